@@ -1,0 +1,152 @@
+/*
+ * liboux -- C ABI of the B200 (sm_100a) explicit compressible-flow time step.
+ *
+ * This is the drop-in boundary for OUxSBLI's GPU hot path.  Each entry point
+ * names the reference interface it replaces (paths relative to the
+ * OUxSBLI repository).  The reference has no C ABI of its own: its Python
+ * layer (ouxsbli/case.py) drives a CUDA-Fortran executable, whose device
+ * work is `RungeKutta` (3D_solver/src/calc_time_dev.f90.fypp:30-114) calling
+ * `calc_EFG` (3D_solver/src/calc_flux_base.f90.fypp:109-198) once per stage.
+ *
+ * Conventions
+ *   - Every call returns an int status: OUX_OK (0) or a negative OUX_E_*.
+ *     oux_last_error() returns a thread-local message for the last failure.
+ *   - Device memory is owned by the caller (e.g. PyTorch tensors): the library
+ *     never allocates device memory for a solve.  oux_state_bytes() and
+ *     oux_scratch_bytes() report the sizes to allocate; oux_bind() attaches them.
+ *   - Calls that take a cudaStream_t (passed as void*) are asynchronous on that
+ *     stream.  A handle is not thread-safe; several handles may share a stream.
+ *   - Device-side faults (NaN / non-positive density or pressure found by the
+ *     status check) set a device status word read by oux_status().
+ *   - No C++ exception crosses this boundary.
+ *
+ * Device state layout ("SoA padded"): for each conservative variable v
+ * (rho, rho u, rho v, [rho w], E, all divided by the cell Jacobian, i.e. the
+ * reference's QJ), a block of nz * ny * row_stride doubles, x fastest, ghost
+ * cells included (g = order/2 per side).  row_stride and var_stride are
+ * reported by oux_layout().  The host-side converters oux_pack_state() /
+ * oux_unpack_state() translate from/to the reference's Q(nx,nv,ny,nz) order.
+ */
+#ifndef OUX_H
+#define OUX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OUX_ABI_VERSION 1
+
+enum oux_status_code {
+  OUX_OK = 0,
+  OUX_E_INVALID = -1,      /* bad argument / unsupported configuration */
+  OUX_E_CUDA = -2,         /* a CUDA runtime call failed */
+  OUX_E_UNBOUND = -3,      /* handle has no device buffers bound */
+  OUX_E_TOO_SMALL = -4,    /* a caller buffer is smaller than required */
+  OUX_E_DEVICE_FAULT = -5  /* the device status word reports a fault */
+};
+
+/* Scheme, physics and option enums; the names follow config.fypp macros. */
+enum oux_scheme { OUX_KEEP = 0, OUX_SLAU = 1, OUX_ROE = 2, OUX_HYBRID = 3 };
+enum oux_visc { OUX_EULER = 0, OUX_NS = 1, OUX_LES = 2 };
+enum oux_visc_stencil { OUX_CENTRAL = 0, OUX_ME4 = 1 };
+enum oux_tvd { OUX_TVD_NONE = 0, OUX_TVD_TVD = 1, OUX_TVD_HYBRID = 2 };
+enum oux_slau_variant { OUX_SLAU1 = 0, OUX_HRSLAU2 = 1 };
+enum oux_precision { OUX_FP64 = 0, OUX_MIXED = 1 };
+/* device status bits (oux_status) */
+enum oux_fault_bits { OUX_FAULT_NAN = 1, OUX_FAULT_NONPOSITIVE = 2, OUX_FAULT_TIMEOUT = 4 };
+
+/*
+ * Solve configuration.  Replaces the compile-time configuration of the
+ * reference: config.fypp macros (VISC, SCHEME, ORDER, TVD, SLAU_VARIANT, RK,
+ * BC_X/Y/Z; VISC_ORDER, VISC_STENCIL) and mod_globals.f90 parameters
+ * (nx, ny, nz incl. ghosts, gamma, R, Pr, Prt, threshold, dt).
+ * dx/dy/dz are the host cell spacings of length n-1 (set_coordinate.f90).
+ */
+typedef struct oux_config {
+  int32_t dim;          /* 2 or 3 */
+  int32_t nx, ny, nz;   /* points incl. ghosts; nz = 1 for dim 2 */
+  int32_t order;        /* convective order 2, 4, 6 */
+  int32_t scheme;       /* enum oux_scheme */
+  int32_t visc;         /* enum oux_visc */
+  int32_t visc_order;   /* 2, 4, 6 (defaults to order when 0) */
+  int32_t visc_stencil; /* enum oux_visc_stencil (ME4 only with visc_order 6) */
+  int32_t tvd;          /* enum oux_tvd */
+  int32_t slau;         /* enum oux_slau_variant */
+  int32_t rk;           /* 3 (TVD-RK3) or 4 (classical RK4) */
+  int32_t bc_x, bc_y, bc_z; /* 0 = periodic (the only boundary built) */
+  int32_t precision;    /* enum oux_precision */
+  double gamma, R, Pr, Prt, threshold, dt;
+  const double *dx, *dy, *dz; /* host arrays, n-1 entries each (dz unused in 2D) */
+} oux_config;
+
+typedef struct oux_handle oux_handle;
+
+typedef struct oux_layout {
+  int32_t nv;          /* conservative variables: dim + 2 */
+  int64_t row_stride;  /* elements between consecutive y rows */
+  int64_t plane_stride;/* elements between consecutive z planes */
+  int64_t var_stride;  /* elements between variables */
+  int64_t elem_bytes;  /* 8 for FP64 state, 4 for the mixed form's state */
+} oux_layout;
+
+/* --- lifetime ----------------------------------------------------------- */
+/* Replaces allocate_device_mem + pre_calc metrics (3D_solver/src/preprocess.f90.fypp:21-103).
+ * Validates the configuration and computes the metric tables on the host. */
+int oux_create(const oux_config* cfg, oux_handle** out);
+int oux_destroy(oux_handle* h);
+const char* oux_last_error(void);
+int oux_abi_version(void);
+
+/* Buffer sizes for a configuration (bytes) and the device layout. */
+int oux_state_bytes(const oux_config* cfg, size_t* bytes);
+int oux_scratch_bytes(const oux_config* cfg, size_t* bytes);
+int oux_layout_of(const oux_handle* h, oux_layout* out);
+
+/* Attach caller-owned device buffers (state = QJ of oux_state_bytes; scratch
+ * of oux_scratch_bytes).  Uploads the metric tables into scratch on `stream`. */
+int oux_bind(oux_handle* h, void* state_dev, void* scratch_dev, size_t scratch_bytes,
+             void* stream);
+
+/* --- host <-> device state (pre_calc H2D :88-95, send_recv_for_print_even D2H) --- */
+/* Copy a host array in the reference order QJ(nx,nv,ny,nz) (Fortran, FP64) to
+ * the bound device state, transposing on the device.  host may be pageable or
+ * pinned; staging uses the scratch buffer. */
+int oux_set_state(oux_handle* h, const double* host_qj, void* stream);
+int oux_get_state(oux_handle* h, double* host_qj, void* stream);
+/* Pure host converters between the reference order and the device layout. */
+int oux_pack_state(const oux_handle* h, const double* ref_qj, void* dev_layout_host);
+int oux_unpack_state(const oux_handle* h, const void* dev_layout_host, double* ref_qj);
+
+/* --- hot path ----------------------------------------------------------- */
+/* Periodic ghost fill: set_bc_cyclic{2,4,6} (3D_solver/src/set_bc_common.f90:101-273). */
+int oux_fill_ghosts(oux_handle* h, void* stream);
+/* Stage residual R = dt*S*(flux differences) of the current state (coef 1), the
+ * quantity calc_R forms (3D_solver/src/calc_steps.f90:8-38) after calc_EFG.
+ * rhs_dev receives nv * (nz-2)*(ny-2)*(nx-2) doubles (3D) in the reference's
+ * Rs(nx-2,nv,ny-2,nz-2) order, interior cells only (ghost entries are 0). */
+int oux_rhs(oux_handle* h, double* rhs_dev, void* stream);
+/* nsteps full time steps: the `do t1 = 1, nt` body of RungeKutta
+ * (3D_solver/src/calc_time_dev.f90.fypp:81-101 RK3, :264-287 RK4;
+ *  2D_solver/src/calc_time_dev.f90.fypp:26-108). */
+int oux_step(oux_handle* h, int32_t nsteps, void* stream);
+/* FP64 domain integrals over interior cells (replaces print_KE / print_entropy,
+ * src/print.f90:42-122, computed on the device in FP64):
+ * out[0] = mean 0.5 rho |u|^2, out[1] = mean rho log(p rho^-gamma),
+ * out[2] = mean 0.5 rho |omega|^2 (enstrophy; no reference counterpart).
+ * Blocking: synchronizes `stream` and copies 3 doubles to the host. */
+int oux_diagnostics(oux_handle* h, double out[3], void* stream);
+/* Device status word (OR of oux_fault_bits); checks the current state for
+ * NaN / non-positive rho or p on `stream` and returns after synchronizing. */
+int oux_check_state(oux_handle* h, int32_t* fault_bits, void* stream);
+int oux_status(oux_handle* h, int32_t* fault_bits);
+
+/* Number of kernel launches the last oux_step call issued (for reporting). */
+int oux_launch_count(const oux_handle* h, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OUX_H */

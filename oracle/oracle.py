@@ -1,0 +1,138 @@
+"""ctypes wrapper of the CPU oracle (oracle.cpp) -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs import
+this module; the product package never does.  See oracle.cpp for what the
+restatement follows and its parity status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+SRC = HERE / "oracle.cpp"
+LIB_PATH = HERE / "liboracle.so"
+# -ffp-contract=off: no fused multiply-add, so the oracle evaluates exactly the
+# operations written; x86-64-v3 keeps the shared object portable to other hosts.
+CFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fopenmp", "-std=c++17", "-fPIC", "-shared"]
+
+SCHEMES = {"KEEP": 0, "SLAU": 1, "Roe": 2, "Hybrid": 3}
+VISC = {"Euler": 0, "NS": 1, "LES": 2}
+STENCILS = {"Central": 0, "ME4Base": 1}
+TVD = {"none": 0, "tvd": 1, "hybrid": 2}
+SLAU_VARIANTS = {"SLAU": 0, "HRSLAU2": 1}
+
+
+def build(force: bool = False) -> pathlib.Path:
+    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < SRC.stat().st_mtime:
+        cmd = ["g++", *CFLAGS, "-o", str(LIB_PATH), str(SRC)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"oracle build failed:\n{r.stderr}")
+    return LIB_PATH
+
+
+class _Cfg(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("dim", "nx", "ny", "nz", "order", "scheme", "visc", "visc_order",
+                                       "visc_stencil", "tvd", "slau", "rk")] + \
+               [(n, C.c_double) for n in ("gamma", "R", "Pr", "Prt", "threshold", "dt")]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(str(LIB_PATH))
+        dp = C.POINTER(C.c_double)
+        cp = C.POINTER(_Cfg)
+        _lib.orc_step.argtypes = [cp, dp, dp, dp, dp, C.c_int]
+        _lib.orc_rhs.argtypes = [cp, dp, dp, dp, dp, dp]
+        _lib.orc_fields.argtypes = [cp, dp, dp, dp, dp, dp]
+        _lib.orc_jacobian.argtypes = [cp, dp, dp, dp, dp]
+        _lib.orc_fill_ghosts.argtypes = [cp, dp]
+        _lib.orc_diag_f32.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                      C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), dp]
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def make_cfg(cfg) -> _Cfg:
+    """Build the oracle config from an object with the SolverConfig attributes."""
+    c = _Cfg()
+    c.dim, c.nx, c.ny = cfg.dim, cfg.nx, cfg.ny
+    c.nz = cfg.nz if cfg.dim == 3 else 1
+    c.order = cfg.order
+    c.scheme = SCHEMES[cfg.scheme]
+    c.visc = VISC[cfg.visc]
+    c.visc_order = cfg.visc_order or cfg.order
+    c.visc_stencil = STENCILS[cfg.visc_stencil]
+    c.tvd = TVD[cfg.tvd]
+    c.slau = SLAU_VARIANTS[cfg.slau]
+    c.rk = cfg.rk
+    c.gamma, c.R, c.Pr, c.Prt, c.threshold, c.dt = cfg.gamma, cfg.R, cfg.Pr, cfg.Prt, cfg.threshold, cfg.dt
+    return c
+
+
+def _axes(cfg):
+    dx = np.ascontiguousarray(cfg.dx, dtype=np.float64)
+    dy = np.ascontiguousarray(cfg.dy, dtype=np.float64)
+    dz = np.ascontiguousarray(cfg.dz if cfg.dim == 3 else np.zeros(1), dtype=np.float64)
+    return dx, dy, dz
+
+
+def step(cfg, qj: np.ndarray, nsteps: int, threads: int | None = None) -> np.ndarray:
+    """Advance a copy of qj (reference layout, Fortran order) by nsteps."""
+    if threads is not None:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    q = np.asfortranarray(qj, dtype=np.float64).copy(order="F")
+    dx, dy, dz = _axes(cfg)
+    c = make_cfg(cfg)
+    rc = lib().orc_step(C.byref(c), _ptr(dx), _ptr(dy), _ptr(dz), _ptr(q), int(nsteps))
+    assert rc == 0
+    return q
+
+
+def rhs(cfg, qj: np.ndarray) -> np.ndarray:
+    """Stage residual (coef 1) in the reference's Rs(nx-2,nv,ny-2[,nz-2]) order."""
+    q = np.asfortranarray(qj, dtype=np.float64)
+    dx, dy, dz = _axes(cfg)
+    nv = cfg.dim + 2
+    shape = (cfg.nx - 2, nv, cfg.ny - 2, cfg.nz - 2) if cfg.dim == 3 else (cfg.nx - 2, nv, cfg.ny - 2)
+    out = np.zeros(shape, dtype=np.float64, order="F")
+    c = make_cfg(cfg)
+    lib().orc_rhs(C.byref(c), _ptr(dx), _ptr(dy), _ptr(dz), _ptr(q), _ptr(out))
+    return out
+
+
+def fields(cfg, qj: np.ndarray) -> dict:
+    q = np.asfortranarray(qj, dtype=np.float64)
+    dx, dy, dz = _axes(cfg)
+    n = cfg.nx * cfg.ny * (cfg.nz if cfg.dim == 3 else 1)
+    out = np.zeros(10 * n)
+    c = make_cfg(cfg)
+    lib().orc_fields(C.byref(c), _ptr(dx), _ptr(dy), _ptr(dz), _ptr(q), _ptr(out))
+    names = ["rho", "u", "v", "w", "p", "T", "mu", "sensor", "mut", "qc2"]
+    shp = (cfg.nx, cfg.ny, cfg.nz) if cfg.dim == 3 else (cfg.nx, cfg.ny)
+    return {nm: out[i * n:(i + 1) * n].reshape(shp, order="F") for i, nm in enumerate(names)}
+
+
+def diag_f32(nx, ny, nz, order, gamma, rho, p, vel) -> tuple[float, float]:
+    """Reference-form KE / entropy (float32 fields, float32 running sum)."""
+    r = np.ascontiguousarray(rho, dtype=np.float32)
+    pp = np.ascontiguousarray(p, dtype=np.float32)
+    v = np.ascontiguousarray(vel, dtype=np.float32)
+    out = np.zeros(2)
+    fp = C.POINTER(C.c_float)
+    lib().orc_diag_f32(nx, ny, nz, order, gamma, r.ctypes.data_as(fp), pp.ctypes.data_as(fp),
+                       v.ctypes.data_as(fp), _ptr(out))
+    return float(out[0]), float(out[1])

@@ -1,0 +1,108 @@
+"""ctypes binding of liboux.so (include/oux.h).
+
+The library is required: importing this module raises if liboux.so has not been
+built (``python -m ouxsbli_b200.build``).  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "liboux.so"
+
+OUX_OK = 0
+OUX_E_INVALID = -1
+OUX_E_CUDA = -2
+OUX_E_UNBOUND = -3
+OUX_E_TOO_SMALL = -4
+OUX_E_DEVICE_FAULT = -5
+
+SCHEMES = {"KEEP": 0, "SLAU": 1, "Roe": 2, "Hybrid": 3}
+VISC = {"Euler": 0, "NS": 1, "LES": 2}
+STENCILS = {"Central": 0, "ME4Base": 1}
+TVD = {"none": 0, "tvd": 1, "hybrid": 2}
+SLAU_VARIANTS = {"SLAU": 0, "HRSLAU2": 1}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+FAULT_NAN = 1
+FAULT_NONPOSITIVE = 2
+FAULT_TIMEOUT = 4
+
+# exported symbols, in include/oux.h order
+SYMBOLS = [
+    "oux_create", "oux_destroy", "oux_last_error", "oux_abi_version", "oux_state_bytes",
+    "oux_scratch_bytes", "oux_layout_of", "oux_bind", "oux_set_state", "oux_get_state",
+    "oux_pack_state", "oux_unpack_state", "oux_fill_ghosts", "oux_rhs", "oux_step",
+    "oux_diagnostics", "oux_check_state", "oux_status", "oux_launch_count",
+]
+
+
+class OuxConfig(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("order", C.c_int32), ("scheme", C.c_int32), ("visc", C.c_int32), ("visc_order", C.c_int32),
+        ("visc_stencil", C.c_int32), ("tvd", C.c_int32), ("slau", C.c_int32), ("rk", C.c_int32),
+        ("bc_x", C.c_int32), ("bc_y", C.c_int32), ("bc_z", C.c_int32), ("precision", C.c_int32),
+        ("gamma", C.c_double), ("R", C.c_double), ("Pr", C.c_double), ("Prt", C.c_double),
+        ("threshold", C.c_double), ("dt", C.c_double),
+        ("dx", C.POINTER(C.c_double)), ("dy", C.POINTER(C.c_double)), ("dz", C.POINTER(C.c_double)),
+    ]
+
+
+class OuxLayout(C.Structure):
+    _fields_ = [("nv", C.c_int32), ("row_stride", C.c_int64), ("plane_stride", C.c_int64),
+                ("var_stride", C.c_int64), ("elem_bytes", C.c_int64)]
+
+
+class OuxError(RuntimeError):
+    """A liboux call returned a negative status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"liboux error {code}: {msg}")
+        self.code = code
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the CUDA library with `python -m ouxsbli_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    vp, i32, i64, dp = C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_double)
+    cfgp = C.POINTER(OuxConfig)
+    sig = {
+        "oux_create": (C.c_int, [cfgp, C.POINTER(vp)]),
+        "oux_destroy": (C.c_int, [vp]),
+        "oux_last_error": (C.c_char_p, []),
+        "oux_abi_version": (C.c_int, []),
+        "oux_state_bytes": (C.c_int, [cfgp, C.POINTER(C.c_size_t)]),
+        "oux_scratch_bytes": (C.c_int, [cfgp, C.POINTER(C.c_size_t)]),
+        "oux_layout_of": (C.c_int, [vp, C.POINTER(OuxLayout)]),
+        "oux_bind": (C.c_int, [vp, vp, vp, C.c_size_t, vp]),
+        "oux_set_state": (C.c_int, [vp, dp, vp]),
+        "oux_get_state": (C.c_int, [vp, dp, vp]),
+        "oux_pack_state": (C.c_int, [vp, dp, vp]),
+        "oux_unpack_state": (C.c_int, [vp, vp, dp]),
+        "oux_fill_ghosts": (C.c_int, [vp, vp]),
+        "oux_rhs": (C.c_int, [vp, vp, vp]),
+        "oux_step": (C.c_int, [vp, i32, vp]),
+        "oux_diagnostics": (C.c_int, [vp, dp, vp]),
+        "oux_check_state": (C.c_int, [vp, C.POINTER(i32), vp]),
+        "oux_status": (C.c_int, [vp, C.POINTER(i32)]),
+        "oux_launch_count": (C.c_int, [vp, C.POINTER(i64)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+LIB = _load()
+
+
+def check(rc: int) -> int:
+    if rc != OUX_OK:
+        msg = LIB.oux_last_error()
+        raise OuxError(rc, msg.decode() if msg else "")
+    return rc

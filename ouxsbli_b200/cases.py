@@ -1,0 +1,236 @@
+"""Case definitions: default parameters and initial fields of the periodic cases.
+
+Each case mirrors a reference case directory (``3D_solver/<CASE>`` or
+``2D_solver/<CASE>``): its config.fypp macros, its mod_globals.f90 parameters
+and its ``set_init``.  Initial fields are built on the host in the reference's
+layout Q(nx, nv, ny[, nz]) (conservative variables, Fortran order), ghosts
+filled periodically.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Callable
+
+import numpy as np
+
+from .grid import cyclic_axis, fill_periodic
+
+
+def sutherland_mu(T: float) -> float:
+    """mu0 of NSTGV/mod_globals.f90:46 (Sutherland with S = 111 K)."""
+    S = 111.0
+    return 1.716e-5 * (273.2 + S) / (T + S) * (T / 273.2) ** 1.5
+
+
+@dataclass
+class CaseDef:
+    name: str
+    dim: int
+    config: dict            # config.fypp macros
+    params: dict            # mod_globals.f90 parameters
+    init: Callable          # (params, xc, yc, zc) -> Q interior-filled
+    derived: Callable = None  # (params) -> params with derived quantities (V0, dt, ...)
+    doc: str = ""
+
+
+# ---------------------------------------------------------------------------
+# Taylor-Green vortex, dimensional form of 3D_solver/NSTGV (mod_globals.f90:42-57,
+# set.f90:16-47).  `rho_mode` = "isothermal" reproduces NSTGV (rho = p / (R T));
+# "uniform" gives rho = rho0 everywhere (the ETGV-style field).
+# ---------------------------------------------------------------------------
+def _tgv_derived(p: dict) -> dict:
+    p = dict(p)
+    T0 = p["T"]
+    p["mu0"] = sutherland_mu(T0)
+    p["V0"] = p["M0"] * math.sqrt(p["gamma"] * p["R"] * T0)
+    p["RHO0"] = p["mu0"] * p["Re"] / (p["V0"] * p["L0"])
+    p["p0"] = p["RHO0"] * p["R"] * T0
+    n = p["nx"]
+    g = p["order"] // 2
+    L = p.get("Lx", 2.0 * math.pi * p["L0"])
+    p.setdefault("Lx", L)
+    p.setdefault("Ly", 2.0 * math.pi * p["L0"])
+    p.setdefault("Lz", 2.0 * math.pi * p["L0"])
+    if p.get("dt") is None:
+        if p.get("cfl_mode", "reference") == "acoustic":
+            # acoustic CFL: dt = CFL * delta / (V0 + c), c = V0 / M0
+            delta = p["Lx"] / (n - 2 * g)
+            p["dt"] = p["CFL"] * delta / (p["V0"] + p["V0"] / p["M0"])
+        else:
+            # NSTGV/mod_globals.f90:53: dt = CFL * (Lx/(nx-1)) / V0
+            p["dt"] = p["CFL"] * (p["Lx"] / float(n - 1)) / p["V0"]
+    p["dtn"] = p["V0"] * p["dt"] / p["L0"]
+    if p.get("nt") is None:
+        p["nt"] = int(20.0 / (float(p["np"]) * p["dtn"]))
+    return p
+
+
+def _tgv_init(p: dict, x, y, z) -> np.ndarray:
+    nx, ny, nz = x.size, y.size, z.size
+    g = p["order"] // 2
+    L0, V0, RHO0, p0, R, T0, gam = p["L0"], p["V0"], p["RHO0"], p["p0"], p["R"], p["T"], p["gamma"]
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    pr = p0 + RHO0 * (V0 ** 2) * (np.cos(2.0 * X / L0) + np.cos(2.0 * Y / L0)) * (np.cos(2.0 * Z / L0) + 2.0) / 16.0
+    if p.get("rho_mode", "isothermal") == "isothermal":
+        rho = pr / (R * T0)
+    else:
+        rho = np.full_like(pr, RHO0)
+    Q = np.zeros((nx, 5, ny, nz), order="F")
+    ru = rho * V0 * np.sin(X / L0) * np.cos(Y / L0) * np.cos(Z / L0)
+    rv = -rho * V0 * np.cos(X / L0) * np.sin(Y / L0) * np.cos(Z / L0)
+    Q[:, 0] = rho
+    Q[:, 1] = ru
+    Q[:, 2] = rv
+    Q[:, 3] = 0.0
+    Q[:, 4] = pr / (gam - 1.0) + 0.5 * (ru ** 2 + rv ** 2) / rho
+    fill_periodic(Q, g)
+    return Q
+
+
+# ---------------------------------------------------------------------------
+# Inviscid Taylor-Green vortex, nondimensional: 3D_solver/ETGV (set.f90:16-45)
+# ---------------------------------------------------------------------------
+def _etgv_init(p: dict, x, y, z) -> np.ndarray:
+    g = p["order"] // 2
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    R0, M0, gam = p["RHO0"], p["M0"], p["gamma"]
+    Q = np.zeros((x.size, 5, y.size, z.size), order="F")
+    ru = R0 * M0 * np.sin(X) * np.cos(Y) * np.cos(Z)
+    rv = -R0 * M0 * np.cos(X) * np.sin(Y) * np.cos(Z)
+    Q[:, 0] = R0
+    Q[:, 1] = ru
+    Q[:, 2] = rv
+    Q[:, 3] = 0.0
+    Q[:, 4] = (1.0 / gam + 0.0625 * R0 * (M0 ** 2) * (np.cos(2.0 * X) + np.cos(2.0 * Y)) * (np.cos(2.0 * Z) + 2.0)) / \
+        (gam - 1.0) + 0.5 * (ru ** 2 + rv ** 2) / R0
+    fill_periodic(Q, g)
+    return Q
+
+
+def _etgv_derived(p: dict) -> dict:
+    p = dict(p)
+    p.setdefault("Lx", 2.0 * math.pi)
+    p.setdefault("Ly", 2.0 * math.pi)
+    p.setdefault("Lz", 2.0 * math.pi)
+    return p
+
+
+# ---------------------------------------------------------------------------
+# Euler vortex convection: 2D_solver/EVC (mod_globals.f90:24-46, set.f90:24-41)
+# ---------------------------------------------------------------------------
+def _evc_derived(p: dict) -> dict:
+    p = dict(p)
+    p["u0"] = p.get("u0") or p["M0"] * math.sqrt(p["gamma"] * p["R"] * p["T0"])
+    p["rho0"] = p["p0"] / (p["R"] * p["T0"])
+    if p.get("dt") is None:
+        p["dt"] = p["CFL"] * p["Lx"] / (float(p["nx"] - 1) * p["u0"])
+    if p.get("nt") is None:
+        T = 2.0 * p["Lx"] / p["u0"]
+        p["nt"] = int(T / (float(p["np"]) * abs(p["dt"])))
+    return p
+
+
+def _evc_init(p: dict, x, y, z=None) -> np.ndarray:
+    nx, ny = x.size, y.size
+    gam, R, T0, u0, beta, Rc, theta = p["gamma"], p["R"], p["T0"], p["u0"], p["beta"], p["Rc"], p["theta"]
+    Cp = R * gam / (gam - 1.0)
+    xc = x[int(nx / 2) - 1]
+    yc = y[int(ny / 2) - 1]
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    ex = np.exp(-0.5 * ((X - xc) ** 2 + (Y - yc) ** 2) / (Rc ** 2))
+    T = T0 - 0.5 * (u0 * beta) ** 2 / Cp * ex ** 2
+    rho = p["rho0"] * (T / T0) ** (1.0 / (gam - 1.0))
+    du = -u0 * beta * (Y - yc) / Rc * ex
+    dv = u0 * beta * (X - xc) / Rc * ex
+    u = u0 * math.cos(theta) + du * math.cos(theta) - dv * math.sin(theta)
+    v = u0 * math.sin(theta) + du * math.sin(theta) + dv * math.cos(theta)
+    pr = rho * R * T
+    Q = np.zeros((nx, 4, ny), order="F")
+    Q[:, 0] = rho
+    Q[:, 1] = rho * u
+    Q[:, 2] = rho * v
+    Q[:, 3] = pr / (gam - 1.0) + 0.5 * rho * (u ** 2 + v ** 2)
+    return Q
+
+
+# ---------------------------------------------------------------------------
+# Isentropic vortex (beta form) for the batched 2D ensemble: nondimensional
+# free stream (rho = 1, p = 1/gamma, c = 1), u_inf = Ma; exact solution = the
+# initial field translated by u_inf * t (periodic).
+# ---------------------------------------------------------------------------
+def isentropic_vortex(nx: int, ny: int, order: int, L: float, beta: float, mach: float,
+                      gamma: float = 1.4, R: float = 1.0, t: float = 0.0) -> np.ndarray:
+    g = order // 2
+    x, _ = cyclic_axis(nx, L, order)
+    y, _ = cyclic_axis(ny, L, order)
+    uinf, vinf = mach, 0.0
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    x0 = 0.5 * L + uinf * t
+    y0 = 0.5 * L + vinf * t
+    dxr = (X - x0 + 0.5 * L) % L - 0.5 * L
+    dyr = (Y - y0 + 0.5 * L) % L - 0.5 * L
+    r2 = dxr ** 2 + dyr ** 2
+    f = np.exp(0.5 * (1.0 - r2))
+    du = -beta / (2.0 * math.pi) * dyr * f
+    dv = beta / (2.0 * math.pi) * dxr * f
+    Tn = 1.0 - (gamma - 1.0) * beta ** 2 / (8.0 * gamma * math.pi ** 2) * np.exp(1.0 - r2)
+    rho = Tn ** (1.0 / (gamma - 1.0))
+    pr = rho ** gamma / gamma
+    u, v = uinf + du, vinf + dv
+    Q = np.zeros((nx, 4, ny), order="F")
+    Q[:, 0] = rho
+    Q[:, 1] = rho * u
+    Q[:, 2] = rho * v
+    Q[:, 3] = pr / (gamma - 1.0) + 0.5 * rho * (u ** 2 + v ** 2)
+    fill_periodic(Q, g)
+    return Q
+
+
+CASES: dict[str, CaseDef] = {
+    "NSTGV": CaseDef(
+        "NSTGV", 3,
+        dict(VISC="NS", SCHEME="SLAU", ORDER=6, TVD="hybrid", SLAU_VARIANT="HRSLAU2", RK=3,
+             BC_X=False, BC_Y=False, BC_Z=False, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=513, ny=513, nz=513, L0=1.524e-3, Re=1600.0, M0=1.25, T=530.0 * 5.0 / 9.0,
+             gamma=1.4, Pr=0.71, Prt=0.9, R=287.03, CFL=0.03, np=100, threshold=0.4, dt=None, nt=None,
+             rho_mode="isothermal", cfl_mode="reference"),
+        _tgv_init, _tgv_derived,
+        "Viscous Taylor-Green vortex (3D_solver/NSTGV)"),
+    "ETGV": CaseDef(
+        "ETGV", 3,
+        dict(VISC="Euler", SCHEME="KEEP", ORDER=6, TVD="hybrid", SLAU_VARIANT="HRSLAU2", RK=4,
+             BC_X=False, BC_Y=False, BC_Z=False, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=66, ny=66, nz=66, nt=200, np=100, dt=0.01, gamma=1.4, Pr=0.71, Prt=0.9, R=287.03,
+             M0=0.4, RHO0=1.0, threshold=0.4),
+        _etgv_init, _etgv_derived,
+        "Inviscid Taylor-Green vortex (3D_solver/ETGV)"),
+    "EVC": CaseDef(
+        "EVC", 2,
+        dict(VISC="Euler", SCHEME="KEEP", ORDER=6, TVD="none", SLAU_VARIANT="HRSLAU2", RK=4,
+             BC_X=False, BC_Y=False, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=258, ny=258, Lx=0.1, Ly=0.1, gamma=1.4, Pr=0.71, Prt=0.9, R=287.15, M0=0.05,
+             beta=1.0 / 50.0, theta=0.0, Rc=0.005, p0=1.0e5, T0=300.0, u0=None, CFL=0.03, np=1,
+             dt=None, nt=None, threshold=0.4),
+        _evc_init, _evc_derived,
+        "Euler vortex convection (2D_solver/EVC)"),
+}
+
+
+def build_initial(case: CaseDef, params: dict):
+    """Return (derived params, xc, yc, zc, dx, dy, dz, Q) for a case."""
+    p = dict(params)
+    order = p["order"]
+    if case.derived:
+        p = case.derived(p)
+    if case.dim == 3:
+        xc, dx = cyclic_axis(p["nx"], p["Lx"], order)
+        yc, dy = cyclic_axis(p["ny"], p["Ly"], order)
+        zc, dz = cyclic_axis(p["nz"], p["Lz"], order)
+        Q = case.init(p, xc, yc, zc)
+    else:
+        xc, dx = cyclic_axis(p["nx"], p["Lx"], order)
+        yc, dy = cyclic_axis(p["ny"], p["Ly"], order)
+        zc, dz = np.zeros(1), None
+        Q = case.init(p, xc, yc, None)
+    return p, xc, yc, zc, dx, dy, dz, Q

@@ -1,0 +1,689 @@
+// Host side of liboux: configuration checks, metric tables, scratch carving,
+// the stage driver that sequences the kernels of oux_kernels.cuh /
+// oux_sweep.cuh, and the C ABI declared in include/oux.h.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "oux.h"
+#include "oux_sweep.cuh"
+#include "oux_dispatch.h"
+
+using namespace oux;
+
+namespace {
+thread_local std::string g_last_error;
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+#define OUX_CUDA(call)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(OUX_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
+  } while (0)
+
+int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+}  // namespace
+
+struct oux_handle {
+  oux_config cfg;
+  Geo G;
+  int nv;
+  int vk;
+  bool les;
+  PhysConst K;
+  std::vector<double> inv_dx, inv_dy, inv_dz, jac, dtdxdy, dtdydz, dtdzdx, dtdx, dtdy;
+  // bound buffers
+  double* Q = nullptr;
+  unsigned char* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  Fields<double> W{};
+  double *Racc = nullptr, *Q2 = nullptr, *Rs = nullptr, *partials = nullptr;
+  int* status = nullptr;
+  Metrics M{};
+  int64_t launches = 0;
+  int diag_blocks = 0;
+};
+
+namespace {
+
+// ---- configuration -------------------------------------------------------------
+int validate(const oux_config* c, std::string& why) {
+  if (!c) { why = "null config"; return OUX_E_INVALID; }
+  if (c->dim != 2 && c->dim != 3) { why = "dim must be 2 or 3"; return OUX_E_INVALID; }
+  if (c->order != 2 && c->order != 4 && c->order != 6) { why = "order must be 2, 4 or 6"; return OUX_E_INVALID; }
+  int g = c->order / 2;
+  int nzc = c->dim == 3 ? c->nz : 1;
+  if (c->nx < 2 * g + 2 || c->ny < 2 * g + 2 || (c->dim == 3 && c->nz < 2 * g + 2)) {
+    why = "grid too small for the stencil (need at least 2 interior cells per axis)";
+    return OUX_E_INVALID;
+  }
+  if ((int64_t)c->nx * c->ny * nzc > (int64_t)1 << 34) { why = "grid too large"; return OUX_E_INVALID; }
+  if (c->scheme < 0 || c->scheme > 3) { why = "unknown scheme"; return OUX_E_INVALID; }
+  if (c->dim == 2 && c->scheme == OUX_ROE) { why = "the 2D solver has no Roe scheme"; return OUX_E_INVALID; }
+  if (c->visc < 0 || c->visc > 2) { why = "unknown visc"; return OUX_E_INVALID; }
+  if (c->dim == 2 && c->visc == OUX_LES) { why = "the 2D solver has no LES model"; return OUX_E_INVALID; }
+  if (c->tvd < 0 || c->tvd > 2) { why = "unknown tvd mode"; return OUX_E_INVALID; }
+  if (c->slau < 0 || c->slau > 1) { why = "unknown SLAU variant"; return OUX_E_INVALID; }
+  if (c->rk != 3 && c->rk != 4) { why = "rk must be 3 or 4"; return OUX_E_INVALID; }
+  if (c->bc_x || c->bc_y || (c->dim == 3 && c->bc_z)) {
+    why = "only periodic boundaries (bc_x = bc_y = bc_z = 0) are built";
+    return OUX_E_INVALID;
+  }
+  if (c->precision != OUX_FP64) { why = "precision: only OUX_FP64 in this library build"; return OUX_E_INVALID; }
+  if (!c->dx || !c->dy || (c->dim == 3 && !c->dz)) { why = "dx/dy/dz host arrays required"; return OUX_E_INVALID; }
+  if (!(c->gamma > 1.0) || !(c->R > 0.0) || !(c->dt > 0.0)) { why = "gamma > 1, R > 0, dt > 0 required"; return OUX_E_INVALID; }
+  if (c->visc != OUX_EULER) {
+    if (!(c->Pr > 0.0)) { why = "Pr > 0 required for viscous runs"; return OUX_E_INVALID; }
+    if (c->visc == OUX_LES && !(c->Prt > 0.0)) { why = "Prt > 0 required for LES"; return OUX_E_INVALID; }
+  }
+  return OUX_OK;
+}
+
+// Viscous kernel family the reference selects for (dim, order, visc_order, stencil):
+// calc_flux_base.f90.fypp:161-177 (3D) and 2D_solver/src/calc_flux_base.f90.fypp:108-132.
+int visc_kind(const oux_config* c, std::string& why) {
+  if (c->visc == OUX_EULER) return VK_EULER;
+  int vo = c->visc_order ? c->visc_order : c->order;
+  if (c->dim == 2) {
+    if (vo == 4) {
+      if (c->order < 4) { why = "2D visc_order 4 needs order >= 4"; return -1; }
+      return VK_2D4;
+    }
+    return VK_GV2;
+  }
+  if (vo == 2) {
+    if (c->order == 6) { why = "order 6 with visc_order 2 has no reference kernel (calc_Ev2_in)"; return -1; }
+    return VK_GV2;
+  }
+  if (vo == 4) {
+    if (c->order < 4) { why = "visc_order 4 needs order >= 4"; return -1; }
+    return VK_C4;
+  }
+  if (vo == 6) {
+    if (c->order != 6) { why = "visc_order 6 is built for order 6 only"; return -1; }
+    return c->visc_stencil == OUX_ME4 ? VK_ME4 : VK_C6;
+  }
+  why = "visc_order must be 2, 4 or 6";
+  return -1;
+}
+
+void build_tables(oux_handle* h) {
+  const oux_config& c = h->cfg;
+  const double* dx = c.dx;
+  const double* dy = c.dy;
+  const double* dz = c.dz;
+  int nx = c.nx, ny = c.ny, nz = c.dim == 3 ? c.nz : 1;
+  h->inv_dx.resize(nx - 1);
+  h->inv_dy.resize(ny - 1);
+  for (int i = 0; i < nx - 1; ++i) h->inv_dx[i] = 1.0 / dx[i];
+  for (int j = 0; j < ny - 1; ++j) h->inv_dy[j] = 1.0 / dy[j];
+  if (c.dim == 3) {
+    h->inv_dz.resize(nz - 1);
+    for (int k = 0; k < nz - 1; ++k) h->inv_dz[k] = 1.0 / dz[k];
+  } else {
+    h->inv_dz.assign(1, 0.0);
+  }
+  // Jacobian: src/set_coordinate.f90:80-117 (1/cell volume, edges copied)
+  h->jac.assign((size_t)nx * ny, 0.0);
+  auto J = [&](int i, int j) -> double& { return h->jac[(size_t)j * nx + i]; };
+  for (int j = 1; j <= ny - 2; ++j)
+    for (int i = 1; i <= nx - 2; ++i) {
+      if (c.dim == 3)
+        J(i, j) = 8.0 / ((dx[i - 1] + dx[i]) * (dy[j - 1] + dy[j]) * 2.0 * dz[0]);
+      else
+        J(i, j) = 4.0 / ((dx[i - 1] + dx[i]) * (dy[j - 1] + dy[j]));
+    }
+  for (int i = 0; i < nx; ++i) { J(i, 0) = J(i, 1); J(i, ny - 1) = J(i, ny - 2); }
+  for (int j = 0; j < ny; ++j) { J(0, j) = J(1, j); J(nx - 1, j) = J(nx - 2, j); }
+  const double dt = c.dt;
+  if (c.dim == 3) {  // 3D_solver/src/preprocess.f90.fypp:76-87
+    h->dtdxdy.resize((size_t)(nx - 2) * (ny - 2));
+    h->dtdydz.resize((size_t)(ny - 2) * (nz - 2));
+    h->dtdzdx.resize((size_t)(nx - 2) * (nz - 2));
+    for (int j = 0; j < ny - 2; ++j)
+      for (int i = 0; i < nx - 2; ++i)
+        h->dtdxdy[(size_t)j * (nx - 2) + i] = 0.25 * dt * (dx[i] + dx[i + 1]) * (dy[j] + dy[j + 1]);
+    for (int k = 0; k < nz - 2; ++k)
+      for (int j = 0; j < ny - 2; ++j)
+        h->dtdydz[(size_t)k * (ny - 2) + j] = 0.25 * dt * (dy[j] + dy[j + 1]) * (dz[k] + dz[k + 1]);
+    for (int k = 0; k < nz - 2; ++k)
+      for (int i = 0; i < nx - 2; ++i)
+        h->dtdzdx[(size_t)k * (nx - 2) + i] = 0.25 * dt * (dz[k] + dz[k + 1]) * (dx[i] + dx[i + 1]);
+  } else {  // 2D_solver/src/preprocess.f90.fypp:96-101
+    h->dtdx.resize(nx - 2);
+    h->dtdy.resize(ny - 2);
+    for (int i = 0; i < nx - 2; ++i) h->dtdx[i] = 0.5 * dt * (dx[i] + dx[i + 1]);
+    for (int j = 0; j < ny - 2; ++j) h->dtdy[j] = 0.5 * dt * (dy[j] + dy[j + 1]);
+  }
+  // derived constants: src/mod_constant.f90.fypp:18-32
+  PhysConst& K = h->K;
+  K.gamma = c.gamma; K.R = c.R; K.Pr = c.Pr; K.Prt = c.Prt; K.threshold = c.threshold;
+  K.gamma_1 = c.gamma - 1.0;
+  K.over_gamma_1 = 1.0 / (c.gamma - 1.0);
+  K.R_over_gamma_1 = c.R / (c.gamma - 1.0);
+  K.Cp = c.gamma * c.R / (c.gamma - 1.0);
+  K.Cp_over_Pr = c.visc != OUX_EULER ? K.Cp / c.Pr : 0.0;
+  K.sutherland = 1.716e-5 * 384.2 * std::pow(273.2, -1.5);
+  K.gamma_over_gamma_1 = c.gamma * K.over_gamma_1;
+  double t10 = std::tan(10.0 * std::acos(-1.0) / 180.0);
+  K.tan10deg2 = t10 * t10;
+}
+
+Geo make_geo(const oux_config& c) {
+  Geo G;
+  G.dim = c.dim; G.nx = c.nx; G.ny = c.ny; G.nz = c.dim == 3 ? c.nz : 1; G.g = c.order / 2;
+  G.sx = round_up(c.nx, 4);
+  G.plane = G.sx * c.ny;
+  G.vs = round_up(G.plane * G.nz, 32);
+  return G;
+}
+
+struct ScratchPlan {
+  size_t fields = 0, racc = 0, q2 = 0, rs = 0, metrics = 0, partials = 0, status = 0, total = 0;
+  int nfield_arrays = 0;
+};
+
+constexpr int DIAG_BLOCKS = 1184;  // 8 blocks per SM on 148 SMs; fixed for a deterministic sum
+
+ScratchPlan plan_scratch(const oux_config& c) {
+  Geo G = make_geo(c);
+  int nv = c.dim + 2;
+  ScratchPlan P;
+  size_t vsb = (size_t)G.vs * sizeof(double);
+  P.nfield_arrays = 10;  // rho,u,v,w,p,T,mu,sensor,mut,qc2 (unused ones are still carved)
+  size_t off = 0;
+  P.fields = off; off += (size_t)P.nfield_arrays * vsb;
+  P.racc = off; off += (size_t)nv * vsb;
+  P.q2 = off; off += (size_t)nv * vsb;
+  P.rs = off; off += (c.rk == 4 ? (size_t)nv * vsb : 0);
+  P.metrics = off;
+  int nx = c.nx, ny = c.ny, nz = c.dim == 3 ? c.nz : 1;
+  size_t mcount = (size_t)(nx - 1) + (ny - 1) + (c.dim == 3 ? nz - 1 : 1) + (size_t)nx * ny;
+  if (c.dim == 3) mcount += (size_t)(nx - 2) * (ny - 2) + (size_t)(ny - 2) * (nz - 2) + (size_t)(nx - 2) * (nz - 2);
+  else mcount += (size_t)(nx - 2) + (ny - 2);
+  off += round_up(mcount * sizeof(double), 256);
+  P.partials = off; off += round_up((size_t)3 * DIAG_BLOCKS * sizeof(double) + 3 * sizeof(double), 256);
+  P.status = off; off += 256;
+  P.total = off;
+  return P;
+}
+
+// ---- small kernels ---------------------------------------------------------------
+// reference order ref[((k*ny + j)*nv + l)*nx + i]  <->  SoA Q[l*vs + k*plane + j*sx + i]
+template <class T>
+__global__ void k_ref_to_soa(const double* __restrict__ ref, T* __restrict__ Q, Geo G, int nv) {
+  int64_t n = (int64_t)G.nx * G.ny * G.nz * nv;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx);
+    int64_t r = t / G.nx;
+    int l = (int)(r % nv); r /= nv;
+    int j = (int)(r % G.ny);
+    int k = (int)(r / G.ny);
+    Q[G.at(i, j, k) + l * G.vs] = (T)ref[t];
+  }
+}
+template <class T>
+__global__ void k_soa_to_ref(const T* __restrict__ Q, double* __restrict__ ref, Geo G, int nv) {
+  int64_t n = (int64_t)G.nx * G.ny * G.nz * nv;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx);
+    int64_t r = t / G.nx;
+    int l = (int)(r % nv); r /= nv;
+    int j = (int)(r % G.ny);
+    int k = (int)(r / G.ny);
+    ref[t] = (double)Q[G.at(i, j, k) + l * G.vs];
+  }
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sm) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sm[wid] = v;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? sm[threadIdx.x] : 0.0;
+  if (wid == 0)
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  return v;
+}
+
+// FP64 domain integrals over interior cells (ke, entropy, enstrophy); W holds the
+// primitives of the current state.  Vorticity uses the central difference of the
+// solve's order (6th: load_smem_visc_cent.f90.fypp:67 form).
+__global__ void k_diag(Geo G, Fields<double> W, Metrics M, double gamma, int order, double* partials) {
+  __shared__ double sm[32];
+  const int g = G.g;
+  const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
+  int64_t n = (int64_t)Nx * Ny * Nz;
+  double ke = 0.0, en = 0.0, ens = 0.0;
+  auto dd = [&](const double* a, int64_t o, int64_t st, double inv) -> double {
+    if (order == 6)
+      return ((1.0 / 60.0) * (-a[o - 3 * st] + a[o + 3 * st]) + 0.15 * (a[o - 2 * st] - a[o + 2 * st]) +
+              0.75 * (-a[o - st] + a[o + st])) * inv;
+    if (order == 4)
+      return ((2.0 / 3.0) * (-a[o - st] + a[o + st]) - (1.0 / 12.0) * (-a[o - 2 * st] + a[o + 2 * st])) * inv;
+    return 0.5 * (-a[o - st] + a[o + st]) * inv;
+  };
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(t % Nx) + g;
+    int64_t r = t / Nx;
+    int j = (int)(r % Ny) + g;
+    int k = (G.dim == 3) ? (int)(r / Ny) + g : 0;
+    int64_t o = G.at(i, j, k);
+    double rho = W.rho[o], u = W.u[o], v = W.v[o], p = W.p[o];
+    double w = (G.dim == 3) ? W.w[o] : 0.0;
+    ke += 0.5 * rho * (u * u + v * v + w * w);
+    en += rho * log(p * pow(rho, -gamma));
+    double ix = M.inv_dx[i], iy = M.inv_dy[j];
+    double dvdx = dd(W.v, o, 1, ix), dudy = dd(W.u, o, G.sx, iy);
+    double om2;
+    if (G.dim == 3) {
+      double iz = M.inv_dz[k];
+      double dwdy = dd(W.w, o, G.sx, iy), dvdz = dd(W.v, o, G.plane, iz);
+      double dudz = dd(W.u, o, G.plane, iz), dwdx = dd(W.w, o, 1, ix);
+      double a = dwdy - dvdz, b = dudz - dwdx, c = dvdx - dudy;
+      om2 = a * a + b * b + c * c;
+    } else {
+      double c = dvdx - dudy;
+      om2 = c * c;
+    }
+    ens += 0.5 * rho * om2;
+  }
+  ke = block_sum(ke, sm);
+  en = block_sum(en, sm);
+  ens = block_sum(ens, sm);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = ke;
+    partials[gridDim.x + blockIdx.x] = en;
+    partials[2 * gridDim.x + blockIdx.x] = ens;
+  }
+}
+__global__ void k_diag_final(const double* partials, int nb, double inv_n, double* out) {
+  __shared__ double sm[32];
+  for (int q = 0; q < 3; ++q) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partials[q * nb + b];
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) out[q] = s * inv_n;
+  }
+}
+
+// status scan: NaN / non-positive density or pressure in interior cells
+__global__ void k_check(const double* __restrict__ Q, Geo G, const double* __restrict__ jac, double gamma_1,
+                        int* status) {
+  const int g = G.g;
+  const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
+  int64_t n = (int64_t)Nx * Ny * Nz;
+  int bits = 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(t % Nx) + g;
+    int64_t r = t / Nx;
+    int j = (int)(r % Ny) + g;
+    int k = (G.dim == 3) ? (int)(r / Ny) + g : 0;
+    int64_t o = G.at(i, j, k);
+    double Jv = jac[(int64_t)j * G.nx + i];
+    double q1 = Q[o], rho = Jv * q1;
+    double ke = 0.0;
+    for (int l = 1; l <= G.dim; ++l) { double vv = Q[o + l * G.vs] / q1; ke += vv * vv; }
+    double p = gamma_1 * (Jv * Q[o + (G.dim + 1) * G.vs] - 0.5 * rho * ke);
+    if (!(rho == rho) || !(p == p)) bits |= OUX_FAULT_NAN;
+    if (!(rho > 0.0) || !(p > 0.0)) bits |= OUX_FAULT_NONPOSITIVE;
+  }
+  if (bits) atomicOr(status, bits);
+}
+
+inline int grid_for(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+void carve(oux_handle* h) {
+  ScratchPlan P = plan_scratch(h->cfg);
+  size_t vsb = (size_t)h->G.vs;
+  double* f = reinterpret_cast<double*>(h->scratch + P.fields);
+  double** fp[10] = {&h->W.rho, &h->W.u, &h->W.v, &h->W.w, &h->W.p, &h->W.T_, &h->W.mu, &h->W.sensor, &h->W.mut, &h->W.qc2};
+  for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
+  h->Racc = reinterpret_cast<double*>(h->scratch + P.racc);
+  h->Q2 = reinterpret_cast<double*>(h->scratch + P.q2);
+  h->Rs = h->cfg.rk == 4 ? reinterpret_cast<double*>(h->scratch + P.rs) : nullptr;
+  double* m = reinterpret_cast<double*>(h->scratch + P.metrics);
+  auto take = [&](const std::vector<double>& v) {
+    double* p = m;
+    m += v.size();
+    return (const double*)p;
+  };
+  h->M.inv_dx = take(h->inv_dx);
+  h->M.inv_dy = take(h->inv_dy);
+  h->M.inv_dz = take(h->inv_dz);
+  h->M.jac = take(h->jac);
+  if (h->cfg.dim == 3) {
+    h->M.dtdxdy = take(h->dtdxdy);
+    h->M.dtdydz = take(h->dtdydz);
+    h->M.dtdzdx = take(h->dtdzdx);
+    h->M.dtdx = h->M.dtdy = nullptr;
+  } else {
+    h->M.dtdx = take(h->dtdx);
+    h->M.dtdy = take(h->dtdy);
+    h->M.dtdxdy = h->M.dtdydz = h->M.dtdzdx = nullptr;
+  }
+  h->partials = reinterpret_cast<double*>(h->scratch + P.partials);
+  h->status = reinterpret_cast<int*>(h->scratch + P.status);
+}
+
+StepArgs<double> base_args(oux_handle* h) {
+  StepArgs<double> A{};
+  A.G = h->G;
+  A.W = h->W;
+  A.M = h->M;
+  A.K = h->K;
+  A.scheme = h->cfg.scheme;
+  A.tvd = h->cfg.tvd;
+  A.slau = h->cfg.slau;
+  A.Racc = h->Racc;
+  A.Rs = h->Rs;
+  return A;
+}
+
+// One stage: primitives of `src`, sensor, SGS viscosity, then the sweeps.
+int run_stage(oux_handle* h, const double* src, StepArgs<double> A, cudaStream_t s) {
+  const Geo& G = h->G;
+  const oux_config& c = h->cfg;
+  int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
+  bool visc = c.visc != OUX_EULER;
+  if (G.dim == 3) {
+    if (visc) k_prim<3, true, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
+    else k_prim<3, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
+  } else {
+    if (visc) k_prim<2, true, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
+    else k_prim<2, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
+  }
+  h->launches++;
+  if (c.scheme != OUX_KEEP) {
+    if (G.dim == 3) {
+      dim3 b(32, 4, 2), gr((G.nx - 2 + 31) / 32, (G.ny - 2 + 3) / 4, (G.nz - 2 + 1) / 2);
+      k_sensor<3, double><<<gr, b, 0, s>>>(G, h->W, h->M);
+    } else {
+      dim3 b(32, 8, 1), gr((G.nx - 2 + 31) / 32, (G.ny - 2 + 7) / 8, 1);
+      k_sensor<2, double><<<gr, b, 0, s>>>(G, h->W, h->M);
+    }
+    h->launches++;
+  }
+  if (h->les) {
+    dim3 b(32, 4, 1), gr((G.nx - 2 + 31) / 32, (G.ny - 2 + 3) / 4, G.nz - 2);
+    k_mut<double><<<gr, b, 0, s>>>(G, h->W, h->M, h->K);
+    k_mut_edges<double><<<grid_for(ncell, 256), 256, 0, s>>>(G, h->W);
+    h->launches += 2;
+  }
+  int rc = launch_sweeps_fp64(G.dim, c.order, h->vk, h->les, A, s);
+  if (rc) return fail(OUX_E_CUDA, std::string("sweep launch: ") + cudaGetErrorString(cudaGetLastError()));
+  h->launches += G.dim;
+  return OUX_OK;
+}
+
+int ghost(oux_handle* h, double* Q, cudaStream_t s) {
+  const Geo& G = h->G;
+  int64_t n = (int64_t)G.nx * G.ny * G.nz;
+  k_ghost<double><<<grid_for(n / 4 + 1, 256), 256, 0, s>>>(Q, G, h->nv);
+  h->launches++;
+  return OUX_OK;
+}
+
+}  // namespace
+
+// ================================ C ABI =========================================
+extern "C" {
+
+const char* oux_last_error(void) { return g_last_error.c_str(); }
+int oux_abi_version(void) { return OUX_ABI_VERSION; }
+
+int oux_state_bytes(const oux_config* cfg, size_t* bytes) {
+  std::string why;
+  int rc = validate(cfg, why);
+  if (rc) return fail(rc, why);
+  if (!bytes) return fail(OUX_E_INVALID, "null output");
+  Geo G = make_geo(*cfg);
+  *bytes = (size_t)(cfg->dim + 2) * G.vs * sizeof(double);
+  return OUX_OK;
+}
+
+int oux_scratch_bytes(const oux_config* cfg, size_t* bytes) {
+  std::string why;
+  int rc = validate(cfg, why);
+  if (rc) return fail(rc, why);
+  if (!bytes) return fail(OUX_E_INVALID, "null output");
+  *bytes = plan_scratch(*cfg).total;
+  return OUX_OK;
+}
+
+int oux_create(const oux_config* cfg, oux_handle** out) {
+  std::string why;
+  int rc = validate(cfg, why);
+  if (rc) return fail(rc, why);
+  if (!out) return fail(OUX_E_INVALID, "null output");
+  int vk = visc_kind(cfg, why);
+  if (vk < 0) return fail(OUX_E_INVALID, why);
+  oux_handle* h = new (std::nothrow) oux_handle();
+  if (!h) return fail(OUX_E_INVALID, "host allocation failed");
+  h->cfg = *cfg;
+  if (h->cfg.dim == 2) { h->cfg.nz = 1; h->cfg.bc_z = 0; }
+  h->G = make_geo(h->cfg);
+  h->nv = cfg->dim + 2;
+  h->vk = vk;
+  h->les = cfg->visc == OUX_LES;
+  build_tables(h);
+  h->cfg.dx = h->cfg.dy = h->cfg.dz = nullptr;  // host arrays are not retained
+  *out = h;
+  return OUX_OK;
+}
+
+int oux_destroy(oux_handle* h) {
+  delete h;
+  return OUX_OK;
+}
+
+int oux_layout_of(const oux_handle* h, oux_layout* out) {
+  if (!h || !out) return fail(OUX_E_INVALID, "null argument");
+  out->nv = h->nv;
+  out->row_stride = h->G.sx;
+  out->plane_stride = h->G.plane;
+  out->var_stride = h->G.vs;
+  out->elem_bytes = sizeof(double);
+  return OUX_OK;
+}
+
+int oux_bind(oux_handle* h, void* state_dev, void* scratch_dev, size_t scratch_bytes, void* stream) {
+  if (!h || !state_dev || !scratch_dev) return fail(OUX_E_INVALID, "null argument");
+  ScratchPlan P = plan_scratch(h->cfg);
+  if (scratch_bytes < P.total)
+    return fail(OUX_E_TOO_SMALL, "scratch buffer smaller than oux_scratch_bytes()");
+  if (((uintptr_t)state_dev & 255) || ((uintptr_t)scratch_dev & 255))
+    return fail(OUX_E_INVALID, "device buffers must be 256-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  h->Q = (double*)state_dev;
+  h->scratch = (unsigned char*)scratch_dev;
+  h->scratch_bytes = scratch_bytes;
+  carve(h);
+  // upload metric tables (contiguous block, same order as carve())
+  std::vector<double> m;
+  auto put = [&](const std::vector<double>& v) { m.insert(m.end(), v.begin(), v.end()); };
+  put(h->inv_dx); put(h->inv_dy); put(h->inv_dz); put(h->jac);
+  if (h->cfg.dim == 3) { put(h->dtdxdy); put(h->dtdydz); put(h->dtdzdx); }
+  else { put(h->dtdx); put(h->dtdy); }
+  OUX_CUDA(cudaMemcpyAsync((void*)h->M.inv_dx, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  OUX_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), s));
+  if (h->Rs) OUX_CUDA(cudaMemsetAsync(h->Rs, 0, (size_t)h->nv * h->G.vs * sizeof(double), s));
+  // the metric upload reads a host vector that goes out of scope: finish it now
+  OUX_CUDA(cudaStreamSynchronize(s));
+  return OUX_OK;
+}
+
+int oux_set_state(oux_handle* h, const double* host_qj, void* stream) {
+  if (!h || !host_qj) return fail(OUX_E_INVALID, "null argument");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo& G = h->G;
+  int64_t n = (int64_t)G.nx * G.ny * G.nz * h->nv;
+  OUX_CUDA(cudaMemcpyAsync(h->Racc, host_qj, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_ref_to_soa<double><<<grid_for(n, 256), 256, 0, s>>>(h->Racc, h->Q, G, h->nv);
+  OUX_CUDA(cudaGetLastError());
+  return OUX_OK;
+}
+
+int oux_get_state(oux_handle* h, double* host_qj, void* stream) {
+  if (!h || !host_qj) return fail(OUX_E_INVALID, "null argument");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo& G = h->G;
+  int64_t n = (int64_t)G.nx * G.ny * G.nz * h->nv;
+  k_soa_to_ref<double><<<grid_for(n, 256), 256, 0, s>>>(h->Q, h->Racc, G, h->nv);
+  OUX_CUDA(cudaGetLastError());
+  OUX_CUDA(cudaMemcpyAsync(host_qj, h->Racc, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  OUX_CUDA(cudaStreamSynchronize(s));
+  return OUX_OK;
+}
+
+int oux_pack_state(const oux_handle* h, const double* ref_qj, void* dev_layout_host) {
+  if (!h || !ref_qj || !dev_layout_host) return fail(OUX_E_INVALID, "null argument");
+  const Geo& G = h->G;
+  double* Q = (double*)dev_layout_host;
+  for (int k = 0; k < G.nz; ++k)
+    for (int j = 0; j < G.ny; ++j)
+      for (int l = 0; l < h->nv; ++l)
+        for (int i = 0; i < G.nx; ++i)
+          Q[G.at(i, j, k) + l * G.vs] = ref_qj[(((int64_t)k * G.ny + j) * h->nv + l) * G.nx + i];
+  return OUX_OK;
+}
+
+int oux_unpack_state(const oux_handle* h, const void* dev_layout_host, double* ref_qj) {
+  if (!h || !ref_qj || !dev_layout_host) return fail(OUX_E_INVALID, "null argument");
+  const Geo& G = h->G;
+  const double* Q = (const double*)dev_layout_host;
+  for (int k = 0; k < G.nz; ++k)
+    for (int j = 0; j < G.ny; ++j)
+      for (int l = 0; l < h->nv; ++l)
+        for (int i = 0; i < G.nx; ++i)
+          ref_qj[(((int64_t)k * G.ny + j) * h->nv + l) * G.nx + i] = Q[G.at(i, j, k) + l * G.vs];
+  return OUX_OK;
+}
+
+int oux_fill_ghosts(oux_handle* h, void* stream) {
+  if (!h) return fail(OUX_E_INVALID, "null handle");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  ghost(h, h->Q, (cudaStream_t)stream);
+  OUX_CUDA(cudaGetLastError());
+  return OUX_OK;
+}
+
+int oux_rhs(oux_handle* h, double* rhs_dev, void* stream) {
+  if (!h || !rhs_dev) return fail(OUX_E_INVALID, "null argument");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo& G = h->G;
+  size_t n = (size_t)h->nv * (G.nx - 2) * (G.ny - 2) * (G.dim == 3 ? G.nz - 2 : 1);
+  OUX_CUDA(cudaMemsetAsync(rhs_dev, 0, n * sizeof(double), s));
+  StepArgs<double> A = base_args(h);
+  A.mode = CM_R_OUT;
+  A.coef = 1.0;
+  A.Rout = rhs_dev;
+  int rc = run_stage(h, h->Q, A, s);
+  if (rc) return rc;
+  OUX_CUDA(cudaGetLastError());
+  return OUX_OK;
+}
+
+int oux_step(oux_handle* h, int32_t nsteps, void* stream) {
+  if (!h) return fail(OUX_E_INVALID, "null handle");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  if (nsteps < 0) return fail(OUX_E_INVALID, "nsteps must be >= 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  h->launches = 0;
+  double* Q = h->Q;
+  double* Q2 = h->Q2;
+  for (int n = 0; n < nsteps; ++n) {
+    StepArgs<double> A = base_args(h);
+    int rc;
+    if (h->cfg.rk == 3) {
+      // calc_time_dev.f90.fypp:81-101
+      A.mode = CM_RK3_1; A.coef = 1.0; A.Qin = Q; A.Qout = Q2;
+      if ((rc = run_stage(h, Q, A, s))) return rc;
+      ghost(h, Q2, s);
+      A.mode = CM_RK3; A.coef = 0.25; A.c1 = 0.75; A.c2 = 0.25; A.c4 = 1.0; A.Qin = Q; A.Qout = Q2;
+      if ((rc = run_stage(h, Q2, A, s))) return rc;
+      ghost(h, Q2, s);
+      A.mode = CM_RK3; A.coef = 2.0; A.c1 = 2.0; A.c2 = 1.0; A.c4 = 1.0 / 3.0; A.Qin = Q2; A.Qout = Q;
+      if ((rc = run_stage(h, Q2, A, s))) return rc;
+      ghost(h, Q, s);
+    } else {
+      // calc_time_dev.f90.fypp:264-287
+      const double c1[3] = {0.5, 0.5, 1.0}, c2[3] = {1.0, 2.0, 2.0};
+      for (int st = 0; st < 3; ++st) {
+        A.mode = CM_RK4_S; A.coef = 1.0; A.c1 = c1[st]; A.c2 = c2[st]; A.Qin = Q; A.Qout = Q2;
+        if ((rc = run_stage(h, st == 0 ? Q : Q2, A, s))) return rc;
+        ghost(h, Q2, s);
+      }
+      A.mode = CM_RK4_4; A.coef = 1.0; A.Qin = Q; A.Qout = Q;
+      if ((rc = run_stage(h, Q2, A, s))) return rc;
+      ghost(h, Q, s);
+    }
+  }
+  OUX_CUDA(cudaGetLastError());
+  return OUX_OK;
+}
+
+int oux_diagnostics(oux_handle* h, double out[3], void* stream) {
+  if (!h || !out) return fail(OUX_E_INVALID, "null argument");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo& G = h->G;
+  int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
+  if (G.dim == 3) k_prim<3, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(h->Q, G, h->W, h->M.jac, h->K);
+  else k_prim<2, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(h->Q, G, h->W, h->M.jac, h->K);
+  k_diag<<<DIAG_BLOCKS, 256, 0, s>>>(G, h->W, h->M, h->K.gamma, h->cfg.order, h->partials);
+  int64_t nint = (int64_t)(G.nx - 2 * G.g) * (G.ny - 2 * G.g) * (G.dim == 3 ? G.nz - 2 * G.g : 1);
+  double* res = h->partials + 3 * DIAG_BLOCKS;
+  k_diag_final<<<1, 256, 0, s>>>(h->partials, DIAG_BLOCKS, 1.0 / (double)nint, res);
+  OUX_CUDA(cudaGetLastError());
+  OUX_CUDA(cudaMemcpyAsync(out, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  OUX_CUDA(cudaStreamSynchronize(s));
+  return OUX_OK;
+}
+
+int oux_check_state(oux_handle* h, int32_t* fault_bits, void* stream) {
+  if (!h || !fault_bits) return fail(OUX_E_INVALID, "null argument");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo& G = h->G;
+  int64_t n = (int64_t)(G.nx - 2 * G.g) * (G.ny - 2 * G.g) * (G.dim == 3 ? G.nz - 2 * G.g : 1);
+  k_check<<<grid_for(n, 256), 256, 0, s>>>(h->Q, G, h->M.jac, h->K.gamma_1, h->status);
+  OUX_CUDA(cudaGetLastError());
+  int v = 0;
+  OUX_CUDA(cudaMemcpyAsync(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  OUX_CUDA(cudaStreamSynchronize(s));
+  *fault_bits = v;
+  return v ? fail(OUX_E_DEVICE_FAULT, "device status word reports a fault") : OUX_OK;
+}
+
+int oux_status(oux_handle* h, int32_t* fault_bits) {
+  if (!h || !fault_bits) return fail(OUX_E_INVALID, "null argument");
+  if (!h->status) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  int v = 0;
+  OUX_CUDA(cudaMemcpy(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost));
+  *fault_bits = v;
+  return OUX_OK;
+}
+
+int oux_launch_count(const oux_handle* h, int64_t* launches) {
+  if (!h || !launches) return fail(OUX_E_INVALID, "null argument");
+  *launches = h->launches;
+  return OUX_OK;
+}
+
+}  // extern "C"

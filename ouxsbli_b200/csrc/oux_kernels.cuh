@@ -1,0 +1,279 @@
+// Kernels of one explicit stage on the ghost-padded SoA layout.
+//
+// Per stage (3D): prim -> [sensor] -> [SGS mut/qc2 + their edge copy] ->
+//   x sweep (faces -> dt*S*dE into Racc) -> y sweep (+= dt*S*dF) ->
+//   z sweep (+= dt*S*dG, then the RK combination) -> ghost fill.
+// Face fluxes never touch HBM: each sweep block computes the 2*ORDER/2 + 32
+// cell tile of its pencil rows into shared memory, evaluates every face of the
+// tile once, and differences neighbouring faces in shared memory.
+#pragma once
+#include <cstdint>
+#include "oux_math.cuh"
+
+namespace oux {
+
+enum ViscKind { VK_EULER = 0, VK_C6 = 1, VK_C4 = 2, VK_ME4 = 3, VK_GV2 = 4, VK_2D4 = 5 };
+enum CombineMode {
+  CM_ACCUM = 0,   // first/middle sweep: Racc (=|+=) c * dF
+  CM_R_OUT = 1,   // last sweep: write R to an output buffer (reference Rs order)
+  CM_RK3 = 2,     // Qout = (c1*Qin + c2*Qout - R) * c4      (calc_step2_3)
+  CM_RK4_S = 3,   // Qs = Qn - c1*R ; Rs = Rs + c2*R          (calc_step)
+  CM_RK4_4 = 4,   // R = Rs + R ; Qn = Qn - R/6 ; Rs = 0      (calc_step4)
+  CM_RK3_1 = 5    // Qs = Qn - R                              (calc_step1)
+};
+
+struct Geo {
+  int dim, nx, ny, nz, g;     // padded extents, ghost width
+  int64_t sx, plane, vs;      // row stride, plane stride, variable stride (elements)
+  __host__ __device__ int64_t at(int i, int j, int k) const { return (int64_t)k * plane + (int64_t)j * sx + i; }
+};
+
+template <class T> struct Fields {
+  // primitive / auxiliary arrays (each vs elements)
+  T *rho, *u, *v, *w, *p, *T_, *mu, *sensor, *mut, *qc2;
+};
+
+struct Metrics {
+  const double *inv_dx, *inv_dy, *inv_dz;   // 1/dx, n-1 each
+  const double *jac;                        // (nx,ny)
+  const double *dtdxdy, *dtdydz, *dtdzdx;   // 3D: (nx-2)(ny-2), (ny-2)(nz-2), (nx-2)(nz-2)
+  const double *dtdx, *dtdy;                // 2D: nx-2, ny-2
+};
+
+template <class T> struct StepArgs {
+  Geo G;
+  Fields<T> W;
+  Metrics M;
+  PhysConst K;
+  int scheme, tvd, slau;
+  // state (conservative / J) and accumulators, nv * vs each
+  T* Qin;       // Q^n (or the stage input for CM_RK3's c1 term)
+  T* Qout;      // output state (may alias Qin's role per mode)
+  T* Rs;        // RK4 accumulator
+  double* Racc; // running flux difference (FP64)
+  double* Rout; // CM_R_OUT destination
+  double coef;  // metric scale (RK3 coef3 or 1)
+  double c1, c2, c4;
+  int mode;
+};
+
+// ---- prim: src/calc_physical_quantities.f90:60-116 (3D), :7-57 (2D) -------
+template <int DIM, bool VISC, class T>
+__global__ void k_prim(const T* __restrict__ Q, Geo G, Fields<T> W, const double* __restrict__ jac,
+                       PhysConst K) {
+  int64_t n = (int64_t)G.nx * G.ny * G.nz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx);
+    int64_t r = t / G.nx;
+    int j = (int)(r % G.ny);
+    int k = (int)(r / G.ny);
+    int64_t o = G.at(i, j, k);
+    T Jv = (T)jac[(int64_t)j * G.nx + i];
+    T q1 = Q[o];
+    T over_Q1 = T(1) / q1;
+    T rho = Jv * q1;
+    T u = Q[o + G.vs] * over_Q1;
+    T v = Q[o + 2 * G.vs] * over_Q1;
+    T w = T(0), p;
+    if constexpr (DIM == 3) {
+      w = Q[o + 3 * G.vs] * over_Q1;
+      p = T(K.gamma_1) * (Jv * Q[o + 4 * G.vs] - T(0.5) * rho * (u * u + v * v + w * w));
+    } else {
+      p = T(K.gamma_1) * (Jv * Q[o + 3 * G.vs] - T(0.5) * rho * (u * u + v * v));
+    }
+    W.rho[o] = rho; W.u[o] = u; W.v[o] = v;
+    if constexpr (DIM == 3) W.w[o] = w;
+    W.p[o] = p;
+    T temp = p / (T(K.R) * rho);
+    W.T_[o] = temp;
+    if constexpr (VISC) W.mu[o] = T(K.sutherland) / (temp + T(111)) * (temp * sqrt(temp));
+  }
+}
+
+// ---- Ducros sensor: 3D_solver/src/calc_hybrid.f90:11-72 (2D twin :11-55) ---
+template <int DIM, class T>
+__global__ void k_sensor(Geo G, Fields<T> W, Metrics M) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  int k = (DIM == 3) ? (int)(blockIdx.z * blockDim.z + threadIdx.z + 1) : 0;
+  if (i > G.nx - 2 || j > G.ny - 2) return;
+  if (DIM == 3 && k > G.nz - 2) return;
+  const T eps = T(1.0e-12);
+  int64_t o = G.at(i, j, k);
+  T dxt = T(0.25) * ((T)M.inv_dx[i - 1] + (T)M.inv_dx[i]);
+  T dyt = T(0.25) * ((T)M.inv_dy[j - 1] + (T)M.inv_dy[j]);
+  T f;
+  if constexpr (DIM == 3) {
+    T dzt = T(0.25) * ((T)M.inv_dz[k - 1] + (T)M.inv_dz[k]);
+    int64_t ox = 1, oy = G.sx, oz = G.plane;
+    T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
+    T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
+    T dwdx = (-W.w[o - ox] + W.w[o + ox]) * dxt;
+    T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
+    T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
+    T dwdy = (-W.w[o - oy] + W.w[o + oy]) * dyt;
+    T dudz = (-W.u[o - oz] + W.u[o + oz]) * dzt;
+    T dvdz = (-W.v[o - oz] + W.v[o + oz]) * dzt;
+    T dwdz = (-W.w[o - oz] + W.w[o + oz]) * dzt;
+    T div = dudx + dvdy + dwdz;
+    T r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
+    f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
+  } else {
+    int64_t ox = 1, oy = G.sx;
+    T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
+    T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
+    T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
+    T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
+    T div = dudx + dvdy;
+    T rot = dvdx - dudy;
+    f = (div * div) / (div * div + rot * rot + eps);
+  }
+  f = fmin_f(T(1), f);
+  W.sensor[o] = f;
+  // edge copies of the reference kernel's tail
+  if (i == 1) W.sensor[G.at(0, j, k)] = f; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = f;
+  if (j == 1) W.sensor[G.at(i, 0, k)] = f; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = f;
+  if constexpr (DIM == 3) {
+    if (k == 1) W.sensor[G.at(i, j, 0)] = f; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = f;
+  }
+}
+
+// ---- SMS sub-grid model: 3D_solver/src/calc_les.f90:30-125 -------------------
+template <class T>
+__device__ __forceinline__ void grad3(const T (&u)[3][3][3], const T (&v)[3][3][3], const T (&w)[3][3][3],
+                                      T dx, T dy, T dz, T d[9]) {  // calc_differential :11-27
+  d[0] = T(0.5) * (-u[1][1][0] + u[1][1][2]) * dx;
+  d[1] = T(0.5) * (-u[1][0][1] + u[1][2][1]) * dy;
+  d[2] = T(0.5) * (-u[0][1][1] + u[2][1][1]) * dz;
+  d[3] = T(0.5) * (-v[1][1][0] + v[1][1][2]) * dx;
+  d[4] = T(0.5) * (-v[1][0][1] + v[1][2][1]) * dy;
+  d[5] = T(0.5) * (-v[0][1][1] + v[2][1][1]) * dz;
+  d[6] = T(0.5) * (-w[1][1][0] + w[1][1][2]) * dx;
+  d[7] = T(0.5) * (-w[1][0][1] + w[1][2][1]) * dy;
+  d[8] = T(0.5) * (-w[0][1][1] + w[2][1][1]) * dz;
+}
+
+template <class T>
+__device__ __forceinline__ T filt(const T* a, int64_t o, int64_t sx, int64_t pl) {  // test_filter :74-80
+  T c = a[o];
+  return c + T(0.25) * (a[o - 1] - T(2) * c + a[o + 1] + a[o - sx] - T(2) * c + a[o + sx] + a[o - pl] -
+                        T(2) * c + a[o + pl]);
+}
+
+template <class T>
+__global__ void k_mut(Geo G, Fields<T> W, Metrics M, PhysConst K) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (i > G.nx - 2 || j > G.ny - 2 || k > G.nz - 2) return;
+  const int64_t sx = G.sx, pl = G.plane;
+  int64_t o = G.at(i, j, k);
+  T u3[3][3][3], v3[3][3][3], w3[3][3][3], ut[3][3][3], vt[3][3][3], wt[3][3][3];
+  bool inner = (2 <= i && i <= G.nx - 3 && 2 <= j && j <= G.ny - 3 && 2 <= k && k <= G.nz - 3);
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        int64_t q = o + (a - 1) + (b - 1) * sx + (c - 1) * pl;
+        u3[c][b][a] = W.u[q]; v3[c][b][a] = W.v[q]; w3[c][b][a] = W.w[q];
+        if (inner) {
+          ut[c][b][a] = filt(W.u, q, sx, pl);
+          vt[c][b][a] = filt(W.v, q, sx, pl);
+          wt[c][b][a] = filt(W.w, q, sx, pl);
+        } else {
+          ut[c][b][a] = u3[c][b][a]; vt[c][b][a] = v3[c][b][a]; wt[c][b][a] = w3[c][b][a];
+        }
+      }
+  T du = u3[1][1][1] - ut[1][1][1], dv = v3[1][1][1] - vt[1][1][1], dw = w3[1][1][1] - wt[1][1][1];
+  T qc2 = T(0.5) * (du * du + dv * dv + dw * dw);
+  // SMS :30-71
+  T dx = (T)M.inv_dx[i], dy = (T)M.inv_dy[j], dz = (T)M.inv_dz[k];
+  T a[9], h[9];
+  grad3(u3, v3, w3, dx, dy, dz, a);
+  grad3(ut, vt, wt, dx, dy, dz, h);
+  T vo1 = a[7] - a[5], vo2 = a[2] - a[6], vo3 = a[3] - a[1];
+  T vh1 = h[7] - h[5], vh2 = h[2] - h[6], vh3 = h[3] - h[1];
+  T vd1 = vo1 - vh1, vd2 = vo2 - vh2, vd3 = vo3 - vh3;
+  T vor2 = vo1 * vo1 + vo2 * vo2 + vo3 * vo3;
+  T vorh2 = vh1 * vh1 + vh2 * vh2 + vh3 * vh3;
+  T vdif2 = vd1 * vd1 + vd2 * vd2 + vd3 * vd3;
+  T svor2 = T(2) * sqrt(vor2) * sqrt(vorh2) + vorh2 + vor2 - vdif2;
+  T tan2 = (fabs(svor2) < T(1.0e-30)) ? T(0)
+                                       : (T(2) * sqrt(vorh2) * sqrt(vor2) - vorh2 - vor2 + vdif2) / svor2;
+  T rth = tan2 / T(K.tan10deg2);
+  T fth = fmin_f(T(1), rth * rth);
+  T S2 = T(2) * (a[0] * a[0] + a[4] * a[4] + a[8] * a[8]) +
+         ((a[3] + a[1]) * (a[3] + a[1]) + (a[7] + a[5]) * (a[7] + a[5]) + (a[2] + a[6]) * (a[2] + a[6]));
+  T mn = fmin_f(fmin_f(dx, dy), dz);
+  T a1 = mn / dx, a2 = mn / dy;
+  T l1 = log(a1), l2 = log(a2);
+  T delta = cosh(sqrt(T(4) * (l1 * l1 - l1 * l2 + l2 * l2) / T(27))) * pow(dx * dy * dz, T(-1.0 / 3.0));
+  const T Cm = T(0.06), alpha = T(0.5);
+  T nut = fth * Cm * pow(S2, T(0.5) * alpha) * pow(qc2, T(0.5) * (T(1) - alpha)) * pow(delta, T(1) + alpha);
+  W.qc2[o] = qc2;
+  W.mut[o] = W.rho[o] * nut;
+}
+
+// set_bc_mut_common (3D_solver/src/set_bc_common.f90:296-335): one ghost layer,
+// images taken at distance n-2 (the reference's composite copy order).
+template <class T>
+__global__ void k_mut_edges(Geo G, Fields<T> W) {
+  int64_t n = (int64_t)G.nx * G.ny * G.nz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx);
+    int64_t r = t / G.nx;
+    int j = (int)(r % G.ny);
+    int k = (int)(r / G.ny);
+    bool edge = (i == 0 || i == G.nx - 1 || j == 0 || j == G.ny - 1 || k == 0 || k == G.nz - 1);
+    if (!edge) continue;
+    int si = i == 0 ? G.nx - 2 : (i == G.nx - 1 ? 1 : i);
+    int sj = j == 0 ? G.ny - 2 : (j == G.ny - 1 ? 1 : j);
+    int sk = k == 0 ? G.nz - 2 : (k == G.nz - 1 ? 1 : k);
+    int64_t o = G.at(i, j, k), s = G.at(si, sj, sk);
+    W.mut[o] = W.mut[s];
+    W.qc2[o] = W.qc2[s];
+  }
+}
+
+// ---- periodic ghost fill: set_bc_cyclic{2,4,6} (set_bc_common.f90:101-273) ---
+// Every ghost cell takes its interior image; the three groups enumerate
+// z-ghost planes, y-ghost rows of interior planes and x-ghost cells of
+// interior rows without touching interior cells.
+template <class T>
+__global__ void k_ghost(T* Q, Geo G, int nv) {
+  const int g = G.g;
+  const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
+  const int gz = (G.dim == 3) ? 2 * g : 0;
+  int64_t nA = (int64_t)gz * G.ny * G.nx;            // z ghost planes
+  int64_t nB = (int64_t)Nz * (2 * g) * G.nx;         // y ghost rows
+  int64_t nC = (int64_t)Nz * Ny * (2 * g);           // x ghost cells
+  int64_t tot = nA + nB + nC;
+  int zo = (G.dim == 3) ? g : 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    if (t < nA) {
+      i = (int)(t % G.nx); int64_t r = t / G.nx; j = (int)(r % G.ny); int kk = (int)(r / G.ny);
+      k = kk < g ? kk : G.nz - 2 * g + kk;
+    } else if (t < nA + nB) {
+      int64_t s = t - nA;
+      i = (int)(s % G.nx); int64_t r = s / G.nx; int jj = (int)(r % (2 * g)); k = (int)(r / (2 * g)) + zo;
+      j = jj < g ? jj : G.ny - 2 * g + jj;
+    } else {
+      int64_t s = t - nA - nB;
+      int ii = (int)(s % (2 * g)); int64_t r = s / (2 * g); j = (int)(r % Ny) + g; k = (int)(r / Ny) + zo;
+      i = ii < g ? ii : G.nx - 2 * g + ii;
+    }
+    int si = (i - g + Nx) % Nx + g;
+    int sj = (j - g + Ny) % Ny + g;
+    int sk = (G.dim == 3) ? (k - g + Nz) % Nz + g : 0;
+    int64_t o = G.at(i, j, k), s = G.at(si, sj, sk);
+    for (int l = 0; l < nv; ++l) Q[o + l * G.vs] = Q[s + l * G.vs];
+  }
+}
+
+}  // namespace oux

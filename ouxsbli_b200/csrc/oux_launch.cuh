@@ -1,0 +1,37 @@
+// Grid/block/shared-memory setup for the three sweeps of one stage.
+#pragma once
+#include "oux_sweep.cuh"
+
+namespace oux {
+
+template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
+int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
+  constexpr size_t smem = sweep_smem<ORDER, DIR, T>();
+  auto kern = k_sweep<DIM, DIR, ORDER, VK, LES, T>;
+  static const cudaError_t attr_rc =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (attr_rc != cudaSuccess) return 1;
+  const Geo& G = A.G;
+  const int g = G.g;
+  const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g, Nz = DIM == 3 ? G.nz - 2 * g : 1;
+  dim3 block(SweepShape<DIR>::TX, SweepShape<DIR>::TY, 1);
+  dim3 grid;
+  if (DIR == 0) grid = dim3((Nx + 31) / 32, (Ny + SWEEP_BR - 1) / SWEEP_BR, Nz);
+  else if (DIR == 1) grid = dim3((Nx + 31) / 32, (Ny + SWEEP_BF - 1) / SWEEP_BF, Nz);
+  else grid = dim3((Nx + 31) / 32, (Nz + SWEEP_BF - 1) / SWEEP_BF, Ny);
+  kern<<<grid, block, smem, s>>>(A, last);
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
+}
+
+template <int DIM, int ORDER, int VK, bool LES, class T>
+int launch_stage_sweeps(const StepArgs<T>& A, cudaStream_t s) {
+  if (launch_one<DIM, 0, ORDER, VK, LES, T>(A, 0, s)) return 1;
+  if constexpr (DIM == 3) {
+    if (launch_one<DIM, 1, ORDER, VK, LES, T>(A, 0, s)) return 1;
+    return launch_one<DIM, 2, ORDER, VK, LES, T>(A, 1, s);
+  } else {
+    return launch_one<DIM, 1, ORDER, VK, LES, T>(A, 1, s);
+  }
+}
+
+}  // namespace oux

@@ -1,0 +1,656 @@
+// Directional flux sweeps: face fluxes (convective + viscous) of a pencil tile
+// evaluated in shared memory and differenced into the stage residual, with the
+// Runge-Kutta combination fused into the last sweep of the stage.
+//
+// Block shapes (cells per block along the sweep, pencil rows):
+//   x sweep: 32 cells x BR rows, threads (33, BR): thread tx owns face tx-1.
+//   y/z sweep: 32 x-cells x BF cells along the sweep, threads (32, BF+1).
+// Tile = the block's cells plus H = ORDER/2 halo cells on each side along the
+// sweep; it holds rho,u,v,w,p,T,mu,mut,qc2,sensor and the four transverse
+// velocity derivatives the viscous stencils need.
+#pragma once
+#include "oux_kernels.cuh"
+
+namespace oux {
+
+constexpr int SWEEP_BR = 4;   // x sweep rows per block
+constexpr int SWEEP_BF = 8;   // y/z sweep cells per block along the sweep
+
+enum TileField { TF_RHO = 0, TF_U, TF_V, TF_W, TF_P, TF_T, TF_MU, TF_MUT, TF_QC2, TF_SEN, TF_D0, TF_D1, TF_D2, TF_D3, TF_COUNT };
+
+template <int DIR> struct SweepShape {
+  static constexpr int TX = (DIR == 0) ? 33 : 32;
+  static constexpr int TY = (DIR == 0) ? SWEEP_BR : SWEEP_BF + 1;
+};
+
+// The tile halo is 3 cells for every order: the widest stencils (6-point
+// convective, Central-6 / ME4 / 2D 4th-order viscous) reach 2 cells left and
+// 3 cells right of a face's left cell.
+constexpr int TILE_HALO = 3;
+template <int ORDER, int DIR> __host__ __device__ constexpr int tile_len() {
+  return DIR == 0 ? 32 + 2 * TILE_HALO : SWEEP_BF + 2 * TILE_HALO;
+}
+template <int ORDER, int DIR> __host__ __device__ constexpr int tile_cells() {
+  return DIR == 0 ? tile_len<ORDER, DIR>() * SWEEP_BR : tile_len<ORDER, DIR>() * 32;
+}
+template <int ORDER, int DIR, class T> __host__ __device__ constexpr size_t sweep_smem() {
+  // TF_COUNT tile fields + 5 face-flux components per face thread (FP64)
+  return sizeof(T) * TF_COUNT * tile_cells<ORDER, DIR>() +
+         sizeof(double) * 5 * SweepShape<DIR>::TX * SweepShape<DIR>::TY;
+}
+
+// transverse node derivative of `a` along axis `ax` at offset o (4th/6th order)
+template <bool SIXTH, class T>
+__device__ __forceinline__ T node_d(const T* __restrict__ a, int64_t o, int64_t st, T inv) {
+  if constexpr (SIXTH)
+    return (T(1.0 / 60.0) * (-a[o - 3 * st] + a[o + 3 * st]) + T(0.15) * (a[o - 2 * st] - a[o + 2 * st]) +
+            T(0.75) * (-a[o - st] + a[o + st])) * inv;
+  else
+    return (T(2.0 / 3.0) * (-a[o - st] + a[o + st]) - T(1.0 / 12.0) * (-a[o - 2 * st] + a[o + 2 * st])) * inv;
+}
+
+// ---- convective face flux: calc_{keep,slau,hybrid,roe}_{x,y,z}_in ---------------
+// s(f,m) reads tile field f at stencil point m (0 .. 2io+1).
+template <int ORDER, class T, class Acc>
+__device__ __forceinline__ void conv_flux(const StepArgs<T>& A, const Acc& s, T fd, int nd, T F[5]) {
+  constexpr int NS = ORDER;  // 2io+2 stencil points
+  T rho[NS], u[NS], v[NS], w[NS], p[NS], Tt[NS];
+#pragma unroll
+  for (int m = 0; m < NS; ++m) {
+    rho[m] = s(TF_RHO, m); u[m] = s(TF_U, m); v[m] = s(TF_V, m); w[m] = s(TF_W, m);
+    p[m] = s(TF_P, m); Tt[m] = s(TF_T, m);
+  }
+  const T* un = nd == 0 ? u : (nd == 1 ? v : w);
+  const int scheme = A.scheme;
+  if (scheme == 0 || (scheme == 3 && fd <= T(A.K.threshold))) {
+    keep_flux<ORDER>(rho, u, v, w, un, p, Tt, nd, T(A.K.R_over_gamma_1), F);
+    return;
+  }
+  T Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, Lp, Rp;
+  const T thr = T(A.K.threshold);
+  reconstruct<ORDER>(A.tvd, thr, fd, rho, Lr, Rr);
+  reconstruct<ORDER>(A.tvd, thr, fd, u, Lu, Ru);
+  reconstruct<ORDER>(A.tvd, thr, fd, v, Lv, Rv);
+  reconstruct<ORDER>(A.tvd, thr, fd, w, Lw, Rw);
+  reconstruct<ORDER>(A.tvd, thr, fd, p, Lp, Rp);
+  if (scheme == 1 || scheme == 3) {
+    T HR;
+    if (scheme == 3 || ORDER == 2) HR = T(1);
+    else if constexpr (ORDER == 6) HR = wiggle(p[1], p[2], p[3], p[4]);
+    else HR = wiggle(p[0], p[1], p[2], p[3]);
+    T un1 = nd == 0 ? Lu : (nd == 1 ? Lv : Lw);
+    T un2 = nd == 0 ? Ru : (nd == 1 ? Rv : Rw);
+    slau_flux(A.slau == 1, Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, un1, un2, Lp, Rp, nd, HR, T(A.K.gamma),
+              T(A.K.gamma_over_gamma_1), F);
+  } else {  // Roe with the normal velocity first (calc_roe_{y,z}_in permutations)
+    T Fr[5];
+    const T g1 = T(A.K.gamma_1), og1 = T(A.K.over_gamma_1), gg = T(A.K.gamma_over_gamma_1);
+    if (nd == 0) {
+      roe_flux(Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, Lp, Rp, g1, og1, gg, Fr);
+      F[0] = Fr[0]; F[1] = Fr[1]; F[2] = Fr[2]; F[3] = Fr[3]; F[4] = Fr[4];
+    } else if (nd == 1) {
+      roe_flux(Lr, Rr, Lv, Rv, Lw, Rw, Lu, Ru, Lp, Rp, g1, og1, gg, Fr);
+      F[0] = Fr[0]; F[2] = Fr[1]; F[3] = Fr[2]; F[1] = Fr[3]; F[4] = Fr[4];
+    } else {
+      roe_flux(Lr, Rr, Lw, Rw, Lu, Ru, Lv, Rv, Lp, Rp, g1, og1, gg, Fr);
+      F[0] = Fr[0]; F[3] = Fr[1]; F[1] = Fr[2]; F[2] = Fr[3]; F[4] = Fr[4];
+    }
+  }
+}
+
+// ---- high-order viscous face terms: calc_visc_high_internal.f90.fypp ----------
+// Stencil points m = 0..5 (C6, ME4) or 0..3 (C4) start at face cell - 2 (- 1).
+// D0,D1 = straight-stress derivatives (cyclic pair), D2,D3 = normal velocity
+// along the two tangential axes in increasing axis order.
+template <int VK, bool LES, class T, class Acc>
+__device__ __forceinline__ void visc_high(const StepArgs<T>& A, const Acc& s, int nd, T inv, T out[4]) {
+  const T two3 = T(2.0 / 3.0);
+  const int ca = nd == 0 ? 1 : 0, cb = nd == 2 ? 1 : 2;
+  const int fn = TF_U + nd, fa = TF_U + ca, fb = TF_U + cb;
+  T tn, ta, tb, wn, wa, wb, kT, Hs = T(0);
+  if constexpr (VK == VK_C6 || VK == VK_C4) {
+    constexpr int N = (VK == VK_C6) ? 6 : 4;
+    T mu[N], mut[N], un[N], ua[N], ub[N], s0[N], s1[N], c0[N], c1[N], Tt[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      mu[m] = s(TF_MU, m); un[m] = s(fn, m); ua[m] = s(fa, m); ub[m] = s(fb, m);
+      s0[m] = s(TF_D0, m); s1[m] = s(TF_D1, m); c0[m] = s(TF_D2, m); c1[m] = s(TF_D3, m);
+      Tt[m] = s(TF_T, m);
+      if constexpr (LES) mut[m] = s(TF_MUT, m);
+    }
+    T mui = v_interp<N>(mu);
+    kT = T(A.K.Cp_over_Pr) * mui * v_diff<N>(inv, Tt);
+    // calc_tau_straight(_LES) / calc_tau_cross(_LES), calc_visc_cent.f90.fypp:23-91
+    {
+      T s0i = v_interp<N>(s0), s1i = v_interp<N>(s1), dn = v_diff<N>(inv, un);
+      tn = two3 * mui * (T(2) * dn - s0i - s1i);
+      wn = v_interp<N>(un) * tn;
+      if constexpr (LES) {
+        T m2 = T(0.5) * (mui + v_interp<N>(mut));
+        tn = two3 * m2 * (T(2) * dn - s0i - s1i);
+      }
+    }
+    {
+      T ci = v_interp<N>(c0), dv = v_diff<N>(inv, ua);
+      ta = mui * (ci + dv);
+      wa = v_interp<N>(ua) * ta;
+      if constexpr (LES) { T m2 = T(0.5) * (mui + v_interp<N>(mut)); ta = m2 * (ci + dv); }
+    }
+    {
+      T ci = v_interp<N>(c1), dv = v_diff<N>(inv, ub);
+      tb = mui * (ci + dv);
+      wb = v_interp<N>(ub) * tb;
+      if constexpr (LES) { T m2 = T(0.5) * (mui + v_interp<N>(mut)); tb = m2 * (ci + dv); }
+    }
+    if constexpr (LES) {
+      T H[N];
+#pragma unroll
+      for (int m = 0; m < N; ++m) {
+        T uu = s(TF_U, m), vv = s(TF_V, m), ww = s(TF_W, m);
+        H[m] = T(A.K.Cp) * Tt[m] + T(0.5) * (uu * uu + vv * vv + ww * ww) + s(TF_QC2, m);
+      }
+      Hs = -v_interp<N>(mut) * v_diff<N>(inv, H) / T(A.K.Prt);
+    }
+  } else {  // VK_ME4: calc_visc_me4_base.f90:4-111 on a 6-point stencil
+    T mu3[3], mut3[3], k3[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      mu3[q] = T(0.0625) * (T(9) * (s(TF_MU, q + 1) + s(TF_MU, q + 2)) - (s(TF_MU, q) + s(TF_MU, q + 3)));
+      if constexpr (LES)
+        mut3[q] = T(0.0625) * (T(9) * (s(TF_MUT, q + 1) + s(TF_MUT, q + 2)) - (s(TF_MUT, q) + s(TF_MUT, q + 3)));
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      k3[q] = T(A.K.Cp_over_Pr) * mu3[q] *
+              (T(1.125) * (-s(TF_T, q + 1) + s(TF_T, q + 2)) - (-s(TF_T, q) + s(TF_T, q + 3)) * T(1.0 / 24.0)) * inv;
+    kT = flux4(k3[0], k3[1], k3[2]);
+    // straight
+    {
+      T t1[3], t2[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        T a0 = s(fn, q), a1 = s(fn, q + 1), a2 = s(fn, q + 2), a3 = s(fn, q + 3);
+        T y0 = s(TF_D0, q), y1 = s(TF_D0, q + 1), y2 = s(TF_D0, q + 2), y3 = s(TF_D0, q + 3);
+        T z0 = s(TF_D1, q), z1 = s(TF_D1, q + 1), z2 = s(TF_D1, q + 2), z3 = s(TF_D1, q + 3);
+        T dd = (T(2.25) * (-a1 + a2) - (-a0 + a3) * T(1.0 / 12.0)) * inv;
+        if constexpr (!LES) {
+          t1[q] = two3 * mu3[q] * (dd - T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3) -
+                                   T(0.0625) * (-z0 + T(9) * (z1 + z2) - z3));
+        } else {
+          t1[q] = dd;
+          t1[q] = t1[q] - T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3);
+          t1[q] = t1[q] - T(0.0625) * (-z0 + T(9) * (z1 + z2) - z3);
+        }
+      }
+      if constexpr (!LES) {
+        tn = flux4(t1[0], t1[1], t1[2]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          t2[q] = T(0.0625) * (-s(fn, q) + T(9) * (s(fn, q + 1) + s(fn, q + 2)) - s(fn, q + 3)) * t1[q];
+        wn = flux4(t2[0], t2[1], t2[2]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) t2[q] = two3 * mu3[q] * t1[q];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          t2[q] = T(0.0625) * (-s(fn, q) + T(9) * (s(fn, q + 1) + s(fn, q + 2)) - s(fn, q + 3)) * t2[q];
+        wn = flux4(t2[0], t2[1], t2[2]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) t2[q] = two3 * (mu3[q] + mut3[q]) * t1[q];
+        tn = flux4(t2[0], t2[1], t2[2]);
+      }
+    }
+    // cross terms (component fa with derivative D2, component fb with D3)
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int fv = side == 0 ? fa : fb, fd_ = side == 0 ? TF_D2 : TF_D3;
+      T t1[3], t2[3], tt, ww;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        T a0 = s(fv, q), a1 = s(fv, q + 1), a2 = s(fv, q + 2), a3 = s(fv, q + 3);
+        T y0 = s(fd_, q), y1 = s(fd_, q + 1), y2 = s(fd_, q + 2), y3 = s(fd_, q + 3);
+        T dd = (T(1.125) * (-a1 + a2) - (-a0 + a3) * T(1.0 / 24.0)) * inv;
+        if constexpr (!LES) t1[q] = mu3[q] * (dd + T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3));
+        else { t1[q] = dd; t1[q] = t1[q] + T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3); }
+      }
+      if constexpr (!LES) {
+        tt = flux4(t1[0], t1[1], t1[2]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          t2[q] = T(0.0625) * (-s(fv, q) + T(9) * (s(fv, q + 1) + s(fv, q + 2)) - s(fv, q + 3)) * t1[q];
+        ww = flux4(t2[0], t2[1], t2[2]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) t2[q] = mu3[q] * t1[q];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          t2[q] = T(0.0625) * (-s(fv, q) + T(9) * (s(fv, q + 1) + s(fv, q + 2)) - s(fv, q + 3)) * t2[q];
+        ww = flux4(t2[0], t2[1], t2[2]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) t2[q] = (mu3[q] + mut3[q]) * t1[q];
+        tt = flux4(t2[0], t2[1], t2[2]);
+      }
+      if (side == 0) { ta = tt; wa = ww; } else { tb = tt; wb = ww; }
+    }
+    if constexpr (LES) {
+      T H[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        T uu = s(TF_U, m + 1), vv = s(TF_V, m + 1), ww = s(TF_W, m + 1);
+        H[m] = T(A.K.Cp) * s(TF_T, m + 1) + T(0.5) * (uu * uu + vv * vv + ww * ww) + s(TF_QC2, m + 1);
+      }
+      Hs = -flux4(mut3[0], mut3[1], mut3[2]) * (T(1.125) * (-H[1] + H[2]) - (-H[0] + H[3]) * T(1.0 / 24.0)) *
+           inv / T(A.K.Prt);
+    }
+  }
+  T t[3], wk[3];
+  t[nd] = tn; t[ca] = ta; t[cb] = tb;
+  wk[nd] = wn; wk[ca] = wa; wk[cb] = wb;
+  out[0] = t[0]; out[1] = t[1]; out[2] = t[2];
+  T e = wk[0] + wk[1] + wk[2] + kT;
+  if constexpr (LES) e = e + Hs;
+  out[3] = e;
+}
+
+// ---- Gaitonde-Visbal 2nd order: 3D_solver/src/calc_visc2.f90.fypp (2D :10-103) ----
+// Reads global arrays directly: face between o and o + st[nd].
+template <int DIM, bool LES, class T>
+__device__ __forceinline__ void visc_gv2(const StepArgs<T>& A, int nd, int64_t o, const int64_t st[3],
+                                         const T invs[3], T out[4]) {
+  const Fields<T>& W = A.W;
+  const int64_t o2 = o + st[nd];
+  const T inv = invs[nd];
+  auto vel = [&](int c, int64_t q) -> T { return c == 0 ? W.u[q] : (c == 1 ? W.v[q] : (DIM == 3 ? W.w[q] : T(0))); };
+  T md = T(0.5) * (W.mu[o] + W.mu[o2]) * inv;
+  T vw = T(A.K.Cp_over_Pr) * md * (-W.T_[o] + W.T_[o2]);
+  T dn[3], sg[3] = {T(0), T(0), T(0)}, Hs = T(0);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dn[c] = md * (-vel(c, o) + vel(c, o2));
+  if constexpr (LES) {
+    T msd = T(0.5) * (W.mut[o] + W.mut[o2]) * inv;
+    auto Hf = [&](int64_t q) {
+      T uu = W.u[q], vv = W.v[q], ww = W.w[q];
+      return T(A.K.Cp) * W.T_[q] + T(0.5) * (uu * uu + vv * vv + ww * ww) + W.qc2[q];
+    };
+    T H1 = Hf(o), H2 = Hf(o2);
+    Hs = -msd * (-H1 + H2) / T(A.K.Prt);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sg[c] = msd * (-vel(c, o) + vel(c, o2));
+  }
+  auto cross = [&](bool sgs, int c, int t) -> T {
+    const T* m = sgs ? W.mut : W.mu;
+    const int64_t s = st[t];
+    T m1 = T(0.0625) * (m[o - s] + m[o] + m[o2 - s] + m[o2]);
+    T m2 = T(0.0625) * (m[o] + m[o + s] + m[o2] + m[o2 + s]);
+    return (m1 * (-vel(c, o - s) - vel(c, o2 - s)) + (m1 - m2) * (vel(c, o) + vel(c, o2)) +
+            m2 * (vel(c, o + s) + vel(c, o2 + s))) * invs[t];
+  };
+  T uS = W.u[o] + W.u[o2], vS = W.v[o] + W.v[o2];
+  T wS = (DIM == 3) ? (W.w[o] + W.w[o2]) : T(0);
+  const T two3 = T(2.0 / 3.0);
+  T s1, s2, s3 = T(0);
+  if constexpr (DIM == 3) {
+    if (nd == 0) {
+      T txx = two3 * (T(2) * dn[0] - cross(false, 1, 1) - cross(false, 2, 2));
+      T txy = cross(false, 0, 1) + dn[1];
+      T txz = dn[2] + cross(false, 0, 2);
+      vw = vw + T(0.5) * (uS * txx + vS * txy + wS * txz);
+      if constexpr (LES) {
+        txx = txx + two3 * (T(2) * sg[0] - cross(true, 1, 1) - cross(true, 2, 2));
+        txy = txy + cross(true, 0, 1) + sg[1];
+        txz = txz + sg[2] + cross(true, 0, 2);
+      }
+      s1 = txx; s2 = txy; s3 = txz;
+    } else if (nd == 1) {
+      T tyx = dn[0] + cross(false, 1, 0);
+      T tyy = two3 * (T(2) * dn[1] - cross(false, 2, 2) - cross(false, 0, 0));
+      T tyz = cross(false, 1, 2) + dn[2];
+      vw = vw + T(0.5) * (uS * tyx + vS * tyy + wS * tyz);
+      if constexpr (LES) {
+        tyx = tyx + sg[0] + cross(true, 1, 0);
+        tyy = tyy + two3 * (T(2) * sg[1] - cross(true, 2, 2) - cross(true, 0, 0));
+        tyz = tyz + cross(true, 1, 2) + sg[2];
+      }
+      s1 = tyx; s2 = tyy; s3 = tyz;
+    } else {
+      T tzx = cross(false, 2, 0) + dn[0];
+      T tzy = dn[1] + cross(false, 2, 1);
+      T tzz = two3 * (T(2) * dn[2] - cross(false, 0, 0) - cross(false, 1, 1));
+      vw = vw + T(0.5) * (uS * tzx + vS * tzy + wS * tzz);
+      if constexpr (LES) {
+        tzx = tzx + cross(true, 2, 0) + sg[0];
+        tzy = tzy + sg[1] + cross(true, 2, 1);
+        tzz = tzz + two3 * (T(2) * sg[2] - cross(true, 0, 0) - cross(true, 1, 1));
+      }
+      s1 = tzx; s2 = tzy; s3 = tzz;
+    }
+  } else {
+    if (nd == 0) {
+      T txx = two3 * (T(2) * dn[0] - cross(false, 1, 1));
+      T txy = cross(false, 0, 1) + dn[1];
+      vw = vw + T(0.5) * (uS * txx + vS * txy);
+      s1 = txx; s2 = txy;
+    } else {
+      T tyx = dn[0] + cross(false, 1, 0);
+      T tyy = two3 * (T(2) * dn[1] - cross(false, 0, 0));
+      vw = vw + T(0.5) * (uS * tyx + vS * tyy);
+      s1 = tyx; s2 = tyy;
+    }
+  }
+  out[0] = s1; out[1] = s2; out[2] = s3;
+  out[3] = LES ? (vw + Hs) : vw;
+}
+
+// ---- 2D 4th-order viscous face with its 2nd-order fallback: 2D_solver/src/calc_visc4.f90.fypp ----
+template <class T, class Acc>
+__device__ __forceinline__ void visc_2d4(const StepArgs<T>& A, const Acc& s, int nd, bool inner,
+                                         int64_t o, const int64_t st[2], const T invs[2], T out[4]) {
+  const T two3 = T(2.0 / 3.0);
+  const int fn = TF_U + nd, fa = TF_U + (1 - nd);
+  const T inv = invs[nd];
+  T tn, ta, wn, wa, kT;
+  if (inner) {
+    T mu3[3], k3[3], t1[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      mu3[q] = T(0.0625) * (T(9) * (s(TF_MU, q + 1) + s(TF_MU, q + 2)) - (s(TF_MU, q) + s(TF_MU, q + 3)));
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      k3[q] = T(A.K.Cp_over_Pr) * mu3[q] *
+              (T(1.125) * (-s(TF_T, q + 1) + s(TF_T, q + 2)) - (-s(TF_T, q) + s(TF_T, q + 3)) * T(1.0 / 24.0)) * inv;
+    kT = flux4(k3[0], k3[1], k3[2]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {  // 2D calc_tau_straight: one transverse derivative (D0)
+      T a0 = s(fn, q), a1 = s(fn, q + 1), a2 = s(fn, q + 2), a3 = s(fn, q + 3);
+      T y0 = s(TF_D0, q), y1 = s(TF_D0, q + 1), y2 = s(TF_D0, q + 2), y3 = s(TF_D0, q + 3);
+      t1[q] = two3 * mu3[q] * ((T(2.25) * (-a1 + a2) - (-a0 + a3) * T(1.0 / 12.0)) * inv -
+                               T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3));
+    }
+    tn = flux4(t1[0], t1[1], t1[2]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      t1[q] = T(0.0625) * (-s(fn, q) + T(9) * (s(fn, q + 1) + s(fn, q + 2)) - s(fn, q + 3)) * t1[q];
+    wn = flux4(t1[0], t1[1], t1[2]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {  // cross: tangential velocity with D2 (normal velocity along tangent)
+      T a0 = s(fa, q), a1 = s(fa, q + 1), a2 = s(fa, q + 2), a3 = s(fa, q + 3);
+      T y0 = s(TF_D2, q), y1 = s(TF_D2, q + 1), y2 = s(TF_D2, q + 2), y3 = s(TF_D2, q + 3);
+      t1[q] = mu3[q] * ((T(1.125) * (-a1 + a2) - (-a0 + a3) * T(1.0 / 24.0)) * inv +
+                        T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3));
+    }
+    ta = flux4(t1[0], t1[1], t1[2]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      t1[q] = T(0.0625) * (-s(fa, q) + T(9) * (s(fa, q + 1) + s(fa, q + 2)) - s(fa, q + 3)) * t1[q];
+    wa = flux4(t1[0], t1[1], t1[2]);
+  } else {
+    const Fields<T>& W = A.W;
+    const int64_t o2 = o + st[nd];
+    const int64_t sa = st[1 - nd];
+    const T inva = invs[1 - nd];
+    T mn = T(0.5) * (W.mu[o] + W.mu[o2]);
+    kT = T(A.K.Cp_over_Pr) * mn * (-W.T_[o] + W.T_[o2]) * inv;
+    T m1 = T(0.25) * (W.mu[o - sa] + W.mu[o] + W.mu[o2 - sa] + W.mu[o2]);
+    T m2 = T(0.25) * (W.mu[o] + W.mu[o + sa] + W.mu[o2] + W.mu[o2 + sa]);
+    auto tder = [&](const T* a) {
+      return T(0.25) * (m1 * (-a[o - sa] + a[o] - a[o2 - sa] + a[o2]) + m2 * (-a[o] + a[o + sa] - a[o2] + a[o2 + sa])) * inva;
+    };
+    const T* vn = nd == 0 ? W.u : W.v;
+    const T* va = nd == 0 ? W.v : W.u;
+    T dnn = mn * (-vn[o] + vn[o2]) * inv;   // mux (x) / mvy (y)
+    T dan = mn * (-va[o] + va[o2]) * inv;   // mvx (x) / muy (y)
+    T dna = tder(vn);                       // muy (x) / mvx (y)
+    T daa = tder(va);                       // mvy (x) / mux (y)
+    tn = two3 * (T(2) * dnn - daa);
+    ta = (nd == 0) ? (dna + dan) : (dan + dna);
+    wn = T(0.5) * (vn[o] + vn[o2]) * tn;
+    wa = T(0.5) * (va[o] + va[o2]) * ta;
+  }
+  // energy in (u, v) order
+  T wu = nd == 0 ? wn : wa, wv = nd == 0 ? wa : wn;
+  out[nd] = tn; out[1 - nd] = ta; out[2] = T(0);
+  out[3] = wu + wv + kT;
+}
+
+}  // namespace oux
+
+namespace oux {
+
+// ---- the sweep kernel -----------------------------------------------------------
+// VK: viscous kind; LES: add the SGS terms.  `last` selects the combination.
+template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
+__global__ void __launch_bounds__(SweepShape<DIR>::TX * SweepShape<DIR>::TY)
+k_sweep(StepArgs<T> A, int last) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int H = ORDER / 2;
+  constexpr int TL = tile_len<ORDER, DIR>();
+  constexpr int NC = tile_cells<ORDER, DIR>();
+  constexpr int TX = SweepShape<DIR>::TX, TY = SweepShape<DIR>::TY;
+  constexpr bool HIGH = (VK == VK_C6 || VK == VK_C4 || VK == VK_ME4 || VK == VK_2D4);
+  constexpr bool SIXTH = (VK == VK_C6);
+  T* tile = reinterpret_cast<T*>(smraw);
+  double* Fs = reinterpret_cast<double*>(smraw + sizeof(T) * TF_COUNT * NC);
+  const Geo& G = A.G;
+  const int g = G.g;
+  const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g;
+  const int Nz = (DIM == 3) ? G.nz - 2 * g : 1;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * TX + tx;
+  const int nthr = TX * TY;
+  // block origin (first owned cell) in padded coordinates
+  int bx0, by0, bz0;
+  if constexpr (DIR == 0) {
+    bx0 = g + 32 * blockIdx.x; by0 = g + SWEEP_BR * blockIdx.y; bz0 = (DIM == 3) ? g + blockIdx.z : 0;
+  } else if constexpr (DIR == 1) {
+    bx0 = g + 32 * blockIdx.x; by0 = g + SWEEP_BF * blockIdx.y; bz0 = (DIM == 3) ? g + blockIdx.z : 0;
+  } else {
+    bx0 = g + 32 * blockIdx.x; bz0 = g + SWEEP_BF * blockIdx.y; by0 = g + blockIdx.z;
+  }
+  const int64_t stv[3] = {1, G.sx, G.plane};
+  const int nsweep = DIR == 0 ? G.nx : (DIR == 1 ? G.ny : G.nz);
+  const int ext[3] = {g + Nx, g + Ny, g + Nz};
+
+  // ---- tile load (cooperative) ----
+  for (int c = tid; c < NC; c += nthr) {
+    int ci[3];
+    int along;
+    if constexpr (DIR == 0) {
+      int t = c % TL, r = c / TL;
+      along = bx0 - TILE_HALO + t; ci[0] = along; ci[1] = by0 + r; ci[2] = bz0;
+    } else {
+      int x = c % 32, t = c / 32;
+      along = (DIR == 1 ? by0 : bz0) - TILE_HALO + t;
+      ci[0] = bx0 + x;
+      ci[1] = (DIR == 1) ? along : by0;
+      ci[2] = (DIR == 2) ? along : bz0;
+    }
+    bool ok = along >= 0 && along < nsweep;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      if (a != DIR && (a < DIM) && ci[a] >= ext[a]) ok = false;
+    if (!ok) continue;
+    const int64_t o = G.at(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
+    tile[TF_RHO * NC + c] = A.W.rho[o];
+    tile[TF_U * NC + c] = A.W.u[o];
+    tile[TF_V * NC + c] = A.W.v[o];
+    tile[TF_W * NC + c] = (DIM == 3) ? A.W.w[o] : T(0);
+    tile[TF_P * NC + c] = A.W.p[o];
+    tile[TF_T * NC + c] = A.W.T_[o];
+    if (A.scheme != 0) tile[TF_SEN * NC + c] = A.W.sensor[o];
+    if constexpr (VK != VK_EULER) tile[TF_MU * NC + c] = A.W.mu[o];
+    if constexpr (LES) { tile[TF_MUT * NC + c] = A.W.mut[o]; tile[TF_QC2 * NC + c] = A.W.qc2[o]; }
+    if constexpr (HIGH) {
+      const T* vel[3] = {A.W.u, A.W.v, A.W.w};
+      const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
+      if constexpr (DIM == 3) {
+        const int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
+        const int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
+        tile[TF_D0 * NC + c] = node_d<SIXTH>(vel[a1], o, stv[a1], (T)invd[a1][ci[a1]]);
+        tile[TF_D1 * NC + c] = node_d<SIXTH>(vel[a2], o, stv[a2], (T)invd[a2][ci[a2]]);
+        tile[TF_D2 * NC + c] = node_d<SIXTH>(vel[n], o, stv[ca], (T)invd[ca][ci[ca]]);
+        tile[TF_D3 * NC + c] = node_d<SIXTH>(vel[n], o, stv[cb], (T)invd[cb][ci[cb]]);
+      } else {
+        const int n = DIR, t = 1 - DIR;
+        tile[TF_D0 * NC + c] = node_d<SIXTH>(vel[t], o, stv[t], (T)invd[t][ci[t]]);
+        tile[TF_D2 * NC + c] = node_d<SIXTH>(vel[n], o, stv[t], (T)invd[t][ci[t]]);
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- faces ----
+  {
+    int fc[3] = {bx0, by0, bz0};  // left cell of this thread's face
+    int base, step;
+    bool rowok;
+    if constexpr (DIR == 0) {
+      fc[0] = bx0 - 1 + tx; fc[1] = by0 + ty;
+      base = ty * TL + tx; step = 1;
+      rowok = fc[1] < ext[1];
+    } else {
+      fc[0] = bx0 + tx;
+      fc[DIR] = (DIR == 1 ? by0 : bz0) - 1 + ty;
+      base = ty * 32 + tx; step = 32;
+      rowok = fc[0] < ext[0];
+    }
+    const int f = fc[DIR];
+    const bool valid = rowok && f >= g - 1 && f <= ext[DIR] - 1;
+    if (valid) {
+      T F[5];
+      // tile position of cell f + off is base + (2 + off) * step
+      auto st0 = [&](int field, int m) -> T { return tile[field * NC + base + m * step]; };
+      const int cb = base + (TILE_HALO - H) * step;
+      auto sc = [&](int field, int m) -> T { return tile[field * NC + cb + m * step]; };
+      T fd = T(0);
+      if (A.scheme != 0) fd = T(0.5) * (st0(TF_SEN, 2) + st0(TF_SEN, 3));
+      conv_flux<ORDER>(A, sc, fd, DIR, F);
+      if constexpr (VK != VK_EULER) {
+        T vo[4];
+        const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
+        const T inv = (T)invd[DIR][f];
+        if constexpr (VK == VK_GV2) {
+          const int64_t o = G.at(fc[0], fc[1], DIM == 3 ? fc[2] : 0);
+          T invs[3] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]], DIM == 3 ? (T)A.M.inv_dz[fc[2]] : T(0)};
+          visc_gv2<DIM, LES>(A, DIR, o, stv, invs, vo);
+        } else if constexpr (VK == VK_2D4) {
+          // inner guard of calc_Ev4 / calc_Fv4 (2D): face 2..n-4, transverse 2..n-3
+          const int nt = DIR == 0 ? G.ny : G.nx;
+          const int tr = fc[1 - DIR];
+          const int nn = DIR == 0 ? G.nx : G.ny;
+          bool inner = (f >= 2 && f <= nn - 4 && tr >= 2 && tr <= nt - 3);
+          const int64_t o = G.at(fc[0], fc[1], 0);
+          T invs[2] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]]};
+          invs[DIR] = inv;
+          auto sv = [&](int field, int m) -> T { return tile[field * NC + base + m * step]; };
+          visc_2d4(A, sv, DIR, inner, o, stv, invs, vo);
+        } else {
+          constexpr int off0 = (VK == VK_C4) ? -1 : -2;
+          const int vb = base + (2 + off0) * step;
+          auto sv = [&](int field, int m) -> T { return tile[field * NC + vb + m * step]; };
+          visc_high<VK, LES>(A, sv, DIR, inv, vo);
+        }
+        if constexpr (DIM == 3) {
+          F[1] = F[1] - vo[0]; F[2] = F[2] - vo[1]; F[3] = F[3] - vo[2]; F[4] = F[4] - vo[3];
+        } else {
+          F[1] = F[1] - vo[0]; F[2] = F[2] - vo[1]; F[4] = F[4] - vo[3];
+        }
+      }
+#pragma unroll
+      for (int l = 0; l < 5; ++l) Fs[l * (TX * TY) + tid] = (double)F[l];
+    }
+  }
+  __syncthreads();
+
+  // ---- cells: difference, accumulate, combine ----
+  {
+    int cc[3];
+    bool ok;
+    int lo, hi;  // flux slots of the left / right faces
+    if constexpr (DIR == 0) {
+      if (tx >= 32) return;
+      cc[0] = bx0 + tx; cc[1] = by0 + ty; cc[2] = bz0;
+      lo = ty * TX + tx; hi = lo + 1;
+    } else {
+      if (ty >= TY - 1) return;
+      cc[0] = bx0 + tx;
+      cc[DIR] = (DIR == 1 ? by0 : bz0) + ty;
+      if (DIR == 1) cc[2] = bz0; else cc[1] = by0;
+      lo = ty * TX + tx; hi = lo + TX;
+    }
+    ok = cc[0] < ext[0] && cc[1] < ext[1] && (DIM == 2 || cc[2] < ext[2]);
+    if (!ok) return;
+    const int i = cc[0], j = cc[1], k = (DIM == 3) ? cc[2] : 0;
+    const int64_t o = G.at(i, j, k);
+    // dt * S metric for this direction, scaled by coef (calc_steps.f90 calc_R)
+    double met;
+    if constexpr (DIM == 3) {
+      if (DIR == 0) met = A.M.dtdydz[(int64_t)(k - 1) * (G.ny - 2) + (j - 1)];
+      else if (DIR == 1) met = A.M.dtdzdx[(int64_t)(k - 1) * (G.nx - 2) + (i - 1)];
+      else met = A.M.dtdxdy[(int64_t)(j - 1) * (G.nx - 2) + (i - 1)];
+    } else {
+      met = (DIR == 0) ? A.M.dtdy[j - 1] : A.M.dtdx[i - 1];
+    }
+    const double cm = A.coef * met;
+    constexpr int NV = DIM + 2;
+    double R[NV];
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
+      const int fl = (DIM == 2 && l == 3) ? 4 : l;  // 2D: energy is flux slot 4
+      double d = cm * (-Fs[fl * (TX * TY) + lo] + Fs[fl * (TX * TY) + hi]);
+      if (DIR == 0) R[l] = d;
+      else R[l] = A.Racc[o + l * G.vs] + d;
+    }
+    if (!last) {
+#pragma unroll
+      for (int l = 0; l < NV; ++l) A.Racc[o + l * G.vs] = R[l];
+      return;
+    }
+    switch (A.mode) {
+      case CM_R_OUT: {
+        // reference Rs(nx-2, nv, ny-2, nz-2) order, cell (i,j,k) -> (i-1, l, j-1, k-1)
+        int64_t base = (((int64_t)(DIM == 3 ? k - 1 : 0) * (G.ny - 2) + (j - 1)) * NV) * (G.nx - 2) + (i - 1);
+#pragma unroll
+        for (int l = 0; l < NV; ++l) A.Rout[base + (int64_t)l * (G.nx - 2)] = R[l];
+        break;
+      }
+      case CM_RK3: {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          const int64_t q = o + l * G.vs;
+          A.Qout[q] = (T)((A.c1 * (double)A.Qin[q] + A.c2 * (double)A.Qout[q] - R[l]) * A.c4);
+        }
+        break;
+      }
+      case CM_RK3_1: {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          const int64_t q = o + l * G.vs;
+          A.Qout[q] = (T)((double)A.Qin[q] - R[l]);
+        }
+        break;
+      }
+      case CM_RK4_S: {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          const int64_t q = o + l * G.vs;
+          A.Qout[q] = (T)((double)A.Qin[q] - A.c1 * R[l]);
+          A.Rs[q] = (T)((double)A.Rs[q] + A.c2 * R[l]);
+        }
+        break;
+      }
+      case CM_RK4_4: {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          const int64_t q = o + l * G.vs;
+          double r = (double)A.Rs[q] + R[l];
+          A.Qout[q] = (T)((double)A.Qout[q] - r * (1.0 / 6.0));
+          A.Rs[q] = T(0);
+        }
+        break;
+      }
+      default: break;
+    }
+  }
+}
+
+}  // namespace oux

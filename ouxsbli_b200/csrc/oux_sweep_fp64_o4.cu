@@ -1,0 +1,16 @@
+// FP64 sweep instantiations for convective order 4 (compiled without FMA
+// contraction so the arithmetic matches the reference operation by operation).
+#include "oux_dispatch.h"
+#include "oux_launch.cuh"
+
+namespace oux {
+int launch_sweeps_fp64_o4(int dim, int vk, bool les, const StepArgs<double>& A, cudaStream_t s) {
+#define OUX_CASE(D, V, L) \
+  if (dim == D && vk == V && les == L) return launch_stage_sweeps<D, 4, V, L, double>(A, s);
+  OUX_CASE(3, VK_EULER, false) OUX_CASE(3, VK_C4, false) OUX_CASE(3, VK_GV2, false)
+  OUX_CASE(3, VK_C4, true) OUX_CASE(3, VK_GV2, true)
+  OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_2D4, false) OUX_CASE(2, VK_GV2, false)
+#undef OUX_CASE
+  return 2;
+}
+}  // namespace oux
