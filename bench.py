@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""Benchmark of the explicit time step on one B200 (or N replicas).
+
+Workload (default): supersonic Taylor-Green vortex, 256^3 interior cells
+(262^3 with the 6th-order ghost layers), Ma = 1.25, Re = 1600, KEEP/SLAU
+hybrid with the Ducros sensor, 6th-order central differences, Central-6
+viscous fluxes, TVD-RK3, FP64.  A "step" is one full time step (three RK
+stages) of that grid.  Metric: Mcell-steps/s = interior cells x steps / s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (one per GPU, torch.distributed for the
+barrier and the max-over-ranks time); the solve itself has no cross-GPU step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s"
+ALG_BYTES_PER_CELL_STEP = 320.0  # FP64 RK3: 8 state accesses x 5 variables x 8 B
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="interior cells per axis")
+    ap.add_argument("--scheme", default="Hybrid")
+    ap.add_argument("--visc", default="NS")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n: int, scheme: str, visc: str):
+    """SolverConfig + initial QJ (reference layout) of the supersonic TGV."""
+    from ouxsbli_b200.cases import CASES, build_initial
+    from ouxsbli_b200.grid import jacobian, to_qj
+    from ouxsbli_b200.solver import SolverConfig
+    case = CASES["NSTGV"]
+    p = dict(case.params)
+    p.update(nx=n + 6, ny=n + 6, nz=n + 6, order=6, M0=1.25, Re=1600.0, rho_mode="uniform",
+             cfl_mode="acoustic", CFL=0.5, dt=None)
+    p, xc, yc, zc, dx, dy, dz, Q = build_initial(case, p)
+    cfg = SolverConfig(dim=3, nx=p["nx"], ny=p["ny"], nz=p["nz"], order=6, scheme=scheme, visc=visc,
+                       tvd="hybrid", slau="HRSLAU2", rk=3, gamma=p["gamma"], R=p["R"], Pr=p["Pr"],
+                       Prt=p["Prt"], threshold=0.4, dt=p["dt"], dx=dx, dy=dy, dz=dz)
+    qj = to_qj(Q, jacobian(dx, dy, dz))
+    return cfg, qj
+
+
+def config_json(args, cfg):
+    return {"workload": f"supersonic Taylor-Green vortex {args.n}^3 (+6 ghost layers), Ma 1.25, Re 1600, "
+                        f"{args.scheme}-6 / {args.visc} Central-6 viscous, TVD-RK3",
+            "grid": [cfg.nx, cfg.ny, cfg.nz], "interior_cells": cfg.interior_cells(), "order": 6,
+            "scheme": args.scheme, "visc": args.visc, "rk": 3, "precision": "fp64",
+            "l2": "inputs larger than L2 (state %.2f GB + stage arrays %.2f GB)" % (
+                5 * cfg.nx * cfg.ny * cfg.nz * 8 / 1e9, 10 * cfg.nx * cfg.ny * cfg.nz * 8 / 1e9)}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(cfg, qj, budget_s: float = 20.0):
+    """The oracle (C++/OpenMP restatement of the reference kernels) on the host cores."""
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    oracle.build()
+    cells = cfg.interior_cells()
+    q = qj
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        q = oracle.step(cfg, q, 1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s * 0.5 or steps >= 3:
+            break
+    return {"value": cells * steps / el / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{steps} full time step(s) of the {cfg.nx}x{cfg.ny}x{cfg.nz} grid "
+                      f"({el:.1f} s, OpenMP over z planes, FP64, no FMA)"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path is the oracle port (the CUDA-Fortran
+    reference has no CPU build and cannot be compiled here)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle
+    oracle.build()
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    # bounded sample per step: a 64^3-interior grid of the same physics (a full
+    # 256^3 step takes tens of seconds on the host), metric is per cell-step
+    ns = 64
+    cfg, qj = workload(ns, args.scheme, args.visc)
+    q = qj
+    for _ in range(args.warmup):
+        q = oracle.step(cfg, q, 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        q = oracle.step(cfg, q, 1)
+    el = time.perf_counter() - t0
+    val = cfg.interior_cells() * args.steps / el / 1e6
+    line = {"metric": METRIC, "value": val, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": config_json(args, workload(args.n, args.scheme, args.visc)[0]) | {
+                "sample_grid": [cfg.nx, cfg.ny, cfg.nz]},
+            "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} timed steps (+{args.warmup} warm-up) of a "
+                                       f"{ns}^3-interior grid with the same scheme and physics"},
+            "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from ouxsbli_b200 import _lib
+    from ouxsbli_b200.solver import Solver
+
+    cfg, qj = workload(args.n, args.scheme, args.visc)
+    s = Solver(cfg, dev)
+    s.set_state(qj)
+    stream = torch.cuda.current_stream(dev)
+    cells = cfg.interior_cells()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # warm-up
+    s.step(args.warmup)
+    barrier()
+    # timed region: per-kernel CUDA events (live, on the launching stream)
+    _lib.check(_lib.LIB.oux_profile(s._h, 1))
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record(stream)
+    s.step(args.steps)
+    ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches_per_step = s.launches() / max(args.steps, 1)
+    kinds = ["prim", "sensor", "sgs", "sgs_edges", "sweep_x", "sweep_y", "sweep_z", "ghost"]
+    kms = (C.c_double * 8)()
+    kcnt = (C.c_int64 * 8)()
+    _lib.check(_lib.LIB.oux_profile_read(s._h, kms, kcnt, 8))
+    _lib.check(_lib.LIB.oux_profile(s._h, 0))
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = cells * args.steps * world / (ms_max / 1e3) / 1e6
+    ms_per_step = ms_max / args.steps
+
+    # end to end through the public API: host (pinned) state in, step, host state out
+    e2e = None
+    if not args.no_e2e:
+        import torch as _t
+        n_el = qj.size
+        h_in = _t.from_numpy(np.ascontiguousarray(qj.ravel(order="F"))).pin_memory()
+        h_out = _t.empty(n_el, dtype=_t.float64).pin_memory()
+        lib = _lib.LIB
+        pin = C.cast(C.c_void_p(h_in.data_ptr()), C.POINTER(C.c_double))
+        pout = C.cast(C.c_void_p(h_out.data_ptr()), C.POINTER(C.c_double))
+        sv = C.c_void_p(stream.cuda_stream)
+        k_e2e = max(1, min(args.steps, 5))
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k_e2e):
+            _lib.check(lib.oux_set_state(s._h, pin, sv))
+            _lib.check(lib.oux_step(s._h, 1, sv))
+            _lib.check(lib.oux_get_state(s._h, pout, sv))  # synchronizes
+        e1.record(stream)
+        barrier()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": cells * k_e2e * world / (float(te.item()) / 1e3) / 1e6, "unit": METRIC,
+               "h2d_bytes_per_step": int(n_el * 8), "d2h_bytes_per_step": int(n_el * 8),
+               "steps": k_e2e,
+               "path": "oux_set_state(pinned host QJ) -> oux_step(1) -> oux_get_state(pinned host QJ)"}
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = ALG_BYTES_PER_CELL_STEP * cells / (ms_per_step / 1e3) / 1e9
+    per_kernel = {}
+    tot = sum(kms[i] for i in range(8)) or 1.0
+    for i, nm in enumerate(kinds):
+        if kcnt[i]:
+            per_kernel[nm] = {"launches": int(kcnt[i]), "avg_ms": kms[i] / kcnt[i], "share": kms[i] / tot}
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["share"]) if per_kernel else None
+    traffic = None
+    try:  # ncu-measured DRAM bytes of one step, scaled to this grid (profiles/)
+        tr = json.load(open(os.path.join(ROOT, "profiles", "step_traffic.json")))
+        traffic = tr["dram_bytes_per_interior_cell_step"] * cells
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic,
+                "kernel": "one RK3 time step (prim, sensor, x/y/z flux sweeps, ghost fill x 3 stages)",
+                "alg_bytes": "320 B per interior cell-step (8 state accesses x 5 vars x 8 B)",
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "dominant_kernel": dom, "per_kernel": per_kernel}
+
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic TGV initial field)",
+            "config": config_json(args, cfg) | {"parallelism": f"{world} independent replicas"},
+            "roofline": roofline, "clocks": clk, "e2e": e2e,
+            "gpu_launches": int(round(launches_per_step * args.steps))}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, qj)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

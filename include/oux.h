@@ -138,10 +138,32 @@ int oux_step(oux_handle* h, int32_t nsteps, void* stream);
  * out[2] = mean 0.5 rho |omega|^2 (enstrophy; no reference counterpart).
  * Blocking: synchronizes `stream` and copies 3 doubles to the host. */
 int oux_diagnostics(oux_handle* h, double out[3], void* stream);
-/* Device status word (OR of oux_fault_bits); checks the current state for
- * NaN / non-positive rho or p on `stream` and returns after synchronizing. */
+/* Device status word (OR of oux_fault_bits).  oux_check_state clears it, scans
+ * the current state's interior for NaN / non-positive rho or p on `stream`,
+ * synchronizes and returns OUX_E_DEVICE_FAULT when a bit is set.  The reference
+ * has no counterpart (it only NaN-checks its rescaling profile,
+ * 3D_solver/src/preprocess.f90.fypp:143-147). */
 int oux_check_state(oux_handle* h, int32_t* fault_bits, void* stream);
 int oux_status(oux_handle* h, int32_t* fault_bits);
+
+/* Per-kernel timing for measurement tools: while enabled, every launch is
+ * bracketed by CUDA events on its stream; oux_profile_read synchronizes and
+ * returns, per kernel kind (0 prim, 1 sensor, 2 sgs, 3 sgs edges, 4 x sweep,
+ * 5 y sweep, 6 z sweep, 7 ghost fill), the summed milliseconds and launch
+ * counts since the last oux_profile call.  No reference counterpart (the
+ * reference is profiled externally with ncu/nsys scripts). */
+int oux_profile(oux_handle* h, int32_t enable);
+int oux_profile_read(oux_handle* h, double* ms, int64_t* count, int32_t nkinds);
+
+/* Host helper for the history files: the reference's KE / entropy arithmetic
+ * (src/print.f90:42-122) on the float32 fields of make_1d_for_print: per-cell
+ * terms in FP64, running sum rounded to float32 after every cell, mean over
+ * (nx-order)(ny-order)(nz-order).  out[0] = ke, out[1] = entropy.  For 2D pass
+ * nz = 1 with order 0 in the z extent handled by the caller (the reference
+ * writes no 2D history). */
+int oux_host_ref_diagnostics(int32_t nx, int32_t ny, int32_t nz, int32_t order, double gamma,
+                             const float* rho_flat, const float* p_flat, const float* vel_flat,
+                             double out[2]);
 
 /* Number of kernel launches the last oux_step call issued (for reporting). */
 int oux_launch_count(const oux_handle* h, int64_t* launches);

@@ -8,7 +8,10 @@ from __future__ import annotations
 import ctypes as C
 import pathlib
 
-LIB_PATH = pathlib.Path(__file__).resolve().parent / "liboux.so"
+import os
+
+# OUX_LIB may point at another build of the same library (e.g. a tuning variant)
+LIB_PATH = pathlib.Path(os.environ.get("OUX_LIB") or (pathlib.Path(__file__).resolve().parent / "liboux.so"))
 
 OUX_OK = 0
 OUX_E_INVALID = -1
@@ -33,7 +36,8 @@ SYMBOLS = [
     "oux_create", "oux_destroy", "oux_last_error", "oux_abi_version", "oux_state_bytes",
     "oux_scratch_bytes", "oux_layout_of", "oux_bind", "oux_set_state", "oux_get_state",
     "oux_pack_state", "oux_unpack_state", "oux_fill_ghosts", "oux_rhs", "oux_step",
-    "oux_diagnostics", "oux_check_state", "oux_status", "oux_launch_count",
+    "oux_diagnostics", "oux_check_state", "oux_status", "oux_profile", "oux_profile_read",
+    "oux_host_ref_diagnostics", "oux_launch_count",
 ]
 
 
@@ -89,6 +93,10 @@ def _load() -> C.CDLL:
         "oux_diagnostics": (C.c_int, [vp, dp, vp]),
         "oux_check_state": (C.c_int, [vp, C.POINTER(i32), vp]),
         "oux_status": (C.c_int, [vp, C.POINTER(i32)]),
+        "oux_profile": (C.c_int, [vp, i32]),
+        "oux_profile_read": (C.c_int, [vp, dp, C.POINTER(i64), i32]),
+        "oux_host_ref_diagnostics": (C.c_int, [i32, i32, i32, i32, C.c_double, C.POINTER(C.c_float),
+                                               C.POINTER(C.c_float), C.POINTER(C.c_float), dp]),
         "oux_launch_count": (C.c_int, [vp, C.POINTER(i64)]),
     }
     for name, (res, args) in sig.items():

@@ -47,6 +47,11 @@ struct oux_handle {
   Metrics M{};
   int64_t launches = 0;
   int diag_blocks = 0;
+  // optional per-kernel timing (oux_profile): CUDA events recorded around each
+  // launch on the launching stream
+  bool profiling = false;
+  struct Rec { int kind; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
 };
 
 namespace {
@@ -195,7 +200,7 @@ ScratchPlan plan_scratch(const oux_config& c) {
   int nv = c.dim + 2;
   ScratchPlan P;
   size_t vsb = (size_t)G.vs * sizeof(double);
-  P.nfield_arrays = 10;  // rho,u,v,w,p,T,mu,sensor,mut,qc2 (unused ones are still carved)
+  P.nfield_arrays = 10;  // rho,u,v,w,p,T,mu,sensor,mut,qc2
   size_t off = 0;
   P.fields = off; off += (size_t)P.nfield_arrays * vsb;
   P.racc = off; off += (size_t)nv * vsb;
@@ -351,6 +356,7 @@ void carve(oux_handle* h) {
   double* f = reinterpret_cast<double*>(h->scratch + P.fields);
   double** fp[10] = {&h->W.rho, &h->W.u, &h->W.v, &h->W.w, &h->W.p, &h->W.T_, &h->W.mu, &h->W.sensor, &h->W.mut, &h->W.qc2};
   for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
+  for (int q = 0; q < 9; ++q) h->W.grad[q] = nullptr;
   h->Racc = reinterpret_cast<double*>(h->scratch + P.racc);
   h->Q2 = reinterpret_cast<double*>(h->scratch + P.q2);
   h->Rs = h->cfg.rk == 4 ? reinterpret_cast<double*>(h->scratch + P.rs) : nullptr;
@@ -378,6 +384,27 @@ void carve(oux_handle* h) {
   h->status = reinterpret_cast<int*>(h->scratch + P.status);
 }
 
+// kinds reported by oux_profile_read
+enum KernelKind { KK_PRIM = 0, KK_SENSOR, KK_MUT, KK_MUT_EDGES, KK_SWEEP_X, KK_SWEEP_Y, KK_SWEEP_Z, KK_GHOST, KK_COUNT };
+
+struct Timed {
+  oux_handle* h;
+  int kind;
+  cudaStream_t s;
+  cudaEvent_t b = nullptr;
+  Timed(oux_handle* h_, int kind_, cudaStream_t s_) : h(h_), kind(kind_), s(s_) {
+    if (!h->profiling) return;
+    cudaEvent_t a;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+    h->recs.push_back({kind, a, b});
+  }
+  ~Timed() {
+    if (b) cudaEventRecord(b, s);
+  }
+};
+
 StepArgs<double> base_args(oux_handle* h) {
   StepArgs<double> A{};
   A.G = h->G;
@@ -398,6 +425,8 @@ int run_stage(oux_handle* h, const double* src, StepArgs<double> A, cudaStream_t
   const oux_config& c = h->cfg;
   int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
   bool visc = c.visc != OUX_EULER;
+  {
+  Timed tm(h, KK_PRIM, s);
   if (G.dim == 3) {
     if (visc) k_prim<3, true, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
     else k_prim<3, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
@@ -405,24 +434,46 @@ int run_stage(oux_handle* h, const double* src, StepArgs<double> A, cudaStream_t
     if (visc) k_prim<2, true, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
     else k_prim<2, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
   }
+  }
   h->launches++;
-  if (c.scheme != OUX_KEEP) {
-    if (G.dim == 3) {
-      dim3 b(32, 4, 2), gr((G.nx - 2 + 31) / 32, (G.ny - 2 + 3) / 4, (G.nz - 2 + 1) / 2);
-      k_sensor<3, double><<<gr, b, 0, s>>>(G, h->W, h->M);
-    } else {
-      dim3 b(32, 8, 1), gr((G.nx - 2 + 31) / 32, (G.ny - 2 + 7) / 8, 1);
-      k_sensor<2, double><<<gr, b, 0, s>>>(G, h->W, h->M);
+  // node gradients for the high-order viscous stencils and the Ducros sensor
+  {
+    const bool sen = c.scheme != OUX_KEEP;
+    const int dord = 0;  // transverse derivatives are formed inside the sweep tiles
+    if (sen || dord) {
+      Timed tm(h, KK_SENSOR, s);
+      const int gb = grid_for(ncell, 256);
+#define OUX_GRAD(D, O, S) \
+  if (G.dim == D && dord == O && sen == S) k_grad<D, O, S, double><<<gb, 256, 0, s>>>(G, h->W, h->M);
+      OUX_GRAD(3, 6, true) OUX_GRAD(3, 6, false) OUX_GRAD(3, 4, true) OUX_GRAD(3, 4, false) OUX_GRAD(3, 0, true)
+      OUX_GRAD(2, 4, true) OUX_GRAD(2, 4, false) OUX_GRAD(2, 0, true)
+#undef OUX_GRAD
+      h->launches++;
     }
-    h->launches++;
   }
   if (h->les) {
     dim3 b(32, 4, 1), gr((G.nx - 2 + 31) / 32, (G.ny - 2 + 3) / 4, G.nz - 2);
-    k_mut<double><<<gr, b, 0, s>>>(G, h->W, h->M, h->K);
-    k_mut_edges<double><<<grid_for(ncell, 256), 256, 0, s>>>(G, h->W);
+    {
+      Timed tm(h, KK_MUT, s);
+      k_mut<double><<<gr, b, 0, s>>>(G, h->W, h->M, h->K);
+    }
+    {
+      Timed tm(h, KK_MUT_EDGES, s);
+      k_mut_edges<double><<<grid_for(ncell, 256), 256, 0, s>>>(G, h->W);
+    }
     h->launches += 2;
   }
-  int rc = launch_sweeps_fp64(G.dim, c.order, h->vk, h->les, A, s);
+  int rc;
+  if (h->profiling) {
+    // one direction at a time so each sweep gets its own event pair
+    rc = 0;
+    for (int d = 0; d < G.dim && !rc; ++d) {
+      Timed tm(h, KK_SWEEP_X + d, s);
+      rc = launch_sweep_dir_fp64(G.dim, c.order, h->vk, h->les, d, A, s);
+    }
+  } else {
+    rc = launch_sweeps_fp64(G.dim, c.order, h->vk, h->les, A, s);
+  }
   if (rc) return fail(OUX_E_CUDA, std::string("sweep launch: ") + cudaGetErrorString(cudaGetLastError()));
   h->launches += G.dim;
   return OUX_OK;
@@ -431,6 +482,7 @@ int run_stage(oux_handle* h, const double* src, StepArgs<double> A, cudaStream_t
 int ghost(oux_handle* h, double* Q, cudaStream_t s) {
   const Geo& G = h->G;
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
+  Timed tm(h, KK_GHOST, s);
   k_ghost<double><<<grid_for(n / 4 + 1, 256), 256, 0, s>>>(Q, G, h->nv);
   h->launches++;
   return OUX_OK;
@@ -485,6 +537,7 @@ int oux_create(const oux_config* cfg, oux_handle** out) {
 }
 
 int oux_destroy(oux_handle* h) {
+  if (h) oux_profile(h, 0);
   delete h;
   return OUX_OK;
 }
@@ -662,6 +715,7 @@ int oux_check_state(oux_handle* h, int32_t* fault_bits, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   const Geo& G = h->G;
   int64_t n = (int64_t)(G.nx - 2 * G.g) * (G.ny - 2 * G.g) * (G.dim == 3 ? G.nz - 2 * G.g : 1);
+  OUX_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), s));
   k_check<<<grid_for(n, 256), 256, 0, s>>>(h->Q, G, h->M.jac, h->K.gamma_1, h->status);
   OUX_CUDA(cudaGetLastError());
   int v = 0;
@@ -677,6 +731,49 @@ int oux_status(oux_handle* h, int32_t* fault_bits) {
   int v = 0;
   OUX_CUDA(cudaMemcpy(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost));
   *fault_bits = v;
+  return OUX_OK;
+}
+
+int oux_profile(oux_handle* h, int32_t enable) {
+  if (!h) return fail(OUX_E_INVALID, "null handle");
+  for (auto& r : h->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  h->recs.clear();
+  h->profiling = enable != 0;
+  return OUX_OK;
+}
+
+int oux_profile_read(oux_handle* h, double* ms, int64_t* count, int32_t nkinds) {
+  if (!h || !ms || !count) return fail(OUX_E_INVALID, "null argument");
+  for (int k = 0; k < nkinds; ++k) { ms[k] = 0.0; count[k] = 0; }
+  for (auto& r : h->recs) {
+    OUX_CUDA(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    OUX_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    if (r.kind < nkinds) { ms[r.kind] += t; count[r.kind] += 1; }
+  }
+  return OUX_OK;
+}
+
+int oux_host_ref_diagnostics(int32_t nx, int32_t ny, int32_t nz, int32_t order, double gamma,
+                              const float* rho_flat, const float* p_flat, const float* vel_flat,
+                              double out[2]) {
+  if (!rho_flat || !p_flat || !vel_flat || !out) return fail(OUX_E_INVALID, "null argument");
+  if (order != 2 && order != 4 && order != 6) return fail(OUX_E_INVALID, "order must be 2, 4 or 6");
+  const int off = order / 2;
+  float ent = 0.0f, ke = 0.0f;
+  for (int k = 1 + off; k <= nz - off; ++k)
+    for (int j = 1 + off; j <= ny - off; ++j)
+      for (int i = 1 + off; i <= nx - off; ++i) {
+        const size_t l = (size_t)(i - 1) + (size_t)(j - 1) * nx + (size_t)(k - 1) * nx * ny;
+        const size_t m = 3 * l;
+        const double r = rho_flat[l];
+        ent = (float)((double)ent + r * std::log((double)p_flat[l] * std::pow(r, -gamma)));
+        const double a = vel_flat[m], b = vel_flat[m + 1], c = vel_flat[m + 2];
+        ke = (float)((double)ke + 0.5 * r * (a * a + b * b + c * c));
+      }
+  const double cnt = (double)((int64_t)(nx - order) * (ny - order) * (nz - order));
+  out[0] = (double)(float)((double)ke / cnt);
+  out[1] = (double)(float)((double)ent / cnt);
   return OUX_OK;
 }
 

@@ -31,6 +31,8 @@ struct Geo {
 template <class T> struct Fields {
   // primitive / auxiliary arrays (each vs elements)
   T *rho, *u, *v, *w, *p, *T_, *mu, *sensor, *mut, *qc2;
+  // node velocity gradient d(vel_c)/d(x_a) at index 3*c + a (3D: 9, 2D: c,a < 2)
+  T* grad[9];
 };
 
 struct Metrics {
@@ -91,51 +93,95 @@ __global__ void k_prim(const T* __restrict__ Q, Geo G, Fields<T> W, const double
   }
 }
 
-// ---- Ducros sensor: 3D_solver/src/calc_hybrid.f90:11-72 (2D twin :11-55) ---
-template <int DIM, class T>
-__global__ void k_sensor(Geo G, Fields<T> W, Metrics M) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  int k = (DIM == 3) ? (int)(blockIdx.z * blockDim.z + threadIdx.z + 1) : 0;
-  if (i > G.nx - 2 || j > G.ny - 2) return;
-  if (DIM == 3 && k > G.nz - 2) return;
-  const T eps = T(1.0e-12);
-  int64_t o = G.at(i, j, k);
-  T dxt = T(0.25) * ((T)M.inv_dx[i - 1] + (T)M.inv_dx[i]);
-  T dyt = T(0.25) * ((T)M.inv_dy[j - 1] + (T)M.inv_dy[j]);
-  T f;
-  if constexpr (DIM == 3) {
-    T dzt = T(0.25) * ((T)M.inv_dz[k - 1] + (T)M.inv_dz[k]);
-    int64_t ox = 1, oy = G.sx, oz = G.plane;
-    T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
-    T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
-    T dwdx = (-W.w[o - ox] + W.w[o + ox]) * dxt;
-    T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
-    T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
-    T dwdy = (-W.w[o - oy] + W.w[o + oy]) * dyt;
-    T dudz = (-W.u[o - oz] + W.u[o + oz]) * dzt;
-    T dvdz = (-W.v[o - oz] + W.v[o + oz]) * dzt;
-    T dwdz = (-W.w[o - oz] + W.w[o + oz]) * dzt;
-    T div = dudx + dvdy + dwdz;
-    T r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
-    f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
-  } else {
-    int64_t ox = 1, oy = G.sx;
-    T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
-    T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
-    T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
-    T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
-    T div = dudx + dvdy;
-    T rot = dvdx - dudy;
-    f = (div * div) / (div * div + rot * rot + eps);
-  }
-  f = fmin_f(T(1), f);
-  W.sensor[o] = f;
-  // edge copies of the reference kernel's tail
-  if (i == 1) W.sensor[G.at(0, j, k)] = f; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = f;
-  if (j == 1) W.sensor[G.at(i, 0, k)] = f; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = f;
-  if constexpr (DIM == 3) {
-    if (k == 1) W.sensor[G.at(i, j, 0)] = f; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = f;
+// ---- node velocity gradients (+ the Ducros sensor) in one pass ----------------
+// Gradients use the transverse-derivative stencils of the viscous loaders:
+// 6th order (load_smem_visc_cent.f90.fypp:51-70) for Central-6, 4th order
+// (load_smem_visc_me4_base.f90:120-127, 2D load_smem_visc4.f90:41-42) for
+// Central-4, ME4 and the 2D 4th-order stencil.  d/dx_a is evaluated where the
+// a-coordinate is interior and at most one other coordinate lies in a ghost
+// layer -- every cell a sweep tile reads.
+template <int DIM, int DORD, bool SENSOR, class T>
+__global__ void k_grad(Geo G, Fields<T> W, Metrics M) {
+  int64_t n = (int64_t)G.nx * G.ny * G.nz;
+  const int g = G.g;
+  const int ext[3] = {G.nx, G.ny, G.nz};
+  const int64_t st[3] = {1, G.sx, G.plane};
+  const double* invd[3] = {M.inv_dx, M.inv_dy, M.inv_dz};
+  const T* vel[3] = {W.u, W.v, W.w};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int c3[3];
+    c3[0] = (int)(t % G.nx);
+    int64_t r = t / G.nx;
+    c3[1] = (int)(r % G.ny);
+    c3[2] = (int)(r / G.ny);
+    const int64_t o = G.at(c3[0], c3[1], c3[2]);
+    if constexpr (DORD > 0) {
+      int outside = 0;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) outside += (c3[a] < g || c3[a] >= ext[a] - g);
+      if (outside <= 1) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          if (c3[a] < g || c3[a] >= ext[a] - g) continue;
+          const T inv = (T)invd[a][c3[a]];
+          const int64_t s = st[a];
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) {
+            const T* q = vel[c];
+            T d;
+            if constexpr (DORD == 6)
+              d = (T(1.0 / 60.0) * (-q[o - 3 * s] + q[o + 3 * s]) + T(0.15) * (q[o - 2 * s] - q[o + 2 * s]) +
+                   T(0.75) * (-q[o - s] + q[o + s])) * inv;
+            else
+              d = (T(2.0 / 3.0) * (-q[o - s] + q[o + s]) - T(1.0 / 12.0) * (-q[o - 2 * s] + q[o + 2 * s])) * inv;
+            W.grad[3 * c + a][o] = d;
+          }
+        }
+      }
+    }
+    if constexpr (SENSOR) {
+      // calc_Ducros (3D_solver/src/calc_hybrid.f90:11-72; 2D twin :11-55) on cells 1..n-2
+      const int i = c3[0], j = c3[1], k = c3[2];
+      if (i < 1 || i > G.nx - 2 || j < 1 || j > G.ny - 2) continue;
+      if (DIM == 3 && (k < 1 || k > G.nz - 2)) continue;
+      const T eps = T(1.0e-12);
+      T dxt = T(0.25) * ((T)M.inv_dx[i - 1] + (T)M.inv_dx[i]);
+      T dyt = T(0.25) * ((T)M.inv_dy[j - 1] + (T)M.inv_dy[j]);
+      T f;
+      if constexpr (DIM == 3) {
+        T dzt = T(0.25) * ((T)M.inv_dz[k - 1] + (T)M.inv_dz[k]);
+        const int64_t ox = 1, oy = G.sx, oz = G.plane;
+        T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
+        T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
+        T dwdx = (-W.w[o - ox] + W.w[o + ox]) * dxt;
+        T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
+        T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
+        T dwdy = (-W.w[o - oy] + W.w[o + oy]) * dyt;
+        T dudz = (-W.u[o - oz] + W.u[o + oz]) * dzt;
+        T dvdz = (-W.v[o - oz] + W.v[o + oz]) * dzt;
+        T dwdz = (-W.w[o - oz] + W.w[o + oz]) * dzt;
+        T div = dudx + dvdy + dwdz;
+        T r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
+        f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
+      } else {
+        const int64_t ox = 1, oy = G.sx;
+        T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
+        T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
+        T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
+        T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
+        T div = dudx + dvdy;
+        T rot = dvdx - dudy;
+        f = (div * div) / (div * div + rot * rot + eps);
+      }
+      f = fmin_f(T(1), f);
+      W.sensor[o] = f;
+      if (i == 1) W.sensor[G.at(0, j, k)] = f; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = f;
+      if (j == 1) W.sensor[G.at(i, 0, k)] = f; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = f;
+      if constexpr (DIM == 3) {
+        if (k == 1) W.sensor[G.at(i, j, 0)] = f; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = f;
+      }
+    }
   }
 }
 

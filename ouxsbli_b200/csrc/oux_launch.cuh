@@ -34,4 +34,15 @@ int launch_stage_sweeps(const StepArgs<T>& A, cudaStream_t s) {
   }
 }
 
+template <int DIM, int ORDER, int VK, bool LES, class T>
+int launch_stage_sweep_dir(const StepArgs<T>& A, int dir, cudaStream_t s) {
+  if (dir == 0) return launch_one<DIM, 0, ORDER, VK, LES, T>(A, 0, s);
+  if constexpr (DIM == 3) {
+    if (dir == 1) return launch_one<DIM, 1, ORDER, VK, LES, T>(A, 0, s);
+    return launch_one<DIM, 2, ORDER, VK, LES, T>(A, 1, s);
+  } else {
+    return launch_one<DIM, 1, ORDER, VK, LES, T>(A, 1, s);
+  }
+}
+
 }  // namespace oux

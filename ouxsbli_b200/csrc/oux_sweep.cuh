@@ -13,8 +13,14 @@
 
 namespace oux {
 
-constexpr int SWEEP_BR = 4;   // x sweep rows per block
-constexpr int SWEEP_BF = 8;   // y/z sweep cells per block along the sweep
+#ifndef OUX_SWEEP_BR
+#define OUX_SWEEP_BR 4
+#endif
+#ifndef OUX_SWEEP_BF
+#define OUX_SWEEP_BF 8
+#endif
+constexpr int SWEEP_BR = OUX_SWEEP_BR;  // x sweep rows per block
+constexpr int SWEEP_BF = OUX_SWEEP_BF;  // y/z sweep cells per block along the sweep
 
 enum TileField { TF_RHO = 0, TF_U, TF_V, TF_W, TF_P, TF_T, TF_MU, TF_MUT, TF_QC2, TF_SEN, TF_D0, TF_D1, TF_D2, TF_D3, TF_COUNT };
 
@@ -418,8 +424,16 @@ namespace oux {
 
 // ---- the sweep kernel -----------------------------------------------------------
 // VK: viscous kind; LES: add the SGS terms.  `last` selects the combination.
+// minimum resident blocks per SM (caps registers; measured on B200: 3 / 2 beat 1 / 1 by 1.5x)
+#ifndef OUX_SWEEP_MINB_X
+#define OUX_SWEEP_MINB_X 3
+#endif
+#ifndef OUX_SWEEP_MINB_YZ
+#define OUX_SWEEP_MINB_YZ 2
+#endif
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
-__global__ void __launch_bounds__(SweepShape<DIR>::TX * SweepShape<DIR>::TY)
+__global__ void __launch_bounds__(SweepShape<DIR>::TX * SweepShape<DIR>::TY,
+                                  DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
 k_sweep(StepArgs<T> A, int last) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int H = ORDER / 2;
@@ -479,7 +493,7 @@ k_sweep(StepArgs<T> A, int last) {
     if (A.scheme != 0) tile[TF_SEN * NC + c] = A.W.sensor[o];
     if constexpr (VK != VK_EULER) tile[TF_MU * NC + c] = A.W.mu[o];
     if constexpr (LES) { tile[TF_MUT * NC + c] = A.W.mut[o]; tile[TF_QC2 * NC + c] = A.W.qc2[o]; }
-    if constexpr (HIGH) {
+    if constexpr (HIGH) {  // transverse node derivatives (the viscous loaders' stencils)
       const T* vel[3] = {A.W.u, A.W.v, A.W.w};
       const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
       if constexpr (DIM == 3) {

@@ -1,0 +1,55 @@
+"""Workload builders shared by the tests (initial fields, configurations)."""
+from __future__ import annotations
+
+import numpy as np
+
+from ouxsbli_b200.cases import CASES, build_initial, isentropic_vortex
+from ouxsbli_b200.grid import cyclic_axis, jacobian, to_qj
+from ouxsbli_b200.solver import SolverConfig
+
+
+def tgv(n: int, order: int = 6, mach: float = 0.1, **kw):
+    """Viscous TGV of the plain-method config: uniform rho, acoustic CFL 0.5."""
+    case = CASES["NSTGV"]
+    p = dict(case.params)
+    p.update(nx=n + order, ny=n + order, nz=n + order, order=order, rho_mode="uniform",
+             cfl_mode="acoustic", CFL=0.5, M0=mach, dt=None)
+    p, xc, yc, zc, dx, dy, dz, Q = build_initial(case, p)
+    cfg = SolverConfig(dim=3, nx=p["nx"], ny=p["ny"], nz=p["nz"], order=order, dt=p["dt"], gamma=p["gamma"],
+                       R=p["R"], Pr=p["Pr"], Prt=p["Prt"], dx=dx, dy=dy, dz=dz, **kw)
+    return cfg, to_qj(Q, jacobian(dx, dy, dz))
+
+
+def random_turbulence(n: int, order: int = 6, seed: int = 0, mt: float = 0.3, **kw):
+    """Seeded solenoidal random-phase velocity (E(k) ~ k^4 exp(-2 (k/k0)^2), k0 = 4) at uniform rho, p."""
+    from ouxsbli_b200.turbulence import decaying_turbulence
+    return decaying_turbulence(n, order=order, seed=seed, mt=mt, **kw)
+
+
+def vortex2d(n: int, order: int = 4, beta: float = 5.0, mach: float = 0.5, L: float = 10.0, cfl: float = 0.4, **kw):
+    Q = isentropic_vortex(n + order, n + order, order, L, beta, mach)
+    _, dx = cyclic_axis(n + order, L, order)
+    dy = dx.copy()
+    dt = cfl * (L / n) / (mach + 1.0)
+    cfg = SolverConfig(dim=2, nx=n + order, ny=n + order, nz=1, order=order, dt=dt, gamma=1.4, R=1.0,
+                       Pr=0.71, dx=dx, dy=dy, dz=None, **kw)
+    return cfg, to_qj(Q, jacobian(dx, dy, None))
+
+
+def interior(a: np.ndarray, g: int, dim: int) -> np.ndarray:
+    """Interior cells of a padded reference-layout array (nx, nv, ny[, nz])."""
+    if dim == 3:
+        return a[g:-g, :, g:-g, g:-g]
+    return a[g:-g, :, g:-g]
+
+
+def rhs_interior(r: np.ndarray, g: int, dim: int) -> np.ndarray:
+    """Interior cells of an Rs(nx-2, nv, ny-2[, nz-2]) array."""
+    s = slice(g - 1, -(g - 1) if g > 1 else None)
+    if dim == 3:
+        return r[s, :, s, s]
+    return r[s, :, s]
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))

@@ -1,0 +1,97 @@
+"""C-ABI checks that need no GPU: exports, configuration validation, sizes, layout."""
+import ctypes as C
+import pathlib
+import re
+
+import numpy as np
+import pytest
+
+from ouxsbli_b200 import _lib
+from ouxsbli_b200.solver import SolverConfig
+
+HEADER = pathlib.Path(__file__).resolve().parents[1] / "include" / "oux.h"
+
+
+def header_functions():
+    txt = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(oux_\w+)\s*\(", txt, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = header_functions()
+    assert len(names) >= 19
+    for n in names:
+        assert hasattr(_lib.LIB, n), f"liboux.so does not export {n}"
+    assert set(_lib.SYMBOLS) <= set(names)
+    assert _lib.LIB.oux_abi_version() == 1
+
+
+def small_cfg(**kw):
+    n = 10 + 6
+    d = np.full(n - 1, 0.1)
+    base = dict(dim=3, nx=n, ny=n, nz=n, order=6, dx=d, dy=d, dz=d, dt=1e-4)
+    base.update(kw)
+    return SolverConfig(**base)
+
+
+def create(cfg):
+    c, keep = cfg.to_c()
+    h = C.c_void_p()
+    rc = _lib.LIB.oux_create(C.byref(c), C.byref(h))
+    return rc, h
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(order=5), "order"),
+    (dict(dim=4), "dim"),
+    (dict(nx=7), "too small"),
+    (dict(rk=2), "rk"),
+    (dict(dim=2, nz=1, scheme="Roe"), "Roe"),
+    (dict(visc="NS", visc_order=2), "calc_Ev2_in"),
+    (dict(order=4, nx=14, ny=14, nz=14, visc="NS", visc_order=6), "order 6"),
+    (dict(dt=0.0), "dt"),
+])
+def test_create_rejects_invalid(kw, msg):
+    rc, h = create(small_cfg(**kw))
+    assert rc == _lib.OUX_E_INVALID
+    assert msg in _lib.LIB.oux_last_error().decode()
+
+
+def test_create_sizes_and_layout():
+    cfg = small_cfg(scheme="Hybrid", visc="NS")
+    rc, h = create(cfg)
+    assert rc == 0
+    lay = _lib.OuxLayout()
+    assert _lib.LIB.oux_layout_of(h, C.byref(lay)) == 0
+    assert lay.nv == 5 and lay.row_stride >= cfg.nx and lay.row_stride % 4 == 0
+    assert lay.plane_stride == lay.row_stride * cfg.ny
+    assert lay.var_stride >= lay.plane_stride * cfg.nz and lay.var_stride % 32 == 0
+    c, keep = cfg.to_c()
+    sb, kb = C.c_size_t(), C.c_size_t()
+    assert _lib.LIB.oux_state_bytes(C.byref(c), C.byref(sb)) == 0
+    assert _lib.LIB.oux_scratch_bytes(C.byref(c), C.byref(kb)) == 0
+    assert sb.value == 5 * lay.var_stride * 8
+    assert kb.value > sb.value
+    # unbound handles refuse device work without touching CUDA
+    assert _lib.LIB.oux_step(h, 1, None) == _lib.OUX_E_UNBOUND
+    assert _lib.LIB.oux_fill_ghosts(h, None) == _lib.OUX_E_UNBOUND
+    assert _lib.LIB.oux_destroy(h) == 0
+
+
+def test_pack_unpack_roundtrip_host():
+    cfg = small_cfg(dim=3, nx=13, ny=17, nz=11, order=2)
+    cfg.dx, cfg.dy, cfg.dz = np.ones(12), np.ones(16), np.ones(10)
+    rc, h = create(cfg)
+    assert rc == 0
+    lay = _lib.OuxLayout()
+    _lib.LIB.oux_layout_of(h, C.byref(lay))
+    ref = np.asfortranarray(np.random.default_rng(0).standard_normal((13, 5, 17, 11)))
+    dev = np.zeros(5 * lay.var_stride)
+    assert _lib.LIB.oux_pack_state(h, ref.ctypes.data_as(C.POINTER(C.c_double)), dev.ctypes.data_as(C.c_void_p)) == 0
+    back = np.zeros_like(ref, order="F")
+    assert _lib.LIB.oux_unpack_state(h, dev.ctypes.data_as(C.c_void_p), back.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    np.testing.assert_array_equal(back, ref)
+    # SoA: variable l of cell (i,j,k) at l*vs + k*plane + j*row + i
+    i, j, k, l = 4, 7, 3, 2
+    assert dev[l * lay.var_stride + k * lay.plane_stride + j * lay.row_stride + i] == ref[i, l, j, k]
+    _lib.LIB.oux_destroy(h)
