@@ -1,0 +1,168 @@
+"""Host-side logic that needs no GPU: patcher, Case configuration, writers, grids."""
+import math
+import re
+import struct
+
+import numpy as np
+import pytest
+
+from ouxsbli_b200 import patch
+from ouxsbli_b200.case import _ALIAS, _RK_NORMALIZE, _VALUE_NORMALIZE, Case
+from ouxsbli_b200.grid import cyclic_axis, fill_periodic, jacobian
+from ouxsbli_b200.ic import PeriodicBC, RiemannIC, TaylorGreenIC, UniformIC, bc_to_params, ic_to_params
+from ouxsbli_b200.output import fortran_e, make_1d_for_print, read_restart, read_vtr, ref_diagnostics, write_restart, write_vtr
+from ouxsbli_b200.patcher import _to_fortran_double
+
+GLOBALS = """module mod_globals
+  implicit none
+  integer, parameter :: nx = 513 ! points incl. ghosts
+  integer, parameter :: ny = 513
+  real(8), parameter :: Re   = 1600.d0
+  real(8), parameter :: CFL  = 0.03d0
+  integer, parameter :: np   = 100
+  integer, parameter :: nt   = int(20.d0 / (dble(np) * dtn))
+end module mod_globals
+"""
+CONFIG = "#:set VISC = 'NS'\n#:set SCHEME = 'SLAU'\n#:set ORDER = 6\n"
+
+
+class TestPatcher:
+    def test_fortran_double(self):
+        assert _to_fortran_double(1600.0) == "1600.0d0"
+        assert float(_to_fortran_double(0.03).replace("d0", "e0")) == pytest.approx(0.03)
+        assert _to_fortran_double(1e-5) == "1d-05"
+
+    def test_parameters_rewritten(self):
+        out = patch(GLOBALS, {"Re": 800.0, "nx": 65, "nt": 500, "CFL": 0.1})
+        lines = {ln.split("::")[1].split("=")[0].strip(): ln for ln in out.splitlines() if "::" in ln}
+        assert "800.0d0" in lines["Re"]
+        assert "= 65" in lines["nx"] and "513" not in lines["nx"]
+        assert "! points incl. ghosts" in lines["nx"]
+        assert "500" in lines["nt"] and "int(" not in lines["nt"]
+        assert "0.1d0" in lines["CFL"]
+        assert "= 513" in lines["ny"]
+        assert "1600" in GLOBALS  # input untouched
+
+    def test_macros_and_append(self):
+        out = patch(CONFIG, {"SCHEME": "KEEP", "ORDER": 4, "RK": 4, "BC_X": False})
+        assert "#:set SCHEME = 'KEEP'" in out
+        assert "#:set ORDER = 4" in out
+        # appended to a fypp file (as the reference's patcher writes them: "NAME =value")
+        assert re.search(r"^#:set RK\s*=\s*4$", out, re.M)
+        assert re.search(r"^#:set BC_X\s*=\s*False$", out, re.M)
+        assert "RK" not in patch(GLOBALS, {"RK": 4})  # never appended to Fortran sources
+
+
+class TestCaseConfig:
+    def test_alias_tables(self):
+        assert _ALIAS["scheme"] == "SCHEME" and _ALIAS["accuracy"] == "ORDER" and _ALIAS["recal"] == "RESTART"
+        assert _VALUE_NORMALIZE["VISC"]["euler"] == "Euler"
+        assert _VALUE_NORMALIZE["TVD"]["minmod"] == "tvd" and _VALUE_NORMALIZE["TVD"]["muscl4"] == "hybrid"
+        assert _RK_NORMALIZE["classical_rk4"] == 4
+
+    def test_routing_and_normalisation(self, tmp_path):
+        c = Case("3D_solver/NSTGV", tmp_path / "w", scheme="keep", visc="euler", accuracy=4, rk="rk4",
+                 nx=20, ny=20, nz=20, Re=800.0, tvd="minmod", visc_stencil="me4", np=1, nt=2)
+        c._setup()
+        assert c.config["SCHEME"] == "KEEP" and c.config["VISC"] == "Euler" and c.config["ORDER"] == 4
+        assert c.config["RK"] == 4 and c.config["TVD"] == "tvd" and c.config["VISC_STENCIL"] == "ME4Base"
+        assert c.globals["nx"] == 20 and c.globals["Re"] == 800.0
+
+    def test_build_validates_without_gpu(self, tmp_path):
+        c = Case("3D_solver/ETGV", tmp_path / "etgv", nx=14, ny=14, nz=14, np=1, nt=1)
+        c.build()
+        assert (tmp_path / "etgv" / "data").is_dir() and (tmp_path / "etgv" / "case.json").exists()
+        with pytest.raises(RuntimeError):
+            Case("3D_solver/ETGV", tmp_path / "x", nx=14, ny=14, nz=14, visc="ns", visc_order=2).build()
+
+    def test_errors(self, tmp_path):
+        with pytest.raises(FileNotFoundError):
+            Case("3D_solver/NOPE", tmp_path / "n").build()
+        with pytest.raises(RuntimeError):
+            Case("3D_solver/ETGV", tmp_path / "r").run()
+        with pytest.raises(RuntimeError):
+            Case("3D_solver/ETGV", tmp_path / "b", bc_x=True).build()
+        with pytest.raises(RuntimeError):
+            Case("3D_solver/ETGV", tmp_path / "rie", ic=RiemannIC()).build()
+
+    def test_ic_bc_specs(self):
+        assert ic_to_params(TaylorGreenIC(Ma=0.2))["Ma"] == 0.2
+        assert ic_to_params({"type": "uniform", "rho": 2.0})["rho0"] == 2.0
+        assert bc_to_params("periodic") == {"BC_X": False, "BC_Y": False, "BC_Z": False}
+        assert bc_to_params(PeriodicBC()) == bc_to_params({"type": "periodic"})
+        with pytest.raises(ValueError):
+            ic_to_params({"type": "nope"})
+        with pytest.raises(ValueError):
+            bc_to_params("wall")
+        assert UniformIC().to_params()["ic_type"] == 1
+
+
+class TestWriters:
+    def test_fortran_e(self):
+        assert fortran_e(1.0) == "  0.1000E+01"
+        assert fortran_e(-3.3e-7) == " -0.3300E-06"
+        assert fortran_e(0.0) == "  0.0000E+00"
+        assert fortran_e(9.99995) == "  0.1000E+02"
+        assert len(fortran_e(123456.7)) == 12
+
+    def test_vtr_layout_and_roundtrip(self, tmp_path):
+        x, y, z = np.arange(3, dtype=np.float32), np.arange(4, dtype=np.float32), np.zeros(2, np.float32)
+        n = 3 * 4 * 2
+        rho = np.linspace(1, 2, n, dtype=np.float32)
+        p = rho * 3
+        vel = np.arange(3 * n, dtype=np.float32)
+        f = tmp_path / "Q00000.vtr"
+        write_vtr(f, x, y, z, rho, p, vel)
+        raw = f.read_bytes()
+        head = raw[:raw.index(b"  _")].decode()
+        assert 'WholeExtent="0    2 0    3 0    1"' in head
+        # offsets advance by 4 + 4*N per block (the reference's header word)
+        assert f'offset="{"{:>12}".format(4 + 12)}"' in head
+        i0 = raw.index(b"  _") + 3
+        assert struct.unpack("<i", raw[i0:i0 + 4])[0] == 4 + 4 * 3
+        assert raw.endswith(b"  </AppendedData>\n</VTKFile>\n")
+        xs, ys, zs, fields = read_vtr(f)
+        np.testing.assert_array_equal(xs, x)
+        np.testing.assert_array_equal(fields["rho"].ravel(), rho)
+        np.testing.assert_array_equal(fields["velocity"].reshape(-1), vel)
+
+    def test_restart_roundtrip(self, tmp_path):
+        q = np.asfortranarray(np.random.default_rng(0).standard_normal((5, 5, 6, 7)))
+        write_restart(tmp_path / "Q00001.dat", q)
+        assert (tmp_path / "Q00001.dat").stat().st_size == q.size * 8
+        np.testing.assert_array_equal(read_restart(tmp_path / "Q00001.dat", q.shape), q)
+
+    def test_reference_diagnostics_match_oracle(self):
+        """liboux's host KE/entropy helper and the oracle's restatement agree exactly."""
+        from oracle import oracle
+        rng = np.random.default_rng(2)
+        nx = ny = nz = 12
+        n = nx * ny * nz
+        rho = (1.0 + 0.1 * rng.random(n)).astype(np.float32)
+        p = (0.7 + 0.1 * rng.random(n)).astype(np.float32)
+        vel = (0.3 * rng.standard_normal(3 * n)).astype(np.float32)
+        a = ref_diagnostics(nx, ny, nz, 6, 1.4, rho, p, vel)
+        b = oracle.diag_f32(nx, ny, nz, 6, 1.4, rho, p, vel)
+        assert a == b
+
+
+class TestGrid:
+    @pytest.mark.parametrize("order", [2, 4, 6])
+    def test_cyclic_axis(self, order):
+        n = 16 + order
+        xc, dx = cyclic_axis(n, 2.0 * math.pi, order)
+        g = order // 2
+        assert np.allclose(dx, 2.0 * math.pi / 16)
+        assert xc[g] == pytest.approx(0.5 * dx[0])  # first interior cell centre at dx/2
+        assert np.allclose(np.diff(xc), dx[0])
+
+    def test_fill_periodic_and_jacobian(self):
+        g = 3
+        q = np.asfortranarray(np.random.default_rng(1).standard_normal((10, 5, 11, 12)))
+        fill_periodic(q, g)
+        # ghost cell c takes the interior image g + (c - g) mod N
+        assert np.array_equal(q[0], q[g + (0 - g) % (10 - 2 * g)])
+        assert np.array_equal(q[:, :, :, 11], q[:, :, :, g + (11 - g) % (12 - 2 * g)])
+        assert np.array_equal(q[:, :, 1, :], q[:, :, g + (1 - g) % (11 - 2 * g), :])
+        J = jacobian(np.full(9, 0.5), np.full(10, 0.25), np.full(11, 0.1))
+        assert J.shape == (10, 11) and np.allclose(J, 1.0 / (0.5 * 0.25 * 0.1))
