@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--visc", default="NS")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--mixed-check-steps", type=int, default=1000,
+                    help="steps of the mixed-vs-FP64 accuracy check (the north star's 1000)")
     return ap.parse_args()
 
 
@@ -266,6 +269,57 @@ def main():
                "steps": k_e2e,
                "path": "oux_set_state(pinned host QJ) -> oux_step(1) -> oux_get_state(pinned host QJ)"}
 
+    # mixed form on the same workload: throughput and its error against FP64 after
+    # the same number of steps from the same initial field
+    mixed = None
+    if not args.no_mixed:
+        import dataclasses
+        n_err = args.mixed_check_steps or (args.warmup + args.steps)
+        s.set_state(qj)
+        s.step(n_err)
+        q64 = s.get_state()
+        sm = Solver(dataclasses.replace(cfg, precision="mixed"), dev)
+        sm.set_state(qj)
+        sm.step(args.warmup)
+        barrier()
+        barrier()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        _lib.check(_lib.LIB.oux_profile(sm._h, 1))
+        m0.record(stream)
+        sm.step(args.steps)
+        m1.record(stream)
+        barrier()
+        mkms = (C.c_double * 8)()
+        mkcnt = (C.c_int64 * 8)()
+        _lib.check(_lib.LIB.oux_profile_read(sm._h, mkms, mkcnt, 8))
+        _lib.check(_lib.LIB.oux_profile(sm._h, 0))
+        mixed_kernels = {kinds[i]: {"launches": int(mkcnt[i]), "avg_ms": mkms[i] / mkcnt[i]}
+                         for i in range(8) if mkcnt[i]}
+        tm = torch.tensor([m0.elapsed_time(m1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        sm.set_state(qj)
+        sm.step(n_err)
+        q32 = sm.get_state()
+        g = cfg.g
+        sl = (slice(g, -g), slice(None), slice(g, -g), slice(g, -g))
+        a32, a64 = q32[sl], q64[sl]
+        errs = [float(np.linalg.norm((a32[:, l] - a64[:, l]).ravel()) / np.linalg.norm(a64[:, l].ravel()))
+                for l in range(5)]
+        mnorm = np.linalg.norm(a64[:, 1:4].ravel())
+        errs_mom = [float(np.linalg.norm((a32[:, l] - a64[:, l]).ravel()) / mnorm) for l in (1, 2, 3)]
+        d64, d32 = s.diagnostics(), sm.diagnostics()
+        mval = cells * args.steps * world / (float(tm.item()) / 1e3) / 1e6
+        mixed = {"value": mval, "unit": METRIC, "ms_per_step": float(tm.item()) / args.steps,
+                 "speedup_vs_fp64": mval / value,
+                 "rel_l2_vs_fp64": errs, "rel_l2_momentum_vector_norm": errs_mom, "after_steps": n_err,
+                 "ke_rel_dev": abs(d32[0] - d64[0]) / abs(d64[0]),
+                 "enstrophy_rel_dev": abs(d32[2] - d64[2]) / abs(d64[2]),
+                 "per_kernel": mixed_kernels,
+                 "form": "FP32 stage increments, primitive fields (p, T as deviations from per-solve references) "
+                         "and face fluxes; FP64 Q^n, flux differences, RK combinations, diagnostics"}
+        sm.close()
+
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -296,7 +350,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic TGV initial field)",
             "config": config_json(args, cfg) | {"parallelism": f"{world} independent replicas"},
-            "roofline": roofline, "clocks": clk, "e2e": e2e,
+            "roofline": roofline, "clocks": clk, "e2e": e2e, "mixed": mixed,
             "gpu_launches": int(round(launches_per_step * args.steps))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, qj)

@@ -34,6 +34,9 @@ UNITS = [
     ("oux_sweep_fp64_o2.cu", ["-fmad=false"]),
     ("oux_sweep_fp64_o4.cu", ["-fmad=false"]),
     ("oux_sweep_fp64_o6.cu", ["-fmad=false"]),
+    ("oux_sweep_mx_o2.cu", []),
+    ("oux_sweep_mx_o4.cu", []),
+    ("oux_sweep_mx_o6.cu", []),
 ]
 
 

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 #include "oux.h"
 #include "oux_sweep.cuh"
@@ -41,8 +42,11 @@ struct oux_handle {
   double* Q = nullptr;
   unsigned char* scratch = nullptr;
   size_t scratch_bytes = 0;
-  Fields<double> W{};
-  double *Racc = nullptr, *Q2 = nullptr, *Rs = nullptr, *partials = nullptr;
+  bool mixed = false;           // FP32 stage states/fields, FP64 Q^n and accumulations
+  Fields<double> W{};           // FP64 form
+  Fields<float> Wf{};           // mixed form
+  double *Racc = nullptr, *Rs = nullptr, *partials = nullptr;
+  void* Qs = nullptr;           // stage state (double or float)
   int* status = nullptr;
   Metrics M{};
   int64_t launches = 0;
@@ -79,7 +83,7 @@ int validate(const oux_config* c, std::string& why) {
     why = "only periodic boundaries (bc_x = bc_y = bc_z = 0) are built";
     return OUX_E_INVALID;
   }
-  if (c->precision != OUX_FP64) { why = "precision: only OUX_FP64 in this library build"; return OUX_E_INVALID; }
+  if (c->precision != OUX_FP64 && c->precision != OUX_MIXED) { why = "unknown precision"; return OUX_E_INVALID; }
   if (!c->dx || !c->dy || (c->dim == 3 && !c->dz)) { why = "dx/dy/dz host arrays required"; return OUX_E_INVALID; }
   if (!(c->gamma > 1.0) || !(c->R > 0.0) || !(c->dt > 0.0)) { why = "gamma > 1, R > 0, dt > 0 required"; return OUX_E_INVALID; }
   if (c->visc != OUX_EULER) {
@@ -175,6 +179,8 @@ void build_tables(oux_handle* h) {
   K.Cp_over_Pr = c.visc != OUX_EULER ? K.Cp / c.Pr : 0.0;
   K.sutherland = 1.716e-5 * 384.2 * std::pow(273.2, -1.5);
   K.gamma_over_gamma_1 = c.gamma * K.over_gamma_1;
+  K.p_ref = 0.0;
+  K.T_ref = 0.0;
   double t10 = std::tan(10.0 * std::acos(-1.0) / 180.0);
   K.tan10deg2 = t10 * t10;
 }
@@ -200,11 +206,12 @@ ScratchPlan plan_scratch(const oux_config& c) {
   int nv = c.dim + 2;
   ScratchPlan P;
   size_t vsb = (size_t)G.vs * sizeof(double);
+  size_t vse = (size_t)G.vs * (c.precision == OUX_MIXED ? sizeof(float) : sizeof(double));
   P.nfield_arrays = 10;  // rho,u,v,w,p,T,mu,sensor,mut,qc2
   size_t off = 0;
-  P.fields = off; off += (size_t)P.nfield_arrays * vsb;
+  P.fields = off; off += round_up((size_t)P.nfield_arrays * vse, 256);
   P.racc = off; off += (size_t)nv * vsb;
-  P.q2 = off; off += (size_t)nv * vsb;
+  P.q2 = off; off += round_up((size_t)nv * vse, 256);
   P.rs = off; off += (c.rk == 4 ? (size_t)nv * vsb : 0);
   P.metrics = off;
   int nx = c.nx, ny = c.ny, nz = c.dim == 3 ? c.nz : 1;
@@ -258,22 +265,25 @@ __device__ __forceinline__ double block_sum(double v, double* sm) {
   return v;
 }
 
-// FP64 domain integrals over interior cells (ke, entropy, enstrophy); W holds the
-// primitives of the current state.  Vorticity uses the central difference of the
-// solve's order (6th: load_smem_visc_cent.f90.fypp:67 form).
-__global__ void k_diag(Geo G, Fields<double> W, Metrics M, double gamma, int order, double* partials) {
+// FP64 domain integrals over interior cells (ke, entropy, enstrophy) of the FP64
+// state Q (= conservative / J): primitives as in calc_quantities_3D, vorticity by
+// the central difference of the solve's order (6th: load_smem_visc_cent.f90.fypp:67).
+__global__ void k_diag(Geo G, const double* __restrict__ Q, Metrics M, double gamma_1, double gamma, int order,
+                       double* partials) {
   __shared__ double sm[32];
   const int g = G.g;
   const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
   int64_t n = (int64_t)Nx * Ny * Nz;
   double ke = 0.0, en = 0.0, ens = 0.0;
-  auto dd = [&](const double* a, int64_t o, int64_t st, double inv) -> double {
+  auto vel = [&](int c, int64_t o) -> double { return Q[o + (1 + c) * G.vs] * (1.0 / Q[o]); };
+  auto dd = [&](int c, int64_t o, int64_t st, double inv) -> double {
     if (order == 6)
-      return ((1.0 / 60.0) * (-a[o - 3 * st] + a[o + 3 * st]) + 0.15 * (a[o - 2 * st] - a[o + 2 * st]) +
-              0.75 * (-a[o - st] + a[o + st])) * inv;
+      return ((1.0 / 60.0) * (-vel(c, o - 3 * st) + vel(c, o + 3 * st)) +
+              0.15 * (vel(c, o - 2 * st) - vel(c, o + 2 * st)) + 0.75 * (-vel(c, o - st) + vel(c, o + st))) * inv;
     if (order == 4)
-      return ((2.0 / 3.0) * (-a[o - st] + a[o + st]) - (1.0 / 12.0) * (-a[o - 2 * st] + a[o + 2 * st])) * inv;
-    return 0.5 * (-a[o - st] + a[o + st]) * inv;
+      return ((2.0 / 3.0) * (-vel(c, o - st) + vel(c, o + st)) -
+              (1.0 / 12.0) * (-vel(c, o - 2 * st) + vel(c, o + 2 * st))) * inv;
+    return 0.5 * (-vel(c, o - st) + vel(c, o + st)) * inv;
   };
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
     int i = (int)(t % Nx) + g;
@@ -281,17 +291,20 @@ __global__ void k_diag(Geo G, Fields<double> W, Metrics M, double gamma, int ord
     int j = (int)(r % Ny) + g;
     int k = (G.dim == 3) ? (int)(r / Ny) + g : 0;
     int64_t o = G.at(i, j, k);
-    double rho = W.rho[o], u = W.u[o], v = W.v[o], p = W.p[o];
-    double w = (G.dim == 3) ? W.w[o] : 0.0;
+    double Jv = M.jac[(int64_t)j * G.nx + i];
+    double q1 = Q[o], over = 1.0 / q1, rho = Jv * q1;
+    double u = Q[o + G.vs] * over, v = Q[o + 2 * G.vs] * over;
+    double w = (G.dim == 3) ? Q[o + 3 * G.vs] * over : 0.0;
+    double p = gamma_1 * (Jv * Q[o + (G.dim + 1) * G.vs] - 0.5 * rho * (u * u + v * v + w * w));
     ke += 0.5 * rho * (u * u + v * v + w * w);
     en += rho * log(p * pow(rho, -gamma));
     double ix = M.inv_dx[i], iy = M.inv_dy[j];
-    double dvdx = dd(W.v, o, 1, ix), dudy = dd(W.u, o, G.sx, iy);
+    double dvdx = dd(1, o, 1, ix), dudy = dd(0, o, G.sx, iy);
     double om2;
     if (G.dim == 3) {
       double iz = M.inv_dz[k];
-      double dwdy = dd(W.w, o, G.sx, iy), dvdz = dd(W.v, o, G.plane, iz);
-      double dudz = dd(W.u, o, G.plane, iz), dwdx = dd(W.w, o, 1, ix);
+      double dwdy = dd(2, o, G.sx, iy), dvdz = dd(1, o, G.plane, iz);
+      double dudz = dd(0, o, G.plane, iz), dwdx = dd(2, o, 1, ix);
       double a = dwdy - dvdz, b = dudz - dwdx, c = dvdx - dudy;
       om2 = a * a + b * b + c * c;
     } else {
@@ -353,12 +366,19 @@ inline int grid_for(int64_t n, int threads) {
 void carve(oux_handle* h) {
   ScratchPlan P = plan_scratch(h->cfg);
   size_t vsb = (size_t)h->G.vs;
-  double* f = reinterpret_cast<double*>(h->scratch + P.fields);
-  double** fp[10] = {&h->W.rho, &h->W.u, &h->W.v, &h->W.w, &h->W.p, &h->W.T_, &h->W.mu, &h->W.sensor, &h->W.mut, &h->W.qc2};
-  for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
-  for (int q = 0; q < 9; ++q) h->W.grad[q] = nullptr;
+  if (!h->mixed) {
+    double* f = reinterpret_cast<double*>(h->scratch + P.fields);
+    double** fp[10] = {&h->W.rho, &h->W.u, &h->W.v, &h->W.w, &h->W.p, &h->W.T_, &h->W.mu, &h->W.sensor, &h->W.mut, &h->W.qc2};
+    for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
+    for (int q = 0; q < 9; ++q) h->W.grad[q] = nullptr;
+  } else {
+    float* f = reinterpret_cast<float*>(h->scratch + P.fields);
+    float** fp[10] = {&h->Wf.rho, &h->Wf.u, &h->Wf.v, &h->Wf.w, &h->Wf.p, &h->Wf.T_, &h->Wf.mu, &h->Wf.sensor, &h->Wf.mut, &h->Wf.qc2};
+    for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
+    for (int q = 0; q < 9; ++q) h->Wf.grad[q] = nullptr;
+  }
   h->Racc = reinterpret_cast<double*>(h->scratch + P.racc);
-  h->Q2 = reinterpret_cast<double*>(h->scratch + P.q2);
+  h->Qs = h->scratch + P.q2;
   h->Rs = h->cfg.rk == 4 ? reinterpret_cast<double*>(h->scratch + P.rs) : nullptr;
   double* m = reinterpret_cast<double*>(h->scratch + P.metrics);
   auto take = [&](const std::vector<double>& v) {
@@ -405,10 +425,15 @@ struct Timed {
   }
 };
 
-StepArgs<double> base_args(oux_handle* h) {
-  StepArgs<double> A{};
+template <class T> Fields<T>& fields_of(oux_handle* h);
+template <> Fields<double>& fields_of<double>(oux_handle* h) { return h->W; }
+template <> Fields<float>& fields_of<float>(oux_handle* h) { return h->Wf; }
+
+template <class T>
+StepArgs<T> base_args(oux_handle* h) {
+  StepArgs<T> A{};
   A.G = h->G;
-  A.W = h->W;
+  A.W = fields_of<T>(h);
   A.M = h->M;
   A.K = h->K;
   A.scheme = h->cfg.scheme;
@@ -416,50 +441,71 @@ StepArgs<double> base_args(oux_handle* h) {
   A.slau = h->cfg.slau;
   A.Racc = h->Racc;
   A.Rs = h->Rs;
+  A.Qn = h->Q;
+  A.Qs = reinterpret_cast<T*>(h->Qs);
   return A;
 }
 
-// One stage: primitives of `src`, sensor, SGS viscosity, then the sweeps.
-int run_stage(oux_handle* h, const double* src, StepArgs<double> A, cudaStream_t s) {
+template <class T>
+int launch_sweeps_t(int dim, int order, int vk, bool les, int dir, const StepArgs<T>& A, cudaStream_t s);
+template <>
+int launch_sweeps_t<double>(int dim, int order, int vk, bool les, int dir, const StepArgs<double>& A, cudaStream_t s) {
+  return dir < 0 ? launch_sweeps_fp64(dim, order, vk, les, A, s) : launch_sweep_dir_fp64(dim, order, vk, les, dir, A, s);
+}
+template <>
+int launch_sweeps_t<float>(int dim, int order, int vk, bool les, int dir, const StepArgs<float>& A, cudaStream_t s) {
+  return dir < 0 ? launch_sweeps_mx(dim, order, vk, les, A, s) : launch_sweep_dir_mx(dim, order, vk, les, dir, A, s);
+}
+
+// One stage: primitives of `src` (FP64 Q^n or the stage state), sensor, SGS
+// viscosity, then the sweeps.
+template <class T, class TS>
+int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   const Geo& G = h->G;
   const oux_config& c = h->cfg;
+  Fields<T>& W = fields_of<T>(h);
   int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
   bool visc = c.visc != OUX_EULER;
   {
-  Timed tm(h, KK_PRIM, s);
-  if (G.dim == 3) {
-    if (visc) k_prim<3, true, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
-    else k_prim<3, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
-  } else {
-    if (visc) k_prim<2, true, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
-    else k_prim<2, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(src, G, h->W, h->M.jac, h->K);
-  }
+    Timed tm(h, KK_PRIM, s);
+    const int gb = grid_for(ncell, 256);
+    if constexpr (sizeof(T) < sizeof(double)) {
+      // mixed form: Q^(s) = Q^n + FP32 increment (no increment for the first stage)
+      const float* dQ = std::is_same<TS, double>::value ? nullptr : reinterpret_cast<const float*>(src);
+      if (G.dim == 3) {
+        if (visc) k_prim_mx<3, true><<<gb, 256, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
+        else k_prim_mx<3, false><<<gb, 256, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
+      } else {
+        if (visc) k_prim_mx<2, true><<<gb, 256, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
+        else k_prim_mx<2, false><<<gb, 256, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
+      }
+    } else {
+      if (G.dim == 3) {
+        if (visc) k_prim<3, true, TS, T><<<gb, 256, 0, s>>>(src, G, W, h->M.jac, h->K);
+        else k_prim<3, false, TS, T><<<gb, 256, 0, s>>>(src, G, W, h->M.jac, h->K);
+      } else {
+        if (visc) k_prim<2, true, TS, T><<<gb, 256, 0, s>>>(src, G, W, h->M.jac, h->K);
+        else k_prim<2, false, TS, T><<<gb, 256, 0, s>>>(src, G, W, h->M.jac, h->K);
+      }
+    }
   }
   h->launches++;
-  // node gradients for the high-order viscous stencils and the Ducros sensor
-  {
-    const bool sen = c.scheme != OUX_KEEP;
-    const int dord = 0;  // transverse derivatives are formed inside the sweep tiles
-    if (sen || dord) {
-      Timed tm(h, KK_SENSOR, s);
-      const int gb = grid_for(ncell, 256);
-#define OUX_GRAD(D, O, S) \
-  if (G.dim == D && dord == O && sen == S) k_grad<D, O, S, double><<<gb, 256, 0, s>>>(G, h->W, h->M);
-      OUX_GRAD(3, 6, true) OUX_GRAD(3, 6, false) OUX_GRAD(3, 4, true) OUX_GRAD(3, 4, false) OUX_GRAD(3, 0, true)
-      OUX_GRAD(2, 4, true) OUX_GRAD(2, 4, false) OUX_GRAD(2, 0, true)
-#undef OUX_GRAD
-      h->launches++;
-    }
+  if (c.scheme != OUX_KEEP) {  // Ducros sensor
+    Timed tm(h, KK_SENSOR, s);
+    const int gb = grid_for(ncell, 256);
+    if (G.dim == 3) k_grad<3, 0, true, T><<<gb, 256, 0, s>>>(G, W, h->M);
+    else k_grad<2, 0, true, T><<<gb, 256, 0, s>>>(G, W, h->M);
+    h->launches++;
   }
   if (h->les) {
     dim3 b(32, 4, 1), gr((G.nx - 2 + 31) / 32, (G.ny - 2 + 3) / 4, G.nz - 2);
     {
       Timed tm(h, KK_MUT, s);
-      k_mut<double><<<gr, b, 0, s>>>(G, h->W, h->M, h->K);
+      k_mut<T><<<gr, b, 0, s>>>(G, W, h->M, h->K);
     }
     {
       Timed tm(h, KK_MUT_EDGES, s);
-      k_mut_edges<double><<<grid_for(ncell, 256), 256, 0, s>>>(G, h->W);
+      k_mut_edges<T><<<grid_for(ncell, 256), 256, 0, s>>>(G, W);
     }
     h->launches += 2;
   }
@@ -469,22 +515,60 @@ int run_stage(oux_handle* h, const double* src, StepArgs<double> A, cudaStream_t
     rc = 0;
     for (int d = 0; d < G.dim && !rc; ++d) {
       Timed tm(h, KK_SWEEP_X + d, s);
-      rc = launch_sweep_dir_fp64(G.dim, c.order, h->vk, h->les, d, A, s);
+      rc = launch_sweeps_t<T>(G.dim, c.order, h->vk, h->les, d, A, s);
     }
   } else {
-    rc = launch_sweeps_fp64(G.dim, c.order, h->vk, h->les, A, s);
+    rc = launch_sweeps_t<T>(G.dim, c.order, h->vk, h->les, -1, A, s);
   }
   if (rc) return fail(OUX_E_CUDA, std::string("sweep launch: ") + cudaGetErrorString(cudaGetLastError()));
   h->launches += G.dim;
   return OUX_OK;
 }
 
-int ghost(oux_handle* h, double* Q, cudaStream_t s) {
+template <class T>
+int ghost(oux_handle* h, T* Q, cudaStream_t s) {
   const Geo& G = h->G;
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   Timed tm(h, KK_GHOST, s);
-  k_ghost<double><<<grid_for(n / 4 + 1, 256), 256, 0, s>>>(Q, G, h->nv);
+  k_ghost<T><<<grid_for(n / 4 + 1, 256), 256, 0, s>>>(Q, G, h->nv);
   h->launches++;
+  return OUX_OK;
+}
+
+// nsteps time steps with compute type T (double: plain FP64 form; float: mixed form)
+template <class T>
+int run_steps(oux_handle* h, int nsteps, cudaStream_t s) {
+  double* Qn = h->Q;
+  T* Qs = reinterpret_cast<T*>(h->Qs);
+  for (int n = 0; n < nsteps; ++n) {
+    StepArgs<T> A = base_args<T>(h);
+    int rc;
+    if (h->cfg.rk == 3) {
+      // calc_time_dev.f90.fypp:81-101
+      A.mode = CM_RK3_1; A.coef = 1.0;
+      if ((rc = run_stage<T, double>(h, Qn, A, s))) return rc;
+      ghost<T>(h, Qs, s);
+      A.mode = CM_RK3_2; A.coef = 0.25; A.c1 = 0.75; A.c2 = 0.25; A.c4 = 1.0;
+      if ((rc = run_stage<T, T>(h, Qs, A, s))) return rc;
+      ghost<T>(h, Qs, s);
+      A.mode = CM_RK3_3; A.coef = 2.0; A.c1 = 2.0; A.c2 = 1.0; A.c4 = 1.0 / 3.0;
+      if ((rc = run_stage<T, T>(h, Qs, A, s))) return rc;
+      ghost<double>(h, Qn, s);
+    } else {
+      // calc_time_dev.f90.fypp:264-287
+      const double c1[3] = {0.5, 0.5, 1.0}, c2[3] = {1.0, 2.0, 2.0};
+      for (int st = 0; st < 3; ++st) {
+        A.mode = CM_RK4_S; A.coef = 1.0; A.c1 = c1[st]; A.c2 = c2[st];
+        if (st == 0) rc = run_stage<T, double>(h, Qn, A, s);
+        else rc = run_stage<T, T>(h, Qs, A, s);
+        if (rc) return rc;
+        ghost<T>(h, Qs, s);
+      }
+      A.mode = CM_RK4_4; A.coef = 1.0;
+      if ((rc = run_stage<T, T>(h, Qs, A, s))) return rc;
+      ghost<double>(h, Qn, s);
+    }
+  }
   return OUX_OK;
 }
 
@@ -530,6 +614,7 @@ int oux_create(const oux_config* cfg, oux_handle** out) {
   h->nv = cfg->dim + 2;
   h->vk = vk;
   h->les = cfg->visc == OUX_LES;
+  h->mixed = cfg->precision == OUX_MIXED;
   build_tables(h);
   h->cfg.dx = h->cfg.dy = h->cfg.dz = nullptr;  // host arrays are not retained
   *out = h;
@@ -584,6 +669,20 @@ int oux_set_state(oux_handle* h, const double* host_qj, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   const Geo& G = h->G;
   int64_t n = (int64_t)G.nx * G.ny * G.nz * h->nv;
+  {
+    // mixed form references: p and T of the first interior cell (any value of
+    // the field's magnitude keeps the FP32 deviations small)
+    const int g = G.g, nv = h->nv;
+    const int kk = G.dim == 3 ? g : 0;
+    auto at = [&](int l) { return host_qj[(((int64_t)kk * G.ny + g) * nv + l) * G.nx + g]; };
+    const double Jv = h->jac[(size_t)g * G.nx + g];
+    const double q1 = at(0), rho = Jv * q1, over = 1.0 / q1;
+    double ke = 0.0;
+    for (int l = 1; l <= G.dim; ++l) { double vv = at(l) * over; ke += vv * vv; }
+    const double p = h->K.gamma_1 * (Jv * at(nv - 1) - 0.5 * rho * ke);
+    h->K.p_ref = h->mixed ? p : 0.0;
+    h->K.T_ref = h->mixed ? p / (h->K.R * rho) : 0.0;
+  }
   OUX_CUDA(cudaMemcpyAsync(h->Racc, host_qj, n * sizeof(double), cudaMemcpyHostToDevice, s));
   k_ref_to_soa<double><<<grid_for(n, 256), 256, 0, s>>>(h->Racc, h->Q, G, h->nv);
   OUX_CUDA(cudaGetLastError());
@@ -630,7 +729,7 @@ int oux_unpack_state(const oux_handle* h, const void* dev_layout_host, double* r
 int oux_fill_ghosts(oux_handle* h, void* stream) {
   if (!h) return fail(OUX_E_INVALID, "null handle");
   if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
-  ghost(h, h->Q, (cudaStream_t)stream);
+  ghost<double>(h, h->Q, (cudaStream_t)stream);
   OUX_CUDA(cudaGetLastError());
   return OUX_OK;
 }
@@ -642,11 +741,16 @@ int oux_rhs(oux_handle* h, double* rhs_dev, void* stream) {
   const Geo& G = h->G;
   size_t n = (size_t)h->nv * (G.nx - 2) * (G.ny - 2) * (G.dim == 3 ? G.nz - 2 : 1);
   OUX_CUDA(cudaMemsetAsync(rhs_dev, 0, n * sizeof(double), s));
-  StepArgs<double> A = base_args(h);
-  A.mode = CM_R_OUT;
-  A.coef = 1.0;
-  A.Rout = rhs_dev;
-  int rc = run_stage(h, h->Q, A, s);
+  int rc;
+  if (h->mixed) {
+    StepArgs<float> A = base_args<float>(h);
+    A.mode = CM_R_OUT; A.coef = 1.0; A.Rout = rhs_dev;
+    rc = run_stage<float, double>(h, h->Q, A, s);
+  } else {
+    StepArgs<double> A = base_args<double>(h);
+    A.mode = CM_R_OUT; A.coef = 1.0; A.Rout = rhs_dev;
+    rc = run_stage<double, double>(h, h->Q, A, s);
+  }
   if (rc) return rc;
   OUX_CUDA(cudaGetLastError());
   return OUX_OK;
@@ -658,35 +762,8 @@ int oux_step(oux_handle* h, int32_t nsteps, void* stream) {
   if (nsteps < 0) return fail(OUX_E_INVALID, "nsteps must be >= 0");
   cudaStream_t s = (cudaStream_t)stream;
   h->launches = 0;
-  double* Q = h->Q;
-  double* Q2 = h->Q2;
-  for (int n = 0; n < nsteps; ++n) {
-    StepArgs<double> A = base_args(h);
-    int rc;
-    if (h->cfg.rk == 3) {
-      // calc_time_dev.f90.fypp:81-101
-      A.mode = CM_RK3_1; A.coef = 1.0; A.Qin = Q; A.Qout = Q2;
-      if ((rc = run_stage(h, Q, A, s))) return rc;
-      ghost(h, Q2, s);
-      A.mode = CM_RK3; A.coef = 0.25; A.c1 = 0.75; A.c2 = 0.25; A.c4 = 1.0; A.Qin = Q; A.Qout = Q2;
-      if ((rc = run_stage(h, Q2, A, s))) return rc;
-      ghost(h, Q2, s);
-      A.mode = CM_RK3; A.coef = 2.0; A.c1 = 2.0; A.c2 = 1.0; A.c4 = 1.0 / 3.0; A.Qin = Q2; A.Qout = Q;
-      if ((rc = run_stage(h, Q2, A, s))) return rc;
-      ghost(h, Q, s);
-    } else {
-      // calc_time_dev.f90.fypp:264-287
-      const double c1[3] = {0.5, 0.5, 1.0}, c2[3] = {1.0, 2.0, 2.0};
-      for (int st = 0; st < 3; ++st) {
-        A.mode = CM_RK4_S; A.coef = 1.0; A.c1 = c1[st]; A.c2 = c2[st]; A.Qin = Q; A.Qout = Q2;
-        if ((rc = run_stage(h, st == 0 ? Q : Q2, A, s))) return rc;
-        ghost(h, Q2, s);
-      }
-      A.mode = CM_RK4_4; A.coef = 1.0; A.Qin = Q; A.Qout = Q;
-      if ((rc = run_stage(h, Q2, A, s))) return rc;
-      ghost(h, Q, s);
-    }
-  }
+  int rc = h->mixed ? run_steps<float>(h, nsteps, s) : run_steps<double>(h, nsteps, s);
+  if (rc) return rc;
   OUX_CUDA(cudaGetLastError());
   return OUX_OK;
 }
@@ -697,9 +774,8 @@ int oux_diagnostics(oux_handle* h, double out[3], void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   const Geo& G = h->G;
   int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
-  if (G.dim == 3) k_prim<3, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(h->Q, G, h->W, h->M.jac, h->K);
-  else k_prim<2, false, double><<<grid_for(ncell, 256), 256, 0, s>>>(h->Q, G, h->W, h->M.jac, h->K);
-  k_diag<<<DIAG_BLOCKS, 256, 0, s>>>(G, h->W, h->M, h->K.gamma, h->cfg.order, h->partials);
+  (void)ncell;
+  k_diag<<<DIAG_BLOCKS, 256, 0, s>>>(G, h->Q, h->M, h->K.gamma_1, h->K.gamma, h->cfg.order, h->partials);
   int64_t nint = (int64_t)(G.nx - 2 * G.g) * (G.ny - 2 * G.g) * (G.dim == 3 ? G.nz - 2 * G.g : 1);
   double* res = h->partials + 3 * DIAG_BLOCKS;
   k_diag_final<<<1, 256, 0, s>>>(h->partials, DIAG_BLOCKS, 1.0 / (double)nint, res);

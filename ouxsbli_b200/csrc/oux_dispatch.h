@@ -26,4 +26,17 @@ inline int launch_sweeps_fp64(int dim, int order, int vk, bool les, const StepAr
   if (order == 4) return launch_sweeps_fp64_o4(dim, vk, les, A, s);
   return launch_sweeps_fp64_o2(dim, vk, les, A, s);
 }
+// mixed form (FP32 fields and face fluxes)
+int launch_sweeps_mx_o2(int dim, int vk, bool les, int dir, const StepArgs<float>& A, cudaStream_t s);
+int launch_sweeps_mx_o4(int dim, int vk, bool les, int dir, const StepArgs<float>& A, cudaStream_t s);
+int launch_sweeps_mx_o6(int dim, int vk, bool les, int dir, const StepArgs<float>& A, cudaStream_t s);
+inline int launch_sweep_dir_mx(int dim, int order, int vk, bool les, int dir, const StepArgs<float>& A,
+                               cudaStream_t s) {
+  if (order == 6) return launch_sweeps_mx_o6(dim, vk, les, dir, A, s);
+  if (order == 4) return launch_sweeps_mx_o4(dim, vk, les, dir, A, s);
+  return launch_sweeps_mx_o2(dim, vk, les, dir, A, s);
+}
+inline int launch_sweeps_mx(int dim, int order, int vk, bool les, const StepArgs<float>& A, cudaStream_t s) {
+  return launch_sweep_dir_mx(dim, order, vk, les, -1, A, s);
+}
 }  // namespace oux

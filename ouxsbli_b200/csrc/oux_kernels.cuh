@@ -13,13 +13,17 @@
 namespace oux {
 
 enum ViscKind { VK_EULER = 0, VK_C6 = 1, VK_C4 = 2, VK_ME4 = 3, VK_GV2 = 4, VK_2D4 = 5 };
+// Stage combinations of 3D_solver/src/calc_steps.f90 with Qn = the FP64 state
+// Q^n and Qs = the stage state (FP64 in the plain form, FP32 in the mixed form);
+// all arithmetic of the combinations is FP64.
 enum CombineMode {
   CM_ACCUM = 0,   // first/middle sweep: Racc (=|+=) c * dF
   CM_R_OUT = 1,   // last sweep: write R to an output buffer (reference Rs order)
-  CM_RK3 = 2,     // Qout = (c1*Qin + c2*Qout - R) * c4      (calc_step2_3)
-  CM_RK4_S = 3,   // Qs = Qn - c1*R ; Rs = Rs + c2*R          (calc_step)
-  CM_RK4_4 = 4,   // R = Rs + R ; Qn = Qn - R/6 ; Rs = 0      (calc_step4)
-  CM_RK3_1 = 5    // Qs = Qn - R                              (calc_step1)
+  CM_RK3_1 = 2,   // Qs = Qn - R                                (calc_step1)
+  CM_RK3_2 = 3,   // Qs = (c1*Qn + c2*Qs - R) * c4              (calc_step2_3, stage 2)
+  CM_RK3_3 = 4,   // Qn = (c1*Qs + c2*Qn - R) * c4              (calc_step2_3, stage 3)
+  CM_RK4_S = 5,   // Qs = Qn - c1*R ; Rs = Rs + c2*R            (calc_step)
+  CM_RK4_4 = 6    // R = Rs + R ; Qn = Qn - R/6 ; Rs = 0        (calc_step4)
 };
 
 struct Geo {
@@ -49,9 +53,9 @@ template <class T> struct StepArgs {
   PhysConst K;
   int scheme, tvd, slau;
   // state (conservative / J) and accumulators, nv * vs each
-  T* Qin;       // Q^n (or the stage input for CM_RK3's c1 term)
-  T* Qout;      // output state (may alias Qin's role per mode)
-  T* Rs;        // RK4 accumulator
+  double* Qn;   // Q^n, FP64
+  T* Qs;        // stage state Q^(1), Q^(2) (RK3) / Q^(s) (RK4)
+  double* Rs;   // RK4 accumulator, FP64
   double* Racc; // running flux difference (FP64)
   double* Rout; // CM_R_OUT destination
   double coef;  // metric scale (RK3 coef3 or 1)
@@ -60,8 +64,8 @@ template <class T> struct StepArgs {
 };
 
 // ---- prim: src/calc_physical_quantities.f90:60-116 (3D), :7-57 (2D) -------
-template <int DIM, bool VISC, class T>
-__global__ void k_prim(const T* __restrict__ Q, Geo G, Fields<T> W, const double* __restrict__ jac,
+template <int DIM, bool VISC, class TS, class T>
+__global__ void k_prim(const TS* __restrict__ Q, Geo G, Fields<T> W, const double* __restrict__ jac,
                        PhysConst K) {
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
@@ -72,17 +76,17 @@ __global__ void k_prim(const T* __restrict__ Q, Geo G, Fields<T> W, const double
     int k = (int)(r / G.ny);
     int64_t o = G.at(i, j, k);
     T Jv = (T)jac[(int64_t)j * G.nx + i];
-    T q1 = Q[o];
+    T q1 = (T)Q[o];
     T over_Q1 = T(1) / q1;
     T rho = Jv * q1;
-    T u = Q[o + G.vs] * over_Q1;
-    T v = Q[o + 2 * G.vs] * over_Q1;
+    T u = (T)Q[o + G.vs] * over_Q1;
+    T v = (T)Q[o + 2 * G.vs] * over_Q1;
     T w = T(0), p;
     if constexpr (DIM == 3) {
-      w = Q[o + 3 * G.vs] * over_Q1;
-      p = T(K.gamma_1) * (Jv * Q[o + 4 * G.vs] - T(0.5) * rho * (u * u + v * v + w * w));
+      w = (T)Q[o + 3 * G.vs] * over_Q1;
+      p = T(K.gamma_1) * (Jv * (T)Q[o + 4 * G.vs] - T(0.5) * rho * (u * u + v * v + w * w));
     } else {
-      p = T(K.gamma_1) * (Jv * Q[o + 3 * G.vs] - T(0.5) * rho * (u * u + v * v));
+      p = T(K.gamma_1) * (Jv * (T)Q[o + 3 * G.vs] - T(0.5) * rho * (u * u + v * v));
     }
     W.rho[o] = rho; W.u[o] = u; W.v[o] = v;
     if constexpr (DIM == 3) W.w[o] = w;
@@ -90,6 +94,41 @@ __global__ void k_prim(const T* __restrict__ Q, Geo G, Fields<T> W, const double
     T temp = p / (T(K.R) * rho);
     W.T_[o] = temp;
     if constexpr (VISC) W.mu[o] = T(K.sutherland) / (temp + T(111)) * (temp * sqrt(temp));
+  }
+}
+
+// ---- mixed-form primitives: Q = Q^n (FP64) + dQ (FP32 stage increment, may be
+// null), evaluated in FP64 like k_prim, stored in FP32 with p and T as deviations
+// from the per-solve references K.p_ref, K.T_ref.
+template <int DIM, bool VISC>
+__global__ void k_prim_mx(const double* __restrict__ Qn, const float* __restrict__ dQ, Geo G, Fields<float> W,
+                          const double* __restrict__ jac, PhysConst K) {
+  int64_t n = (int64_t)G.nx * G.ny * G.nz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx);
+    int64_t r = t / G.nx;
+    int j = (int)(r % G.ny);
+    int k = (int)(r / G.ny);
+    int64_t o = G.at(i, j, k);
+    double q[5];
+#pragma unroll
+    for (int l = 0; l < DIM + 2; ++l) q[l] = Qn[o + l * G.vs] + (dQ ? (double)dQ[o + l * G.vs] : 0.0);
+    double Jv = jac[(int64_t)j * G.nx + i];
+    double over = 1.0 / q[0], rho = Jv * q[0];
+    double u = q[1] * over, v = q[2] * over, w = 0.0, p;
+    if constexpr (DIM == 3) {
+      w = q[3] * over;
+      p = K.gamma_1 * (Jv * q[4] - 0.5 * rho * (u * u + v * v + w * w));
+    } else {
+      p = K.gamma_1 * (Jv * q[3] - 0.5 * rho * (u * u + v * v));
+    }
+    double temp = p / (K.R * rho);
+    W.rho[o] = (float)rho; W.u[o] = (float)u; W.v[o] = (float)v;
+    if constexpr (DIM == 3) W.w[o] = (float)w;
+    W.p[o] = (float)(p - K.p_ref);
+    W.T_[o] = (float)(temp - K.T_ref);
+    if constexpr (VISC) W.mu[o] = (float)(K.sutherland / (temp + 111.0) * (temp * sqrt(temp)));
   }
 }
 

@@ -19,6 +19,8 @@ struct PhysConst {
   double gamma, R, Pr, Prt, threshold;
   double gamma_1, over_gamma_1, R_over_gamma_1, Cp, Cp_over_Pr, sutherland;
   double gamma_over_gamma_1, tan10deg2;
+  // mixed form only: FP32 pressure / temperature fields hold p - p_ref, T - T_ref
+  double p_ref, T_ref;
 };
 
 template <class T> __device__ __forceinline__ T sgn1(T b) { return signbit(b) ? T(-1) : T(1); }
@@ -102,16 +104,29 @@ template <class T> __device__ __forceinline__ T wiggle(T p1, T p2, T p3, T p4) {
 
 // ---- KEEP split form: 3D_solver/src/calc_keep_3d.f90 ------------------------
 // s[] holds 2io+2 stencil points; un = normal velocity; nd = normal axis.
-template <int ORDER, class T>
+// MX (mixed form): p and Tt are deviations from pr / tr; the momentum-flux
+// pressure is formed from the deviations (its stencil weights sum to 1, so the
+// constant cancels in the face difference), every other use adds the reference back.
+template <int ORDER, class T, bool MX = false>
 __device__ __forceinline__ void keep_flux(const T* rho, const T* u, const T* v, const T* w,
-                                          const T* un, const T* p, const T* Tt, int nd, T Rg1,
-                                          T F[5]) {
+                                          const T* un, const T* pd, const T* Td, int nd, T Rg1,
+                                          T F[5], T pr = T(0), T tr = T(0)) {
   const T n2 = nd == 0 ? T(1) : T(0), n3 = nd == 1 ? T(1) : T(0), n4 = nd == 2 ? T(1) : T(0);
+  constexpr int NS = ORDER;
+  T pf[NS], Tf[NS];
+  const T* p = pd;
+  const T* Tt = Td;
+  if constexpr (MX) {
+#pragma unroll
+    for (int m = 0; m < NS; ++m) { pf[m] = pd[m] + pr; Tf[m] = Td[m] + tr; }
+    p = pf;
+    Tt = Tf;
+  }
   if constexpr (ORDER == 2) {  // KEEP2 :1-15
     F[0] = T(0.25) * (rho[0] + rho[1]) * (un[0] + un[1]);
-    F[1] = T(0.5) * (F[0] * (u[0] + u[1]) + (p[0] + p[1]) * n2);
-    F[2] = T(0.5) * (F[0] * (v[0] + v[1]) + (p[0] + p[1]) * n3);
-    F[3] = T(0.5) * (F[0] * (w[0] + w[1]) + (p[0] + p[1]) * n4);
+    F[1] = T(0.5) * (F[0] * (u[0] + u[1]) + (pd[0] + pd[1]) * n2);
+    F[2] = T(0.5) * (F[0] * (v[0] + v[1]) + (pd[0] + pd[1]) * n3);
+    F[3] = T(0.5) * (F[0] * (w[0] + w[1]) + (pd[0] + pd[1]) * n4);
     F[4] = F[0] * T(0.5) * (Tt[0] + Tt[1]) * Rg1;
     F[4] = F[4] + T(0.5) * (un[0] * p[1] + un[1] * p[0]);
     F[4] = F[4] + T(0.5) * F[0] * (u[0] * u[1] + v[0] * v[1] + w[0] * w[1]);
@@ -125,7 +140,7 @@ __device__ __forceinline__ void keep_flux(const T* rho, const T* u, const T* v, 
     B = c48 * B;
     Cc = c48 * Cc;
     T AB = A - B, AC = A - Cc;
-    T pres = -c12 * p[0] + c712 * (p[1] + p[2]) - c12 * p[3];
+    T pres = -c12 * pd[0] + c712 * (pd[1] + pd[2]) - c12 * pd[3];
     F[1] = -Cc * u[0] + AB * u[1] + AC * u[2] - B * u[3] + pres * n2;
     F[2] = -Cc * v[0] + AB * v[1] + AC * v[2] - B * v[3] + pres * n3;
     F[3] = -Cc * w[0] + AB * w[1] + AC * w[2] - B * w[3] + pres * n4;
@@ -150,7 +165,7 @@ __device__ __forceinline__ void keep_flux(const T* rho, const T* u, const T* v, 
     a5 = a5 * c240;
     a6 = a6 * c240;
     T w35 = -a3 + a5, w124 = a1 - a2 + a4, w136 = a1 - a3 + a6, w25 = -a2 + a5;
-    T pres = (p[0] - T(8) * p[1] + T(37) * (p[2] + p[3]) - T(8) * p[4] + p[5]) * c60;
+    T pres = (pd[0] - T(8) * pd[1] + T(37) * (pd[2] + pd[3]) - T(8) * pd[4] + pd[5]) * c60;
     T m1 = a6 * u[0] + w35 * u[1] + w124 * u[2] + w136 * u[3] + w25 * u[4] + a4 * u[5];
     m1 = m1 + pres * n2;
     T m2 = a6 * v[0] + w35 * v[1] + w124 * v[2] + w136 * v[3] + w25 * v[4] + a4 * v[5];
@@ -170,11 +185,13 @@ __device__ __forceinline__ void keep_flux(const T* rho, const T* u, const T* v, 
 }
 
 // ---- SLAU family: 3D_solver/src/calc_slau_3d.f90 -----------------------------
-template <class T>
+// MX: pd1, pd2 are pressure deviations from pr (see keep_flux)
+template <class T, bool MX = false>
 __device__ __forceinline__ void slau_flux(bool hr2, T r1, T r2, T u1, T u2, T v1, T v2, T w1, T w2,
-                                          T un1, T un2, T p1, T p2, int nd, T HR, T gam, T g_g1,
-                                          T F[5]) {
+                                          T un1, T un2, T pd1, T pd2, int nd, T HR, T gam, T g_g1,
+                                          T F[5], T pr = T(0)) {
   const T n2 = nd == 0 ? T(1) : T(0), n3 = nd == 1 ? T(1) : T(0), n4 = nd == 2 ? T(1) : T(0);
+  const T p1 = MX ? pd1 + pr : pd1, p2 = MX ? pd2 + pr : pd2;
   T or1 = T(1) / r1, or2 = T(1) / r2;
   // SLAU_common :1-36
   T cl = sqrt(gam * p1 * or1);
@@ -188,21 +205,29 @@ __device__ __forceinline__ void slau_flux(bool hr2, T r1, T r2, T u1, T u2, T v1
   T Vtm = gv + g * fabs(un2);
   T bp = (fabs(Mp) < T(1)) ? T(0.25) * (T(2) - Mp) * ((Mp + T(1)) * (Mp + T(1))) : T(0.5) * (T(1) + sgn1(Mp));
   T bm = (fabs(Mm) < T(1)) ? T(0.25) * (T(2) + Mm) * ((Mm - T(1)) * (Mm - T(1))) : T(0.5) * (T(1) + sgn1(-Mm));
-  T dp = -p1 + p2;
+  T dp = -pd1 + pd2;
   T k1 = T(0.5) * (u1 * u1 + v1 * v1 + w1 * w1);
   T k2 = T(0.5) * (u2 * u2 + v2 * v2 + w2 * w2);
+  // bp + bm - 1 multiplies rho*c*|V| ~ 1/M: in the mixed form the subsonic branch
+  // uses the identical factored polynomial 0.25 (Mp - Mm)(3 - Mp^2 - Mp Mm - Mm^2),
+  // which has no cancellation in FP32
+  T bsum1 = bp + bm - T(1);
+  if constexpr (MX) {
+    if (fabs(Mp) < T(1) && fabs(Mm) < T(1))
+      bsum1 = T(0.25) * ((un1 - un2) * oc) * (T(3) - (Mp * Mp + Mp * Mm + Mm * Mm));
+  }
   T mass, pres;
   if (!hr2) {  // SLAU1 :49-76
     T M = fmin_f(T(1), sqrt(k1 + k2) * oc);
     T x = (T(1) - M) * (T(1) - M);
     mass = T(0.25) * (r1 * (un1 + Vtp) + r2 * (un2 - Vtm) - x * dp * oc);
-    pres = T(0.5) * (p1 + p2 + (bp - bm) * (-dp) + (T(1) - x) * (bp + bm - T(1)) * (p1 + p2));
+    pres = T(0.5) * (pd1 + pd2 + (bp - bm) * (-dp) + (T(1) - x) * bsum1 * (p1 + p2));
   } else {  // HRSLAU2 :79-104
     T V2 = sqrt(k1 + k2);
     T M = fmin_f(T(1), V2 * oc);
     T x = (T(1) - M) * (T(1) - M);
     mass = T(0.25) * (r1 * (un1 + Vtp) + r2 * (un2 - Vtm) - x * dp * oc);
-    pres = T(0.5) * (p1 + p2 + (bp - bm) * (-dp) + HR * V2 * (bp + bm - T(1)) * T(0.5) * (r1 + r2) * c);
+    pres = T(0.5) * (pd1 + pd2 + (bp - bm) * (-dp) + HR * V2 * bsum1 * T(0.5) * (r1 + r2) * c);
   }
   T m1 = mass + fabs(mass), m2 = mass - fabs(mass);
   F[0] = m1 + m2;
@@ -214,20 +239,26 @@ __device__ __forceinline__ void slau_flux(bool hr2, T r1, T r2, T u1, T u2, T v1
 }
 
 // ---- Roe: 3D_solver/src/calc_roe_3d.f90 (normal velocity first) ---------------
-template <class T>
-__device__ __forceinline__ void roe_flux(T r1, T r2, T u1, T u2, T v1, T v2, T w1, T w2, T p1, T p2,
-                                         T g1, T og1, T g_g1, T F[5]) {
+// MX: pd1, pd2 are pressure deviations from pr; the central pressure term and the
+// energy jump dQ5 use deviations, the enthalpies and the central energy flux full values
+template <class T, bool MX = false>
+__device__ __forceinline__ void roe_flux(T r1, T r2, T u1, T u2, T v1, T v2, T w1, T w2, T pd1, T pd2,
+                                         T g1, T og1, T g_g1, T F[5], T pr = T(0)) {
+  const T p1 = MX ? pd1 + pr : pd1, p2 = MX ? pd2 + pr : pd2;
   T k1 = T(0.5) * (u1 * u1 + v1 * v1 + w1 * w1);
   T k2 = T(0.5) * (u2 * u2 + v2 * v2 + w2 * w2);
   T e1 = p1 * og1 + r1 * k1;  // calc_Roe_common :53-77
   T e2 = p2 * og1 + r2 * k2;
   T ru1 = r1 * u1, ru2 = r2 * u2;
   T F1 = T(0.5) * (ru1 + ru2);
-  T F2 = T(0.5) * (ru1 * u1 + ru2 * u2 + (p1 + p2));
+  T F2 = T(0.5) * (ru1 * u1 + ru2 * u2 + (pd1 + pd2));
   T F3 = T(0.5) * (ru1 * v1 + ru2 * v2);
   T F4 = T(0.5) * (ru1 * w1 + ru2 * w2);
   T F5 = T(0.5) * ((e1 + p1) * u1 + (e2 + p2) * u2);
-  T q1 = -r1 + r2, q2 = -r1 * u1 + r2 * u2, q3 = -r1 * v1 + r2 * v2, q4 = -r1 * w1 + r2 * w2, q5 = -e1 + e2;
+  T q5;
+  if constexpr (MX) q5 = -(pd1 * og1 + r1 * k1) + (pd2 * og1 + r2 * k2);
+  else q5 = -e1 + e2;
+  T q1 = -r1 + r2, q2 = -r1 * u1 + r2 * u2, q3 = -r1 * v1 + r2 * v2, q4 = -r1 * w1 + r2 * w2;
   T H1 = g_g1 * p1 / r1 + k1;  // calc_Roe_ave :37-50
   T H2 = g_g1 * p2 / r2 + k2;
   T sl = sqrt(r1), sr = sqrt(r2);

@@ -68,8 +68,11 @@ __device__ __forceinline__ void conv_flux(const StepArgs<T>& A, const Acc& s, T 
   }
   const T* un = nd == 0 ? u : (nd == 1 ? v : w);
   const int scheme = A.scheme;
+  // mixed form: the tile's p and T are deviations from the per-solve references
+  constexpr bool MX = sizeof(T) < sizeof(double);
+  const T pr = MX ? T(A.K.p_ref) : T(0), tr = MX ? T(A.K.T_ref) : T(0);
   if (scheme == 0 || (scheme == 3 && fd <= T(A.K.threshold))) {
-    keep_flux<ORDER>(rho, u, v, w, un, p, Tt, nd, T(A.K.R_over_gamma_1), F);
+    keep_flux<ORDER, T, MX>(rho, u, v, w, un, p, Tt, nd, T(A.K.R_over_gamma_1), F, pr, tr);
     return;
   }
   T Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, Lp, Rp;
@@ -86,19 +89,37 @@ __device__ __forceinline__ void conv_flux(const StepArgs<T>& A, const Acc& s, T 
     else HR = wiggle(p[0], p[1], p[2], p[3]);
     T un1 = nd == 0 ? Lu : (nd == 1 ? Lv : Lw);
     T un2 = nd == 0 ? Ru : (nd == 1 ? Rv : Rw);
-    slau_flux(A.slau == 1, Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, un1, un2, Lp, Rp, nd, HR, T(A.K.gamma),
-              T(A.K.gamma_over_gamma_1), F);
+    slau_flux<T, MX>(A.slau == 1, Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, un1, un2, Lp, Rp, nd, HR, T(A.K.gamma),
+                     T(A.K.gamma_over_gamma_1), F, pr);
   } else {  // Roe with the normal velocity first (calc_roe_{y,z}_in permutations)
+    // rotate so the normal velocity leads: x (u,v,w), y (v,w,u), z (w,u,v)
+    T a1 = nd == 0 ? Lu : (nd == 1 ? Lv : Lw), b1 = nd == 0 ? Ru : (nd == 1 ? Rv : Rw);
+    T a2 = nd == 0 ? Lv : (nd == 1 ? Lw : Lu), b2 = nd == 0 ? Rv : (nd == 1 ? Rw : Ru);
+    T a3 = nd == 0 ? Lw : (nd == 1 ? Lu : Lv), b3 = nd == 0 ? Rw : (nd == 1 ? Ru : Rv);
     T Fr[5];
-    const T g1 = T(A.K.gamma_1), og1 = T(A.K.over_gamma_1), gg = T(A.K.gamma_over_gamma_1);
+    bool wide = false;
+    if constexpr (sizeof(T) < sizeof(double)) {
+      // mixed form: the eigen-decomposition stays FP64 where |u_n| or |u_n| - c is
+      // small against c (stagnation / sonic points), where FP32 |lambda| loses digits
+      T cl = sqrt(T(A.K.gamma) * (Lp + pr) / Lr), cr = sqrt(T(A.K.gamma) * (Rp + pr) / Rr);
+      T un = T(0.5) * (a1 + b1), cm = T(0.5) * (cl + cr);
+      wide = fabs(un) < T(0.05) * cm || fabs(fabs(un) - cm) < T(0.05) * cm;
+    }
+    if (wide) {
+      double Fd[5];
+      roe_flux<double, MX>(Lr, Rr, a1, b1, a2, b2, a3, b3, Lp, Rp, A.K.gamma_1, A.K.over_gamma_1,
+                           A.K.gamma_over_gamma_1, Fd, A.K.p_ref);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) Fr[q] = (T)Fd[q];
+    } else {
+      roe_flux<T, MX>(Lr, Rr, a1, b1, a2, b2, a3, b3, Lp, Rp, T(A.K.gamma_1), T(A.K.over_gamma_1),
+                      T(A.K.gamma_over_gamma_1), Fr, pr);
+    }
     if (nd == 0) {
-      roe_flux(Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, Lp, Rp, g1, og1, gg, Fr);
       F[0] = Fr[0]; F[1] = Fr[1]; F[2] = Fr[2]; F[3] = Fr[3]; F[4] = Fr[4];
     } else if (nd == 1) {
-      roe_flux(Lr, Rr, Lv, Rv, Lw, Rw, Lu, Ru, Lp, Rp, g1, og1, gg, Fr);
       F[0] = Fr[0]; F[2] = Fr[1]; F[3] = Fr[2]; F[1] = Fr[3]; F[4] = Fr[4];
     } else {
-      roe_flux(Lr, Rr, Lw, Rw, Lu, Ru, Lv, Rv, Lp, Rp, g1, og1, gg, Fr);
       F[0] = Fr[0]; F[3] = Fr[1]; F[1] = Fr[2]; F[2] = Fr[3]; F[4] = Fr[4];
     }
   }
@@ -619,6 +640,8 @@ k_sweep(StepArgs<T> A, int last) {
       for (int l = 0; l < NV; ++l) A.Racc[o + l * G.vs] = R[l];
       return;
     }
+    // mixed form: the stage state holds the FP32 increment Q^(s) - Q^n
+    constexpr bool MXC = sizeof(T) < sizeof(double);
     switch (A.mode) {
       case CM_R_OUT: {
         // reference Rs(nx-2, nv, ny-2, nz-2) order, cell (i,j,k) -> (i-1, l, j-1, k-1)
@@ -627,19 +650,30 @@ k_sweep(StepArgs<T> A, int last) {
         for (int l = 0; l < NV; ++l) A.Rout[base + (int64_t)l * (G.nx - 2)] = R[l];
         break;
       }
-      case CM_RK3: {
-#pragma unroll
-        for (int l = 0; l < NV; ++l) {
-          const int64_t q = o + l * G.vs;
-          A.Qout[q] = (T)((A.c1 * (double)A.Qin[q] + A.c2 * (double)A.Qout[q] - R[l]) * A.c4);
-        }
-        break;
-      }
       case CM_RK3_1: {
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           const int64_t q = o + l * G.vs;
-          A.Qout[q] = (T)((double)A.Qin[q] - R[l]);
+          if constexpr (MXC) A.Qs[q] = (T)(-R[l]);  // stage increment Q1 - Qn
+          else A.Qs[q] = (T)(A.Qn[q] - R[l]);
+        }
+        break;
+      }
+      case CM_RK3_2: {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          const int64_t q = o + l * G.vs;
+          if constexpr (MXC) A.Qs[q] = (T)((A.c2 * (double)A.Qs[q] - R[l]) * A.c4);  // c1 + c2 = 1
+          else A.Qs[q] = (T)((A.c1 * A.Qn[q] + A.c2 * (double)A.Qs[q] - R[l]) * A.c4);
+        }
+        break;
+      }
+      case CM_RK3_3: {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          const int64_t q = o + l * G.vs;
+          if constexpr (MXC) A.Qn[q] = A.Qn[q] + (A.c1 * (double)A.Qs[q] - R[l]) * A.c4;  // (c1 + c2) c4 = 1
+          else A.Qn[q] = (A.c1 * (double)A.Qs[q] + A.c2 * A.Qn[q] - R[l]) * A.c4;
         }
         break;
       }
@@ -647,8 +681,9 @@ k_sweep(StepArgs<T> A, int last) {
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           const int64_t q = o + l * G.vs;
-          A.Qout[q] = (T)((double)A.Qin[q] - A.c1 * R[l]);
-          A.Rs[q] = (T)((double)A.Rs[q] + A.c2 * R[l]);
+          if constexpr (MXC) A.Qs[q] = (T)(-A.c1 * R[l]);
+          else A.Qs[q] = (T)(A.Qn[q] - A.c1 * R[l]);
+          A.Rs[q] = A.Rs[q] + A.c2 * R[l];
         }
         break;
       }
@@ -656,9 +691,9 @@ k_sweep(StepArgs<T> A, int last) {
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           const int64_t q = o + l * G.vs;
-          double r = (double)A.Rs[q] + R[l];
-          A.Qout[q] = (T)((double)A.Qout[q] - r * (1.0 / 6.0));
-          A.Rs[q] = T(0);
+          double r = A.Rs[q] + R[l];
+          A.Qn[q] = A.Qn[q] - r * (1.0 / 6.0);
+          A.Rs[q] = 0.0;
         }
         break;
       }

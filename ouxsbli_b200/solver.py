@@ -32,6 +32,7 @@ class SolverConfig:
     tvd: str = "hybrid"            # TVD: none | tvd | hybrid
     slau: str = "HRSLAU2"          # SLAU_VARIANT
     rk: int = 3
+    precision: str = "fp64"        # fp64 | mixed (FP32 stage states/fluxes, FP64 Q^n + accumulation)
     gamma: float = 1.4
     R: float = 287.03
     Pr: float = 0.71
@@ -75,7 +76,7 @@ class SolverConfig:
         c.slau = _lib.SLAU_VARIANTS[self.slau]
         c.rk = self.rk
         c.bc_x = c.bc_y = c.bc_z = 0
-        c.precision = 0
+        c.precision = _lib.PRECISION[self.precision]
         c.gamma, c.R, c.Pr, c.Prt, c.threshold, c.dt = (self.gamma, self.R, self.Pr, self.Prt,
                                                          self.threshold, self.dt)
         c.dx = arr(self.dx)

@@ -1,0 +1,87 @@
+"""The reference's own known-answer tests, run through the drop-in Case API on the GPU.
+
+* ETGV (ouxsbli/tests/test_etgv.py:15-61): Euler KEEP-2, RK4, 66^3, 20000 steps of
+  dt = 0.01: final (s0 - s)/s0 < 3e-3 and 0.75 < ke/ke0 < 1.01 read back from the
+  data/*.d history files.
+* EVC (ouxsbli/tests/test_evc.py:50-133): 2D Euler vortex convection on 64/128/256
+  grids with the reference parameters; L2(rho) against the initial field gives a
+  least-squares convergence order >= 3.6 (KEEP-4) and >= 5.7 (KEEP-6).  The
+  reference test needs FP64 fields (its note asks for io = 8), so the FP64
+  device state is used instead of the float32 VTK files.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import interior, tgv
+from ouxsbli_b200 import Case
+
+pytestmark = pytest.mark.gpu
+
+
+def test_etgv_ke_and_entropy_preserved(tmp_path, cuda_device):
+    case = Case(source="3D_solver/ETGV", workdir=str(tmp_path / "etgv"), visc="euler", scheme="keep",
+                accuracy=2, rk="rk4", nx=66, ny=66, nz=66, nt=20000, np=1, dt=0.01e0)
+    case.build()
+    case.run(nranks=2, device=cuda_device)
+    data = tmp_path / "etgv" / "data"
+    ent = np.loadtxt(data / "entropy.d")
+    ke = np.loadtxt(data / "kinetic_energy.d")
+    assert ent.shape == (2, 2) and ke.shape == (2, 3)
+    assert abs(ent[-1, -1]) < 3.0e-3
+    assert 0.75 < ke[-1, -1] < 1.0 + 0.01
+    assert (data / "Q00000.vtr").exists() and (data / "Q00001.vtr").exists()
+    assert (tmp_path / "etgv" / "recal" / "Q00001.dat").stat().st_size == 66 ** 3 * 5 * 8
+
+
+def _evc_l2(tmp_path, accuracy, n, device):
+    Lx, gamma, R, M0, T0 = 0.1, 1.4, 287.15, 0.05, 300.0
+    u0 = M0 * math.sqrt(gamma * R * T0)
+    case = Case(source="2D_solver/EVC", workdir=str(tmp_path / f"evc{accuracy}_{n}"), scheme="keep",
+                accuracy=accuracy, visc="euler", tvd="none", nx=n + accuracy, ny=n + accuracy, Lx=Lx, Ly=Lx,
+                gamma=gamma, Pr=0.71, R=R, M0=M0, beta=1.0 / 50.0, theta=0.0, Rc=0.005, p0=1.0e5, T0=T0, u0=u0)
+    case.build()
+    case.run(device=device)
+    from ouxsbli_b200.grid import jacobian
+    p, xc, yc, zc, dx, dy, dz, Q0 = case._initial()
+    J = jacobian(dx, dy, None)
+    q1 = case.solver.get_state()
+    g = accuracy // 2
+    rho0 = Q0[g:-g, 0, g:-g]
+    rho1 = (J[:, None, :] * q1)[g:-g, 0, g:-g]
+    return math.sqrt(np.mean((rho1 - rho0) ** 2))
+
+
+@pytest.mark.parametrize("accuracy,min_order", [(4, 3.6), (6, 5.7)])
+def test_evc_grid_convergence(tmp_path, accuracy, min_order, cuda_device):
+    grids = [64, 128, 256]
+    errs = [_evc_l2(tmp_path, accuracy, n, cuda_device) for n in grids]
+    order = np.polyfit(np.log([1.0 / n for n in grids]), np.log(errs), 1)[0]
+    assert order >= min_order, (errs, order)
+
+
+@pytest.mark.parametrize("scheme,visc,precision", [("Hybrid", "NS", "fp64"), ("Roe", "Euler", "fp64"),
+                                                   ("SLAU", "NS", "fp64"), ("Hybrid", "NS", "mixed")])
+def test_conservation(scheme, visc, precision, cuda_device):
+    """Periodic finite-volume update: sums over interior cells of Q/J are conserved
+    (mass and energy to 1e-12 of their totals, momenta to 1e-12 of the total |momentum|;
+    1e-8 for the mixed form, whose FP32 stage increments are rounded before they are
+    added back to the FP64 state).
+
+    LES is left out on purpose: the reference's SGS viscosity is not periodic in the
+    outer ghost layers (calc_les.f90:118-122 and set_bc_mut_common), so its fluxes at
+    the periodic seam do not telescope; the GPU path reproduces that."""
+    from ouxsbli_b200.solver import Solver
+    cfg, qj = tgv(24, mach=1.25, scheme=scheme, visc=visc, precision=precision)
+    s = Solver(cfg, cuda_device)
+    s.set_state(qj)
+    s.step(20)
+    q = s.get_state()
+    a, b = interior(qj, cfg.g, 3), interior(q, cfg.g, 3)
+    mom_scale = sum(np.abs(a[:, l]).sum() for l in (1, 2, 3))
+    for l in range(5):
+        tot0, tot1 = a[:, l].sum(), b[:, l].sum()
+        scale = mom_scale if l in (1, 2, 3) else np.abs(a[:, l]).sum()
+        tol = 1e-12 if precision == "fp64" else 1e-8
+        assert abs(tot1 - tot0) <= tol * scale, (l, tot0, tot1)
