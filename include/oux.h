@@ -168,6 +168,38 @@ int oux_host_ref_diagnostics(int32_t nx, int32_t ny, int32_t nz, int32_t order, 
 /* Number of kernel launches the last oux_step call issued (for reporting). */
 int oux_launch_count(const oux_handle* h, int64_t* launches);
 
+/* --- allocation-free residual ---------------------------------------------
+ * No counterpart in the reference.  The same stage residual as oux_rhs, for
+ * callers that cannot allocate device memory when they call: a host program
+ * that has no device allocator of its own and does not want to size, own and
+ * bind a scratch buffer (a Fortran or C driver holding only plain pointers), or
+ * code running where every free byte is already reserved by another allocator
+ * (a caching allocator's pool) or where an allocation's implicit device
+ * synchronisation is not acceptable.  It needs no handle and calls no
+ * cudaMalloc / cudaFree or other allocating routine.
+ *
+ * Scratch: a fixed device array of OUX_NOALLOC_SCRATCH_BYTES inside the library,
+ * created on every GPU where the library's device code is loaded and held until
+ * the process exits.  A grid whose oux_scratch_bytes() exceeds that size is
+ * rejected with OUX_E_TOO_SMALL and a message giving both sizes; that is about
+ * 200 000 cells (59^3 with ghosts) in 3D FP64.
+ *
+ * Inputs: cfg (precision must be OUX_FP64); state_dev, a 256-byte aligned
+ * device array in the layout oux_layout_of() reports for cfg (the state buffer
+ * of oux_bind, ghost cells already filled), only read.  Output: rhs_dev as for
+ * oux_rhs.  Asynchronous on `stream`; dx/dy/dz are copied on `stream`, so when
+ * they are page-locked they must stay valid until the stream reaches the call.
+ *
+ * The first call on a device looks up the array's device address on that
+ * device (cudaGetSymbolAddress, once per device, with that device current);
+ * make that first call before any stream capture.  Every call on a device
+ * shares the one array, which keeps the previous call's contents (the call
+ * clears what must start at zero), so calls whose GPU work overlaps (other
+ * streams, other host threads) race and give wrong results: order them on one
+ * stream or synchronise between them. */
+#define OUX_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+int oux_rhs_noalloc(const oux_config* cfg, const double* state_dev, double* rhs_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

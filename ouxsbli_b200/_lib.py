@@ -37,8 +37,9 @@ SYMBOLS = [
     "oux_scratch_bytes", "oux_layout_of", "oux_bind", "oux_set_state", "oux_get_state",
     "oux_pack_state", "oux_unpack_state", "oux_fill_ghosts", "oux_rhs", "oux_step",
     "oux_diagnostics", "oux_check_state", "oux_status", "oux_profile", "oux_profile_read",
-    "oux_host_ref_diagnostics", "oux_launch_count",
+    "oux_host_ref_diagnostics", "oux_launch_count", "oux_rhs_noalloc",
 ]
+NOALLOC_SCRATCH_BYTES = 32 << 20  # OUX_NOALLOC_SCRATCH_BYTES
 
 
 class OuxConfig(C.Structure):
@@ -98,6 +99,7 @@ def _load() -> C.CDLL:
         "oux_host_ref_diagnostics": (C.c_int, [i32, i32, i32, i32, C.c_double, C.POINTER(C.c_float),
                                                C.POINTER(C.c_float), C.POINTER(C.c_float), dp]),
         "oux_launch_count": (C.c_int, [vp, C.POINTER(i64)]),
+        "oux_rhs_noalloc": (C.c_int, [cfgp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

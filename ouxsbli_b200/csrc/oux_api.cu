@@ -2,6 +2,7 @@
 // the stage driver that sequences the kernels of oux_kernels.cuh /
 // oux_sweep.cuh, and the C ABI declared in include/oux.h.
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -572,6 +573,106 @@ int run_steps(oux_handle* h, int nsteps, cudaStream_t s) {
   return OUX_OK;
 }
 
+// ---- allocation-free residual (oux_rhs_noalloc) ------------------------------------
+// Scratch for oux_rhs_noalloc: a fixed array in the library's own device image,
+// created when the library's module is loaded on a device and held until the
+// process exits.  Every oux_rhs_noalloc call on a device uses the same bytes.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[OUX_NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::atomic<unsigned char*> g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+
+// Device address of g_noalloc_scratch on the current device, looked up once per
+// device (cudaGetSymbolAddress with that device current) and cached.
+int noalloc_scratch(unsigned char** out) {
+  int dev = -1;
+  OUX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(OUX_E_INVALID, "device ordinal out of range");
+  unsigned char* p = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    void* a = nullptr;
+    OUX_CUDA(cudaGetSymbolAddress(&a, g_noalloc_scratch));
+    p = static_cast<unsigned char*>(a);
+    g_noalloc_ptr[dev].store(p, std::memory_order_release);
+  }
+  *out = p;
+  return OUX_OK;
+}
+
+// Physical constants of a configuration (src/mod_constant.f90.fypp:18-32),
+// without the host metric tables.
+PhysConst consts_of(const oux_config& c) {
+  PhysConst K{};
+  K.gamma = c.gamma; K.R = c.R; K.Pr = c.Pr; K.Prt = c.Prt; K.threshold = c.threshold;
+  K.gamma_1 = c.gamma - 1.0;
+  K.over_gamma_1 = 1.0 / (c.gamma - 1.0);
+  K.R_over_gamma_1 = c.R / (c.gamma - 1.0);
+  K.Cp = c.gamma * c.R / (c.gamma - 1.0);
+  K.Cp_over_Pr = c.visc != OUX_EULER ? K.Cp / c.Pr : 0.0;
+  K.sutherland = 1.716e-5 * 384.2 * std::pow(273.2, -1.5);
+  K.gamma_over_gamma_1 = c.gamma * K.over_gamma_1;
+  K.p_ref = 0.0;
+  K.T_ref = 0.0;
+  double t10 = std::tan(10.0 * std::acos(-1.0) / 180.0);
+  K.tan10deg2 = t10 * t10;
+  return K;
+}
+
+// Metric tables on the device from the raw spacings d = [dx | dy | dz] (same
+// arithmetic and order of operations as build_tables, so the values are the
+// same bits): 1/d, the Jacobian with clamped edges, and the dt * face-area
+// tables of preprocess.f90.fypp.
+__global__ void k_noalloc_tables(const double* __restrict__ d, Geo G, double dt, Metrics M) {
+  const int nx = G.nx, ny = G.ny, nz = G.nz;
+  const double* dx = d;
+  const double* dy = d + (nx - 1);
+  const double* dz = dy + (ny - 1);
+  double* inv_dx = const_cast<double*>(M.inv_dx);
+  double* inv_dy = const_cast<double*>(M.inv_dy);
+  double* inv_dz = const_cast<double*>(M.inv_dz);
+  double* jac = const_cast<double*>(M.jac);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (int64_t t = t0; t < nx - 1; t += stride) inv_dx[t] = 1.0 / dx[t];
+  for (int64_t t = t0; t < ny - 1; t += stride) inv_dy[t] = 1.0 / dy[t];
+  if (G.dim == 3) {
+    for (int64_t t = t0; t < nz - 1; t += stride) inv_dz[t] = 1.0 / dz[t];
+  } else if (t0 == 0) {
+    inv_dz[0] = 0.0;
+  }
+  for (int64_t t = t0; t < (int64_t)nx * ny; t += stride) {
+    int i = (int)(t % nx), j = (int)(t / nx);
+    i = i < 1 ? 1 : (i > nx - 2 ? nx - 2 : i);
+    j = j < 1 ? 1 : (j > ny - 2 ? ny - 2 : j);
+    if (G.dim == 3)
+      jac[t] = 8.0 / ((dx[i - 1] + dx[i]) * (dy[j - 1] + dy[j]) * 2.0 * dz[0]);
+    else
+      jac[t] = 4.0 / ((dx[i - 1] + dx[i]) * (dy[j - 1] + dy[j]));
+  }
+  if (G.dim == 3) {
+    double* dtdxdy = const_cast<double*>(M.dtdxdy);
+    double* dtdydz = const_cast<double*>(M.dtdydz);
+    double* dtdzdx = const_cast<double*>(M.dtdzdx);
+    for (int64_t t = t0; t < (int64_t)(nx - 2) * (ny - 2); t += stride) {
+      int i = (int)(t % (nx - 2)), j = (int)(t / (nx - 2));
+      dtdxdy[t] = 0.25 * dt * (dx[i] + dx[i + 1]) * (dy[j] + dy[j + 1]);
+    }
+    for (int64_t t = t0; t < (int64_t)(ny - 2) * (nz - 2); t += stride) {
+      int j = (int)(t % (ny - 2)), k = (int)(t / (ny - 2));
+      dtdydz[t] = 0.25 * dt * (dy[j] + dy[j + 1]) * (dz[k] + dz[k + 1]);
+    }
+    for (int64_t t = t0; t < (int64_t)(nx - 2) * (nz - 2); t += stride) {
+      int i = (int)(t % (nx - 2)), k = (int)(t / (nx - 2));
+      dtdzdx[t] = 0.25 * dt * (dz[k] + dz[k + 1]) * (dx[i] + dx[i + 1]);
+    }
+  } else {
+    double* dtdx = const_cast<double*>(M.dtdx);
+    double* dtdy = const_cast<double*>(M.dtdy);
+    for (int64_t t = t0; t < nx - 2; t += stride) dtdx[t] = 0.5 * dt * (dx[t] + dx[t + 1]);
+    for (int64_t t = t0; t < ny - 2; t += stride) dtdy[t] = 0.5 * dt * (dy[t] + dy[t + 1]);
+  }
+}
+
 }  // namespace
 
 // ================================ C ABI =========================================
@@ -856,6 +957,75 @@ int oux_host_ref_diagnostics(int32_t nx, int32_t ny, int32_t nz, int32_t order, 
 int oux_launch_count(const oux_handle* h, int64_t* launches) {
   if (!h || !launches) return fail(OUX_E_INVALID, "null argument");
   *launches = h->launches;
+  return OUX_OK;
+}
+
+int oux_rhs_noalloc(const oux_config* cfg, const double* state_dev, double* rhs_dev, void* stream) {
+  std::string why;
+  int rc = validate(cfg, why);
+  if (rc) return fail(rc, why);
+  if (!state_dev || !rhs_dev) return fail(OUX_E_INVALID, "null argument");
+  if (cfg->precision != OUX_FP64) return fail(OUX_E_INVALID, "oux_rhs_noalloc computes the FP64 form only");
+  if ((uintptr_t)state_dev & 255) return fail(OUX_E_INVALID, "state buffer must be 256-byte aligned");
+  int vk = visc_kind(cfg, why);
+  if (vk < 0) return fail(OUX_E_INVALID, why);
+  // a handle on the stack: its host tables stay empty (nothing is allocated)
+  oux_handle h;
+  h.cfg = *cfg;
+  if (h.cfg.dim == 2) { h.cfg.nz = 1; h.cfg.bc_z = 0; }
+  const ScratchPlan P = plan_scratch(h.cfg);
+  if (P.total > (size_t)OUX_NOALLOC_SCRATCH_BYTES)
+    return fail(OUX_E_TOO_SMALL, "oux_rhs_noalloc: this grid needs " + std::to_string(P.total) +
+                                     " scratch bytes, more than the fixed OUX_NOALLOC_SCRATCH_BYTES = " +
+                                     std::to_string((size_t)OUX_NOALLOC_SCRATCH_BYTES));
+  h.G = make_geo(h.cfg);
+  h.nv = h.cfg.dim + 2;
+  h.vk = vk;
+  h.les = h.cfg.visc == OUX_LES;
+  h.mixed = false;
+  h.K = consts_of(h.cfg);
+  unsigned char* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  h.Q = const_cast<double*>(state_dev);  // read only: the residual mode writes no state
+  h.scratch = scratch;
+  h.scratch_bytes = OUX_NOALLOC_SCRATCH_BYTES;
+  carve(&h);
+  // metric tables: same carve order as oux_bind's upload (1/dx, 1/dy, 1/dz, J, dt*area)
+  const Geo& G = h.G;
+  const int nx = G.nx, ny = G.ny, nz = G.nz;
+  double* m = reinterpret_cast<double*>(scratch + P.metrics);
+  h.M.inv_dx = m; m += nx - 1;
+  h.M.inv_dy = m; m += ny - 1;
+  h.M.inv_dz = m; m += (G.dim == 3 ? nz - 1 : 1);
+  h.M.jac = m; m += (size_t)nx * ny;
+  if (G.dim == 3) {
+    h.M.dtdxdy = m; m += (size_t)(nx - 2) * (ny - 2);
+    h.M.dtdydz = m; m += (size_t)(ny - 2) * (nz - 2);
+    h.M.dtdzdx = m;
+    h.M.dtdx = h.M.dtdy = nullptr;
+  } else {
+    h.M.dtdx = m; m += nx - 2;
+    h.M.dtdy = m;
+    h.M.dtdxdy = h.M.dtdydz = h.M.dtdzdx = nullptr;
+  }
+  // raw spacings staged in the (unused here) stage-state region, then expanded on the device
+  double* d = reinterpret_cast<double*>(scratch + P.q2);
+  OUX_CUDA(cudaMemcpyAsync(d, cfg->dx, (size_t)(nx - 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+  OUX_CUDA(cudaMemcpyAsync(d + (nx - 1), cfg->dy, (size_t)(ny - 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (G.dim == 3)
+    OUX_CUDA(cudaMemcpyAsync(d + (nx - 1) + (ny - 1), cfg->dz, (size_t)(nz - 1) * sizeof(double),
+                             cudaMemcpyHostToDevice, s));
+  k_noalloc_tables<<<grid_for((int64_t)nx * ny, 256), 256, 0, s>>>(d, G, h.cfg.dt, h.M);
+  OUX_CUDA(cudaGetLastError());
+  // what must start at zero: the status word and the output (ghost entries stay 0)
+  OUX_CUDA(cudaMemsetAsync(h.status, 0, sizeof(int), s));
+  const size_t n = (size_t)h.nv * (nx - 2) * (ny - 2) * (G.dim == 3 ? nz - 2 : 1);
+  OUX_CUDA(cudaMemsetAsync(rhs_dev, 0, n * sizeof(double), s));
+  StepArgs<double> A = base_args<double>(&h);
+  A.mode = CM_R_OUT; A.coef = 1.0; A.Rout = rhs_dev;
+  if ((rc = run_stage<double, double>(&h, h.Q, A, s))) return rc;
+  OUX_CUDA(cudaGetLastError());
   return OUX_OK;
 }
 
