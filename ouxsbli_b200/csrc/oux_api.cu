@@ -494,8 +494,8 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   if (c.scheme != OUX_KEEP) {  // Ducros sensor
     Timed tm(h, KK_SENSOR, s);
     const int gb = grid_for(ncell, 256);
-    if (G.dim == 3) k_grad<3, 0, true, T><<<gb, 256, 0, s>>>(G, W, h->M);
-    else k_grad<2, 0, true, T><<<gb, 256, 0, s>>>(G, W, h->M);
+    if (G.dim == 3) k_sensor<3, T><<<gb, 256, 0, s>>>(G, W, h->M);
+    else k_sensor<2, T><<<gb, 256, 0, s>>>(G, W, h->M);
     h->launches++;
   }
   if (h->les) {

@@ -64,164 +64,141 @@ template <class T> struct StepArgs {
 };
 
 // ---- prim: src/calc_physical_quantities.f90:60-116 (3D), :7-57 (2D) -------
+// One padded cell t (x fastest over nx, then ny, then nz).
+template <int DIM, bool VISC, class TS, class T>
+__device__ __forceinline__ void prim_cell(const TS* Q, const Geo& G, const Fields<T>& W, const double* jac,
+                                          const PhysConst& K, int64_t t) {
+  int i = (int)(t % G.nx);
+  int64_t r = t / G.nx;
+  int j = (int)(r % G.ny);
+  int k = (int)(r / G.ny);
+  int64_t o = G.at(i, j, k);
+  T Jv = (T)jac[(int64_t)j * G.nx + i];
+  T q1 = (T)Q[o];
+  T over_Q1 = T(1) / q1;
+  T rho = Jv * q1;
+  T u = (T)Q[o + G.vs] * over_Q1;
+  T v = (T)Q[o + 2 * G.vs] * over_Q1;
+  T w = T(0), p;
+  if constexpr (DIM == 3) {
+    w = (T)Q[o + 3 * G.vs] * over_Q1;
+    p = T(K.gamma_1) * (Jv * (T)Q[o + 4 * G.vs] - T(0.5) * rho * (u * u + v * v + w * w));
+  } else {
+    p = T(K.gamma_1) * (Jv * (T)Q[o + 3 * G.vs] - T(0.5) * rho * (u * u + v * v));
+  }
+  W.rho[o] = rho; W.u[o] = u; W.v[o] = v;
+  if constexpr (DIM == 3) W.w[o] = w;
+  W.p[o] = p;
+  T temp = p / (T(K.R) * rho);
+  W.T_[o] = temp;
+  if constexpr (VISC) W.mu[o] = T(K.sutherland) / (temp + T(111)) * (temp * sqrt(temp));
+}
+
 template <int DIM, bool VISC, class TS, class T>
 __global__ void k_prim(const TS* __restrict__ Q, Geo G, Fields<T> W, const double* __restrict__ jac,
                        PhysConst K) {
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    int i = (int)(t % G.nx);
-    int64_t r = t / G.nx;
-    int j = (int)(r % G.ny);
-    int k = (int)(r / G.ny);
-    int64_t o = G.at(i, j, k);
-    T Jv = (T)jac[(int64_t)j * G.nx + i];
-    T q1 = (T)Q[o];
-    T over_Q1 = T(1) / q1;
-    T rho = Jv * q1;
-    T u = (T)Q[o + G.vs] * over_Q1;
-    T v = (T)Q[o + 2 * G.vs] * over_Q1;
-    T w = T(0), p;
-    if constexpr (DIM == 3) {
-      w = (T)Q[o + 3 * G.vs] * over_Q1;
-      p = T(K.gamma_1) * (Jv * (T)Q[o + 4 * G.vs] - T(0.5) * rho * (u * u + v * v + w * w));
-    } else {
-      p = T(K.gamma_1) * (Jv * (T)Q[o + 3 * G.vs] - T(0.5) * rho * (u * u + v * v));
-    }
-    W.rho[o] = rho; W.u[o] = u; W.v[o] = v;
-    if constexpr (DIM == 3) W.w[o] = w;
-    W.p[o] = p;
-    T temp = p / (T(K.R) * rho);
-    W.T_[o] = temp;
-    if constexpr (VISC) W.mu[o] = T(K.sutherland) / (temp + T(111)) * (temp * sqrt(temp));
-  }
+       t += (int64_t)gridDim.x * blockDim.x)
+    prim_cell<DIM, VISC, TS, T>(Q, G, W, jac, K, t);
 }
 
 // ---- mixed-form primitives: Q = Q^n (FP64) + dQ (FP32 stage increment, may be
 // null), evaluated in FP64 like k_prim, stored in FP32 with p and T as deviations
 // from the per-solve references K.p_ref, K.T_ref.
 template <int DIM, bool VISC>
+__device__ __forceinline__ void prim_mx_cell(const double* Qn, const float* dQ, const Geo& G,
+                                             const Fields<float>& W, const double* jac, const PhysConst& K,
+                                             int64_t t) {
+  int i = (int)(t % G.nx);
+  int64_t r = t / G.nx;
+  int j = (int)(r % G.ny);
+  int k = (int)(r / G.ny);
+  int64_t o = G.at(i, j, k);
+  double q[5];
+#pragma unroll
+  for (int l = 0; l < DIM + 2; ++l) q[l] = Qn[o + l * G.vs] + (dQ ? (double)dQ[o + l * G.vs] : 0.0);
+  double Jv = jac[(int64_t)j * G.nx + i];
+  double over = 1.0 / q[0], rho = Jv * q[0];
+  double u = q[1] * over, v = q[2] * over, w = 0.0, p;
+  if constexpr (DIM == 3) {
+    w = q[3] * over;
+    p = K.gamma_1 * (Jv * q[4] - 0.5 * rho * (u * u + v * v + w * w));
+  } else {
+    p = K.gamma_1 * (Jv * q[3] - 0.5 * rho * (u * u + v * v));
+  }
+  double temp = p / (K.R * rho);
+  W.rho[o] = (float)rho; W.u[o] = (float)u; W.v[o] = (float)v;
+  if constexpr (DIM == 3) W.w[o] = (float)w;
+  W.p[o] = (float)(p - K.p_ref);
+  W.T_[o] = (float)(temp - K.T_ref);
+  if constexpr (VISC) W.mu[o] = (float)(K.sutherland / (temp + 111.0) * (temp * sqrt(temp)));
+}
+
+template <int DIM, bool VISC>
 __global__ void k_prim_mx(const double* __restrict__ Qn, const float* __restrict__ dQ, Geo G, Fields<float> W,
                           const double* __restrict__ jac, PhysConst K) {
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    int i = (int)(t % G.nx);
-    int64_t r = t / G.nx;
-    int j = (int)(r % G.ny);
-    int k = (int)(r / G.ny);
-    int64_t o = G.at(i, j, k);
-    double q[5];
-#pragma unroll
-    for (int l = 0; l < DIM + 2; ++l) q[l] = Qn[o + l * G.vs] + (dQ ? (double)dQ[o + l * G.vs] : 0.0);
-    double Jv = jac[(int64_t)j * G.nx + i];
-    double over = 1.0 / q[0], rho = Jv * q[0];
-    double u = q[1] * over, v = q[2] * over, w = 0.0, p;
-    if constexpr (DIM == 3) {
-      w = q[3] * over;
-      p = K.gamma_1 * (Jv * q[4] - 0.5 * rho * (u * u + v * v + w * w));
-    } else {
-      p = K.gamma_1 * (Jv * q[3] - 0.5 * rho * (u * u + v * v));
-    }
-    double temp = p / (K.R * rho);
-    W.rho[o] = (float)rho; W.u[o] = (float)u; W.v[o] = (float)v;
-    if constexpr (DIM == 3) W.w[o] = (float)w;
-    W.p[o] = (float)(p - K.p_ref);
-    W.T_[o] = (float)(temp - K.T_ref);
-    if constexpr (VISC) W.mu[o] = (float)(K.sutherland / (temp + 111.0) * (temp * sqrt(temp)));
+       t += (int64_t)gridDim.x * blockDim.x)
+    prim_mx_cell<DIM, VISC>(Qn, dQ, G, W, jac, K, t);
+}
+
+// ---- Ducros sensor: calc_Ducros (3D_solver/src/calc_hybrid.f90:11-72; 2D twin
+// :11-55) on cells 1..n-2, with the reference's copies to the outer faces.
+template <int DIM, class T>
+__device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, const Metrics& M, int64_t t) {
+  const int i = (int)(t % G.nx);
+  const int64_t r = t / G.nx;
+  const int j = (int)(r % G.ny);
+  const int k = (int)(r / G.ny);
+  if (i < 1 || i > G.nx - 2 || j < 1 || j > G.ny - 2) return;
+  if (DIM == 3 && (k < 1 || k > G.nz - 2)) return;
+  const int64_t o = G.at(i, j, k);
+  const T eps = T(1.0e-12);
+  T dxt = T(0.25) * ((T)M.inv_dx[i - 1] + (T)M.inv_dx[i]);
+  T dyt = T(0.25) * ((T)M.inv_dy[j - 1] + (T)M.inv_dy[j]);
+  T f;
+  if constexpr (DIM == 3) {
+    T dzt = T(0.25) * ((T)M.inv_dz[k - 1] + (T)M.inv_dz[k]);
+    const int64_t ox = 1, oy = G.sx, oz = G.plane;
+    T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
+    T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
+    T dwdx = (-W.w[o - ox] + W.w[o + ox]) * dxt;
+    T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
+    T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
+    T dwdy = (-W.w[o - oy] + W.w[o + oy]) * dyt;
+    T dudz = (-W.u[o - oz] + W.u[o + oz]) * dzt;
+    T dvdz = (-W.v[o - oz] + W.v[o + oz]) * dzt;
+    T dwdz = (-W.w[o - oz] + W.w[o + oz]) * dzt;
+    T div = dudx + dvdy + dwdz;
+    T r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
+    f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
+  } else {
+    const int64_t ox = 1, oy = G.sx;
+    T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
+    T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
+    T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
+    T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
+    T div = dudx + dvdy;
+    T rot = dvdx - dudy;
+    f = (div * div) / (div * div + rot * rot + eps);
+  }
+  f = fmin_f(T(1), f);
+  W.sensor[o] = f;
+  if (i == 1) W.sensor[G.at(0, j, k)] = f; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = f;
+  if (j == 1) W.sensor[G.at(i, 0, k)] = f; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = f;
+  if constexpr (DIM == 3) {
+    if (k == 1) W.sensor[G.at(i, j, 0)] = f; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = f;
   }
 }
 
-// ---- node velocity gradients (+ the Ducros sensor) in one pass ----------------
-// Gradients use the transverse-derivative stencils of the viscous loaders:
-// 6th order (load_smem_visc_cent.f90.fypp:51-70) for Central-6, 4th order
-// (load_smem_visc_me4_base.f90:120-127, 2D load_smem_visc4.f90:41-42) for
-// Central-4, ME4 and the 2D 4th-order stencil.  d/dx_a is evaluated where the
-// a-coordinate is interior and at most one other coordinate lies in a ghost
-// layer -- every cell a sweep tile reads.
-template <int DIM, int DORD, bool SENSOR, class T>
-__global__ void k_grad(Geo G, Fields<T> W, Metrics M) {
+template <int DIM, class T>
+__global__ void k_sensor(Geo G, Fields<T> W, Metrics M) {
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
-  const int g = G.g;
-  const int ext[3] = {G.nx, G.ny, G.nz};
-  const int64_t st[3] = {1, G.sx, G.plane};
-  const double* invd[3] = {M.inv_dx, M.inv_dy, M.inv_dz};
-  const T* vel[3] = {W.u, W.v, W.w};
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    int c3[3];
-    c3[0] = (int)(t % G.nx);
-    int64_t r = t / G.nx;
-    c3[1] = (int)(r % G.ny);
-    c3[2] = (int)(r / G.ny);
-    const int64_t o = G.at(c3[0], c3[1], c3[2]);
-    if constexpr (DORD > 0) {
-      int outside = 0;
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) outside += (c3[a] < g || c3[a] >= ext[a] - g);
-      if (outside <= 1) {
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) {
-          if (c3[a] < g || c3[a] >= ext[a] - g) continue;
-          const T inv = (T)invd[a][c3[a]];
-          const int64_t s = st[a];
-#pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            const T* q = vel[c];
-            T d;
-            if constexpr (DORD == 6)
-              d = (T(1.0 / 60.0) * (-q[o - 3 * s] + q[o + 3 * s]) + T(0.15) * (q[o - 2 * s] - q[o + 2 * s]) +
-                   T(0.75) * (-q[o - s] + q[o + s])) * inv;
-            else
-              d = (T(2.0 / 3.0) * (-q[o - s] + q[o + s]) - T(1.0 / 12.0) * (-q[o - 2 * s] + q[o + 2 * s])) * inv;
-            W.grad[3 * c + a][o] = d;
-          }
-        }
-      }
-    }
-    if constexpr (SENSOR) {
-      // calc_Ducros (3D_solver/src/calc_hybrid.f90:11-72; 2D twin :11-55) on cells 1..n-2
-      const int i = c3[0], j = c3[1], k = c3[2];
-      if (i < 1 || i > G.nx - 2 || j < 1 || j > G.ny - 2) continue;
-      if (DIM == 3 && (k < 1 || k > G.nz - 2)) continue;
-      const T eps = T(1.0e-12);
-      T dxt = T(0.25) * ((T)M.inv_dx[i - 1] + (T)M.inv_dx[i]);
-      T dyt = T(0.25) * ((T)M.inv_dy[j - 1] + (T)M.inv_dy[j]);
-      T f;
-      if constexpr (DIM == 3) {
-        T dzt = T(0.25) * ((T)M.inv_dz[k - 1] + (T)M.inv_dz[k]);
-        const int64_t ox = 1, oy = G.sx, oz = G.plane;
-        T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
-        T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
-        T dwdx = (-W.w[o - ox] + W.w[o + ox]) * dxt;
-        T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
-        T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
-        T dwdy = (-W.w[o - oy] + W.w[o + oy]) * dyt;
-        T dudz = (-W.u[o - oz] + W.u[o + oz]) * dzt;
-        T dvdz = (-W.v[o - oz] + W.v[o + oz]) * dzt;
-        T dwdz = (-W.w[o - oz] + W.w[o + oz]) * dzt;
-        T div = dudx + dvdy + dwdz;
-        T r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
-        f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
-      } else {
-        const int64_t ox = 1, oy = G.sx;
-        T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
-        T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
-        T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
-        T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
-        T div = dudx + dvdy;
-        T rot = dvdx - dudy;
-        f = (div * div) / (div * div + rot * rot + eps);
-      }
-      f = fmin_f(T(1), f);
-      W.sensor[o] = f;
-      if (i == 1) W.sensor[G.at(0, j, k)] = f; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = f;
-      if (j == 1) W.sensor[G.at(i, 0, k)] = f; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = f;
-      if constexpr (DIM == 3) {
-        if (k == 1) W.sensor[G.at(i, j, 0)] = f; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = f;
-      }
-    }
-  }
+       t += (int64_t)gridDim.x * blockDim.x)
+    sensor_cell<DIM, T>(G, W, M, t);
 }
 
 // ---- SMS sub-grid model: 3D_solver/src/calc_les.f90:30-125 -------------------
@@ -246,12 +223,10 @@ __device__ __forceinline__ T filt(const T* a, int64_t o, int64_t sx, int64_t pl)
                         T(2) * c + a[o + pl]);
 }
 
+// One cell (i, j, k) of calc_mut, 1 <= i,j,k <= n-2.
 template <class T>
-__global__ void k_mut(Geo G, Fields<T> W, Metrics M, PhysConst K) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-  if (i > G.nx - 2 || j > G.ny - 2 || k > G.nz - 2) return;
+__device__ __forceinline__ void mut_cell(const Geo& G, const Fields<T>& W, const Metrics& M, const PhysConst& K,
+                                         int i, int j, int k) {
   const int64_t sx = G.sx, pl = G.plane;
   int64_t o = G.at(i, j, k);
   T u3[3][3][3], v3[3][3][3], w3[3][3][3], ut[3][3][3], vt[3][3][3], wt[3][3][3];
@@ -302,63 +277,88 @@ __global__ void k_mut(Geo G, Fields<T> W, Metrics M, PhysConst K) {
   W.mut[o] = W.rho[o] * nut;
 }
 
+template <class T>
+__global__ void k_mut(Geo G, Fields<T> W, Metrics M, PhysConst K) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (i > G.nx - 2 || j > G.ny - 2 || k > G.nz - 2) return;
+  mut_cell<T>(G, W, M, K, i, j, k);
+}
+
 // set_bc_mut_common (3D_solver/src/set_bc_common.f90:296-335): one ghost layer,
 // images taken at distance n-2 (the reference's composite copy order).
+template <class T>
+__device__ __forceinline__ void mut_edge_cell(const Geo& G, const Fields<T>& W, int64_t t) {
+  int i = (int)(t % G.nx);
+  int64_t r = t / G.nx;
+  int j = (int)(r % G.ny);
+  int k = (int)(r / G.ny);
+  bool edge = (i == 0 || i == G.nx - 1 || j == 0 || j == G.ny - 1 || k == 0 || k == G.nz - 1);
+  if (!edge) return;
+  int si = i == 0 ? G.nx - 2 : (i == G.nx - 1 ? 1 : i);
+  int sj = j == 0 ? G.ny - 2 : (j == G.ny - 1 ? 1 : j);
+  int sk = k == 0 ? G.nz - 2 : (k == G.nz - 1 ? 1 : k);
+  int64_t o = G.at(i, j, k), s = G.at(si, sj, sk);
+  W.mut[o] = W.mut[s];
+  W.qc2[o] = W.qc2[s];
+}
+
 template <class T>
 __global__ void k_mut_edges(Geo G, Fields<T> W) {
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    int i = (int)(t % G.nx);
-    int64_t r = t / G.nx;
-    int j = (int)(r % G.ny);
-    int k = (int)(r / G.ny);
-    bool edge = (i == 0 || i == G.nx - 1 || j == 0 || j == G.ny - 1 || k == 0 || k == G.nz - 1);
-    if (!edge) continue;
-    int si = i == 0 ? G.nx - 2 : (i == G.nx - 1 ? 1 : i);
-    int sj = j == 0 ? G.ny - 2 : (j == G.ny - 1 ? 1 : j);
-    int sk = k == 0 ? G.nz - 2 : (k == G.nz - 1 ? 1 : k);
-    int64_t o = G.at(i, j, k), s = G.at(si, sj, sk);
-    W.mut[o] = W.mut[s];
-    W.qc2[o] = W.qc2[s];
-  }
+       t += (int64_t)gridDim.x * blockDim.x)
+    mut_edge_cell<T>(G, W, t);
 }
 
 // ---- periodic ghost fill: set_bc_cyclic{2,4,6} (set_bc_common.f90:101-273) ---
 // Every ghost cell takes its interior image; the three groups enumerate
 // z-ghost planes, y-ghost rows of interior planes and x-ghost cells of
 // interior rows without touching interior cells.
+// Number of ghost cells the fill enumerates (x-ghosts of interior rows, y-ghost
+// rows of interior planes, whole z-ghost planes).
+__host__ __device__ inline int64_t ghost_cells(const Geo& G) {
+  const int g = G.g;
+  const int Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
+  const int gz = (G.dim == 3) ? 2 * g : 0;
+  return (int64_t)gz * G.ny * G.nx + (int64_t)Nz * (2 * g) * G.nx + (int64_t)Nz * Ny * (2 * g);
+}
+
 template <class T>
-__global__ void k_ghost(T* Q, Geo G, int nv) {
+__device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t) {
   const int g = G.g;
   const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
   const int gz = (G.dim == 3) ? 2 * g : 0;
   int64_t nA = (int64_t)gz * G.ny * G.nx;            // z ghost planes
   int64_t nB = (int64_t)Nz * (2 * g) * G.nx;         // y ghost rows
-  int64_t nC = (int64_t)Nz * Ny * (2 * g);           // x ghost cells
-  int64_t tot = nA + nB + nC;
   int zo = (G.dim == 3) ? g : 0;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    int i, j, k;
-    if (t < nA) {
-      i = (int)(t % G.nx); int64_t r = t / G.nx; j = (int)(r % G.ny); int kk = (int)(r / G.ny);
-      k = kk < g ? kk : G.nz - 2 * g + kk;
-    } else if (t < nA + nB) {
-      int64_t s = t - nA;
-      i = (int)(s % G.nx); int64_t r = s / G.nx; int jj = (int)(r % (2 * g)); k = (int)(r / (2 * g)) + zo;
-      j = jj < g ? jj : G.ny - 2 * g + jj;
-    } else {
-      int64_t s = t - nA - nB;
-      int ii = (int)(s % (2 * g)); int64_t r = s / (2 * g); j = (int)(r % Ny) + g; k = (int)(r / Ny) + zo;
-      i = ii < g ? ii : G.nx - 2 * g + ii;
-    }
-    int si = (i - g + Nx) % Nx + g;
-    int sj = (j - g + Ny) % Ny + g;
-    int sk = (G.dim == 3) ? (k - g + Nz) % Nz + g : 0;
-    int64_t o = G.at(i, j, k), s = G.at(si, sj, sk);
-    for (int l = 0; l < nv; ++l) Q[o + l * G.vs] = Q[s + l * G.vs];
+  int i, j, k;
+  if (t < nA) {
+    i = (int)(t % G.nx); int64_t r = t / G.nx; j = (int)(r % G.ny); int kk = (int)(r / G.ny);
+    k = kk < g ? kk : G.nz - 2 * g + kk;
+  } else if (t < nA + nB) {
+    int64_t s = t - nA;
+    i = (int)(s % G.nx); int64_t r = s / G.nx; int jj = (int)(r % (2 * g)); k = (int)(r / (2 * g)) + zo;
+    j = jj < g ? jj : G.ny - 2 * g + jj;
+  } else {
+    int64_t s = t - nA - nB;
+    int ii = (int)(s % (2 * g)); int64_t r = s / (2 * g); j = (int)(r % Ny) + g; k = (int)(r / Ny) + zo;
+    i = ii < g ? ii : G.nx - 2 * g + ii;
   }
+  int si = (i - g + Nx) % Nx + g;
+  int sj = (j - g + Ny) % Ny + g;
+  int sk = (G.dim == 3) ? (k - g + Nz) % Nz + g : 0;
+  int64_t o = G.at(i, j, k), s = G.at(si, sj, sk);
+  for (int l = 0; l < nv; ++l) Q[o + l * G.vs] = Q[s + l * G.vs];
+}
+
+template <class T>
+__global__ void k_ghost(T* Q, Geo G, int nv) {
+  const int64_t tot = ghost_cells(G);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x)
+    ghost_cell<T>(Q, G, nv, t);
 }
 
 }  // namespace oux

@@ -24,30 +24,33 @@ constexpr int SWEEP_BF = OUX_SWEEP_BF;  // y/z sweep cells per block along the s
 
 enum TileField { TF_RHO = 0, TF_U, TF_V, TF_W, TF_P, TF_T, TF_MU, TF_MUT, TF_QC2, TF_SEN, TF_D0, TF_D1, TF_D2, TF_D3, TF_COUNT };
 
-template <int DIR> struct SweepShape {
+// ROWS: pencil rows per x-sweep tile, or cells along the sweep per y/z tile.
+template <int DIR> __host__ __device__ constexpr int default_rows() { return DIR == 0 ? SWEEP_BR : SWEEP_BF; }
+template <int DIR, int ROWS = default_rows<DIR>()> struct SweepShape {
   static constexpr int TX = (DIR == 0) ? 33 : 32;
-  static constexpr int TY = (DIR == 0) ? SWEEP_BR : SWEEP_BF + 1;
+  static constexpr int TY = (DIR == 0) ? ROWS : ROWS + 1;
 };
 
 // The tile halo is 3 cells for every order: the widest stencils (6-point
 // convective, Central-6 / ME4 / 2D 4th-order viscous) reach 2 cells left and
 // 3 cells right of a face's left cell.
 constexpr int TILE_HALO = 3;
-template <int ORDER, int DIR> __host__ __device__ constexpr int tile_len() {
-  return DIR == 0 ? 32 + 2 * TILE_HALO : SWEEP_BF + 2 * TILE_HALO;
+template <int ORDER, int DIR, int ROWS = default_rows<DIR>()> __host__ __device__ constexpr int tile_len() {
+  return DIR == 0 ? 32 + 2 * TILE_HALO : ROWS + 2 * TILE_HALO;
 }
-template <int ORDER, int DIR> __host__ __device__ constexpr int tile_cells() {
-  return DIR == 0 ? tile_len<ORDER, DIR>() * SWEEP_BR : tile_len<ORDER, DIR>() * 32;
+template <int ORDER, int DIR, int ROWS = default_rows<DIR>()> __host__ __device__ constexpr int tile_cells() {
+  return DIR == 0 ? tile_len<ORDER, DIR, ROWS>() * ROWS : tile_len<ORDER, DIR, ROWS>() * 32;
 }
-template <int ORDER, int DIR, class T> __host__ __device__ constexpr size_t sweep_smem() {
+template <int ORDER, int DIR, class T, int ROWS = default_rows<DIR>()>
+__host__ __device__ constexpr size_t sweep_smem() {
   // TF_COUNT tile fields + 5 face-flux components per face thread (FP64)
-  return sizeof(T) * TF_COUNT * tile_cells<ORDER, DIR>() +
-         sizeof(double) * 5 * SweepShape<DIR>::TX * SweepShape<DIR>::TY;
+  return sizeof(T) * TF_COUNT * tile_cells<ORDER, DIR, ROWS>() +
+         sizeof(double) * 5 * SweepShape<DIR, ROWS>::TX * SweepShape<DIR, ROWS>::TY;
 }
 
 // transverse node derivative of `a` along axis `ax` at offset o (4th/6th order)
 template <bool SIXTH, class T>
-__device__ __forceinline__ T node_d(const T* __restrict__ a, int64_t o, int64_t st, T inv) {
+__device__ __forceinline__ T node_d(const T* a, int64_t o, int64_t st, T inv) {
   if constexpr (SIXTH)
     return (T(1.0 / 60.0) * (-a[o - 3 * st] + a[o + 3 * st]) + T(0.15) * (a[o - 2 * st] - a[o + 2 * st]) +
             T(0.75) * (-a[o - st] + a[o + st])) * inv;
@@ -452,15 +455,16 @@ namespace oux {
 #ifndef OUX_SWEEP_MINB_YZ
 #define OUX_SWEEP_MINB_YZ 2
 #endif
-template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
-__global__ void __launch_bounds__(SweepShape<DIR>::TX * SweepShape<DIR>::TY,
-                                  DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
-k_sweep(StepArgs<T> A, int last) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+// One sweep tile: block-tile indices (b0, b1, b2) as the grid of launch_one
+// enumerates them; `tid` / `nthr_all` are the calling block's linear thread index
+// and size (>= TX*TY: threads beyond the tile shape only help load the tile).
+template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>()>
+__device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
+                                           unsigned char* smraw, int tid, int nthr_all) {
   constexpr int H = ORDER / 2;
-  constexpr int TL = tile_len<ORDER, DIR>();
-  constexpr int NC = tile_cells<ORDER, DIR>();
-  constexpr int TX = SweepShape<DIR>::TX, TY = SweepShape<DIR>::TY;
+  constexpr int TL = tile_len<ORDER, DIR, ROWS>();
+  constexpr int NC = tile_cells<ORDER, DIR, ROWS>();
+  constexpr int TX = SweepShape<DIR, ROWS>::TX, TY = SweepShape<DIR, ROWS>::TY;
   constexpr bool HIGH = (VK == VK_C6 || VK == VK_C4 || VK == VK_ME4 || VK == VK_2D4);
   constexpr bool SIXTH = (VK == VK_C6);
   T* tile = reinterpret_cast<T*>(smraw);
@@ -469,17 +473,17 @@ k_sweep(StepArgs<T> A, int last) {
   const int g = G.g;
   const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g;
   const int Nz = (DIM == 3) ? G.nz - 2 * g : 1;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = ty * TX + tx;
-  const int nthr = TX * TY;
+  const bool act = tid < TX * TY;  // thread owns a face / cell slot of the tile shape
+  const int tx = tid % TX, ty = tid / TX;
+  const int nthr = nthr_all;
   // block origin (first owned cell) in padded coordinates
   int bx0, by0, bz0;
   if constexpr (DIR == 0) {
-    bx0 = g + 32 * blockIdx.x; by0 = g + SWEEP_BR * blockIdx.y; bz0 = (DIM == 3) ? g + blockIdx.z : 0;
+    bx0 = g + 32 * b0; by0 = g + ROWS * b1; bz0 = (DIM == 3) ? g + b2 : 0;
   } else if constexpr (DIR == 1) {
-    bx0 = g + 32 * blockIdx.x; by0 = g + SWEEP_BF * blockIdx.y; bz0 = (DIM == 3) ? g + blockIdx.z : 0;
+    bx0 = g + 32 * b0; by0 = g + ROWS * b1; bz0 = (DIM == 3) ? g + b2 : 0;
   } else {
-    bx0 = g + 32 * blockIdx.x; bz0 = g + SWEEP_BF * blockIdx.y; by0 = g + blockIdx.z;
+    bx0 = g + 32 * b0; bz0 = g + ROWS * b1; by0 = g + b2;
   }
   const int64_t stv[3] = {1, G.sx, G.plane};
   const int nsweep = DIR == 0 ? G.nx : (DIR == 1 ? G.ny : G.nz);
@@ -549,7 +553,7 @@ k_sweep(StepArgs<T> A, int last) {
       rowok = fc[0] < ext[0];
     }
     const int f = fc[DIR];
-    const bool valid = rowok && f >= g - 1 && f <= ext[DIR] - 1;
+    const bool valid = act && rowok && f >= g - 1 && f <= ext[DIR] - 1;
     if (valid) {
       T F[5];
       // tile position of cell f + off is base + (2 + off) * step
@@ -597,6 +601,7 @@ k_sweep(StepArgs<T> A, int last) {
   __syncthreads();
 
   // ---- cells: difference, accumulate, combine ----
+  if (!act) return;
   {
     int cc[3];
     bool ok;
@@ -700,6 +705,16 @@ k_sweep(StepArgs<T> A, int last) {
       default: break;
     }
   }
+}
+
+template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
+__global__ void __launch_bounds__(SweepShape<DIR>::TX * SweepShape<DIR>::TY,
+                                  DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
+k_sweep(StepArgs<T> A, int last) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int TX = SweepShape<DIR>::TX, TY = SweepShape<DIR>::TY;
+  sweep_tile<DIM, DIR, ORDER, VK, LES, T>(A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw,
+                                          threadIdx.y * TX + threadIdx.x, TX * TY);
 }
 
 }  // namespace oux
