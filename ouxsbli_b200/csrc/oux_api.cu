@@ -12,15 +12,21 @@
 #include "oux.h"
 #include "oux_sweep.cuh"
 #include "oux_dispatch.h"
+#include "oux_internal.h"
 
 using namespace oux;
 
 namespace {
 thread_local std::string g_last_error;
-int fail(int code, const std::string& msg) {
+}  // namespace
+
+int oux_internal_fail(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
 }
+
+namespace {
+int fail(int code, const std::string& msg) { return oux_internal_fail(code, msg); }
 #define OUX_CUDA(call)                                                                    \
   do {                                                                                    \
     cudaError_t e_ = (call);                                                              \
@@ -30,34 +36,6 @@ int fail(int code, const std::string& msg) {
 
 int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 }  // namespace
-
-struct oux_handle {
-  oux_config cfg;
-  Geo G;
-  int nv;
-  int vk;
-  bool les;
-  PhysConst K;
-  std::vector<double> inv_dx, inv_dy, inv_dz, jac, dtdxdy, dtdydz, dtdzdx, dtdx, dtdy;
-  // bound buffers
-  double* Q = nullptr;
-  unsigned char* scratch = nullptr;
-  size_t scratch_bytes = 0;
-  bool mixed = false;           // FP32 stage states/fields, FP64 Q^n and accumulations
-  Fields<double> W{};           // FP64 form
-  Fields<float> Wf{};           // mixed form
-  double *Racc = nullptr, *Rs = nullptr, *partials = nullptr;
-  void* Qs = nullptr;           // stage state (double or float)
-  int* status = nullptr;
-  Metrics M{};
-  int64_t launches = 0;
-  int diag_blocks = 0;
-  // optional per-kernel timing (oux_profile): CUDA events recorded around each
-  // launch on the launching stream
-  bool profiling = false;
-  struct Rec { int kind; cudaEvent_t a, b; };
-  std::vector<Rec> recs;
-};
 
 namespace {
 
@@ -425,27 +403,6 @@ struct Timed {
     if (b) cudaEventRecord(b, s);
   }
 };
-
-template <class T> Fields<T>& fields_of(oux_handle* h);
-template <> Fields<double>& fields_of<double>(oux_handle* h) { return h->W; }
-template <> Fields<float>& fields_of<float>(oux_handle* h) { return h->Wf; }
-
-template <class T>
-StepArgs<T> base_args(oux_handle* h) {
-  StepArgs<T> A{};
-  A.G = h->G;
-  A.W = fields_of<T>(h);
-  A.M = h->M;
-  A.K = h->K;
-  A.scheme = h->cfg.scheme;
-  A.tvd = h->cfg.tvd;
-  A.slau = h->cfg.slau;
-  A.Racc = h->Racc;
-  A.Rs = h->Rs;
-  A.Qn = h->Q;
-  A.Qs = reinterpret_cast<T*>(h->Qs);
-  return A;
-}
 
 template <class T>
 int launch_sweeps_t(int dim, int order, int vk, bool les, int dir, const StepArgs<T>& A, cudaStream_t s);
