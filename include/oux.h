@@ -168,6 +168,44 @@ int oux_host_ref_diagnostics(int32_t nx, int32_t ny, int32_t nz, int32_t order, 
 /* Number of kernel launches the last oux_step call issued (for reporting). */
 int oux_launch_count(const oux_handle* h, int64_t* launches);
 
+/* --- batched solves ---------------------------------------------------------
+ * No reference counterpart: the reference runs one solve per executable.  A
+ * batch advances many bound handles (independent periodic solves of any grid
+ * sizes) with ONE persistent kernel launch per time step over a phase-major
+ * tile work list; each solve computes what oux_step computes for it (bit for
+ * bit in FP64).
+ *
+ * Members must share dim, order, visc, visc_order / visc_stencil, precision and
+ * rk; scheme, tvd, slau, gamma, R, Pr, Prt, threshold, dt and the grid may
+ * differ.  The batch snapshots each member's bound buffers and constants at
+ * oux_batch_bind (for the mixed form: the pressure / temperature references of
+ * the member's last oux_set_state), so set the states before binding. */
+typedef struct oux_batch oux_batch;
+
+typedef struct oux_batch_tuning {
+  int32_t pencil;        /* sweep tiles per work item, >= 1 (consecutive along the sweep) */
+  int32_t chunk;         /* cells per point-wise work item, >= 1 */
+  int32_t blocks_per_sm; /* persistent blocks per SM; 0 = as many as fit */
+  int32_t use_graph;     /* 1: each step replays one captured CUDA graph */
+} oux_batch_tuning;
+
+/* tuning may be NULL (pencil 4, chunk 1152, all resident blocks, graphs on). */
+int oux_batch_create(oux_handle* const* members, int32_t n, const oux_batch_tuning* tuning,
+                     oux_batch** out);
+/* Device workspace (step arguments, work list, counters) the batch needs. */
+int oux_batch_workspace_bytes(const oux_batch* b, size_t* bytes);
+/* Attach a caller-owned, 256-byte aligned workspace and upload the work list on
+ * `stream` (synchronises it). */
+int oux_batch_bind(oux_batch* b, void* workspace_dev, size_t bytes, void* stream);
+/* nsteps time steps of every member: per step a counter reset and one kernel
+ * launch (or one CUDA-graph replay); asynchronous on `stream`, no allocation. */
+int oux_batch_step(oux_batch* b, int32_t nsteps, void* stream);
+/* Batch status word: OUX_FAULT_TIMEOUT if a dependency wait gave up. */
+int oux_batch_status(oux_batch* b, int32_t* fault_bits);
+/* Work-list size, phases per step and the persistent grid. */
+int oux_batch_info(const oux_batch* b, int64_t* items, int32_t* phases, int32_t* grid);
+int oux_batch_destroy(oux_batch* b);
+
 /* --- allocation-free residual ---------------------------------------------
  * No counterpart in the reference.  The same stage residual as oux_rhs, for
  * callers that cannot allocate device memory when they call: a host program

@@ -38,6 +38,8 @@ SYMBOLS = [
     "oux_pack_state", "oux_unpack_state", "oux_fill_ghosts", "oux_rhs", "oux_step",
     "oux_diagnostics", "oux_check_state", "oux_status", "oux_profile", "oux_profile_read",
     "oux_host_ref_diagnostics", "oux_launch_count", "oux_rhs_noalloc",
+    "oux_batch_create", "oux_batch_workspace_bytes", "oux_batch_bind", "oux_batch_step",
+    "oux_batch_status", "oux_batch_info", "oux_batch_destroy",
 ]
 NOALLOC_SCRATCH_BYTES = 32 << 20  # OUX_NOALLOC_SCRATCH_BYTES
 
@@ -57,6 +59,11 @@ class OuxConfig(C.Structure):
 class OuxLayout(C.Structure):
     _fields_ = [("nv", C.c_int32), ("row_stride", C.c_int64), ("plane_stride", C.c_int64),
                 ("var_stride", C.c_int64), ("elem_bytes", C.c_int64)]
+
+
+class OuxBatchTuning(C.Structure):
+    _fields_ = [("pencil", C.c_int32), ("chunk", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("use_graph", C.c_int32)]
 
 
 class OuxError(RuntimeError):
@@ -100,6 +107,13 @@ def _load() -> C.CDLL:
                                                C.POINTER(C.c_float), C.POINTER(C.c_float), dp]),
         "oux_launch_count": (C.c_int, [vp, C.POINTER(i64)]),
         "oux_rhs_noalloc": (C.c_int, [cfgp, vp, vp, vp]),
+        "oux_batch_create": (C.c_int, [C.POINTER(vp), i32, C.POINTER(OuxBatchTuning), C.POINTER(vp)]),
+        "oux_batch_workspace_bytes": (C.c_int, [vp, C.POINTER(C.c_size_t)]),
+        "oux_batch_bind": (C.c_int, [vp, vp, C.c_size_t, vp]),
+        "oux_batch_step": (C.c_int, [vp, i32, vp]),
+        "oux_batch_status": (C.c_int, [vp, C.POINTER(i32)]),
+        "oux_batch_info": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]),
+        "oux_batch_destroy": (C.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -37,6 +37,13 @@ UNITS = [
     ("oux_sweep_mx_o2.cu", []),
     ("oux_sweep_mx_o4.cu", []),
     ("oux_sweep_mx_o6.cu", []),
+    ("oux_batch_api.cu", ["-fmad=false"]),
+    ("oux_batch_fp64_o2.cu", ["-fmad=false"]),
+    ("oux_batch_fp64_o4.cu", ["-fmad=false"]),
+    ("oux_batch_fp64_o6.cu", ["-fmad=false"]),
+    ("oux_batch_mx_o2.cu", []),
+    ("oux_batch_mx_o4.cu", []),
+    ("oux_batch_mx_o6.cu", []),
 ]
 
 
