@@ -234,3 +234,47 @@ def build_initial(case: CaseDef, params: dict):
         zc, dz = np.zeros(1), None
         Q = case.init(p, xc, yc, None)
     return p, xc, yc, zc, dx, dy, dz, Q
+
+
+# ---- batched 2D ensemble: independent isentropic-vortex convection solves -------
+VORTEX_SIZES = (64, 96, 128, 192, 256, 384, 512)
+
+
+@dataclass
+class VortexMember:
+    n: int          # interior cells per side
+    beta: float     # vortex strength
+    mach: float     # free-stream Mach number (= u_inf; c_inf = 1)
+    L: float        # periodic box side
+    dt: float
+
+
+def vortex_member(m: VortexMember, order: int = 4, **cfg_kw):
+    """SolverConfig and initial QJ of one 2D vortex (gamma 1.4, R 1, c_inf = 1)."""
+    from .grid import jacobian, to_qj
+    from .solver import SolverConfig
+    nx = m.n + order
+    Q = isentropic_vortex(nx, nx, order, m.L, m.beta, m.mach)
+    _, dx = cyclic_axis(nx, m.L, order)
+    cfg = SolverConfig(dim=2, nx=nx, ny=nx, nz=1, order=order, dt=m.dt, gamma=1.4, R=1.0, Pr=0.71,
+                       dx=dx, dy=dx.copy(), dz=None, **cfg_kw)
+    return cfg, to_qj(Q, jacobian(dx, dx.copy(), None))
+
+
+def vortex_exact(m: VortexMember, order: int, t: float) -> np.ndarray:
+    """The exact solution at time t: the initial vortex translated by u_inf t (periodic)."""
+    nx = m.n + order
+    return isentropic_vortex(nx, nx, order, m.L, m.beta, m.mach, t=t)
+
+
+def vortex_ensemble(count: int = 64, seed: int = 0, sizes=VORTEX_SIZES, L: float = 10.0, cfl: float = 0.4):
+    """Seeded ensemble: side lengths uniform over `sizes`, beta ~ U[1, 5], Mach ~ U[0.1, 0.8];
+    dt = cfl * h / (u_inf + 1) per member."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.choice(sizes))
+        beta = float(rng.uniform(1.0, 5.0))
+        mach = float(rng.uniform(0.1, 0.8))
+        out.append(VortexMember(n, beta, mach, L, cfl * (L / n) / (mach + 1.0)))
+    return out
