@@ -44,10 +44,19 @@ enum PhaseKind {
 constexpr int BATCH_MAX_PHASES = 40;
 constexpr int BATCH_THREADS = 288;   // 32 x 9: the y/z sweep tile shape
 constexpr int BATCH_ROWS_X = 8;      // x-sweep tile 33 x 8 (264 of the 288 threads)
+constexpr int BATCH_ROWS_YZ = 8;     // y/z-sweep tile 32 x (8 + 1)
+static_assert(32 * (BATCH_ROWS_YZ + 1) == BATCH_THREADS, "y/z tile shape must fill the batch block");
+static_assert(33 * BATCH_ROWS_X <= BATCH_THREADS, "x tile shape must fit the batch block");
 #ifndef OUX_BATCH_SPIN_LIMIT
 #define OUX_BATCH_SPIN_LIMIT (1 << 22)  // polls of >= 64 ns each: a few seconds at most
 #endif
 constexpr int BATCH_FAULT_TIMEOUT = 4;  // OUX_FAULT_TIMEOUT of the C ABI
+#ifndef OUX_BATCH_MINB
+#define OUX_BATCH_MINB 2  // resident blocks per SM the 3D register budget is sized for
+#endif
+// 2D steps fit 3 resident blocks per SM without spills (measured: the 64-vortex
+// FP64 ensemble runs 1.39x faster than at 2); 3D sweeps need the larger budget.
+constexpr int batch_minb(int dim) { return dim == 2 ? 3 : OUX_BATCH_MINB; }
 
 struct PhaseDesc {
   int kind;
@@ -85,7 +94,7 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
 template <int ORDER, class T>
 __host__ __device__ constexpr size_t batch_smem() {
   constexpr size_t a = sweep_smem<ORDER, 0, T, BATCH_ROWS_X>();
-  constexpr size_t b = sweep_smem<ORDER, 1, T, SWEEP_BF>();
+  constexpr size_t b = sweep_smem<ORDER, 1, T, BATCH_ROWS_YZ>();
   return a > b ? a : b;
 }
 
@@ -95,21 +104,22 @@ __host__ __device__ inline void sweep_grid(const Geo& G, int n[3]) {
   const int g = G.g;
   const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g, Nz = G.dim == 3 ? G.nz - 2 * g : 1;
   if (DIR == 0) { n[0] = (Nx + 31) / 32; n[1] = (Ny + BATCH_ROWS_X - 1) / BATCH_ROWS_X; n[2] = Nz; }
-  else if (DIR == 1) { n[0] = (Nx + 31) / 32; n[1] = (Ny + SWEEP_BF - 1) / SWEEP_BF; n[2] = Nz; }
-  else { n[0] = (Nx + 31) / 32; n[1] = (Nz + SWEEP_BF - 1) / SWEEP_BF; n[2] = Ny; }
+  else if (DIR == 1) { n[0] = (Nx + 31) / 32; n[1] = (Ny + BATCH_ROWS_YZ - 1) / BATCH_ROWS_YZ; n[2] = Nz; }
+  else { n[0] = (Nx + 31) / 32; n[1] = (Nz + BATCH_ROWS_YZ - 1) / BATCH_ROWS_YZ; n[2] = Ny; }
 }
 
-template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
+template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool KONLY>
 __device__ __forceinline__ void batch_sweep(const StepArgs<T>& A, int last, int first, int count,
                                             unsigned char* smraw) {
-  constexpr int ROWS = DIR == 0 ? BATCH_ROWS_X : SWEEP_BF;
+  constexpr int ROWS = DIR == 0 ? BATCH_ROWS_X : BATCH_ROWS_YZ;
   int n[3];
   sweep_grid<DIR>(A.G, n);
   for (int t = first; t < first + count; ++t) {
     int b0, b1, b2;
     if (DIR == 0) { b0 = t % n[0]; b1 = (t / n[0]) % n[1]; b2 = t / (n[0] * n[1]); }
     else { b1 = t % n[1]; b0 = (t / n[1]) % n[0]; b2 = t / (n[0] * n[1]); }  // pencil along the sweep
-    sweep_tile<DIM, DIR, ORDER, VK, LES, T, ROWS>(A, last, b0, b1, b2, smraw, threadIdx.x, BATCH_THREADS);
+    sweep_tile<DIM, DIR, ORDER, VK, LES, T, ROWS, false, KONLY>(A, last, b0, b1, b2, smraw, threadIdx.x,
+                                                              BATCH_THREADS);
     __syncthreads();
   }
 }
@@ -120,8 +130,9 @@ __device__ __forceinline__ int64_t batch_end(int64_t c0, int count, int chunk, i
   return e < n ? e : n;
 }
 
-template <int DIM, int ORDER, int VK, bool LES, class T>
-__global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch_step(BatchArgs<T> B) {
+// KONLY: every member uses KEEP (no sensor phase, KEEP flux only).
+template <int DIM, int ORDER, int VK, bool LES, class T, bool KONLY>
+__global__ void __launch_bounds__(BATCH_THREADS, batch_minb(DIM)) k_batch_step(BatchArgs<T> B) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ int s_item, s_abort;
   const int tid = threadIdx.x;
@@ -177,8 +188,10 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch_step(BatchArgs<T> B)
         break;
       }
       case PH_SENSOR: {
-        const int64_t c1 = batch_end(c0, bi.count, B.chunk, ncell);
-        for (int64_t t = c0 + tid; t < c1; t += BATCH_THREADS) sensor_cell<DIM, T>(G, A.W, A.M, t);
+        if constexpr (!KONLY) {
+          const int64_t c1 = batch_end(c0, bi.count, B.chunk, ncell);
+          for (int64_t t = c0 + tid; t < c1; t += BATCH_THREADS) sensor_cell<DIM, T>(G, A.W, A.M, t);
+        }
         break;
       }
       case PH_MUT: {
@@ -201,13 +214,13 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch_step(BatchArgs<T> B)
         break;
       }
       case PH_SWEEP_X:
-        batch_sweep<DIM, 0, ORDER, VK, LES, T>(A, ph.last, bi.first, bi.count, smraw);
+        batch_sweep<DIM, 0, ORDER, VK, LES, T, KONLY>(A, ph.last, bi.first, bi.count, smraw);
         break;
       case PH_SWEEP_Y:
-        batch_sweep<DIM, 1, ORDER, VK, LES, T>(A, ph.last, bi.first, bi.count, smraw);
+        batch_sweep<DIM, 1, ORDER, VK, LES, T, KONLY>(A, ph.last, bi.first, bi.count, smraw);
         break;
       case PH_SWEEP_Z:
-        if constexpr (DIM == 3) batch_sweep<DIM, 2, ORDER, VK, LES, T>(A, ph.last, bi.first, bi.count, smraw);
+        if constexpr (DIM == 3) batch_sweep<DIM, 2, ORDER, VK, LES, T, KONLY>(A, ph.last, bi.first, bi.count, smraw);
         break;
       case PH_GHOST_QS:
       case PH_GHOST_QN: {

@@ -40,6 +40,7 @@ struct oux_batch {
   oux_batch_tuning tune{};
   int dim = 0, order = 0, vk = 0, rk = 0;
   bool les = false, mixed = false;
+  bool keep_only = false;  // every member uses KEEP: the KEEP-only kernel
   std::vector<PhaseDesc> phases;
   std::vector<int> phase_stage;
   std::vector<BatchItem> items;
@@ -83,6 +84,7 @@ int build_lists(oux_batch* b) {
   const int stages = b->rk == 3 ? 3 : 4;
   bool any_sensor = false;
   for (auto* h : b->members) any_sensor |= h->cfg.scheme != OUX_KEEP;
+  b->keep_only = !any_sensor;
   b->phases.clear();
   b->phase_stage.clear();
   auto add = [&](int kind, int src_qs, int last, int st) {
@@ -160,9 +162,9 @@ void fill_args(oux_batch* b, BatchArgs<T>& B) {
 
 int launch(oux_batch* b, cudaStream_t s, int dry) {
   int rc = b->mixed ? batch_launch(b->dim, b->order, b->vk, b->les, b->B32, b->tune.blocks_per_sm, b->nsm,
-                                   &b->grid, s, dry)
+                                   &b->grid, s, dry, b->keep_only)
                     : batch_launch(b->dim, b->order, b->vk, b->les, b->B64, b->tune.blocks_per_sm, b->nsm,
-                                   &b->grid, s, dry);
+                                   &b->grid, s, dry, b->keep_only);
   if (rc == 2) return fail(OUX_E_INVALID, "no batched kernel built for this configuration");
   if (rc) return fail(OUX_E_CUDA, std::string("batched step launch: ") + cudaGetErrorString(cudaGetLastError()));
   return OUX_OK;

@@ -5,9 +5,10 @@
 
 namespace oux {
 int batch_launch_fp64_o2(int dim, int vk, bool les, const BatchArgs<double>& B, int bps, int nsm, int* grid,
-                         cudaStream_t s, int dry) {
+                         cudaStream_t s, int dry, bool konly) {
 #define OUX_CASE(D, V, L) \
-  if (dim == D && vk == V && les == L) return batch_launch_t<D, 2, V, L, double>(B, bps, nsm, grid, s, dry);
+  if (dim == D && vk == V && les == L) return konly ? batch_launch_t<D, 2, V, L, double, true>(B, bps, nsm, grid, s, dry) \
+                 : batch_launch_t<D, 2, V, L, double, false>(B, bps, nsm, grid, s, dry);
   OUX_CASE(3, VK_EULER, false) OUX_CASE(3, VK_GV2, false) OUX_CASE(3, VK_GV2, true)
   OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_GV2, false)
 #undef OUX_CASE

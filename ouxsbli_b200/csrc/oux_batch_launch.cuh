@@ -8,10 +8,10 @@ namespace oux {
 // dry != 0: set the kernel's shared-memory attribute, size the grid into *grid
 // and launch nothing (done once, outside any stream capture).  dry == 0: launch
 // with the grid sized before.
-template <int DIM, int ORDER, int VK, bool LES, class T>
+template <int DIM, int ORDER, int VK, bool LES, class T, bool KONLY>
 int batch_launch_t(const BatchArgs<T>& B, int blocks_per_sm, int nsm, int* grid, cudaStream_t s, int dry) {
   constexpr size_t smem = batch_smem<ORDER, T>();
-  auto kern = k_batch_step<DIM, ORDER, VK, LES, T>;
+  auto kern = k_batch_step<DIM, ORDER, VK, LES, T, KONLY>;
   if (dry) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return 1;

@@ -63,9 +63,19 @@ template <class T> struct StepArgs {
   int mode;
 };
 
+// Load through the read-only data path when the caller guarantees the array is
+// not written during the kernel (RO = true: the single-solve kernels); plain
+// coherent load otherwise (the batched kernel, where other blocks of the same
+// launch produce the fields).
+template <bool RO, class T>
+__device__ __forceinline__ T ldro(const T* p) {
+  if constexpr (RO) return __ldg(p);
+  else return *p;
+}
+
 // ---- prim: src/calc_physical_quantities.f90:60-116 (3D), :7-57 (2D) -------
 // One padded cell t (x fastest over nx, then ny, then nz).
-template <int DIM, bool VISC, class TS, class T>
+template <int DIM, bool VISC, class TS, class T, bool RO = false>
 __device__ __forceinline__ void prim_cell(const TS* Q, const Geo& G, const Fields<T>& W, const double* jac,
                                           const PhysConst& K, int64_t t) {
   int i = (int)(t % G.nx);
@@ -73,18 +83,18 @@ __device__ __forceinline__ void prim_cell(const TS* Q, const Geo& G, const Field
   int j = (int)(r % G.ny);
   int k = (int)(r / G.ny);
   int64_t o = G.at(i, j, k);
-  T Jv = (T)jac[(int64_t)j * G.nx + i];
-  T q1 = (T)Q[o];
+  T Jv = (T)__ldg(jac + (int64_t)j * G.nx + i);
+  T q1 = (T)ldro<RO>(Q + o);
   T over_Q1 = T(1) / q1;
   T rho = Jv * q1;
-  T u = (T)Q[o + G.vs] * over_Q1;
-  T v = (T)Q[o + 2 * G.vs] * over_Q1;
+  T u = (T)ldro<RO>(Q + o + G.vs) * over_Q1;
+  T v = (T)ldro<RO>(Q + o + 2 * G.vs) * over_Q1;
   T w = T(0), p;
   if constexpr (DIM == 3) {
-    w = (T)Q[o + 3 * G.vs] * over_Q1;
-    p = T(K.gamma_1) * (Jv * (T)Q[o + 4 * G.vs] - T(0.5) * rho * (u * u + v * v + w * w));
+    w = (T)ldro<RO>(Q + o + 3 * G.vs) * over_Q1;
+    p = T(K.gamma_1) * (Jv * (T)ldro<RO>(Q + o + 4 * G.vs) - T(0.5) * rho * (u * u + v * v + w * w));
   } else {
-    p = T(K.gamma_1) * (Jv * (T)Q[o + 3 * G.vs] - T(0.5) * rho * (u * u + v * v));
+    p = T(K.gamma_1) * (Jv * (T)ldro<RO>(Q + o + 3 * G.vs) - T(0.5) * rho * (u * u + v * v));
   }
   W.rho[o] = rho; W.u[o] = u; W.v[o] = v;
   if constexpr (DIM == 3) W.w[o] = w;
@@ -100,13 +110,13 @@ __global__ void k_prim(const TS* __restrict__ Q, Geo G, Fields<T> W, const doubl
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x)
-    prim_cell<DIM, VISC, TS, T>(Q, G, W, jac, K, t);
+    prim_cell<DIM, VISC, TS, T, true>(Q, G, W, jac, K, t);
 }
 
 // ---- mixed-form primitives: Q = Q^n (FP64) + dQ (FP32 stage increment, may be
 // null), evaluated in FP64 like k_prim, stored in FP32 with p and T as deviations
 // from the per-solve references K.p_ref, K.T_ref.
-template <int DIM, bool VISC>
+template <int DIM, bool VISC, bool RO = false>
 __device__ __forceinline__ void prim_mx_cell(const double* Qn, const float* dQ, const Geo& G,
                                              const Fields<float>& W, const double* jac, const PhysConst& K,
                                              int64_t t) {
@@ -117,8 +127,9 @@ __device__ __forceinline__ void prim_mx_cell(const double* Qn, const float* dQ, 
   int64_t o = G.at(i, j, k);
   double q[5];
 #pragma unroll
-  for (int l = 0; l < DIM + 2; ++l) q[l] = Qn[o + l * G.vs] + (dQ ? (double)dQ[o + l * G.vs] : 0.0);
-  double Jv = jac[(int64_t)j * G.nx + i];
+  for (int l = 0; l < DIM + 2; ++l)
+    q[l] = ldro<RO>(Qn + o + l * G.vs) + (dQ ? (double)ldro<RO>(dQ + o + l * G.vs) : 0.0);
+  double Jv = __ldg(jac + (int64_t)j * G.nx + i);
   double over = 1.0 / q[0], rho = Jv * q[0];
   double u = q[1] * over, v = q[2] * over, w = 0.0, p;
   if constexpr (DIM == 3) {
@@ -141,12 +152,12 @@ __global__ void k_prim_mx(const double* __restrict__ Qn, const float* __restrict
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x)
-    prim_mx_cell<DIM, VISC>(Qn, dQ, G, W, jac, K, t);
+    prim_mx_cell<DIM, VISC, true>(Qn, dQ, G, W, jac, K, t);
 }
 
 // ---- Ducros sensor: calc_Ducros (3D_solver/src/calc_hybrid.f90:11-72; 2D twin
 // :11-55) on cells 1..n-2, with the reference's copies to the outer faces.
-template <int DIM, class T>
+template <int DIM, class T, bool RO = false>
 __device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, const Metrics& M, int64_t t) {
   const int i = (int)(t % G.nx);
   const int64_t r = t / G.nx;
@@ -156,30 +167,33 @@ __device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, co
   if (DIM == 3 && (k < 1 || k > G.nz - 2)) return;
   const int64_t o = G.at(i, j, k);
   const T eps = T(1.0e-12);
-  T dxt = T(0.25) * ((T)M.inv_dx[i - 1] + (T)M.inv_dx[i]);
-  T dyt = T(0.25) * ((T)M.inv_dy[j - 1] + (T)M.inv_dy[j]);
+  auto U = [&](int64_t q) { return ldro<RO>(W.u + q); };
+  auto V = [&](int64_t q) { return ldro<RO>(W.v + q); };
+  auto Wv = [&](int64_t q) { return ldro<RO>(W.w + q); };
+  T dxt = T(0.25) * ((T)__ldg(M.inv_dx + i - 1) + (T)__ldg(M.inv_dx + i));
+  T dyt = T(0.25) * ((T)__ldg(M.inv_dy + j - 1) + (T)__ldg(M.inv_dy + j));
   T f;
   if constexpr (DIM == 3) {
-    T dzt = T(0.25) * ((T)M.inv_dz[k - 1] + (T)M.inv_dz[k]);
+    T dzt = T(0.25) * ((T)__ldg(M.inv_dz + k - 1) + (T)__ldg(M.inv_dz + k));
     const int64_t ox = 1, oy = G.sx, oz = G.plane;
-    T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
-    T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
-    T dwdx = (-W.w[o - ox] + W.w[o + ox]) * dxt;
-    T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
-    T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
-    T dwdy = (-W.w[o - oy] + W.w[o + oy]) * dyt;
-    T dudz = (-W.u[o - oz] + W.u[o + oz]) * dzt;
-    T dvdz = (-W.v[o - oz] + W.v[o + oz]) * dzt;
-    T dwdz = (-W.w[o - oz] + W.w[o + oz]) * dzt;
+    T dudx = (-U(o - ox) + U(o + ox)) * dxt;
+    T dvdx = (-V(o - ox) + V(o + ox)) * dxt;
+    T dwdx = (-Wv(o - ox) + Wv(o + ox)) * dxt;
+    T dudy = (-U(o - oy) + U(o + oy)) * dyt;
+    T dvdy = (-V(o - oy) + V(o + oy)) * dyt;
+    T dwdy = (-Wv(o - oy) + Wv(o + oy)) * dyt;
+    T dudz = (-U(o - oz) + U(o + oz)) * dzt;
+    T dvdz = (-V(o - oz) + V(o + oz)) * dzt;
+    T dwdz = (-Wv(o - oz) + Wv(o + oz)) * dzt;
     T div = dudx + dvdy + dwdz;
     T r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
     f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
   } else {
     const int64_t ox = 1, oy = G.sx;
-    T dudx = (-W.u[o - ox] + W.u[o + ox]) * dxt;
-    T dvdx = (-W.v[o - ox] + W.v[o + ox]) * dxt;
-    T dudy = (-W.u[o - oy] + W.u[o + oy]) * dyt;
-    T dvdy = (-W.v[o - oy] + W.v[o + oy]) * dyt;
+    T dudx = (-U(o - ox) + U(o + ox)) * dxt;
+    T dvdx = (-V(o - ox) + V(o + ox)) * dxt;
+    T dudy = (-U(o - oy) + U(o + oy)) * dyt;
+    T dvdy = (-V(o - oy) + V(o + oy)) * dyt;
     T div = dudx + dvdy;
     T rot = dvdx - dudy;
     f = (div * div) / (div * div + rot * rot + eps);
@@ -198,7 +212,7 @@ __global__ void k_sensor(Geo G, Fields<T> W, Metrics M) {
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x)
-    sensor_cell<DIM, T>(G, W, M, t);
+    sensor_cell<DIM, T, false>(G, W, M, t);  // measured faster than the read-only path
 }
 
 // ---- SMS sub-grid model: 3D_solver/src/calc_les.f90:30-125 -------------------

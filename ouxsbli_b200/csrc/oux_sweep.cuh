@@ -49,18 +49,21 @@ __host__ __device__ constexpr size_t sweep_smem() {
 }
 
 // transverse node derivative of `a` along axis `ax` at offset o (4th/6th order)
-template <bool SIXTH, class T>
+template <bool SIXTH, bool RO, class T>
 __device__ __forceinline__ T node_d(const T* a, int64_t o, int64_t st, T inv) {
+  auto A = [&](int64_t q) { return ldro<RO>(a + q); };
   if constexpr (SIXTH)
-    return (T(1.0 / 60.0) * (-a[o - 3 * st] + a[o + 3 * st]) + T(0.15) * (a[o - 2 * st] - a[o + 2 * st]) +
-            T(0.75) * (-a[o - st] + a[o + st])) * inv;
+    return (T(1.0 / 60.0) * (-A(o - 3 * st) + A(o + 3 * st)) + T(0.15) * (A(o - 2 * st) - A(o + 2 * st)) +
+            T(0.75) * (-A(o - st) + A(o + st))) * inv;
   else
-    return (T(2.0 / 3.0) * (-a[o - st] + a[o + st]) - T(1.0 / 12.0) * (-a[o - 2 * st] + a[o + 2 * st])) * inv;
+    return (T(2.0 / 3.0) * (-A(o - st) + A(o + st)) - T(1.0 / 12.0) * (-A(o - 2 * st) + A(o + 2 * st))) * inv;
 }
 
 // ---- convective face flux: calc_{keep,slau,hybrid,roe}_{x,y,z}_in ---------------
 // s(f,m) reads tile field f at stencil point m (0 .. 2io+1).
-template <int ORDER, class T, class Acc>
+// KONLY: every solve of the launch uses KEEP (compile-time; the other schemes'
+// code and registers drop out).
+template <int ORDER, bool KONLY, class T, class Acc>
 __device__ __forceinline__ void conv_flux(const StepArgs<T>& A, const Acc& s, T fd, int nd, T F[5]) {
   constexpr int NS = ORDER;  // 2io+2 stencil points
   T rho[NS], u[NS], v[NS], w[NS], p[NS], Tt[NS];
@@ -74,7 +77,7 @@ __device__ __forceinline__ void conv_flux(const StepArgs<T>& A, const Acc& s, T 
   // mixed form: the tile's p and T are deviations from the per-solve references
   constexpr bool MX = sizeof(T) < sizeof(double);
   const T pr = MX ? T(A.K.p_ref) : T(0), tr = MX ? T(A.K.T_ref) : T(0);
-  if (scheme == 0 || (scheme == 3 && fd <= T(A.K.threshold))) {
+  if (KONLY || scheme == 0 || (scheme == 3 && fd <= T(A.K.threshold))) {
     keep_flux<ORDER, T, MX>(rho, u, v, w, un, p, Tt, nd, T(A.K.R_over_gamma_1), F, pr, tr);
     return;
   }
@@ -284,10 +287,17 @@ __device__ __forceinline__ void visc_high(const StepArgs<T>& A, const Acc& s, in
 
 // ---- Gaitonde-Visbal 2nd order: 3D_solver/src/calc_visc2.f90.fypp (2D :10-103) ----
 // Reads global arrays directly: face between o and o + st[nd].
-template <int DIM, bool LES, class T>
+template <int DIM, bool LES, bool RO, class T>
 __device__ __forceinline__ void visc_gv2(const StepArgs<T>& A, int nd, int64_t o, const int64_t st[3],
                                          const T invs[3], T out[4]) {
-  const Fields<T>& W = A.W;
+  // read-only view of the fields: W.f[q] loads through ldro<RO>
+  struct RoField {
+    const T* p;
+    __device__ T operator[](int64_t q) const { return ldro<RO>(p + q); }
+  };
+  struct {
+    RoField u, v, w, mu, T_, mut, qc2;
+  } W{{A.W.u}, {A.W.v}, {A.W.w}, {A.W.mu}, {A.W.T_}, {A.W.mut}, {A.W.qc2}};
   const int64_t o2 = o + st[nd];
   const T inv = invs[nd];
   auto vel = [&](int c, int64_t q) -> T { return c == 0 ? W.u[q] : (c == 1 ? W.v[q] : (DIM == 3 ? W.w[q] : T(0))); };
@@ -308,7 +318,7 @@ __device__ __forceinline__ void visc_gv2(const StepArgs<T>& A, int nd, int64_t o
     for (int c = 0; c < 3; ++c) sg[c] = msd * (-vel(c, o) + vel(c, o2));
   }
   auto cross = [&](bool sgs, int c, int t) -> T {
-    const T* m = sgs ? W.mut : W.mu;
+    const RoField m = sgs ? W.mut : W.mu;
     const int64_t s = st[t];
     T m1 = T(0.0625) * (m[o - s] + m[o] + m[o2 - s] + m[o2]);
     T m2 = T(0.0625) * (m[o] + m[o + s] + m[o2] + m[o2 + s]);
@@ -458,7 +468,8 @@ namespace oux {
 // One sweep tile: block-tile indices (b0, b1, b2) as the grid of launch_one
 // enumerates them; `tid` / `nthr_all` are the calling block's linear thread index
 // and size (>= TX*TY: threads beyond the tile shape only help load the tile).
-template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>()>
+template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
+          bool RO = false, bool KONLY = false>
 __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
                                            unsigned char* smraw, int tid, int nthr_all) {
   constexpr int H = ORDER / 2;
@@ -509,29 +520,32 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       if (a != DIR && (a < DIM) && ci[a] >= ext[a]) ok = false;
     if (!ok) continue;
     const int64_t o = G.at(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
-    tile[TF_RHO * NC + c] = A.W.rho[o];
-    tile[TF_U * NC + c] = A.W.u[o];
-    tile[TF_V * NC + c] = A.W.v[o];
-    tile[TF_W * NC + c] = (DIM == 3) ? A.W.w[o] : T(0);
-    tile[TF_P * NC + c] = A.W.p[o];
-    tile[TF_T * NC + c] = A.W.T_[o];
-    if (A.scheme != 0) tile[TF_SEN * NC + c] = A.W.sensor[o];
-    if constexpr (VK != VK_EULER) tile[TF_MU * NC + c] = A.W.mu[o];
-    if constexpr (LES) { tile[TF_MUT * NC + c] = A.W.mut[o]; tile[TF_QC2 * NC + c] = A.W.qc2[o]; }
+    tile[TF_RHO * NC + c] = ldro<RO>(A.W.rho + o);
+    tile[TF_U * NC + c] = ldro<RO>(A.W.u + o);
+    tile[TF_V * NC + c] = ldro<RO>(A.W.v + o);
+    tile[TF_W * NC + c] = (DIM == 3) ? ldro<RO>(A.W.w + o) : T(0);
+    tile[TF_P * NC + c] = ldro<RO>(A.W.p + o);
+    tile[TF_T * NC + c] = ldro<RO>(A.W.T_ + o);
+    if (!KONLY && A.scheme != 0) tile[TF_SEN * NC + c] = ldro<RO>(A.W.sensor + o);
+    if constexpr (VK != VK_EULER) tile[TF_MU * NC + c] = ldro<RO>(A.W.mu + o);
+    if constexpr (LES) {
+      tile[TF_MUT * NC + c] = ldro<RO>(A.W.mut + o);
+      tile[TF_QC2 * NC + c] = ldro<RO>(A.W.qc2 + o);
+    }
     if constexpr (HIGH) {  // transverse node derivatives (the viscous loaders' stencils)
       const T* vel[3] = {A.W.u, A.W.v, A.W.w};
       const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
       if constexpr (DIM == 3) {
         const int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
         const int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
-        tile[TF_D0 * NC + c] = node_d<SIXTH>(vel[a1], o, stv[a1], (T)invd[a1][ci[a1]]);
-        tile[TF_D1 * NC + c] = node_d<SIXTH>(vel[a2], o, stv[a2], (T)invd[a2][ci[a2]]);
-        tile[TF_D2 * NC + c] = node_d<SIXTH>(vel[n], o, stv[ca], (T)invd[ca][ci[ca]]);
-        tile[TF_D3 * NC + c] = node_d<SIXTH>(vel[n], o, stv[cb], (T)invd[cb][ci[cb]]);
+        tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[a1], o, stv[a1], (T)__ldg(invd[a1] + ci[a1]));
+        tile[TF_D1 * NC + c] = node_d<SIXTH, RO>(vel[a2], o, stv[a2], (T)__ldg(invd[a2] + ci[a2]));
+        tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[ca], (T)__ldg(invd[ca] + ci[ca]));
+        tile[TF_D3 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[cb], (T)__ldg(invd[cb] + ci[cb]));
       } else {
         const int n = DIR, t = 1 - DIR;
-        tile[TF_D0 * NC + c] = node_d<SIXTH>(vel[t], o, stv[t], (T)invd[t][ci[t]]);
-        tile[TF_D2 * NC + c] = node_d<SIXTH>(vel[n], o, stv[t], (T)invd[t][ci[t]]);
+        tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[t], o, stv[t], (T)__ldg(invd[t] + ci[t]));
+        tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[t], (T)__ldg(invd[t] + ci[t]));
       }
     }
   }
@@ -561,16 +575,17 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       const int cb = base + (TILE_HALO - H) * step;
       auto sc = [&](int field, int m) -> T { return tile[field * NC + cb + m * step]; };
       T fd = T(0);
-      if (A.scheme != 0) fd = T(0.5) * (st0(TF_SEN, 2) + st0(TF_SEN, 3));
-      conv_flux<ORDER>(A, sc, fd, DIR, F);
+      if (!KONLY && A.scheme != 0) fd = T(0.5) * (st0(TF_SEN, 2) + st0(TF_SEN, 3));
+      conv_flux<ORDER, KONLY>(A, sc, fd, DIR, F);
       if constexpr (VK != VK_EULER) {
         T vo[4];
         const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
-        const T inv = (T)invd[DIR][f];
+        const T inv = (T)__ldg(invd[DIR] + f);
         if constexpr (VK == VK_GV2) {
           const int64_t o = G.at(fc[0], fc[1], DIM == 3 ? fc[2] : 0);
-          T invs[3] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]], DIM == 3 ? (T)A.M.inv_dz[fc[2]] : T(0)};
-          visc_gv2<DIM, LES>(A, DIR, o, stv, invs, vo);
+          T invs[3] = {(T)__ldg(A.M.inv_dx + fc[0]), (T)__ldg(A.M.inv_dy + fc[1]),
+                        DIM == 3 ? (T)__ldg(A.M.inv_dz + fc[2]) : T(0)};
+          visc_gv2<DIM, LES, RO>(A, DIR, o, stv, invs, vo);
         } else if constexpr (VK == VK_2D4) {
           // inner guard of calc_Ev4 / calc_Fv4 (2D): face 2..n-4, transverse 2..n-3
           const int nt = DIR == 0 ? G.ny : G.nx;
@@ -578,7 +593,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
           const int nn = DIR == 0 ? G.nx : G.ny;
           bool inner = (f >= 2 && f <= nn - 4 && tr >= 2 && tr <= nt - 3);
           const int64_t o = G.at(fc[0], fc[1], 0);
-          T invs[2] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]]};
+          T invs[2] = {(T)__ldg(A.M.inv_dx + fc[0]), (T)__ldg(A.M.inv_dy + fc[1])};
           invs[DIR] = inv;
           auto sv = [&](int field, int m) -> T { return tile[field * NC + base + m * step]; };
           visc_2d4(A, sv, DIR, inner, o, stv, invs, vo);
@@ -624,11 +639,11 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     // dt * S metric for this direction, scaled by coef (calc_steps.f90 calc_R)
     double met;
     if constexpr (DIM == 3) {
-      if (DIR == 0) met = A.M.dtdydz[(int64_t)(k - 1) * (G.ny - 2) + (j - 1)];
-      else if (DIR == 1) met = A.M.dtdzdx[(int64_t)(k - 1) * (G.nx - 2) + (i - 1)];
-      else met = A.M.dtdxdy[(int64_t)(j - 1) * (G.nx - 2) + (i - 1)];
+      if (DIR == 0) met = __ldg(A.M.dtdydz + (int64_t)(k - 1) * (G.ny - 2) + (j - 1));
+      else if (DIR == 1) met = __ldg(A.M.dtdzdx + (int64_t)(k - 1) * (G.nx - 2) + (i - 1));
+      else met = __ldg(A.M.dtdxdy + (int64_t)(j - 1) * (G.nx - 2) + (i - 1));
     } else {
-      met = (DIR == 0) ? A.M.dtdy[j - 1] : A.M.dtdx[i - 1];
+      met = (DIR == 0) ? __ldg(A.M.dtdy + j - 1) : __ldg(A.M.dtdx + i - 1);
     }
     const double cm = A.coef * met;
     constexpr int NV = DIM + 2;
@@ -713,8 +728,9 @@ __global__ void __launch_bounds__(SweepShape<DIR>::TX * SweepShape<DIR>::TY,
 k_sweep(StepArgs<T> A, int last) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int TX = SweepShape<DIR>::TX, TY = SweepShape<DIR>::TY;
-  sweep_tile<DIM, DIR, ORDER, VK, LES, T>(A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw,
-                                          threadIdx.y * TX + threadIdx.x, TX * TY);
+  // coherent loads: measured as fast as the read-only path for y/z and faster for x
+  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false>(A, last, blockIdx.x, blockIdx.y, blockIdx.z,
+                                                                     smraw, threadIdx.y * TX + threadIdx.x, TX * TY);
 }
 
 }  // namespace oux
