@@ -83,7 +83,7 @@ __device__ __forceinline__ void prim_cell(const TS* Q, const Geo& G, const Field
   int j = (int)(r % G.ny);
   int k = (int)(r / G.ny);
   int64_t o = G.at(i, j, k);
-  T Jv = (T)__ldg(jac + (int64_t)j * G.nx + i);
+  T Jv = (T)ldro<RO>(jac + (int64_t)j * G.nx + i);
   T q1 = (T)ldro<RO>(Q + o);
   T over_Q1 = T(1) / q1;
   T rho = Jv * q1;
@@ -129,7 +129,7 @@ __device__ __forceinline__ void prim_mx_cell(const double* Qn, const float* dQ, 
 #pragma unroll
   for (int l = 0; l < DIM + 2; ++l)
     q[l] = ldro<RO>(Qn + o + l * G.vs) + (dQ ? (double)ldro<RO>(dQ + o + l * G.vs) : 0.0);
-  double Jv = __ldg(jac + (int64_t)j * G.nx + i);
+  double Jv = ldro<RO>(jac + (int64_t)j * G.nx + i);
   double over = 1.0 / q[0], rho = Jv * q[0];
   double u = q[1] * over, v = q[2] * over, w = 0.0, p;
   if constexpr (DIM == 3) {
@@ -170,11 +170,11 @@ __device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, co
   auto U = [&](int64_t q) { return ldro<RO>(W.u + q); };
   auto V = [&](int64_t q) { return ldro<RO>(W.v + q); };
   auto Wv = [&](int64_t q) { return ldro<RO>(W.w + q); };
-  T dxt = T(0.25) * ((T)__ldg(M.inv_dx + i - 1) + (T)__ldg(M.inv_dx + i));
-  T dyt = T(0.25) * ((T)__ldg(M.inv_dy + j - 1) + (T)__ldg(M.inv_dy + j));
+  T dxt = T(0.25) * ((T)M.inv_dx[i - 1] + (T)M.inv_dx[i]);
+  T dyt = T(0.25) * ((T)M.inv_dy[j - 1] + (T)M.inv_dy[j]);
   T f;
   if constexpr (DIM == 3) {
-    T dzt = T(0.25) * ((T)__ldg(M.inv_dz + k - 1) + (T)__ldg(M.inv_dz + k));
+    T dzt = T(0.25) * ((T)M.inv_dz[k - 1] + (T)M.inv_dz[k]);
     const int64_t ox = 1, oy = G.sx, oz = G.plane;
     T dudx = (-U(o - ox) + U(o + ox)) * dxt;
     T dvdx = (-V(o - ox) + V(o + ox)) * dxt;
@@ -212,7 +212,7 @@ __global__ void k_sensor(Geo G, Fields<T> W, Metrics M) {
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x)
-    sensor_cell<DIM, T, false>(G, W, M, t);  // measured faster than the read-only path
+    sensor_cell<DIM, T, false>(G, W, M, t);
 }
 
 // ---- SMS sub-grid model: 3D_solver/src/calc_les.f90:30-125 -------------------

@@ -538,14 +538,14 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       if constexpr (DIM == 3) {
         const int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
         const int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
-        tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[a1], o, stv[a1], (T)__ldg(invd[a1] + ci[a1]));
-        tile[TF_D1 * NC + c] = node_d<SIXTH, RO>(vel[a2], o, stv[a2], (T)__ldg(invd[a2] + ci[a2]));
-        tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[ca], (T)__ldg(invd[ca] + ci[ca]));
-        tile[TF_D3 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[cb], (T)__ldg(invd[cb] + ci[cb]));
+        tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[a1], o, stv[a1], (T)invd[a1][ci[a1]]);
+        tile[TF_D1 * NC + c] = node_d<SIXTH, RO>(vel[a2], o, stv[a2], (T)invd[a2][ci[a2]]);
+        tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[ca], (T)invd[ca][ci[ca]]);
+        tile[TF_D3 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[cb], (T)invd[cb][ci[cb]]);
       } else {
         const int n = DIR, t = 1 - DIR;
-        tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[t], o, stv[t], (T)__ldg(invd[t] + ci[t]));
-        tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[t], (T)__ldg(invd[t] + ci[t]));
+        tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[t], o, stv[t], (T)invd[t][ci[t]]);
+        tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[t], (T)invd[t][ci[t]]);
       }
     }
   }
@@ -580,11 +580,10 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       if constexpr (VK != VK_EULER) {
         T vo[4];
         const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
-        const T inv = (T)__ldg(invd[DIR] + f);
+        const T inv = (T)invd[DIR][f];
         if constexpr (VK == VK_GV2) {
           const int64_t o = G.at(fc[0], fc[1], DIM == 3 ? fc[2] : 0);
-          T invs[3] = {(T)__ldg(A.M.inv_dx + fc[0]), (T)__ldg(A.M.inv_dy + fc[1]),
-                        DIM == 3 ? (T)__ldg(A.M.inv_dz + fc[2]) : T(0)};
+          T invs[3] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]], DIM == 3 ? (T)A.M.inv_dz[fc[2]] : T(0)};
           visc_gv2<DIM, LES, RO>(A, DIR, o, stv, invs, vo);
         } else if constexpr (VK == VK_2D4) {
           // inner guard of calc_Ev4 / calc_Fv4 (2D): face 2..n-4, transverse 2..n-3
@@ -593,7 +592,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
           const int nn = DIR == 0 ? G.nx : G.ny;
           bool inner = (f >= 2 && f <= nn - 4 && tr >= 2 && tr <= nt - 3);
           const int64_t o = G.at(fc[0], fc[1], 0);
-          T invs[2] = {(T)__ldg(A.M.inv_dx + fc[0]), (T)__ldg(A.M.inv_dy + fc[1])};
+          T invs[2] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]]};
           invs[DIR] = inv;
           auto sv = [&](int field, int m) -> T { return tile[field * NC + base + m * step]; };
           visc_2d4(A, sv, DIR, inner, o, stv, invs, vo);
@@ -639,11 +638,11 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     // dt * S metric for this direction, scaled by coef (calc_steps.f90 calc_R)
     double met;
     if constexpr (DIM == 3) {
-      if (DIR == 0) met = __ldg(A.M.dtdydz + (int64_t)(k - 1) * (G.ny - 2) + (j - 1));
-      else if (DIR == 1) met = __ldg(A.M.dtdzdx + (int64_t)(k - 1) * (G.nx - 2) + (i - 1));
-      else met = __ldg(A.M.dtdxdy + (int64_t)(j - 1) * (G.nx - 2) + (i - 1));
+      if (DIR == 0) met = A.M.dtdydz[(int64_t)(k - 1) * (G.ny - 2) + (j - 1)];
+      else if (DIR == 1) met = A.M.dtdzdx[(int64_t)(k - 1) * (G.nx - 2) + (i - 1)];
+      else met = A.M.dtdxdy[(int64_t)(j - 1) * (G.nx - 2) + (i - 1)];
     } else {
-      met = (DIR == 0) ? __ldg(A.M.dtdy + j - 1) : __ldg(A.M.dtdx + i - 1);
+      met = (DIR == 0) ? A.M.dtdy[j - 1] : A.M.dtdx[i - 1];
     }
     const double cm = A.coef * met;
     constexpr int NV = DIM + 2;
