@@ -191,3 +191,39 @@ class Autotuner:
                            "trials": [[m, asdict(c)] for m, c in results]}
         self.save()
         return best
+
+
+def _main(argv=None) -> int:
+    """Run the seeded 2D vortex ensemble as one batch (a driver for profiling):
+
+        python -m ouxsbli_b200.batch [--count 64] [--seed 0] [--steps 5] [--precision fp64]
+                                     [--pencil 8] [--chunk 2304]
+    """
+    import argparse
+    from .cases import vortex_ensemble, vortex_member
+    ap = argparse.ArgumentParser(prog="python -m ouxsbli_b200.batch")
+    ap.add_argument("--count", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--pencil", type=int, default=8)
+    ap.add_argument("--chunk", type=int, default=8 * BATCH_THREADS)
+    a = ap.parse_args(argv)
+    dev = torch.device("cuda:0")
+    solvers = []
+    for m in vortex_ensemble(a.count, a.seed):
+        cfg, qj = vortex_member(m, order=4, scheme="KEEP", visc="Euler", rk=4, precision=a.precision)
+        s = Solver(cfg, dev)
+        s.set_state(qj)
+        solvers.append(s)
+    b = Batch(solvers, Tuning(pencil=a.pencil, chunk=a.chunk))
+    ms = _event_timer(b, a.steps)
+    st = b.status()
+    print(json.dumps({"solves": a.count, "interior_cells": b.interior_cells(), "ms_per_step": ms,
+                      "status": st, **b.info()}))
+    b.close()
+    return 0 if st == 0 else 1
+
+
+if __name__ == "__main__":
+    raise SystemExit(_main())
