@@ -187,9 +187,16 @@ typedef struct oux_batch_tuning {
   int32_t chunk;         /* cells per point-wise work item, >= 1 */
   int32_t blocks_per_sm; /* persistent blocks per SM; 0 = as many as fit */
   int32_t use_graph;     /* 1: each step replays one captured CUDA graph */
+  int32_t mode;          /* enum oux_batch_mode */
 } oux_batch_tuning;
 
-/* tuning may be NULL (pencil 4, chunk 1152, all resident blocks, graphs on). */
+/* OUX_BATCH_PERSISTENT: one persistent kernel per step over the tile work list
+ * (pencil / chunk / blocks_per_sm apply).  OUX_BATCH_GRAPH: one CUDA graph per
+ * step in which every solve's own stage kernels (those of oux_step) run on a
+ * branch of their own, so the solves overlap on the device (always graphed). */
+enum oux_batch_mode { OUX_BATCH_PERSISTENT = 0, OUX_BATCH_GRAPH = 1 };
+
+/* tuning may be NULL (persistent, pencil 4, chunk 1152, all resident blocks, graphs on). */
 int oux_batch_create(oux_handle* const* members, int32_t n, const oux_batch_tuning* tuning,
                      oux_batch** out);
 /* Device workspace (step arguments, work list, counters) the batch needs. */

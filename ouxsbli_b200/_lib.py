@@ -63,7 +63,10 @@ class OuxLayout(C.Structure):
 
 class OuxBatchTuning(C.Structure):
     _fields_ = [("pencil", C.c_int32), ("chunk", C.c_int32), ("blocks_per_sm", C.c_int32),
-                ("use_graph", C.c_int32)]
+                ("use_graph", C.c_int32), ("mode", C.c_int32)]
+
+
+BATCH_MODES = {"persistent": 0, "graph": 1}
 
 
 class OuxError(RuntimeError):

@@ -19,7 +19,7 @@ from typing import Callable, Sequence
 
 import torch
 
-from ._lib import LIB, OuxBatchTuning, check
+from ._lib import BATCH_MODES, LIB, OuxBatchTuning, check
 from .solver import Solver
 
 BATCH_THREADS = 288  # threads per block of the persistent kernel (csrc/oux_batch.cuh)
@@ -31,11 +31,16 @@ class Tuning:
     chunk: int = 4 * BATCH_THREADS  # cells per point-wise work item
     blocks_per_sm: int = 0          # persistent blocks per SM; 0 = as many as fit
     use_graph: bool = True          # replay one captured CUDA graph per step
+    # "persistent": one persistent kernel per step over the tile work list;
+    # "graph": one CUDA graph per step with every solve's own stage kernels on a
+    # branch of their own (the work-list fields do not apply)
+    mode: str = "persistent"
 
     def to_c(self) -> OuxBatchTuning:
         t = OuxBatchTuning()
         t.pencil, t.chunk, t.blocks_per_sm = self.pencil, self.chunk, self.blocks_per_sm
         t.use_graph = int(self.use_graph)
+        t.mode = BATCH_MODES[self.mode]
         return t
 
 
@@ -102,7 +107,7 @@ class Batch:
 
 # ---------------------------------------------------------------- autotuner --
 CANDIDATES = tuple(Tuning(pencil=p, chunk=c * BATCH_THREADS, blocks_per_sm=b)
-                   for p in (1, 2, 4, 8) for c in (2, 4, 8) for b in (0, 1))
+                   for p in (1, 2, 4, 8) for c in (2, 4, 8) for b in (0, 1)) + (Tuning(mode="graph"),)
 
 
 def size_class(total_interior_cells: int) -> int:
@@ -152,6 +157,22 @@ class Autotuner:
     def lookup(self, key: str) -> Tuning | None:
         e = self.cache.get(key)
         return Tuning(**e["tuning"]) if e else None
+
+    def lookup_nearest(self, key: str) -> Tuning | None:
+        """The cached tuning of `key`, else that of the nearest size class with the
+        same dimension, scheme, order, viscous model, precision and RK."""
+        hit = self.lookup(key)
+        if hit is not None:
+            return hit
+        stem, _, cls = key.rpartition("/2^")
+        best = None
+        for k, e in self.cache.items():
+            s2, _, c2 = k.rpartition("/2^")
+            if s2 == stem:
+                d = abs(int(c2) - int(cls))
+                if best is None or d < best[0]:
+                    best = (d, e)
+        return Tuning(**best[1]["tuning"]) if best else None
 
     def save(self) -> None:
         self.path.parent.mkdir(parents=True, exist_ok=True)

@@ -632,6 +632,10 @@ __global__ void k_noalloc_tables(const double* __restrict__ d, Geo G, double dt,
 
 }  // namespace
 
+int oux_internal_run_steps(oux_handle* h, int nsteps, cudaStream_t s) {
+  return h->mixed ? run_steps<float>(h, nsteps, s) : run_steps<double>(h, nsteps, s);
+}
+
 // ================================ C ABI =========================================
 extern "C" {
 

@@ -55,6 +55,10 @@ struct oux_batch {
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // OUX_BATCH_GRAPH: one capture branch (stream + join event) per member
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> joined;
+  cudaEvent_t fork = nullptr;
 };
 
 namespace {
@@ -182,16 +186,41 @@ void release_graph(oux_batch* b) {
   b->graph = nullptr;
 }
 
+// OUX_BATCH_GRAPH capture of one step: fork every member onto its own branch,
+// run the member's stage kernels there, join all branches back.
+int capture_branches(oux_batch* b) {
+  OUX_CUDA(cudaEventRecord(b->fork, b->cap));
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    OUX_CUDA(cudaStreamWaitEvent(b->branch[i], b->fork, 0));
+    int rc = oux_internal_run_steps(b->members[i], 1, b->branch[i]);
+    if (rc) return rc;
+    OUX_CUDA(cudaEventRecord(b->joined[i], b->branch[i]));
+    OUX_CUDA(cudaStreamWaitEvent(b->cap, b->joined[i], 0));
+  }
+  return OUX_OK;
+}
+
+void release_branches(oux_batch* b) {
+  for (auto s : b->branch) cudaStreamDestroy(s);
+  for (auto e : b->joined) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  b->branch.clear();
+  b->joined.clear();
+  b->fork = nullptr;
+}
+
 }  // namespace
 
 extern "C" {
 
 int oux_batch_create(oux_handle* const* members, int32_t n, const oux_batch_tuning* tuning, oux_batch** out) {
   if (!members || !out || n < 1) return fail(OUX_E_INVALID, "need at least one member and an output");
-  oux_batch_tuning t{4, 4 * BATCH_THREADS, 0, 1};
+  oux_batch_tuning t{4, 4 * BATCH_THREADS, 0, 1, OUX_BATCH_PERSISTENT};
   if (tuning) t = *tuning;
   if (t.pencil < 1 || t.chunk < 1 || t.blocks_per_sm < 0)
     return fail(OUX_E_INVALID, "tuning: pencil >= 1, chunk >= 1, blocks_per_sm >= 0");
+  if (t.mode != OUX_BATCH_PERSISTENT && t.mode != OUX_BATCH_GRAPH) return fail(OUX_E_INVALID, "unknown batch mode");
+  if (t.mode == OUX_BATCH_GRAPH) t.use_graph = 1;
   oux_handle* h0 = members[0];
   for (int i = 0; i < n; ++i) {
     const oux_handle* h = members[i];
@@ -261,9 +290,22 @@ int oux_batch_bind(oux_batch* b, void* workspace_dev, size_t bytes, void* stream
   OUX_CUDA(cudaMemsetAsync(b->ws + b->off_status, 0, sizeof(int), s));
   OUX_CUDA(cudaStreamSynchronize(s));
   // size the persistent grid and set the kernel attribute before any capture
-  int rc = launch(b, s, 1);
-  if (rc) return rc;
+  if (b->tune.mode == OUX_BATCH_PERSISTENT) {
+    int rc = launch(b, s, 1);
+    if (rc) return rc;
+  }
   if (b->tune.use_graph && !b->cap) OUX_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  if (b->tune.mode == OUX_BATCH_GRAPH && b->branch.empty()) {
+    OUX_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    for (size_t i = 0; i < b->members.size(); ++i) {
+      cudaStream_t st = nullptr;
+      cudaEvent_t ev = nullptr;
+      OUX_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      b->branch.push_back(st);
+      OUX_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      b->joined.push_back(ev);
+    }
+  }
   return OUX_OK;
 }
 
@@ -274,8 +316,12 @@ int oux_batch_step(oux_batch* b, int32_t nsteps, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (b->tune.use_graph) {
     if (!b->exec) {
-      OUX_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
-      int rc = one_step(b, b->cap);
+      // relaxed: the members' kernels may set their shared-memory attribute on
+      // their first launch, which happens inside this capture
+      const bool branches = b->tune.mode == OUX_BATCH_GRAPH;
+      OUX_CUDA(cudaStreamBeginCapture(b->cap, branches ? cudaStreamCaptureModeRelaxed
+                                                       : cudaStreamCaptureModeThreadLocal));
+      int rc = branches ? capture_branches(b) : one_step(b, b->cap);
       cudaGraph_t g = nullptr;
       cudaError_t e = cudaStreamEndCapture(b->cap, &g);
       if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -317,6 +363,7 @@ int oux_batch_info(const oux_batch* b, int64_t* items, int32_t* phases, int32_t*
 int oux_batch_destroy(oux_batch* b) {
   if (!b) return OUX_OK;
   release_graph(b);
+  release_branches(b);
   if (b->cap) cudaStreamDestroy(b->cap);
   delete b;
   return OUX_OK;

@@ -10,6 +10,9 @@
 // Sets the thread-local message oux_last_error() returns; returns `code`.
 int oux_internal_fail(int code, const std::string& msg);
 
+// nsteps time steps of a bound handle on `s` (the body of oux_step).
+int oux_internal_run_steps(oux_handle* h, int nsteps, cudaStream_t s);
+
 struct oux_handle {
   oux_config cfg;
   oux::Geo G;

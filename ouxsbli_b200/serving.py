@@ -120,14 +120,15 @@ class Server:
                                                        precision="mixed"))
     tuner: Autotuner | None = None      # cached tunings are used when present
     keep_states: bool = False           # return each final state (host copy)
+    default_tuning: Tuning = field(default_factory=Tuning)  # when the tuner has nothing cached
     stats: dict = field(default_factory=dict)
 
     def _tuning(self, solvers) -> Tuning:
         if self.tuner is not None:
-            t = self.tuner.lookup(tuning_key(solvers))
+            t = self.tuner.lookup_nearest(tuning_key(solvers))
             if t is not None:
                 return t
-        return Tuning()
+        return self.default_tuning
 
     def run(self, requests: Sequence[SolveRequest], clock: Callable[[], float] = time.perf_counter,
             sleep: Callable[[float], None] = time.sleep) -> list[SolveResult]:

@@ -94,3 +94,14 @@ def test_vortex_ensemble_is_seeded():
     a, b = vortex_ensemble(64, seed=0), vortex_ensemble(64, seed=0)
     assert a == b and len(a) == 64
     assert all(m.n in VORTEX_SIZES and 1.0 <= m.beta <= 5.0 and 0.1 <= m.mach <= 0.8 for m in a)
+
+
+def test_autotuner_nearest_size_class(tmp_path):
+    t = Autotuner(tmp_path / "t.json")
+    t.cache["3d/SLAU/o6/LES-Central-6/mixed/rk3/2^20"] = {"tuning": {"mode": "graph"}}
+    t.cache["3d/SLAU/o6/LES-Central-6/mixed/rk3/2^12"] = {"tuning": {"pencil": 1}}
+    t.cache["2d/KEEP/o4/Euler/fp64/rk4/2^21"] = {"tuning": {"pencil": 8}}
+    assert t.lookup_nearest("3d/SLAU/o6/LES-Central-6/mixed/rk3/2^19") == Tuning(mode="graph")
+    assert t.lookup_nearest("3d/SLAU/o6/LES-Central-6/mixed/rk3/2^13") == Tuning(pencil=1)
+    assert t.lookup_nearest("3d/KEEP/o6/NS-Central-6/fp64/rk3/2^20") is None
+    assert Tuning(mode="graph").to_c().mode == 1

@@ -121,3 +121,18 @@ def test_autotuner_caches_choice(tmp_path, cuda_device):
     assert again.tune(solvers, candidates=()) == best  # served from the cache
     for s in solvers:
         s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_graph_mode_bitexact(precision, cuda_device):
+    """Graph mode runs every member's own stage kernels on a graph branch: bit for bit
+    the single-solve result, in the mixed form too."""
+    cases = [random_turbulence(n, seed=s, scheme="SLAU", visc="LES", precision=precision)
+             for n, s in ((12, 1), (16, 2), (14, 3))]
+    ref = singles(cases, 4, cuda_device)
+    got = batched(cases, 4, cuda_device, Tuning(mode="graph"))
+    for x, y in zip(ref, got):
+        np.testing.assert_array_equal(x, y)
+    cases2 = vortex_ensemble()
+    for x, y in zip(singles(cases2, 5, cuda_device), batched(cases2, 5, cuda_device, Tuning(mode="graph"))):
+        np.testing.assert_array_equal(x, y)
