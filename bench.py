@@ -246,14 +246,32 @@ def bench_ensemble(dev, steps: int, check_steps: int, single_steps: int, count: 
 
 def bench_serving(dev, count: int, rate: float, budget_gb: float, seed: int = 0):
     """Serving stream of 3D decaying-turbulence LES requests (SLAU-6, SMS, RK3, mixed)."""
-    from ouxsbli_b200.batch import Autotuner
-    from ouxsbli_b200.serving import Server, poisson_stream, summarize
-    reqs = poisson_stream(count, rate, seed)
+    import dataclasses
+    from ouxsbli_b200.batch import Autotuner, Tuning, tuning_key
+    from ouxsbli_b200.serving import GRID_SIZES, Server, SolveRequest, poisson_stream, summarize
+    from ouxsbli_b200.solver import Solver
     srv = Server(device=dev, hbm_budget=int(budget_gb * (1 << 30)), quantum=100, tuner=Autotuner())
+    # tune once on a representative mix (one request of every grid size); the server
+    # then reuses the cached choice of the nearest size class
+    rep = []
+    for i, n in enumerate(GRID_SIZES):
+        cfg, qj = SolveRequest(rid=i, n=n, steps=1, seed=1000 + i).build(srv.physics)
+        s = Solver(cfg, dev)
+        s.set_state(qj)
+        rep.append(s)
+    cands = (Tuning(), Tuning(pencil=8, chunk=2304), Tuning(mode="graph"))
+    chosen = srv.tuner.tune(rep, steps=3, candidates=cands, force=True)
+    key = tuning_key(rep)
+    trials = srv.tuner.cache[key]["trials"]
+    for s in rep:
+        s.close()
+    reqs = poisson_stream(count, rate, seed)
     res = srv.run(reqs)
     return summarize(res) | {"unit_latency": "s", "arrival_rate_per_s": rate, "hbm_budget_gb": budget_gb,
                              "grids": sorted({r.n for r in reqs}), "steps_range": [200, 2000],
                              "physics": "SLAU-6 HRSLAU2, SMS LES, TVD-RK3, mixed FP32/FP64",
+                             "tuning": dataclasses.asdict(chosen),
+                             "tuning_trials_ms_per_step": {t[1]["mode"] + (f"-p{t[1]['pencil']}" if t[1]["mode"] == "persistent" else ""): t[0] for t in trials},
                              "server": srv.stats}
 
 
