@@ -48,6 +48,31 @@ __host__ __device__ constexpr size_t sweep_smem() {
          sizeof(double) * 5 * SweepShape<DIR, ROWS>::TX * SweepShape<DIR, ROWS>::TY;
 }
 
+// Shared-memory bytes of the operand prefetch of a y/z sweep (PF): for every
+// owned cell, nv (<= 5) values each of Racc, Q^n, Rs (FP64) and Qs (T).
+template <int DIR, class T, int ROWS = default_rows<DIR>()>
+__host__ __device__ constexpr size_t sweep_pf_bytes() {
+  return DIR == 0 ? 0 : (size_t)5 * 32 * ROWS * (3 * sizeof(double) + sizeof(T));
+}
+
+// Where k_sweep prefetches: the last sweep of a stage (the one that applies the RK
+// combination) in the mixed form.  Measured on B200: the FP32 z sweep runs 1.37x
+// faster; in FP64 the extra 40 KB per block cost more L1 hits than the overlap
+// gained (y sweep 1.28x slower, z unchanged).
+template <int DIM, int DIR, class T>
+__host__ __device__ constexpr bool sweep_pf_on() {
+  return sizeof(T) < sizeof(double) && DIR == DIM - 1;
+}
+
+// asynchronous global -> shared copies (the issuing thread waits for its own)
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // transverse node derivative of `a` along axis `ax` at offset o (4th/6th order)
 template <bool SIXTH, bool RO, class T>
 __device__ __forceinline__ T node_d(const T* a, int64_t o, int64_t st, T inv) {
@@ -468,8 +493,11 @@ namespace oux {
 // One sweep tile: block-tile indices (b0, b1, b2) as the grid of launch_one
 // enumerates them; `tid` / `nthr_all` are the calling block's linear thread index
 // and size (>= TX*TY: threads beyond the tile shape only help load the tile).
+// PF: prefetch the cell operands of the difference / combination (accumulator,
+// Q^n, Qs, Rs) into shared memory when the tile starts, so their latency overlaps
+// the face fluxes; needs sweep_pf_bytes() more dynamic shared memory.
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
-          bool RO = false, bool KONLY = false>
+          bool RO = false, bool KONLY = false, bool PF = false>
 __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
                                            unsigned char* smraw, int tid, int nthr_all) {
   constexpr int H = ORDER / 2;
@@ -499,6 +527,41 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   const int64_t stv[3] = {1, G.sx, G.plane};
   const int nsweep = DIR == 0 ? G.nx : (DIR == 1 ? G.ny : G.nz);
   const int ext[3] = {g + Nx, g + Ny, g + Nz};
+
+  // ---- operand prefetch (y/z sweeps): the thread that owns a cell copies it ----
+  constexpr bool PF_ON = PF && DIR != 0;
+  constexpr bool MXC = sizeof(T) < sizeof(double);
+  constexpr int PFC = 32 * ROWS;  // owned cells per tile
+  double* pfR = reinterpret_cast<double*>(smraw + sweep_smem<ORDER, DIR, T, ROWS>());
+  double* pfQn = pfR + 5 * PFC;
+  double* pfRs = pfQn + 5 * PFC;
+  T* pfQs = reinterpret_cast<T*>(pfRs + 5 * PFC);
+  const int md = last ? A.mode : CM_ACCUM;
+  const bool needQn = (!MXC && (md == CM_RK3_1 || md == CM_RK3_2 || md == CM_RK4_S)) || md == CM_RK3_3 ||
+                      md == CM_RK4_4;
+  const bool needQs = md == CM_RK3_2 || md == CM_RK3_3;
+  const bool needRs = md == CM_RK4_S || md == CM_RK4_4;
+  const int slot = ty * 32 + tx;
+  if constexpr (PF_ON) {
+    if (act && ty < TY - 1) {
+      int pc[3];
+      pc[0] = bx0 + tx;
+      pc[DIR] = (DIR == 1 ? by0 : bz0) + ty;
+      if (DIR == 1) pc[2] = bz0; else pc[1] = by0;
+      if (pc[0] < ext[0] && pc[1] < ext[1] && (DIM == 2 || pc[2] < ext[2])) {
+        const int64_t po = G.at(pc[0], pc[1], DIM == 3 ? pc[2] : 0);
+#pragma unroll
+        for (int l = 0; l < DIM + 2; ++l) {
+          const int64_t q = po + l * G.vs;
+          cp_async<8>(pfR + l * PFC + slot, A.Racc + q);
+          if (needQn) cp_async<8>(pfQn + l * PFC + slot, A.Qn + q);
+          if (needRs) cp_async<8>(pfRs + l * PFC + slot, A.Rs + q);
+          if (needQs) cp_async<sizeof(T)>(pfQs + l * PFC + slot, A.Qs + q);
+        }
+      }
+    }
+    cp_async_commit();
+  }
 
   // ---- tile load (cooperative) ----
   for (int c = tid; c < NC; c += nthr) {
@@ -635,6 +698,24 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     if (!ok) return;
     const int i = cc[0], j = cc[1], k = (DIM == 3) ? cc[2] : 0;
     const int64_t o = G.at(i, j, k);
+    if constexpr (PF_ON) cp_async_wait_all();
+    // operands of the difference / combination: prefetched copy or global
+    auto RACC = [&](int l) -> double {
+      if constexpr (PF_ON) return pfR[l * PFC + slot];
+      else return A.Racc[o + l * G.vs];
+    };
+    auto QN = [&](int l) -> double {
+      if constexpr (PF_ON) return pfQn[l * PFC + slot];
+      else return A.Qn[o + l * G.vs];
+    };
+    auto QS = [&](int l) -> T {
+      if constexpr (PF_ON) return pfQs[l * PFC + slot];
+      else return A.Qs[o + l * G.vs];
+    };
+    auto RS = [&](int l) -> double {
+      if constexpr (PF_ON) return pfRs[l * PFC + slot];
+      else return A.Rs[o + l * G.vs];
+    };
     // dt * S metric for this direction, scaled by coef (calc_steps.f90 calc_R)
     double met;
     if constexpr (DIM == 3) {
@@ -652,7 +733,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       const int fl = (DIM == 2 && l == 3) ? 4 : l;  // 2D: energy is flux slot 4
       double d = cm * (-Fs[fl * (TX * TY) + lo] + Fs[fl * (TX * TY) + hi]);
       if (DIR == 0) R[l] = d;
-      else R[l] = A.Racc[o + l * G.vs] + d;
+      else R[l] = RACC(l) + d;
     }
     if (!last) {
 #pragma unroll
@@ -660,7 +741,6 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       return;
     }
     // mixed form: the stage state holds the FP32 increment Q^(s) - Q^n
-    constexpr bool MXC = sizeof(T) < sizeof(double);
     switch (A.mode) {
       case CM_R_OUT: {
         // reference Rs(nx-2, nv, ny-2, nz-2) order, cell (i,j,k) -> (i-1, l, j-1, k-1)
@@ -674,7 +754,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         for (int l = 0; l < NV; ++l) {
           const int64_t q = o + l * G.vs;
           if constexpr (MXC) A.Qs[q] = (T)(-R[l]);  // stage increment Q1 - Qn
-          else A.Qs[q] = (T)(A.Qn[q] - R[l]);
+          else A.Qs[q] = (T)(QN(l) - R[l]);
         }
         break;
       }
@@ -682,8 +762,8 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           const int64_t q = o + l * G.vs;
-          if constexpr (MXC) A.Qs[q] = (T)((A.c2 * (double)A.Qs[q] - R[l]) * A.c4);  // c1 + c2 = 1
-          else A.Qs[q] = (T)((A.c1 * A.Qn[q] + A.c2 * (double)A.Qs[q] - R[l]) * A.c4);
+          if constexpr (MXC) A.Qs[q] = (T)((A.c2 * (double)QS(l) - R[l]) * A.c4);  // c1 + c2 = 1
+          else A.Qs[q] = (T)((A.c1 * QN(l) + A.c2 * (double)QS(l) - R[l]) * A.c4);
         }
         break;
       }
@@ -691,8 +771,8 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           const int64_t q = o + l * G.vs;
-          if constexpr (MXC) A.Qn[q] = A.Qn[q] + (A.c1 * (double)A.Qs[q] - R[l]) * A.c4;  // (c1 + c2) c4 = 1
-          else A.Qn[q] = (A.c1 * (double)A.Qs[q] + A.c2 * A.Qn[q] - R[l]) * A.c4;
+          if constexpr (MXC) A.Qn[q] = QN(l) + (A.c1 * (double)QS(l) - R[l]) * A.c4;  // (c1 + c2) c4 = 1
+          else A.Qn[q] = (A.c1 * (double)QS(l) + A.c2 * QN(l) - R[l]) * A.c4;
         }
         break;
       }
@@ -701,8 +781,8 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         for (int l = 0; l < NV; ++l) {
           const int64_t q = o + l * G.vs;
           if constexpr (MXC) A.Qs[q] = (T)(-A.c1 * R[l]);
-          else A.Qs[q] = (T)(A.Qn[q] - A.c1 * R[l]);
-          A.Rs[q] = A.Rs[q] + A.c2 * R[l];
+          else A.Qs[q] = (T)(QN(l) - A.c1 * R[l]);
+          A.Rs[q] = RS(l) + A.c2 * R[l];
         }
         break;
       }
@@ -710,8 +790,8 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           const int64_t q = o + l * G.vs;
-          double r = A.Rs[q] + R[l];
-          A.Qn[q] = A.Qn[q] - r * (1.0 / 6.0);
+          double r = RS(l) + R[l];
+          A.Qn[q] = QN(l) - r * (1.0 / 6.0);
           A.Rs[q] = 0.0;
         }
         break;
@@ -728,8 +808,8 @@ k_sweep(StepArgs<T> A, int last) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int TX = SweepShape<DIR>::TX, TY = SweepShape<DIR>::TY;
   // coherent loads: measured as fast as the read-only path for y/z and faster for x
-  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false>(A, last, blockIdx.x, blockIdx.y, blockIdx.z,
-                                                                     smraw, threadIdx.y * TX + threadIdx.x, TX * TY);
+  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_on<DIM, DIR, T>()>(
+      A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.y * TX + threadIdx.x, TX * TY);
 }
 
 }  // namespace oux
