@@ -6,7 +6,7 @@ namespace oux {
 
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
 int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
-  constexpr size_t smem = sweep_smem<ORDER, DIR, T>() + (sweep_pf_on<DIM, DIR, T>() ? sweep_pf_bytes<DIR, T>() : 0);
+  constexpr size_t smem = sweep_smem<ORDER, DIR, T>() + sweep_pf_bytes<DIR, T>(sweep_pf_mode<DIM, DIR, T>());
   auto kern = k_sweep<DIM, DIR, ORDER, VK, LES, T>;
   static const cudaError_t attr_rc =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

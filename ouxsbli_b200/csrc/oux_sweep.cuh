@@ -48,20 +48,22 @@ __host__ __device__ constexpr size_t sweep_smem() {
          sizeof(double) * 5 * SweepShape<DIR, ROWS>::TX * SweepShape<DIR, ROWS>::TY;
 }
 
-// Shared-memory bytes of the operand prefetch of a y/z sweep (PF): for every
-// owned cell, nv (<= 5) values each of Racc, Q^n, Rs (FP64) and Qs (T).
+// Operand prefetch of a y/z sweep (PF): for every owned cell, nv (<= 5) values of
+// Q^n and of Qs or Rs (never needed together), and with PF = 2 also the
+// accumulator Racc, copied into shared memory when the tile starts.
 template <int DIR, class T, int ROWS = default_rows<DIR>()>
-__host__ __device__ constexpr size_t sweep_pf_bytes() {
-  return DIR == 0 ? 0 : (size_t)5 * 32 * ROWS * (3 * sizeof(double) + sizeof(T));
+__host__ __device__ constexpr size_t sweep_pf_bytes(int pf) {
+  return (DIR == 0 || pf == 0) ? 0 : (size_t)5 * 32 * ROWS * sizeof(double) * (pf == 2 ? 3 : 2);
 }
 
-// Where k_sweep prefetches: the last sweep of a stage (the one that applies the RK
-// combination) in the mixed form.  Measured on B200: the FP32 z sweep runs 1.37x
-// faster; in FP64 the extra 40 KB per block cost more L1 hits than the overlap
-// gained (y sweep 1.28x slower, z unchanged).
+// Which prefetch k_sweep uses: only the last sweep of a stage (the one that applies
+// the RK combination).  Measured on B200: prefetching Q^n / Qs / Rs there moves
+// their latency under the face fluxes; the mixed form (smaller FP32 tile) also
+// prefetches the accumulator, while in FP64 shared memory beyond ~80 KB per block
+// costs more L1 hits than it saves.
 template <int DIM, int DIR, class T>
-__host__ __device__ constexpr bool sweep_pf_on() {
-  return sizeof(T) < sizeof(double) && DIR == DIM - 1;
+__host__ __device__ constexpr int sweep_pf_mode() {
+  return DIR != DIM - 1 ? 0 : (sizeof(T) < sizeof(double) ? 2 : 1);
 }
 
 // asynchronous global -> shared copies (the issuing thread waits for its own)
@@ -493,11 +495,11 @@ namespace oux {
 // One sweep tile: block-tile indices (b0, b1, b2) as the grid of launch_one
 // enumerates them; `tid` / `nthr_all` are the calling block's linear thread index
 // and size (>= TX*TY: threads beyond the tile shape only help load the tile).
-// PF: prefetch the cell operands of the difference / combination (accumulator,
-// Q^n, Qs, Rs) into shared memory when the tile starts, so their latency overlaps
-// the face fluxes; needs sweep_pf_bytes() more dynamic shared memory.
+// PF: prefetch the cell operands of the combination (Q^n, Qs / Rs; PF = 2: and the
+// accumulator) into shared memory when the tile starts, so their latency overlaps
+// the face fluxes; needs sweep_pf_bytes(PF) more dynamic shared memory.
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
-          bool RO = false, bool KONLY = false, bool PF = false>
+          bool RO = false, bool KONLY = false, int PF = 0>
 __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
                                            unsigned char* smraw, int tid, int nthr_all) {
   constexpr int H = ORDER / 2;
@@ -529,13 +531,15 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   const int ext[3] = {g + Nx, g + Ny, g + Nz};
 
   // ---- operand prefetch (y/z sweeps): the thread that owns a cell copies it ----
-  constexpr bool PF_ON = PF && DIR != 0;
+  constexpr bool PF_ON = PF > 0 && DIR != 0;
+  constexpr bool PF_R = PF_ON && PF == 2;
   constexpr bool MXC = sizeof(T) < sizeof(double);
   constexpr int PFC = 32 * ROWS;  // owned cells per tile
-  double* pfR = reinterpret_cast<double*>(smraw + sweep_smem<ORDER, DIR, T, ROWS>());
-  double* pfQn = pfR + 5 * PFC;
-  double* pfRs = pfQn + 5 * PFC;
-  T* pfQs = reinterpret_cast<T*>(pfRs + 5 * PFC);
+  double* pfQn = reinterpret_cast<double*>(smraw + sweep_smem<ORDER, DIR, T, ROWS>());
+  double* pfX = pfQn + 5 * PFC;             // Qs (as T) or Rs
+  T* pfQs = reinterpret_cast<T*>(pfX);
+  double* pfRs = pfX;
+  double* pfR = pfX + 5 * PFC;              // PF = 2 only
   const int md = last ? A.mode : CM_ACCUM;
   const bool needQn = (!MXC && (md == CM_RK3_1 || md == CM_RK3_2 || md == CM_RK4_S)) || md == CM_RK3_3 ||
                       md == CM_RK4_4;
@@ -553,10 +557,10 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
 #pragma unroll
         for (int l = 0; l < DIM + 2; ++l) {
           const int64_t q = po + l * G.vs;
-          cp_async<8>(pfR + l * PFC + slot, A.Racc + q);
+          if (PF_R) cp_async<8>(pfR + l * PFC + slot, A.Racc + q);
           if (needQn) cp_async<8>(pfQn + l * PFC + slot, A.Qn + q);
           if (needRs) cp_async<8>(pfRs + l * PFC + slot, A.Rs + q);
-          if (needQs) cp_async<sizeof(T)>(pfQs + l * PFC + slot, A.Qs + q);
+          else if (needQs) cp_async<sizeof(T)>(pfQs + l * PFC + slot, A.Qs + q);
         }
       }
     }
@@ -701,7 +705,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     if constexpr (PF_ON) cp_async_wait_all();
     // operands of the difference / combination: prefetched copy or global
     auto RACC = [&](int l) -> double {
-      if constexpr (PF_ON) return pfR[l * PFC + slot];
+      if constexpr (PF_R) return pfR[l * PFC + slot];
       else return A.Racc[o + l * G.vs];
     };
     auto QN = [&](int l) -> double {
@@ -808,7 +812,7 @@ k_sweep(StepArgs<T> A, int last) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int TX = SweepShape<DIR>::TX, TY = SweepShape<DIR>::TY;
   // coherent loads: measured as fast as the read-only path for y/z and faster for x
-  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_on<DIM, DIR, T>()>(
+  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>()>(
       A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.y * TX + threadIdx.x, TX * TY);
 }
 
