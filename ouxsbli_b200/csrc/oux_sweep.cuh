@@ -48,22 +48,25 @@ __host__ __device__ constexpr size_t sweep_smem() {
          sizeof(double) * 5 * SweepShape<DIR, ROWS>::TX * SweepShape<DIR, ROWS>::TY;
 }
 
-// Operand prefetch of a y/z sweep (PF): for every owned cell, nv (<= 5) values of
-// Q^n and of Qs or Rs (never needed together), and with PF = 2 also the
-// accumulator Racc, copied into shared memory when the tile starts.
+// Operand prefetch of a y/z sweep, PF = bit mask: 1 = the combination operands
+// (nv values of Q^n and of Qs or Rs, never needed together), 2 = the accumulator
+// Racc; copied into shared memory when the tile starts.
 template <int DIR, class T, int ROWS = default_rows<DIR>()>
 __host__ __device__ constexpr size_t sweep_pf_bytes(int pf) {
-  return (DIR == 0 || pf == 0) ? 0 : (size_t)5 * 32 * ROWS * sizeof(double) * (pf == 2 ? 3 : 2);
+  return DIR == 0 ? 0 : (size_t)5 * 32 * ROWS * sizeof(double) * ((pf & 1 ? 2 : 0) + (pf & 2 ? 1 : 0));
 }
 
-// Which prefetch k_sweep uses: only the last sweep of a stage (the one that applies
-// the RK combination).  Measured on B200: prefetching Q^n / Qs / Rs there moves
-// their latency under the face fluxes; the mixed form (smaller FP32 tile) also
-// prefetches the accumulator, while in FP64 shared memory beyond ~80 KB per block
-// costs more L1 hits than it saves.
+// Which prefetch k_sweep uses (measured on B200, 256^3 Hybrid-6 / NS C6):
+//  - last sweep of a stage (applies the RK combination): Q^n / Qs / Rs, which moves
+//    their latency under the face fluxes (FP64 z sweep 1.79 -> 1.37 ms);
+//  - the mixed form, whose FP32 tile is half as large, also prefetches the
+//    accumulator, in every y/z sweep (y 0.89 -> 0.85 ms);
+//  - in FP64 the accumulator prefetch costs more L1 hits than it saves (y 1.20 ->
+//    1.24 ms), so FP64 y sweeps in 3D prefetch nothing.
 template <int DIM, int DIR, class T>
 __host__ __device__ constexpr int sweep_pf_mode() {
-  return DIR != DIM - 1 ? 0 : (sizeof(T) < sizeof(double) ? 2 : 1);
+  constexpr bool mx = sizeof(T) < sizeof(double);
+  return DIR == 0 ? 0 : (DIR != DIM - 1 ? (mx ? 2 : 0) : (mx ? 3 : 1));
 }
 
 // asynchronous global -> shared copies (the issuing thread waits for its own)
@@ -532,14 +535,15 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
 
   // ---- operand prefetch (y/z sweeps): the thread that owns a cell copies it ----
   constexpr bool PF_ON = PF > 0 && DIR != 0;
-  constexpr bool PF_R = PF_ON && PF == 2;
+  constexpr bool PF_C = PF_ON && (PF & 1);  // combination operands
+  constexpr bool PF_R = PF_ON && (PF & 2);  // accumulator
   constexpr bool MXC = sizeof(T) < sizeof(double);
   constexpr int PFC = 32 * ROWS;  // owned cells per tile
   double* pfQn = reinterpret_cast<double*>(smraw + sweep_smem<ORDER, DIR, T, ROWS>());
   double* pfX = pfQn + 5 * PFC;             // Qs (as T) or Rs
   T* pfQs = reinterpret_cast<T*>(pfX);
   double* pfRs = pfX;
-  double* pfR = pfX + 5 * PFC;              // PF = 2 only
+  double* pfR = pfQn + (PF_C ? 10 : 0) * PFC;
   const int md = last ? A.mode : CM_ACCUM;
   const bool needQn = (!MXC && (md == CM_RK3_1 || md == CM_RK3_2 || md == CM_RK4_S)) || md == CM_RK3_3 ||
                       md == CM_RK4_4;
@@ -558,9 +562,9 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         for (int l = 0; l < DIM + 2; ++l) {
           const int64_t q = po + l * G.vs;
           if (PF_R) cp_async<8>(pfR + l * PFC + slot, A.Racc + q);
-          if (needQn) cp_async<8>(pfQn + l * PFC + slot, A.Qn + q);
-          if (needRs) cp_async<8>(pfRs + l * PFC + slot, A.Rs + q);
-          else if (needQs) cp_async<sizeof(T)>(pfQs + l * PFC + slot, A.Qs + q);
+          if (PF_C && needQn) cp_async<8>(pfQn + l * PFC + slot, A.Qn + q);
+          if (PF_C && needRs) cp_async<8>(pfRs + l * PFC + slot, A.Rs + q);
+          else if (PF_C && needQs) cp_async<sizeof(T)>(pfQs + l * PFC + slot, A.Qs + q);
         }
       }
     }
@@ -709,15 +713,15 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       else return A.Racc[o + l * G.vs];
     };
     auto QN = [&](int l) -> double {
-      if constexpr (PF_ON) return pfQn[l * PFC + slot];
+      if constexpr (PF_C) return pfQn[l * PFC + slot];
       else return A.Qn[o + l * G.vs];
     };
     auto QS = [&](int l) -> T {
-      if constexpr (PF_ON) return pfQs[l * PFC + slot];
+      if constexpr (PF_C) return pfQs[l * PFC + slot];
       else return A.Qs[o + l * G.vs];
     };
     auto RS = [&](int l) -> double {
-      if constexpr (PF_ON) return pfRs[l * PFC + slot];
+      if constexpr (PF_C) return pfRs[l * PFC + slot];
       else return A.Rs[o + l * G.vs];
     };
     // dt * S metric for this direction, scaled by coef (calc_steps.f90 calc_R)
