@@ -116,6 +116,11 @@ int oux_bind(oux_handle* h, void* state_dev, void* scratch_dev, size_t scratch_b
  * pinned; staging uses the scratch buffer. */
 int oux_set_state(oux_handle* h, const double* host_qj, void* stream);
 int oux_get_state(oux_handle* h, double* host_qj, void* stream);
+/* oux_get_state without the final synchronisation: the copy into host_qj (pinned
+ * memory for real asynchrony) completes when `stream` reaches it.  The handle's
+ * scratch stages the copy, so further work on the handle must be ordered after it
+ * (the same stream does that).  Same reference counterpart as oux_get_state. */
+int oux_get_state_async(oux_handle* h, double* host_qj, void* stream);
 /* Pure host converters between the reference order and the device layout. */
 int oux_pack_state(const oux_handle* h, const double* ref_qj, void* dev_layout_host);
 int oux_unpack_state(const oux_handle* h, const void* dev_layout_host, double* ref_qj);

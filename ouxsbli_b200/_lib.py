@@ -35,7 +35,7 @@ FAULT_TIMEOUT = 4
 SYMBOLS = [
     "oux_create", "oux_destroy", "oux_last_error", "oux_abi_version", "oux_state_bytes",
     "oux_scratch_bytes", "oux_layout_of", "oux_bind", "oux_set_state", "oux_get_state",
-    "oux_pack_state", "oux_unpack_state", "oux_fill_ghosts", "oux_rhs", "oux_step",
+    "oux_pack_state", "oux_unpack_state", "oux_fill_ghosts", "oux_rhs", "oux_step", "oux_get_state_async",
     "oux_diagnostics", "oux_check_state", "oux_status", "oux_profile", "oux_profile_read",
     "oux_host_ref_diagnostics", "oux_launch_count", "oux_rhs_noalloc",
     "oux_batch_create", "oux_batch_workspace_bytes", "oux_batch_bind", "oux_batch_step",
@@ -96,6 +96,7 @@ def _load() -> C.CDLL:
         "oux_bind": (C.c_int, [vp, vp, vp, C.c_size_t, vp]),
         "oux_set_state": (C.c_int, [vp, dp, vp]),
         "oux_get_state": (C.c_int, [vp, dp, vp]),
+        "oux_get_state_async": (C.c_int, [vp, dp, vp]),
         "oux_pack_state": (C.c_int, [vp, dp, vp]),
         "oux_unpack_state": (C.c_int, [vp, vp, dp]),
         "oux_fill_ghosts": (C.c_int, [vp, vp]),

@@ -764,6 +764,18 @@ int oux_get_state(oux_handle* h, double* host_qj, void* stream) {
   return OUX_OK;
 }
 
+int oux_get_state_async(oux_handle* h, double* host_qj, void* stream) {
+  if (!h || !host_qj) return fail(OUX_E_INVALID, "null argument");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo& G = h->G;
+  int64_t n = (int64_t)G.nx * G.ny * G.nz * h->nv;
+  k_soa_to_ref<double><<<grid_for(n, 256), 256, 0, s>>>(h->Q, h->Racc, G, h->nv);
+  OUX_CUDA(cudaGetLastError());
+  OUX_CUDA(cudaMemcpyAsync(host_qj, h->Racc, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  return OUX_OK;
+}
+
 int oux_pack_state(const oux_handle* h, const double* ref_qj, void* dev_layout_host) {
   if (!h || !ref_qj || !dev_layout_host) return fail(OUX_E_INVALID, "null argument");
   const Geo& G = h->G;
