@@ -53,3 +53,26 @@ def rhs_interior(r: np.ndarray, g: int, dim: int) -> np.ndarray:
 
 def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def diagnostics_numpy(cfg, qj):
+    """FP64 KE, entropy and enstrophy means of a 3D state from the oracle's
+    primitive fields (the definitions liboux's diagnostics use: vorticity by the
+    6th-order central difference)."""
+    from oracle import oracle
+    f = oracle.fields(cfg, qj)
+    g = cfg.g
+    sl = (slice(g, -g),) * 3
+    rho, u, v, w, p = (f[k][sl] for k in ("rho", "u", "v", "w", "p"))
+    ke = np.mean(0.5 * rho * (u * u + v * v + w * w))
+    ent = np.mean(rho * np.log(p * rho ** (-cfg.gamma)))
+    inv = 1.0 / cfg.dx[0]
+
+    def d6(a, axis):
+        r = lambda m: np.roll(a, -m, axis=axis)
+        return ((1.0 / 60.0) * (-r(-3) + r(3)) + 0.15 * (r(-2) - r(2)) + 0.75 * (-r(-1) + r(1))) * inv
+
+    U, V, W = (f[k] for k in ("u", "v", "w"))
+    om = [d6(W, 1) - d6(V, 2), d6(U, 2) - d6(W, 0), d6(V, 0) - d6(U, 1)]
+    ens = np.mean(0.5 * f["rho"][sl] * sum(o[sl] ** 2 for o in om))
+    return float(ke), float(ent), float(ens)
