@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--mixed-check-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy check (the north star's 1000)")
+    ap.add_argument("--workload", default="tgv256", choices=["tgv256", "large512"],
+                    help="large512: FP64 vs mixed on the 512^3 ME4 supersonic TGV (opt-in, minutes)")
+    ap.add_argument("--large-steps", type=int, default=2000)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched 2D ensemble section")
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream section")
@@ -56,7 +59,7 @@ def parse():
     return ap.parse_args()
 
 
-def workload(n: int, scheme: str, visc: str):
+def workload(n: int, scheme: str, visc: str, **kw):
     """SolverConfig + initial QJ (reference layout) of the supersonic TGV."""
     from ouxsbli_b200.cases import CASES, build_initial
     from ouxsbli_b200.grid import jacobian, to_qj
@@ -68,7 +71,7 @@ def workload(n: int, scheme: str, visc: str):
     p, xc, yc, zc, dx, dy, dz, Q = build_initial(case, p)
     cfg = SolverConfig(dim=3, nx=p["nx"], ny=p["ny"], nz=p["nz"], order=6, scheme=scheme, visc=visc,
                        tvd="hybrid", slau="HRSLAU2", rk=3, gamma=p["gamma"], R=p["R"], Pr=p["Pr"],
-                       Prt=p["Prt"], threshold=0.4, dt=p["dt"], dx=dx, dy=dy, dz=dz)
+                       Prt=p["Prt"], threshold=0.4, dt=p["dt"], dx=dx, dy=dy, dz=dz, **kw)
     qj = to_qj(Q, jacobian(dx, dy, dz))
     return cfg, qj
 
@@ -316,10 +319,64 @@ def run_reference(args):
     return 0
 
 
+def run_large(args):
+    """512^3 supersonic TGV (Ma 1.25, Re 1600, Hybrid-6, ME4 viscous, TVD-RK3): plain FP64
+    against the mixed form over --large-steps steps -- throughput, HBM roofline at
+    320 B / cell-step, per-field error and the enstrophy history and its peak."""
+    import dataclasses
+    import torch
+    from ouxsbli_b200.solver import Solver
+    dev = torch.device("cuda", 0)
+    cfg, qj = workload(512, "Hybrid", "NS", visc_order=6, visc_stencil="ME4Base")
+    cells = cfg.interior_cells()
+    every = 50
+    out = {"workload": "large512", "config": config_json(args, cfg) | {"visc_stencil": "ME4Base"},
+           "steps": args.large_steps, "history_every": every}
+    finals = {}
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    for prec in ("fp64", "mixed"):
+        s = Solver(dataclasses.replace(cfg, precision=prec), dev)
+        s.set_state(qj)
+        st = torch.cuda.current_stream(dev)
+        hist, ms = [s.diagnostics()], 0.0
+        for n in range(0, args.large_steps, every):
+            k = min(every, args.large_steps - n)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            s.step(k)
+            b.record(st)
+            b.synchronize()
+            ms += a.elapsed_time(b)
+            hist.append(s.diagnostics())
+        finals[prec] = s.get_state()
+        s.close()
+        v = cells * args.large_steps / (ms / 1e3) / 1e6
+        ens = [h[2] for h in hist]
+        ipk = int(np.argmax(ens))
+        out[prec] = {"value": v, "unit": METRIC, "ms_per_step": ms / args.large_steps,
+                     "hbm_gbs_at_320B": 320.0 * v * 1e6 / 1e9,
+                     "roofline_frac_at_320B": 320.0 * v * 1e6 / 1e9 / float(peaks.get("hbm_gbs", 6650.0)),
+                     "enstrophy_history": ens, "ke_history": [h[0] for h in hist],
+                     "enstrophy_peak": ens[ipk], "enstrophy_peak_step": ipk * every}
+    g = cfg.g
+    sl = (slice(g, -g), slice(None), slice(g, -g), slice(g, -g))
+    a32, a64 = finals["mixed"][sl], finals["fp64"][sl]
+    out["mixed_vs_fp64"] = {
+        "rel_l2": [float(np.linalg.norm(a32[:, l] - a64[:, l]) / np.linalg.norm(a64[:, l])) for l in range(5)],
+        "enstrophy_peak_rel_dev": abs(out["mixed"]["enstrophy_peak"] - out["fp64"]["enstrophy_peak"])
+        / abs(out["fp64"]["enstrophy_peak"]),
+        "speedup": out["mixed"]["value"] / out["fp64"]["value"]}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "large512":
+        return run_large(args)
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
