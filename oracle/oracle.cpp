@@ -48,6 +48,7 @@ typedef struct orc_config {
   int tvd;            // ORC_TVD_*
   int slau;           // ORC_SLAU1 / ORC_HRSLAU2
   int rk;             // 3 or 4
+  int bc_x;           // 0 periodic; 1 non-periodic x (boundary flux kernels, zero-gradient boundary cells)
   double gamma, R, Pr, Prt, threshold, dt;
 } orc_config;
 
@@ -532,10 +533,13 @@ void ducros(Ctx& C) {
 
 // ---- convective face flux (calc_{keep,slau,hybrid,roe}_kernel_internal) ----------
 // dir: 0 x, 1 y, 2 z.  Face between cells c and c+1 along dir; (i,j,k) is cell c.
-void conv_face(const Ctx& C, int dir, int i, int j, int k, double F[5]) {
+// ord: the stencil order of this face -- the configured order for the interior
+// kernels; lower next to a non-periodic boundary (2D_solver/src/calc_slau_kernel,
+// calc_keep_kernel, calc_hybrid_kernel .f90.fypp: 6 -> 4 -> 2 / first order).
+void conv_face(const Ctx& C, int dir, int i, int j, int k, double F[5], int ord) {
   Prim P{C};
   const Consts& K = C.K;
-  int io = C.c.order / 2 - 1;
+  int io = ord / 2 - 1;
   int n = 2 * io + 2;
   double rho[6], u[6], v[6], w[6], p[6], T[6];
   for (int m = 0; m < n; ++m) {
@@ -546,25 +550,25 @@ void conv_face(const Ctx& C, int dir, int i, int j, int k, double F[5]) {
   }
   const double* un = dir == 0 ? u : dir == 1 ? v : w;
   int scheme = C.c.scheme;
-  if (scheme == ORC_KEEP) { keep_flux(C.c.order, rho, u, v, w, un, p, T, dir, K, F); return; }
+  if (scheme == ORC_KEEP) { keep_flux(ord, rho, u, v, w, un, p, T, dir, K, F); return; }
   double s0 = C.w.sensor[C.sidx(i, j, k)];
   double s1 = C.w.sensor[C.sidx(i + (dir == 0), j + (dir == 1), k + (dir == 2))];
   double fd = 0.5 * (s0 + s1);
   if (scheme == ORC_HYBRID && fd <= K.threshold) {
-    keep_flux(C.c.order, rho, u, v, w, un, p, T, dir, K, F);
+    keep_flux(ord, rho, u, v, w, un, p, T, dir, K, F);
     return;
   }
   double L[5], Rr[5];
   double* arr[5] = {rho, u, v, w, p};
   for (int q = 0; q < 5; ++q) {
-    if (C.c.order == 2) { L[q] = arr[q][0]; Rr[q] = arr[q][1]; }
-    else if (C.c.order == 4) delta4(C.c.tvd, K.threshold, fd, arr[q], L[q], Rr[q]);
+    if (ord == 2) { L[q] = arr[q][0]; Rr[q] = arr[q][1]; }
+    else if (ord == 4) delta4(C.c.tvd, K.threshold, fd, arr[q], L[q], Rr[q]);
     else delta6(C.c.tvd, K.threshold, fd, arr[q], L[q], Rr[q]);
   }
   if (scheme == ORC_SLAU) {
     double HR;
-    if (C.c.order == 2) HR = 1.0;
-    else HR = wiggle(p + (C.c.order == 6 ? 1 : 0));  // p(2:5) for 6th, p(1:4) for 4th
+    if (ord == 2) HR = 1.0;
+    else HR = wiggle(p + (ord == 6 ? 1 : 0));  // p(2:5) for 6th, p(1:4) for 4th
     double un1 = dir == 0 ? L[1] : dir == 1 ? L[2] : L[3];
     double un2 = dir == 0 ? Rr[1] : dir == 1 ? Rr[2] : Rr[3];
     slau_flux(C.c.slau, L[0], Rr[0], L[1], Rr[1], L[2], Rr[2], L[3], Rr[3], un1, un2, L[4], Rr[4],
@@ -594,12 +598,18 @@ void calc_conv(Ctx& C) {
   int io = C.c.order / 2 - 1;
   double F[5];
   int kz0 = C.c.dim == 3 ? 2 : 1, kz1 = C.c.dim == 3 ? nz - 1 : 1;
-  // x faces: i in io+1..nx-(io+1), j 2..ny-1, k 2..nz-1
+  // x faces: i in io+1..nx-(io+1) (interior kernels) or, with a non-periodic x
+  // (bc_x = 1), every face 1..nx-1 with the order lowered next to the boundary;
+  // j 2..ny-1, k 2..nz-1
+  const int ord = C.c.order;
+  const int i0 = C.c.bc_x ? 1 : io + 1, i1 = C.c.bc_x ? nx - 1 : nx - (io + 1);
 #pragma omp parallel for schedule(static) private(F)
   for (int k = kz0; k <= kz1; ++k)
     for (int j = 2; j <= ny - 1; ++j)
-      for (int i = io + 1; i <= nx - (io + 1); ++i) {
-        conv_face(C, 0, i, j, k, F);
+      for (int i = i0; i <= i1; ++i) {
+        int o = ord;
+        if (C.c.bc_x) o = (ord == 6 && 3 <= i && i <= nx - 3) ? 6 : (ord >= 4 && 2 <= i && i <= nx - 2) ? 4 : 2;
+        conv_face(C, 0, i, j, k, F, o);
         if (C.c.dim == 2) F[3] = F[4];  // 2D variables: rho, rho u, rho v, E
         for (int l = 0; l < C.nv; ++l) C.w.E[C.eidx(l + 1, i, j - 1, C.c.dim == 3 ? k - 1 : 1)] = F[l];
       }
@@ -607,7 +617,7 @@ void calc_conv(Ctx& C) {
   for (int k = kz0; k <= kz1; ++k)
     for (int j = io + 1; j <= ny - (io + 1); ++j)
       for (int i = 2; i <= nx - 1; ++i) {
-        conv_face(C, 1, i, j, k, F);
+        conv_face(C, 1, i, j, k, F, ord);
         if (C.c.dim == 2) F[3] = F[4];
         for (int l = 0; l < C.nv; ++l) C.w.F[C.fidx(l + 1, i - 1, j, C.c.dim == 3 ? k - 1 : 1)] = F[l];
       }
@@ -616,7 +626,7 @@ void calc_conv(Ctx& C) {
     for (int k = io + 1; k <= nz - (io + 1); ++k)
       for (int j = 2; j <= ny - 1; ++j)
         for (int i = 2; i <= nx - 1; ++i) {
-          conv_face(C, 2, i, j, k, F);
+          conv_face(C, 2, i, j, k, F, ord);
           for (int l = 0; l < 5; ++l) C.w.G[C.gidx(l + 1, i - 1, j - 1, k)] = F[l];
         }
 }
@@ -1257,11 +1267,14 @@ void fill_ghosts(const Ctx& C, double* Q) {
     t = ((t % N) + N) % N;
     return t + g + 1;
   };
+  // non-periodic x (bc_x = 1): boundary cells 1 and nx take their neighbour's value
+  // (the zero-gradient copy of 2D_solver/ST/set.f90 set_bc); y stays periodic
+  auto xsrc = [&](int i) { return C.c.bc_x ? (i < 2 ? 2 : (i > nx - 1 ? nx - 1 : i)) : wrap(i, g, Nx); };
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
-        int ii = wrap(i, g, Nx), jj = wrap(j, g, Ny);
+        int ii = xsrc(i), jj = wrap(j, g, Ny);
         int kk = C.c.dim == 3 ? wrap(k, g, Nz) : 1;
         if (ii == i && jj == j && kk == k) continue;
         for (int l = 1; l <= nv; ++l) Q[C.qidx(i, l, j, k)] = Q[C.qidx(ii, l, jj, kk)];

@@ -38,7 +38,7 @@ def build(force: bool = False) -> pathlib.Path:
 
 class _Cfg(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("dim", "nx", "ny", "nz", "order", "scheme", "visc", "visc_order",
-                                       "visc_stencil", "tvd", "slau", "rk")] + \
+                                       "visc_stencil", "tvd", "slau", "rk", "bc_x")] + \
                [(n, C.c_double) for n in ("gamma", "R", "Pr", "Prt", "threshold", "dt")]
 
 
@@ -79,6 +79,7 @@ def make_cfg(cfg) -> _Cfg:
     c.tvd = TVD[cfg.tvd]
     c.slau = SLAU_VARIANTS[cfg.slau]
     c.rk = cfg.rk
+    c.bc_x = getattr(cfg, "bc_x", 0)
     c.gamma, c.R, c.Pr, c.Prt, c.threshold, c.dt = cfg.gamma, cfg.R, cfg.Pr, cfg.Prt, cfg.threshold, cfg.dt
     return c
 

@@ -104,6 +104,8 @@ class Case:
         if ic_type == 1:
             glob["uniform"] = {k: glob.pop(k) for k in ("rho0", "u0", "v0", "w0", "p0") if k in glob}
         for key in ("BC_X", "BC_Y", "BC_Z", "RESCALE", "COMMZ"):
+            if key == "BC_X" and case.bc_x:
+                continue  # built: non-periodic x (2D Euler, zero-gradient boundary cells)
             if config.get(key):
                 raise RuntimeError(f"{key}=True needs wall/inflow or multi-rank code paths, which are not built "
                                    "(only fully periodic rectilinear cases)")
@@ -117,7 +119,8 @@ class Case:
             order=int(c["ORDER"]), scheme=c["SCHEME"], visc=c["VISC"], visc_order=int(c.get("VISC_ORDER", 0) or 0),
             visc_stencil=c.get("VISC_STENCIL", "Central"), tvd=c["TVD"], slau=c["SLAU_VARIANT"], rk=int(c["RK"]),
             gamma=p["gamma"], R=p["R"], Pr=p.get("Pr", 0.71), Prt=p.get("Prt", 0.9),
-            threshold=p.get("threshold", 0.4), dt=p["dt"], dx=dx, dy=dy, dz=dz)
+            threshold=p.get("threshold", 0.4), dt=p["dt"], dx=dx, dy=dy, dz=dz,
+            bc_x=1 if c.get("BC_X") else 0)
 
     def _initial(self):
         p = dict(self.globals)

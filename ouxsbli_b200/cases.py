@@ -32,6 +32,8 @@ class CaseDef:
     init: Callable          # (params, xc, yc, zc) -> Q interior-filled
     derived: Callable = None  # (params) -> params with derived quantities (V0, dt, ...)
     doc: str = ""
+    grid: Callable = None     # (params) -> (x, dx, y, dy) for node-based grids; default: periodic cell centres
+    bc_x: bool = False        # the case's x boundaries are non-periodic (BC_X = True)
 
 
 # ---------------------------------------------------------------------------
@@ -187,6 +189,53 @@ def isentropic_vortex(nx: int, ny: int, order: int, L: float, beta: float, mach:
     return Q
 
 
+# ---------------------------------------------------------------------------
+# Inviscid shock tube (Sod): 2D_solver/ST (mod_globals.f90:22-45, set.f90:9-46).
+# x is non-periodic with zero-gradient boundary cells; y is periodic here (the
+# reference's y-wall / symmetry rows leave the 1D flow unchanged).
+# ---------------------------------------------------------------------------
+def _st_derived(p: dict) -> dict:
+    p = dict(p)
+    p["mu0"] = p["C"] * p["T0"] ** 1.5 / (p["T0"] + p["S"])
+    p["p0"] = p["rho0"] * p["R"] * p["T0"]
+    p["rho1"] = 0.125 * p["rho0"]
+    p["p1"] = 0.1 * p["p0"]
+    p["Lx"] = p["Re"] * p["mu0"] / math.sqrt(p["rho0"] * p["p0"])
+    p["Ly"] = 0.1 * p["Lx"]
+    c0 = math.sqrt(p["p0"] / p["rho0"])
+    if p.get("dt") is None:
+        p["dt"] = p["CFL"] * p["Lx"] / (float(p["nx"] - 1) * c0)
+    p["endT"] = 0.2136 * p["Lx"] / c0
+    if p.get("nt") is None:
+        p["nt"] = int(p["endT"] / (float(p["np"]) * p["dt"]))
+    return p
+
+
+def _st_grid(p: dict):
+    """set_grid: nodes x(1) = 0, x(i+1) = x(i) + Lx / (nx-1); same in y."""
+    nx, ny = p["nx"], p["ny"]
+    dx0, dy0 = p["Lx"] / (nx - 1), p["Ly"] / (ny - 1)
+    x = np.zeros(nx)
+    for i in range(nx - 1):
+        x[i + 1] = x[i] + dx0
+    y = np.zeros(ny)
+    for j in range(ny - 1):
+        y[j + 1] = y[j] + dy0
+    return x, np.full(nx - 1, dx0), y, np.full(ny - 1, dy0)
+
+
+def _st_init(p: dict, x, y, z=None) -> np.ndarray:
+    """set_init: the left state in cells 1..nx/2 (1-based), the right state after."""
+    nx, ny, gam = x.size, y.size, p["gamma"]
+    Q = np.zeros((nx, 4, ny), order="F")
+    half = nx // 2
+    Q[:half, 0] = p["rho0"]
+    Q[:half, 3] = p["p0"] / (gam - 1.0)
+    Q[half:, 0] = p["rho1"]
+    Q[half:, 3] = p["p1"] / (gam - 1.0)
+    return Q
+
+
 CASES: dict[str, CaseDef] = {
     "NSTGV": CaseDef(
         "NSTGV", 3,
@@ -214,6 +263,15 @@ CASES: dict[str, CaseDef] = {
              dt=None, nt=None, threshold=0.4),
         _evc_init, _evc_derived,
         "Euler vortex convection (2D_solver/EVC)"),
+    "ST": CaseDef(
+        "ST", 2,
+        dict(VISC="NS", SCHEME="KEEP", ORDER=6, TVD="none", SLAU_VARIANT="HRSLAU2", RK=3,
+             BC_X=True, BC_Y=False, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=4097, ny=257, gamma=1.4, Pr=0.71, Prt=0.9, R=287.03, T0=300.0, C=1.461e-6, S=110.3,
+             Re=25000.0, rho0=1.293, CFL=0.1, np=100, dt=None, nt=None, threshold=0.4),
+        _st_init, _st_derived,
+        "Inviscid shock tube, Sod problem (2D_solver/ST)",
+        grid=_st_grid, bc_x=True),
 }
 
 
@@ -229,10 +287,22 @@ def build_initial(case: CaseDef, params: dict):
         zc, dz = cyclic_axis(p["nz"], p["Lz"], order)
         Q = case.init(p, xc, yc, zc)
     else:
-        xc, dx = cyclic_axis(p["nx"], p["Lx"], order)
-        yc, dy = cyclic_axis(p["ny"], p["Ly"], order)
+        if case.grid is not None:
+            xc, dx, yc, dy = case.grid(p)
+        else:
+            xc, dx = cyclic_axis(p["nx"], p["Lx"], order)
+            yc, dy = cyclic_axis(p["ny"], p["Ly"], order)
         zc, dz = np.zeros(1), None
         Q = case.init(p, xc, yc, None)
+        if case.bc_x:
+            from .grid import fill_periodic
+            g = order // 2
+            # boundary cells copy their neighbour; y ghost rows take the periodic images
+            Q[0], Q[-1] = Q[1], Q[-2]
+            ny = Q.shape[2]
+            N = ny - 2 * g
+            for j in list(range(g)) + list(range(ny - g, ny)):
+                Q[:, :, j] = Q[:, :, g + (j - g) % N]
     return p, xc, yc, zc, dx, dy, dz, Q
 
 

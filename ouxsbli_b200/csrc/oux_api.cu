@@ -46,8 +46,8 @@ int validate(const oux_config* c, std::string& why) {
   if (c->order != 2 && c->order != 4 && c->order != 6) { why = "order must be 2, 4 or 6"; return OUX_E_INVALID; }
   int g = c->order / 2;
   int nzc = c->dim == 3 ? c->nz : 1;
-  if (c->nx < 2 * g + 2 || c->ny < 2 * g + 2 || (c->dim == 3 && c->nz < 2 * g + 2)) {
-    why = "grid too small for the stencil (need at least 2 interior cells per axis)";
+  if (c->nx < 2 * g + 1 || c->ny < 2 * g + 1 || (c->dim == 3 && c->nz < 2 * g + 1) || c->nx < 4) {
+    why = "grid too small for the stencil (need at least 1 interior cell per axis)";
     return OUX_E_INVALID;
   }
   if ((int64_t)c->nx * c->ny * nzc > (int64_t)1 << 34) { why = "grid too large"; return OUX_E_INVALID; }
@@ -58,8 +58,12 @@ int validate(const oux_config* c, std::string& why) {
   if (c->tvd < 0 || c->tvd > 2) { why = "unknown tvd mode"; return OUX_E_INVALID; }
   if (c->slau < 0 || c->slau > 1) { why = "unknown SLAU variant"; return OUX_E_INVALID; }
   if (c->rk != 3 && c->rk != 4) { why = "rk must be 3 or 4"; return OUX_E_INVALID; }
-  if (c->bc_x || c->bc_y || (c->dim == 3 && c->bc_z)) {
-    why = "only periodic boundaries (bc_x = bc_y = bc_z = 0) are built";
+  if (c->bc_y || (c->dim == 3 && c->bc_z) || c->bc_x < 0 || c->bc_x > 1) {
+    why = "boundaries: bc_y = bc_z = 0 (periodic); bc_x = 0 (periodic) or 1 (non-periodic x, 2D Euler)";
+    return OUX_E_INVALID;
+  }
+  if (c->bc_x == 1 && (c->dim != 2 || c->visc != OUX_EULER)) {
+    why = "non-periodic x (bc_x = 1) is built for 2D Euler solves";
     return OUX_E_INVALID;
   }
   if (c->precision != OUX_FP64 && c->precision != OUX_MIXED) { why = "unknown precision"; return OUX_E_INVALID; }
@@ -167,6 +171,8 @@ void build_tables(oux_handle* h) {
 Geo make_geo(const oux_config& c) {
   Geo G;
   G.dim = c.dim; G.nx = c.nx; G.ny = c.ny; G.nz = c.dim == 3 ? c.nz : 1; G.g = c.order / 2;
+  G.bcx = c.bc_x;
+  G.gx = c.bc_x ? 1 : G.g;
   G.sx = round_up(c.nx, 4);
   G.plane = G.sx * c.ny;
   G.vs = round_up(G.plane * G.nz, 32);

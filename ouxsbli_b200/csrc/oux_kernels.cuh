@@ -28,6 +28,7 @@ enum CombineMode {
 
 struct Geo {
   int dim, nx, ny, nz, g;     // padded extents, ghost width
+  int gx, bcx;                // x ghost width of the cell ranges (g, or 1 for a non-periodic x), bc_x
   int64_t sx, plane, vs;      // row stride, plane stride, variable stride (elements)
   __host__ __device__ int64_t at(int i, int j, int k) const { return (int64_t)k * plane + (int64_t)j * sx + i; }
 };
@@ -336,13 +337,13 @@ __host__ __device__ inline int64_t ghost_cells(const Geo& G) {
   const int g = G.g;
   const int Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
   const int gz = (G.dim == 3) ? 2 * g : 0;
-  return (int64_t)gz * G.ny * G.nx + (int64_t)Nz * (2 * g) * G.nx + (int64_t)Nz * Ny * (2 * g);
+  return (int64_t)gz * G.ny * G.nx + (int64_t)Nz * (2 * g) * G.nx + (int64_t)Nz * Ny * (2 * G.gx);
 }
 
 template <class T>
 __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t) {
-  const int g = G.g;
-  const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
+  const int g = G.g, gx = G.gx;
+  const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
   const int gz = (G.dim == 3) ? 2 * g : 0;
   int64_t nA = (int64_t)gz * G.ny * G.nx;            // z ghost planes
   int64_t nB = (int64_t)Nz * (2 * g) * G.nx;         // y ghost rows
@@ -357,10 +358,12 @@ __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t
     j = jj < g ? jj : G.ny - 2 * g + jj;
   } else {
     int64_t s = t - nA - nB;
-    int ii = (int)(s % (2 * g)); int64_t r = s / (2 * g); j = (int)(r % Ny) + g; k = (int)(r / Ny) + zo;
-    i = ii < g ? ii : G.nx - 2 * g + ii;
+    int ii = (int)(s % (2 * gx)); int64_t r = s / (2 * gx); j = (int)(r % Ny) + g; k = (int)(r / Ny) + zo;
+    i = ii < gx ? ii : G.nx - 2 * gx + ii;
   }
-  int si = (i - g + Nx) % Nx + g;
+  // periodic image; with a non-periodic x the boundary cells copy their neighbour
+  // (zero gradient), and ghost rows read the interior value, never another ghost
+  int si = G.bcx ? (i < 1 ? 1 : (i > G.nx - 2 ? G.nx - 2 : i)) : (i - gx + Nx) % Nx + gx;
   int sj = (j - g + Ny) % Ny + g;
   int sk = (G.dim == 3) ? (k - g + Nz) % Nz + g : 0;
   int64_t o = G.at(i, j, k), s = G.at(si, sj, sk);

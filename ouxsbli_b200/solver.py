@@ -33,6 +33,7 @@ class SolverConfig:
     slau: str = "HRSLAU2"          # SLAU_VARIANT
     rk: int = 3
     precision: str = "fp64"        # fp64 | mixed (FP32 stage states/fluxes, FP64 Q^n + accumulation)
+    bc_x: int = 0                  # 0 periodic; 1 non-periodic x (boundary flux kernels, zero-gradient cells; 2D Euler)
     gamma: float = 1.4
     R: float = 287.03
     Pr: float = 0.71
@@ -75,7 +76,8 @@ class SolverConfig:
         c.tvd = _lib.TVD[self.tvd]
         c.slau = _lib.SLAU_VARIANTS[self.slau]
         c.rk = self.rk
-        c.bc_x = c.bc_y = c.bc_z = 0
+        c.bc_x = self.bc_x
+        c.bc_y = c.bc_z = 0
         c.precision = _lib.PRECISION[self.precision]
         c.gamma, c.R, c.Pr, c.Prt, c.threshold, c.dt = (self.gamma, self.R, self.Pr, self.Prt,
                                                          self.threshold, self.dt)

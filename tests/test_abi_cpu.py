@@ -44,7 +44,10 @@ def create(cfg):
 @pytest.mark.parametrize("kw,msg", [
     (dict(order=5), "order"),
     (dict(dim=4), "dim"),
-    (dict(nx=7), "too small"),
+    (dict(nx=6), "too small"),
+    (dict(bc_x=1), "non-periodic x"),
+    (dict(bc_x=2), "boundaries"),
+    (dict(dim=2, nz=1, bc_x=1, visc="NS"), "2D Euler"),
     (dict(rk=2), "rk"),
     (dict(dim=2, nz=1, scheme="Roe"), "Roe"),
     (dict(visc="NS", visc_order=2), "calc_Ev2_in"),

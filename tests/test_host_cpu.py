@@ -166,3 +166,22 @@ class TestGrid:
         assert np.array_equal(q[:, :, 1, :], q[:, :, g + (1 - g) % (11 - 2 * g), :])
         J = jacobian(np.full(9, 0.5), np.full(10, 0.25), np.full(11, 0.1))
         assert J.shape == (10, 11) and np.allclose(J, 1.0 / (0.5 * 0.25 * 0.1))
+
+
+class TestSodExact:
+    def test_star_state_matches_published_values(self):
+        """Sod's problem (rho 1 / 0.125, p 1 / 0.1, gamma 1.4): p* = 0.30313, u* = 0.92745
+        (Toro, Riemann Solvers and Numerical Methods for Fluid Dynamics, Table 4.3)."""
+        from sod_exact import star_state
+        ps, us = star_state(1.0, 0.0, 1.0, 0.125, 0.0, 0.1)
+        assert abs(ps - 0.30313) < 5e-5 and abs(us - 0.92745) < 5e-5
+
+    def test_profile_structure(self):
+        from sod_exact import solve
+        x = np.linspace(0.0, 1.0, 2001)
+        rho, u, p = solve(x, 0.2, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1, x0=0.5)
+        assert rho[0] == 1.0 and rho[-1] == 0.125 and p[0] == 1.0 and p[-1] == 0.1
+        assert np.all(np.diff(p) <= 1e-12)          # pressure falls monotonically
+        assert abs(u.max() - 0.92745) < 5e-5       # the star velocity
+        # mass conservation: integral of rho over [0, 1] equals the initial one
+        assert abs(np.trapezoid(rho, x) - 0.5625) < 2e-3
