@@ -167,6 +167,7 @@ class Case:
         from .output import HistoryWriter, make_1d_for_print, read_restart, ref_diagnostics, write_restart, write_vtr
         from .solver import Solver
         p, xc, yc, zc, dx, dy, dz, Q = self._initial()
+        self.globals_used = p  # the derived parameters of this run (dt, nt, ...)
         dim = self._case.dim
         J = jacobian(dx, dy, dz if dim == 3 else None)
         nv = dim + 2
