@@ -76,7 +76,11 @@ typedef struct oux_config {
   int32_t tvd;          /* enum oux_tvd */
   int32_t slau;         /* enum oux_slau_variant */
   int32_t rk;           /* 3 (TVD-RK3) or 4 (classical RK4) */
-  int32_t bc_x, bc_y, bc_z; /* 0 = periodic (the only boundary built) */
+  int32_t bc_x, bc_y, bc_z; /* 0 = periodic.  bc_x = 1 (2D Euler): non-periodic x -- every x
+                               face with the order lowered next to the boundary, as the
+                               reference's calc_{slau,keep,hybrid}_x boundary kernels do
+                               (2D_solver/src/calc_*_kernel.f90.fypp), and zero-gradient
+                               boundary cells (2D_solver/ST/set.f90 set_bc) */
   int32_t precision;    /* enum oux_precision */
   double gamma, R, Pr, Prt, threshold, dt;
   const double *dx, *dy, *dz; /* host arrays, n-1 entries each (dz unused in 2D) */

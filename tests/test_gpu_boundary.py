@@ -95,3 +95,20 @@ def test_shock_tube_vs_exact_sod(tmp_path, cuda_device):
     l1_rho = np.mean(np.abs(rho_num - rho_ex)) / np.mean(rho_ex)
     l1_p = np.mean(np.abs(p_num - p_ex)) / np.mean(p_ex)
     assert l1_rho < 0.01 and l1_p < 0.01, (l1_rho, l1_p)
+
+
+def test_boundary_mixed_close_to_fp64(cuda_device):
+    """The mixed form with a non-periodic x: smooth flow (KEEP-4, RK4), relative L2
+    against FP64 within the mixed form's bound for switch-free schemes (1e-5)."""
+    import dataclasses
+    cfg, qj = tube(45, 14, order=4, scheme="KEEP", rk=4)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = Solver(dataclasses.replace(cfg, precision=prec), cuda_device)
+        s.set_state(qj)
+        s.step(20)
+        out[prec] = s.get_state()
+        s.close()
+    for l in range(4):
+        a, b = out["mixed"][:, l], out["fp64"][:, l]
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-5, l
