@@ -422,11 +422,9 @@ def main():
     kcnt = (C.c_int64 * 8)()
     _lib.check(_lib.LIB.oux_profile_read(s._h, kms, kcnt, 8))
     _lib.check(_lib.LIB.oux_profile(s._h, 0))
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = cells * args.steps * world / (ms_max / 1e3) / 1e6
+    from ouxsbli_b200.replicas import job_rate, max_over_ranks
+    value, ms_max = job_rate(cells * args.steps, ms, dev)
+    value /= 1e6
     ms_per_step = ms_max / args.steps
 
     # end to end through the public API: every step is an independent job that copies
@@ -469,10 +467,7 @@ def main():
                 stream.wait_event(ev)
             e1.record(stream)
             barrier()
-            te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-            if world > 1:
-                dist.all_reduce(te, op=dist.ReduceOp.MAX)
-            return float(te.item())
+            return max_over_ranks(e0.elapsed_time(e1), dev)
 
         pipelined(NPIPE)  # warm-up
         ms_pipe = timed_multi(pipelined, k_e2e)
@@ -527,9 +522,7 @@ def main():
         _lib.check(_lib.LIB.oux_profile(sm._h, 0))
         mixed_kernels = {kinds[i]: {"launches": int(mkcnt[i]), "avg_ms": mkms[i] / mkcnt[i]}
                          for i in range(8) if mkcnt[i]}
-        tm = torch.tensor([m0.elapsed_time(m1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        tm = torch.tensor([max_over_ranks(m0.elapsed_time(m1), dev)], dtype=torch.float64)
         sm.set_state(qj)
         sm.step(n_err)
         q32 = sm.get_state()
@@ -598,9 +591,10 @@ def main():
             "roofline": roofline, "clocks": clk, "e2e": e2e, "mixed": mixed,
             "gpu_launches": int(round(launches_per_step * args.steps))}
     s.close()
-    if not args.no_ensemble:
+    # the batched-ensemble and serving sections run on rank 0 (their own GPU) only
+    if rank == 0 and not args.no_ensemble:
         line["ensemble2d"] = bench_ensemble(dev, args.ensemble_steps, 1000, 50)
-    if not args.no_serving:
+    if rank == 0 and not args.no_serving:
         line["serving"] = bench_serving(dev, args.serving_requests, args.serving_rate, args.serving_budget_gb)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, qj)
