@@ -79,8 +79,12 @@ typedef struct oux_config {
   int32_t bc_x, bc_y, bc_z; /* 0 = periodic.  bc_x = 1 (2D Euler): non-periodic x -- every x
                                face with the order lowered next to the boundary, as the
                                reference's calc_{slau,keep,hybrid}_x boundary kernels do
-                               (2D_solver/src/calc_*_kernel.f90.fypp), and zero-gradient
-                               boundary cells (2D_solver/ST/set.f90 set_bc) */
+                               (2D_solver/src/calc_*_kernel.f90.fypp), and one boundary
+                               cell on each side, zero-gradient unless oux_set_boundary
+                               gives its face another rule (2D_solver/ST/set.f90 set_bc).
+                               bc_y = 1 (2D Euler, with bc_x = 1): the same for y
+                               (calc_*_y), as the BC_X = BC_Y = True cases build them
+                               (2D_solver/OS).  bc_z must be 0. */
   int32_t precision;    /* enum oux_precision */
   double gamma, R, Pr, Prt, threshold, dt;
   const double *dx, *dy, *dz; /* host arrays, n-1 entries each (dz unused in 2D) */
@@ -129,8 +133,30 @@ int oux_get_state_async(oux_handle* h, double* host_qj, void* stream);
 int oux_pack_state(const oux_handle* h, const double* ref_qj, void* dev_layout_host);
 int oux_unpack_state(const oux_handle* h, const void* dev_layout_host, double* ref_qj);
 
+/* --- boundary cells of non-periodic directions --------------------------- */
+/* Replaces the case's own set_bc subroutine (2D_solver/OS/set.f90:50-90,
+ * 2D_solver/ST/set.f90 set_bc), which the reference compiles into each case.
+ * Faces: x low, x high, y low, y high.  Rules, applied to the one boundary cell of
+ * every row (x faces) or column (y faces) from the adjacent interior cell:
+ *   ZERO_GRADIENT  the neighbour's Q/J (the default of every non-periodic face)
+ *   SLIP_WALL      the neighbour's Q/J with the normal momentum negated
+ *   FIXED          caller values: fixed_dev holds nv x len doubles of Q/J, variable-
+ *                  major ([l * len + pos]; len = ny for x faces, nx for y faces),
+ *                  device memory owned by the caller and read at every fill until
+ *                  the face is set again.  In the mixed form the stage increments
+ *                  of FIXED cells are 0 (Q^n holds the values).
+ * y faces are applied first over every column, then x faces over every row, so a
+ * corner takes its x rule applied to the y-boundary cell next to it (the order of
+ * 2D_solver/OS/set.f90).  The face's direction must be non-periodic.  Set rules
+ * before oux_batch_create when the handle joins a batch. */
+enum oux_face { OUX_FACE_X_LO = 0, OUX_FACE_X_HI = 1, OUX_FACE_Y_LO = 2, OUX_FACE_Y_HI = 3 };
+enum oux_bc_kind { OUX_BC_ZERO_GRADIENT = 0, OUX_BC_SLIP_WALL = 1, OUX_BC_FIXED = 2 };
+int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fixed_dev);
+
 /* --- hot path ----------------------------------------------------------- */
-/* Periodic ghost fill: set_bc_cyclic{2,4,6} (3D_solver/src/set_bc_common.f90:101-273). */
+/* Ghost / boundary-cell fill: periodic images, set_bc_cyclic{2,4,6}
+ * (3D_solver/src/set_bc_common.f90:101-273), and the rules of oux_set_boundary on
+ * non-periodic faces. */
 int oux_fill_ghosts(oux_handle* h, void* stream);
 /* Stage residual R = dt*S*(flux differences) of the current state (coef 1), the
  * quantity calc_R forms (3D_solver/src/calc_steps.f90:8-38) after calc_EFG.

@@ -9,15 +9,17 @@
 // Parity status: the reference is CUDA Fortran with no CPU build and cannot be
 // compiled here (no Fortran compiler, no NVHPC).  This restatement is pinned by
 // the reference's own known-answer tests (ETGV entropy/KE bounds, EVC
-// convergence order) re-run in tests/, not by golden vectors from the
-// reference itself: "parity unpinned" against a run of the reference.
+// convergence order, the ST shock tube against the exact Sod solution, the OS
+// reflected oblique shock against the shock relations) re-run in tests/, not by
+// golden vectors from the reference itself: "parity unpinned" against a run of
+// the reference.
 //
 // Layout follows the reference exactly (Fortran column-major, 1-based indices
 // in the accessors below): QJ(nx,nv,ny,nz) with nv = dim+2, x fastest, then the
 // variable, then y, then z.  Ghost cells are stored (g = order/2 per side).
 //
 // Rounding conventions chosen where the Fortran source leaves them to the
-// compiler (documented in DESIGN.md):
+// compiler:
 //   * SIGN(1,x) follows copysign (a -0.0 argument gives -1).
 //   * MIN(a,b) returns b only when b < a, else a.
 //   * No FMA contraction (build with -ffp-contract=off); operations are
@@ -48,8 +50,12 @@ typedef struct orc_config {
   int tvd;            // ORC_TVD_*
   int slau;           // ORC_SLAU1 / ORC_HRSLAU2
   int rk;             // 3 or 4
-  int bc_x;           // 0 periodic; 1 non-periodic x (boundary flux kernels, zero-gradient boundary cells)
+  int bc_x;           // 0 periodic; 1 non-periodic x (boundary flux kernels, one boundary cell a side)
   double gamma, R, Pr, Prt, threshold, dt;
+  int bc_y;           // 0 periodic; 1 non-periodic y (2D, with bc_x = 1)
+  int bkind[4];       // boundary-cell rule of the faces x lo, x hi, y lo, y hi:
+                      // 0 zero gradient, 1 slip wall, 2 fixed values
+  const double* bfix[4];  // fixed values of Q/J, nv x (ny for x faces, nx for y faces), variable-major
 } orc_config;
 
 }  // extern "C"
@@ -613,11 +619,16 @@ void calc_conv(Ctx& C) {
         if (C.c.dim == 2) F[3] = F[4];  // 2D variables: rho, rho u, rho v, E
         for (int l = 0; l < C.nv; ++l) C.w.E[C.eidx(l + 1, i, j - 1, C.c.dim == 3 ? k - 1 : 1)] = F[l];
       }
+  // y faces: j in io+1..ny-(io+1), or every face 1..ny-1 with a non-periodic y
+  // (calc_*_y, 2D_solver/src/calc_slau_kernel.f90.fypp:116-204); i 2..nx-1
+  const int j0 = C.c.bc_y ? 1 : io + 1, j1 = C.c.bc_y ? ny - 1 : ny - (io + 1);
 #pragma omp parallel for schedule(static) private(F)
   for (int k = kz0; k <= kz1; ++k)
-    for (int j = io + 1; j <= ny - (io + 1); ++j)
+    for (int j = j0; j <= j1; ++j)
       for (int i = 2; i <= nx - 1; ++i) {
-        conv_face(C, 1, i, j, k, F, ord);
+        int o = ord;
+        if (C.c.bc_y) o = (ord == 6 && 3 <= j && j <= ny - 3) ? 6 : (ord >= 4 && 2 <= j && j <= ny - 2) ? 4 : 2;
+        conv_face(C, 1, i, j, k, F, o);
         if (C.c.dim == 2) F[3] = F[4];
         for (int l = 0; l < C.nv; ++l) C.w.F[C.fidx(l + 1, i - 1, j, C.c.dim == 3 ? k - 1 : 1)] = F[l];
       }
@@ -1258,26 +1269,65 @@ void residual(Ctx& C, double coef, std::vector<double>& Rout) {
   }
 }
 
-// ---- periodic ghost fill: set_bc_common.f90 set_bc_cyclic{2,4,6} (3D :101-273, 2D :74-210) ----
+// ---- ghost / boundary-cell fill ----------------------------------------------------
+// Periodic directions: set_bc_common.f90 set_bc_cyclic{2,4,6} (3D :101-273, 2D :74-210).
+// Non-periodic directions (bc_x / bc_y = 1): one boundary cell a side, set from the
+// adjacent interior cell by the face's rule -- what a case's set_bc does
+// (2D_solver/OS/set.f90:50-90: y rows first for every column, then x columns for every
+// row; 2D_solver/ST/set.f90: zero-gradient x).  Rules: 0 copy, 1 copy with the normal
+// momentum negated, 2 the given values.
+void bc_rule(const Ctx& C, int f, int pos, double* v) {  // pos: 1-based j (x faces) / i (y faces)
+  int kind = C.c.bkind[f];
+  if (kind == 1) {
+    int n = f < 2 ? 1 : 2;
+    v[n] = -v[n];
+  } else if (kind == 2) {
+    int len = f < 2 ? C.ny : C.nx;
+    for (int l = 0; l < C.nv; ++l) v[l] = C.c.bfix[f][(size_t)l * len + (pos - 1)];
+  }
+}
+
 void fill_ghosts(const Ctx& C, double* Q) {
   int nx = C.nx, ny = C.ny, nz = C.nz, nv = C.nv, g = C.c.order / 2;
-  int Nx = nx - 2 * g, Ny = ny - 2 * g, Nz = nz - 2 * g;
+  int gx = C.c.bc_x ? 1 : g, gy = C.c.bc_y ? 1 : g;
+  int Nx = nx - 2 * gx, Ny = ny - 2 * gy, Nz = nz - 2 * g;
   auto wrap = [](int i, int g, int N) {  // 1-based padded index -> 1-based interior image
     int t = i - g - 1;
     t = ((t % N) + N) % N;
     return t + g + 1;
   };
-  // non-periodic x (bc_x = 1): boundary cells 1 and nx take their neighbour's value
-  // (the zero-gradient copy of 2D_solver/ST/set.f90 set_bc); y stays periodic
-  auto xsrc = [&](int i) { return C.c.bc_x ? (i < 2 ? 2 : (i > nx - 1 ? nx - 1 : i)) : wrap(i, g, Nx); };
+  // every value comes from interior cells only, so the cells can be set in place in
+  // any order
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
-        int ii = xsrc(i), jj = wrap(j, g, Ny);
+        bool xb = C.c.bc_x && (i == 1 || i == nx), yb = C.c.bc_y && (j == 1 || j == ny);
         int kk = C.c.dim == 3 ? wrap(k, g, Nz) : 1;
-        if (ii == i && jj == j && kk == k) continue;
-        for (int l = 1; l <= nv; ++l) Q[C.qidx(i, l, j, k)] = Q[C.qidx(ii, l, jj, kk)];
+        double v[5];
+        if (!xb && !yb) {
+          int ii = wrap(i, gx, Nx), jj = wrap(j, gy, Ny);
+          if (ii == i && jj == j && kk == k) continue;
+          for (int l = 1; l <= nv; ++l) Q[C.qidx(i, l, j, k)] = Q[C.qidx(ii, l, jj, kk)];
+          continue;
+        } else if (xb) {
+          int in = i == 1 ? 2 : nx - 1;
+          if (yb) {
+            int jn = j == 1 ? 2 : ny - 1;
+            for (int l = 1; l <= nv; ++l) v[l - 1] = Q[C.qidx(in, l, jn, kk)];
+            bc_rule(C, j == 1 ? 2 : 3, in, v);
+          } else {
+            int jj = C.c.bc_y ? j : wrap(j, gy, Ny);
+            for (int l = 1; l <= nv; ++l) v[l - 1] = Q[C.qidx(in, l, jj, kk)];
+          }
+          bc_rule(C, i == 1 ? 0 : 1, j, v);
+        } else {
+          int jn = j == 1 ? 2 : ny - 1;
+          int ii = C.c.bc_x ? i : wrap(i, gx, Nx);
+          for (int l = 1; l <= nv; ++l) v[l - 1] = Q[C.qidx(ii, l, jn, kk)];
+          bc_rule(C, j == 1 ? 2 : 3, i, v);
+        }
+        for (int l = 1; l <= nv; ++l) Q[C.qidx(i, l, j, k)] = v[l - 1];
       }
 }
 

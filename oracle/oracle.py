@@ -39,7 +39,8 @@ def build(force: bool = False) -> pathlib.Path:
 class _Cfg(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("dim", "nx", "ny", "nz", "order", "scheme", "visc", "visc_order",
                                        "visc_stencil", "tvd", "slau", "rk", "bc_x")] + \
-               [(n, C.c_double) for n in ("gamma", "R", "Pr", "Prt", "threshold", "dt")]
+               [(n, C.c_double) for n in ("gamma", "R", "Pr", "Prt", "threshold", "dt")] + \
+               [("bc_y", C.c_int), ("bkind", C.c_int * 4), ("bfix", C.POINTER(C.c_double) * 4)]
 
 
 _lib = None
@@ -80,6 +81,14 @@ def make_cfg(cfg) -> _Cfg:
     c.slau = SLAU_VARIANTS[cfg.slau]
     c.rk = cfg.rk
     c.bc_x = getattr(cfg, "bc_x", 0)
+    c.bc_y = getattr(cfg, "bc_y", 0)
+    c._keep = []
+    rules = cfg.boundary_rules() if hasattr(cfg, "boundary_rules") else []
+    for face, kind, vals in rules:
+        c.bkind[face] = kind
+        if vals is not None:
+            c._keep.append(vals)
+            c.bfix[face] = _ptr(vals)
     c.gamma, c.R, c.Pr, c.Prt, c.threshold, c.dt = cfg.gamma, cfg.R, cfg.Pr, cfg.Prt, cfg.threshold, cfg.dt
     return c
 
@@ -125,6 +134,15 @@ def fields(cfg, qj: np.ndarray) -> dict:
     names = ["rho", "u", "v", "w", "p", "T", "mu", "sensor", "mut", "qc2"]
     shp = (cfg.nx, cfg.ny, cfg.nz) if cfg.dim == 3 else (cfg.nx, cfg.ny)
     return {nm: out[i * n:(i + 1) * n].reshape(shp, order="F") for i, nm in enumerate(names)}
+
+
+def fill_ghosts(cfg, qj: np.ndarray) -> np.ndarray:
+    """A copy of qj with its ghost / boundary cells set (periodic images and the
+    boundary-cell rules of the non-periodic faces)."""
+    q = np.asfortranarray(qj, dtype=np.float64).copy(order="F")
+    c = make_cfg(cfg)
+    assert lib().orc_fill_ghosts(C.byref(c), _ptr(q)) == 0
+    return q
 
 
 def diag_f32(nx, ny, nz, order, gamma, rho, p, vel) -> tuple[float, float]:

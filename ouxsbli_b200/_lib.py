@@ -35,13 +35,15 @@ FAULT_TIMEOUT = 4
 SYMBOLS = [
     "oux_create", "oux_destroy", "oux_last_error", "oux_abi_version", "oux_state_bytes",
     "oux_scratch_bytes", "oux_layout_of", "oux_bind", "oux_set_state", "oux_get_state",
-    "oux_pack_state", "oux_unpack_state", "oux_fill_ghosts", "oux_rhs", "oux_step", "oux_get_state_async",
+    "oux_pack_state", "oux_unpack_state", "oux_set_boundary", "oux_fill_ghosts", "oux_rhs", "oux_step", "oux_get_state_async",
     "oux_diagnostics", "oux_check_state", "oux_status", "oux_profile", "oux_profile_read",
     "oux_host_ref_diagnostics", "oux_launch_count", "oux_rhs_noalloc",
     "oux_batch_create", "oux_batch_workspace_bytes", "oux_batch_bind", "oux_batch_step",
     "oux_batch_status", "oux_batch_info", "oux_batch_destroy",
 ]
 NOALLOC_SCRATCH_BYTES = 32 << 20  # OUX_NOALLOC_SCRATCH_BYTES
+FACES = {"x_lo": 0, "x_hi": 1, "y_lo": 2, "y_hi": 3}                  # enum oux_face
+BC_KINDS = {"zero_gradient": 0, "slip_wall": 1, "fixed": 2}          # enum oux_bc_kind
 
 
 class OuxConfig(C.Structure):
@@ -99,6 +101,7 @@ def _load() -> C.CDLL:
         "oux_get_state_async": (C.c_int, [vp, dp, vp]),
         "oux_pack_state": (C.c_int, [vp, dp, vp]),
         "oux_unpack_state": (C.c_int, [vp, vp, dp]),
+        "oux_set_boundary": (C.c_int, [vp, C.c_int32, C.c_int32, vp]),
         "oux_fill_ghosts": (C.c_int, [vp, vp]),
         "oux_rhs": (C.c_int, [vp, vp, vp]),
         "oux_step": (C.c_int, [vp, i32, vp]),

@@ -34,6 +34,8 @@ class CaseDef:
     doc: str = ""
     grid: Callable = None     # (params) -> (x, dx, y, dy) for node-based grids; default: periodic cell centres
     bc_x: bool = False        # the case's x boundaries are non-periodic (BC_X = True)
+    bc_y: bool = False        # the case's y boundaries are non-periodic (BC_Y = True)
+    boundary: Callable = None  # (params, J) -> rules of the non-periodic faces (SolverConfig.boundary)
 
 
 # ---------------------------------------------------------------------------
@@ -236,6 +238,80 @@ def _st_init(p: dict, x, y, z=None) -> np.ndarray:
     return Q
 
 
+# ---------------------------------------------------------------------------
+# Reflection of an oblique shock from a slip wall: 2D_solver/OS (mod_globals.f90,
+# set.f90).  Supersonic inflow at x low, zero-gradient outflow at x high, a slip wall
+# at y low and, at y high, the free stream up to 0.1 Lx and the state behind an
+# incident shock of angle beta after it (that shock enters the domain there).
+# ---------------------------------------------------------------------------
+def _os_derived(p: dict) -> dict:
+    """The free-stream and post-incident-shock states of mod_globals.f90 (the
+    oblique-shock relations for the angle beta)."""
+    p = dict(p)
+    g, R, M0 = p["gamma"], p["R"], p["M0"]
+    p.setdefault("Lx", 5.0 * p["blt"])
+    p.setdefault("Ly", 2.0 * p["blt"])
+    p["p0"] = p["p_tot"] / ((1.0 + 0.5 * (g - 1.0) * M0 ** 2) ** (g / (g - 1.0)))
+    p["T0"] = p["T_tot"] / (1.0 + 0.5 * (g - 1.0) * M0 ** 2)
+    p["u0"] = M0 * math.sqrt(g * R * p["T0"])
+    p["rho0"] = p["p0"] / (R * p["T0"])
+    beta = p["beta"]
+    Ms = M0 * math.sin(beta)
+    Ms2 = Ms ** 2
+    p["theta"] = math.atan(2.0 * (1.0 / math.tan(beta)) * (Ms2 - 1.0) / (M0 ** 2 * (g + math.cos(2.0 * beta)) + 2.0))
+    p["T2"] = p["T0"] * (1.0 + 2.0 * (g - 1.0) * (Ms2 - 1.0) * (1.0 + g * Ms2) / (Ms2 * (g + 1.0) ** 2))
+    p["p2"] = p["p0"] * (1.0 + 2.0 * g * (Ms2 - 1.0) / (g + 1.0))
+    p["rho2"] = p["p2"] / (R * p["T2"])
+    u1 = p["u0"] * math.sin(beta)
+    a1 = p["u0"] / M0
+    u2 = u1 - 2.0 * a1 * (Ms - 1.0 / Ms) / (g + 1.0)
+    v2 = p["u0"] * math.cos(beta)
+    umag = math.sqrt(u2 ** 2 + v2 ** 2)
+    p["ux"] = umag * math.cos(p["theta"])
+    p["uy"] = -umag * math.sin(p["theta"])
+    if p.get("nt") is None:
+        p["nt"] = int(p["endT"] / (float(p["np"]) * p["dt"]))
+    return p
+
+
+def _os_states(p: dict) -> tuple[np.ndarray, np.ndarray]:
+    """Conservative (rho, rho u, rho v, E) of the free stream and of the post-shock state."""
+    og1 = 1.0 / (p["gamma"] - 1.0)
+    free = np.array([p["rho0"], p["rho0"] * p["u0"], 0.0, p["p0"] * og1 + 0.5 * p["rho0"] * p["u0"] ** 2])
+    r2, ux, uy = p["rho2"], p["ux"], p["uy"]
+    post = np.array([r2, r2 * ux, r2 * uy, p["p2"] * og1 + 0.5 * r2 * (ux ** 2 + uy ** 2)])
+    return free, post
+
+
+def _os_first_post(nx: int) -> int:
+    """0-based first column of the post-shock part of the top row (1-based int(0.1 nx))."""
+    return int(0.1 * nx) - 1
+
+
+def _os_init(p: dict, x, y, z=None) -> np.ndarray:
+    """set_init: the free stream everywhere, the post-shock state on the top row from
+    column int(0.1 nx) (1-based) on."""
+    nx, ny = x.size, y.size
+    free, post = _os_states(p)
+    Q = np.zeros((nx, 4, ny), order="F")
+    Q[:] = free[None, :, None]
+    Q[_os_first_post(nx):, :, ny - 1] = post
+    return Q
+
+
+def _os_boundary(p: dict, J: np.ndarray) -> dict:
+    """set_bc: inflow (fixed free stream) at x low, zero gradient at x high, a slip
+    wall at y low, the fixed top row at y high (values of Q/J)."""
+    nx, ny = J.shape
+    free, post = _os_states(p)
+    top = np.empty((4, nx))
+    top[:] = free[:, None]
+    top[:, _os_first_post(nx):] = post[:, None]
+    top = top * (1.0 / J[0, ny - 2])
+    inflow = free[:, None] * (1.0 / J[0, :])[None, :]
+    return {"x_lo": ("fixed", inflow), "x_hi": "zero_gradient", "y_lo": "slip_wall", "y_hi": ("fixed", top)}
+
+
 CASES: dict[str, CaseDef] = {
     "NSTGV": CaseDef(
         "NSTGV", 3,
@@ -272,6 +348,16 @@ CASES: dict[str, CaseDef] = {
         _st_init, _st_derived,
         "Inviscid shock tube, Sod problem (2D_solver/ST)",
         grid=_st_grid, bc_x=True),
+    "OS": CaseDef(
+        "OS", 2,
+        dict(VISC="Euler", SCHEME="SLAU", ORDER=6, TVD="hybrid", SLAU_VARIANT="HRSLAU2", RK=3,
+             BC_X=True, BC_Y=True, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=257, ny=129, blt=1.0e-3, endT=0.1e-3, np=10, dt=3.0e-9, nt=None, R=287.03, gamma=1.4,
+             Pr=0.72, Prt=0.9, M0=2.0, p_tot=100.0e3, T_tot=295.0, beta=math.pi * 37.2 / 180.0,
+             threshold=0.4),
+        _os_init, _os_derived,
+        "Reflection of an oblique shock from a slip wall (2D_solver/OS)",
+        grid=_st_grid, bc_x=True, bc_y=True, boundary=_os_boundary),
 }
 
 
@@ -294,7 +380,7 @@ def build_initial(case: CaseDef, params: dict):
             yc, dy = cyclic_axis(p["ny"], p["Ly"], order)
         zc, dz = np.zeros(1), None
         Q = case.init(p, xc, yc, None)
-        if case.bc_x:
+        if case.bc_x and not case.bc_y:
             from .grid import fill_periodic
             g = order // 2
             # boundary cells copy their neighbour; y ghost rows take the periodic images

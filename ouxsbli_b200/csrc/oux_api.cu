@@ -58,12 +58,16 @@ int validate(const oux_config* c, std::string& why) {
   if (c->tvd < 0 || c->tvd > 2) { why = "unknown tvd mode"; return OUX_E_INVALID; }
   if (c->slau < 0 || c->slau > 1) { why = "unknown SLAU variant"; return OUX_E_INVALID; }
   if (c->rk != 3 && c->rk != 4) { why = "rk must be 3 or 4"; return OUX_E_INVALID; }
-  if (c->bc_y || (c->dim == 3 && c->bc_z) || c->bc_x < 0 || c->bc_x > 1) {
-    why = "boundaries: bc_y = bc_z = 0 (periodic); bc_x = 0 (periodic) or 1 (non-periodic x, 2D Euler)";
+  if ((c->dim == 3 && c->bc_z) || c->bc_x < 0 || c->bc_x > 1 || c->bc_y < 0 || c->bc_y > 1) {
+    why = "boundaries: bc_z = 0 (periodic); bc_x, bc_y = 0 (periodic) or 1 (non-periodic, 2D Euler)";
     return OUX_E_INVALID;
   }
-  if (c->bc_x == 1 && (c->dim != 2 || c->visc != OUX_EULER)) {
-    why = "non-periodic x (bc_x = 1) is built for 2D Euler solves";
+  if ((c->bc_x == 1 || c->bc_y == 1) && (c->dim != 2 || c->visc != OUX_EULER)) {
+    why = "non-periodic x / y (bc_x = 1, bc_y = 1) is built for 2D Euler solves";
+    return OUX_E_INVALID;
+  }
+  if (c->bc_y == 1 && (c->bc_x != 1 || c->ny < 4)) {
+    why = "non-periodic y (bc_y = 1) needs a non-periodic x (bc_x = 1) and ny >= 4";
     return OUX_E_INVALID;
   }
   if (c->precision != OUX_FP64 && c->precision != OUX_MIXED) { why = "unknown precision"; return OUX_E_INVALID; }
@@ -173,6 +177,10 @@ Geo make_geo(const oux_config& c) {
   G.dim = c.dim; G.nx = c.nx; G.ny = c.ny; G.nz = c.dim == 3 ? c.nz : 1; G.g = c.order / 2;
   G.bcx = c.bc_x;
   G.gx = c.bc_x ? 1 : G.g;
+  G.bcy = c.bc_y;
+  G.gy = c.bc_y ? 1 : G.g;
+  G.bkind = 0;  // zero-gradient boundary cells until oux_set_boundary says otherwise
+  for (int f = 0; f < 4; ++f) G.bfix[f] = nullptr;
   G.sx = round_up(c.nx, 4);
   G.plane = G.sx * c.ny;
   G.vs = round_up(G.plane * G.nz, 32);
@@ -321,13 +329,13 @@ __global__ void k_diag_final(const double* partials, int nb, double inv_n, doubl
 __global__ void k_check(const double* __restrict__ Q, Geo G, const double* __restrict__ jac, double gamma_1,
                         int* status) {
   const int g = G.g;
-  const int Nx = G.nx - 2 * g, Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
+  const int Nx = G.nx - 2 * G.gx, Ny = G.ny - 2 * G.gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
   int64_t n = (int64_t)Nx * Ny * Nz;
   int bits = 0;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-    int i = (int)(t % Nx) + g;
+    int i = (int)(t % Nx) + G.gx;
     int64_t r = t / Nx;
-    int j = (int)(r % Ny) + g;
+    int j = (int)(r % Ny) + G.gy;
     int k = (G.dim == 3) ? (int)(r / Ny) + g : 0;
     int64_t o = G.at(i, j, k);
     double Jv = jac[(int64_t)j * G.nx + i];
@@ -811,6 +819,20 @@ int oux_fill_ghosts(oux_handle* h, void* stream) {
   if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
   ghost<double>(h, h->Q, (cudaStream_t)stream);
   OUX_CUDA(cudaGetLastError());
+  return OUX_OK;
+}
+
+int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fixed_dev) {
+  if (!h) return fail(OUX_E_INVALID, "null handle");
+  if (face < 0 || face > 3) return fail(OUX_E_INVALID, "face must be 0..3 (x low, x high, y low, y high)");
+  if (kind < OUX_BC_ZERO_GRADIENT || kind > OUX_BC_FIXED) return fail(OUX_E_INVALID, "unknown boundary rule");
+  if (!(face < 2 ? h->G.bcx : h->G.bcy))
+    return fail(OUX_E_INVALID, "the face's direction is periodic (set bc_x / bc_y = 1)");
+  if (kind == OUX_BC_FIXED && !fixed_dev) return fail(OUX_E_INVALID, "a fixed rule needs its device values");
+  if (kind == OUX_BC_FIXED && (reinterpret_cast<uintptr_t>(fixed_dev) & 7))
+    return fail(OUX_E_INVALID, "fixed values must be 8-byte aligned");
+  h->G.bkind = (h->G.bkind & ~(15 << (4 * face))) | (kind << (4 * face));
+  h->G.bfix[face] = kind == OUX_BC_FIXED ? fixed_dev : nullptr;
   return OUX_OK;
 }
 

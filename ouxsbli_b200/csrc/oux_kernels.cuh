@@ -29,7 +29,11 @@ enum CombineMode {
 struct Geo {
   int dim, nx, ny, nz, g;     // padded extents, ghost width
   int gx, bcx;                // x ghost width of the cell ranges (g, or 1 for a non-periodic x), bc_x
+  int gy, bcy;                // the same for y
+  int bkind;                  // boundary-cell rule of face f (enum oux_bc_kind) in bits 4f..4f+3;
+                              // faces 0..3: x low, x high, y low, y high
   int64_t sx, plane, vs;      // row stride, plane stride, variable stride (elements)
+  const double* bfix[4];      // OUX_BC_FIXED faces: nv x (ny for x faces, nx for y faces) values of Q/J
   __host__ __device__ int64_t at(int i, int j, int k) const { return (int64_t)k * plane + (int64_t)j * sx + i; }
 };
 
@@ -327,26 +331,49 @@ __global__ void k_mut_edges(Geo G, Fields<T> W) {
     mut_edge_cell<T>(G, W, t);
 }
 
-// ---- periodic ghost fill: set_bc_cyclic{2,4,6} (set_bc_common.f90:101-273) ---
-// Every ghost cell takes its interior image; the three groups enumerate
-// z-ghost planes, y-ghost rows of interior planes and x-ghost cells of
-// interior rows without touching interior cells.
-// Number of ghost cells the fill enumerates (x-ghosts of interior rows, y-ghost
-// rows of interior planes, whole z-ghost planes).
+// ---- ghost / boundary-cell fill ------------------------------------------------
+// Periodic directions: every ghost cell takes its interior image (set_bc_cyclic{2,4,6},
+// set_bc_common.f90:101-273).  Non-periodic directions (2D): one boundary cell on
+// each side, set by the face's rule from the adjacent interior cell -- the roles of a
+// case's set_bc (2D_solver/ST/set.f90, 2D_solver/OS/set.f90:50-90):
+//   OUX_BC_ZERO_GRADIENT  copy of the neighbour
+//   OUX_BC_SLIP_WALL      copy with the normal momentum negated
+//   OUX_BC_FIXED          caller-given Q/J values (stage increments of the mixed form: 0)
+// With both x and y non-periodic the y faces are set first for every column and the
+// x faces after them for every row (2D_solver/OS/set.f90 order), so a corner takes
+// its x rule applied to the y-boundary value next to it.  Every value is computed
+// from interior cells only, so the cells can be filled in any order.
+// The three groups enumerate z-ghost planes, y-ghost rows of interior planes and
+// x-ghost cells of interior rows without touching interior cells.
 __host__ __device__ inline int64_t ghost_cells(const Geo& G) {
-  const int g = G.g;
-  const int Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
+  const int g = G.g, gy = G.gy;
+  const int Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
   const int gz = (G.dim == 3) ? 2 * g : 0;
-  return (int64_t)gz * G.ny * G.nx + (int64_t)Nz * (2 * g) * G.nx + (int64_t)Nz * Ny * (2 * G.gx);
+  return (int64_t)gz * G.ny * G.nx + (int64_t)Nz * (2 * gy) * G.nx + (int64_t)Nz * Ny * (2 * G.gx);
+}
+
+// Apply face f's rule to the neighbour values v (in place); pos: position along the
+// face (j for x faces, i for y faces).  INCR: v are mixed-form stage increments.
+template <class T, bool INCR>
+__device__ __forceinline__ void bc_rule(const Geo& G, int f, int pos, int nv, T (&v)[5]) {
+  const int kind = (G.bkind >> (4 * f)) & 15;
+  if (kind == 1) {  // slip wall: normal momentum (rho u for x faces, rho v for y faces) negated
+    const int n = f < 2 ? 1 : 2;
+    v[n] = -v[n];
+  } else if (kind == 2) {  // fixed
+    const int len = f < 2 ? G.ny : G.nx;
+    for (int l = 0; l < nv; ++l) v[l] = INCR ? T(0) : (T)G.bfix[f][(int64_t)l * len + pos];
+  }
 }
 
 template <class T>
 __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t) {
-  const int g = G.g, gx = G.gx;
-  const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * g, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
+  constexpr bool INCR = sizeof(T) < sizeof(double);  // mixed form: Q holds stage increments
+  const int g = G.g, gx = G.gx, gy = G.gy;
+  const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
   const int gz = (G.dim == 3) ? 2 * g : 0;
   int64_t nA = (int64_t)gz * G.ny * G.nx;            // z ghost planes
-  int64_t nB = (int64_t)Nz * (2 * g) * G.nx;         // y ghost rows
+  int64_t nB = (int64_t)Nz * (2 * gy) * G.nx;        // y ghost rows
   int zo = (G.dim == 3) ? g : 0;
   int i, j, k;
   if (t < nA) {
@@ -354,20 +381,50 @@ __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t
     k = kk < g ? kk : G.nz - 2 * g + kk;
   } else if (t < nA + nB) {
     int64_t s = t - nA;
-    i = (int)(s % G.nx); int64_t r = s / G.nx; int jj = (int)(r % (2 * g)); k = (int)(r / (2 * g)) + zo;
-    j = jj < g ? jj : G.ny - 2 * g + jj;
+    i = (int)(s % G.nx); int64_t r = s / G.nx; int jj = (int)(r % (2 * gy)); k = (int)(r / (2 * gy)) + zo;
+    j = jj < gy ? jj : G.ny - 2 * gy + jj;
   } else {
     int64_t s = t - nA - nB;
-    int ii = (int)(s % (2 * gx)); int64_t r = s / (2 * gx); j = (int)(r % Ny) + g; k = (int)(r / Ny) + zo;
+    int ii = (int)(s % (2 * gx)); int64_t r = s / (2 * gx); j = (int)(r % Ny) + gy; k = (int)(r / Ny) + zo;
     i = ii < gx ? ii : G.nx - 2 * gx + ii;
   }
-  // periodic image; with a non-periodic x the boundary cells copy their neighbour
-  // (zero gradient), and ghost rows read the interior value, never another ghost
-  int si = G.bcx ? (i < 1 ? 1 : (i > G.nx - 2 ? G.nx - 2 : i)) : (i - gx + Nx) % Nx + gx;
-  int sj = (j - g + Ny) % Ny + g;
-  int sk = (G.dim == 3) ? (k - g + Nz) % Nz + g : 0;
-  int64_t o = G.at(i, j, k), s = G.at(si, sj, sk);
-  for (int l = 0; l < nv; ++l) Q[o + l * G.vs] = Q[s + l * G.vs];
+  const int64_t o = G.at(i, j, k);
+  const bool xb = G.bcx && (i == 0 || i == G.nx - 1);  // x boundary cell
+  const bool yb = G.bcy && (j == 0 || j == G.ny - 1);  // y boundary cell
+  if (!xb && !yb) {  // periodic images only
+    int si = (i - gx + Nx) % Nx + gx;
+    int sj = (j - gy + Ny) % Ny + gy;
+    int sk = (G.dim == 3) ? (k - g + Nz) % Nz + g : 0;
+    int64_t s = G.at(si, sj, sk);
+    for (int l = 0; l < nv; ++l) Q[o + l * G.vs] = Q[s + l * G.vs];
+    return;
+  }
+  T v[5];
+  const int sk = (G.dim == 3) ? (k - g + Nz) % Nz + g : 0;
+  if (xb) {
+    // x face: the neighbour column's value in this row -- a periodic image of an
+    // interior row, or (non-periodic y) that column's y-boundary value
+    const int fx = i == 0 ? 0 : 1, in = i == 0 ? 1 : G.nx - 2;
+    if (G.bcy && (j == 0 || j == G.ny - 1)) {
+      const int fy = j == 0 ? 2 : 3, jn = j == 0 ? 1 : G.ny - 2;
+      const int64_t s = G.at(in, jn, sk);
+      for (int l = 0; l < nv; ++l) v[l] = Q[s + l * G.vs];
+      bc_rule<T, INCR>(G, fy, in, nv, v);
+    } else {
+      const int sj = G.bcy ? j : (j - gy + Ny) % Ny + gy;
+      const int64_t s = G.at(in, sj, sk);
+      for (int l = 0; l < nv; ++l) v[l] = Q[s + l * G.vs];
+    }
+    bc_rule<T, INCR>(G, fx, j, nv, v);
+  } else {
+    // y face of an interior column (or a periodic-x ghost column's image)
+    const int fy = j == 0 ? 2 : 3, jn = j == 0 ? 1 : G.ny - 2;
+    const int si = G.bcx ? i : (i - gx + Nx) % Nx + gx;
+    const int64_t s = G.at(si, jn, sk);
+    for (int l = 0; l < nv; ++l) v[l] = Q[s + l * G.vs];
+    bc_rule<T, INCR>(G, fy, i, nv, v);
+  }
+  for (int l = 0; l < nv; ++l) Q[o + l * G.vs] = v[l];
 }
 
 template <class T>

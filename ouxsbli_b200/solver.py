@@ -33,7 +33,12 @@ class SolverConfig:
     slau: str = "HRSLAU2"          # SLAU_VARIANT
     rk: int = 3
     precision: str = "fp64"        # fp64 | mixed (FP32 stage states/fluxes, FP64 Q^n + accumulation)
-    bc_x: int = 0                  # 0 periodic; 1 non-periodic x (boundary flux kernels, zero-gradient cells; 2D Euler)
+    bc_x: int = 0                  # 0 periodic; 1 non-periodic x (boundary flux kernels, boundary cells; 2D Euler)
+    bc_y: int = 0                  # the same for y (2D Euler, with bc_x = 1)
+    # rules of the non-periodic faces ("x_lo", "x_hi", "y_lo", "y_hi"): "zero_gradient"
+    # (the default), "slip_wall" or ("fixed", values (nv, ny) for x faces / (nv, nx) for
+    # y faces, of Q/J)
+    boundary: dict = field(default=None, repr=False)
     gamma: float = 1.4
     R: float = 287.03
     Pr: float = 0.71
@@ -54,8 +59,27 @@ class SolverConfig:
 
     def interior_cells(self) -> int:
         g = self.g
-        n = (self.nx - 2 * g) * (self.ny - 2 * g)
+        gx, gy = (1 if self.bc_x else g), (1 if self.bc_y else g)
+        n = (self.nx - 2 * gx) * (self.ny - 2 * gy)
         return n * (self.nz - 2 * g if self.dim == 3 else 1)
+
+    def boundary_rules(self) -> list[tuple[int, int, np.ndarray | None]]:
+        """(face, kind, fixed values as a C-contiguous (nv, len) array or None) per given face."""
+        out = []
+        for name, rule in (self.boundary or {}).items():
+            face = _lib.FACES[name]
+            if isinstance(rule, str):
+                out.append((face, _lib.BC_KINDS[rule], None))
+                continue
+            kind, vals = rule
+            if kind != "fixed":
+                raise ValueError(f"unknown boundary rule {rule!r}")
+            n = self.ny if face < 2 else self.nx
+            v = np.ascontiguousarray(vals, dtype=np.float64)
+            if v.shape != (self.nv, n):
+                raise ValueError(f"fixed values of face {name} must have shape {(self.nv, n)}, got {v.shape}")
+            out.append((face, _lib.BC_KINDS["fixed"], v))
+        return out
 
     def to_c(self) -> tuple[OuxConfig, list]:
         keep = []
@@ -77,7 +101,8 @@ class SolverConfig:
         c.slau = _lib.SLAU_VARIANTS[self.slau]
         c.rk = self.rk
         c.bc_x = self.bc_x
-        c.bc_y = c.bc_z = 0
+        c.bc_y = self.bc_y
+        c.bc_z = 0
         c.precision = _lib.PRECISION[self.precision]
         c.gamma, c.R, c.Pr, c.Prt, c.threshold, c.dt = (self.gamma, self.R, self.Pr, self.Prt,
                                                          self.threshold, self.dt)
@@ -115,6 +140,14 @@ class Solver:
         lay = _lib.OuxLayout()
         check(LIB.oux_layout_of(self._h, C.byref(lay)))
         self.layout = lay
+        self._bfix = {}  # device copies of fixed boundary values (the library reads them every fill)
+        for face, kind, vals in cfg.boundary_rules():
+            ptr = None
+            if vals is not None:
+                t = torch.from_numpy(vals.ravel()).to(self.device)
+                self._bfix[face] = t
+                ptr = C.c_void_p(t.data_ptr())
+            check(LIB.oux_set_boundary(self._h, face, kind, ptr))
 
     # -- lifetime --
     def close(self) -> None:

@@ -1,13 +1,16 @@
-"""Non-periodic x (bc_x = 1, 2D Euler) on the GPU.
+"""Non-periodic x and y (bc_x = 1, bc_y = 1, 2D Euler) on the GPU.
 
 * Parity: the boundary flux faces with the reference's order fallback
-  (2D_solver/src/calc_{slau,keep,hybrid}_kernel.f90.fypp) and the zero-gradient
-  boundary cells, against the oracle's restatement: bit-identical states and
-  stage residuals (FP64, no FMA contraction on either side).
-* Known answer (ouxsbli/tests/test_st.py:15-71): the inviscid shock tube through
+  (2D_solver/src/calc_{slau,keep,hybrid}_kernel.f90.fypp, calc_*_x / calc_*_y) and
+  the boundary-cell rules (zero gradient, slip wall, fixed values), against the
+  oracle's restatement: bit-identical states and stage residuals (FP64, no FMA
+  contraction on either side).
+* Known answers: the inviscid shock tube (ouxsbli/tests/test_st.py:15-71) through
   the Case API with the reference test's settings (SLAU, TVD hybrid, 6th order,
   TVD-RK3, nx 513, ny 7, one output interval) against the exact Sod solution:
-  relative L1 error of density and pressure < 1 %.
+  relative L1 error of density and pressure < 1 %; the oblique shock reflected
+  from a slip wall (ouxsbli/tests/test_os.py) with that test's settings against
+  the shock relations: pre-shock and post-reflection means within 3 %.
 """
 import math
 
@@ -112,3 +115,131 @@ def test_boundary_mixed_close_to_fp64(cuda_device):
     for l in range(4):
         a, b = out["mixed"][:, l], out["fp64"][:, l]
         assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-5, l
+
+
+def duct(nx, ny, order, rules, **kw):
+    """A smooth supersonic field on a box non-periodic in x and y, with boundary rules."""
+    L = 1.0
+    dx = np.full(nx - 1, L / (nx - 1))
+    dy = np.full(ny - 1, 0.6 * L / (ny - 1))
+    x = np.concatenate([[0.0], np.cumsum(dx)])
+    y = np.concatenate([[0.0], np.cumsum(dy)])
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    gam = 1.4
+    rho = 1.0 + 0.2 * np.sin(2 * math.pi * X) * np.cos(math.pi * Y)
+    u = 1.8 + 0.1 * np.cos(2 * math.pi * Y)
+    v = 0.1 * np.sin(2 * math.pi * X) * np.sin(math.pi * Y / 0.6)
+    p = 1.0 / gam + 0.1 * np.cos(2 * math.pi * (X - Y))
+    Q = np.zeros((nx, 4, ny), order="F")
+    Q[:, 0], Q[:, 1], Q[:, 2] = rho, rho * u, rho * v
+    Q[:, 3] = p / (gam - 1.0) + 0.5 * rho * (u * u + v * v)
+    J = jacobian(dx, dy, None)
+    qj = to_qj(Q, J)
+    bnd = {}
+    for face, kind in rules.items():
+        if kind == "fixed":
+            if face.startswith("x"):
+                bnd[face] = ("fixed", np.ascontiguousarray(qj[0 if face == "x_lo" else -1, :, :]))
+            else:
+                bnd[face] = ("fixed", np.ascontiguousarray(qj[:, :, 0 if face == "y_lo" else -1].T))
+        else:
+            bnd[face] = kind
+    dt = 0.3 * dx[0] / (2.0 + math.sqrt(gam * 1.2))
+    cfg = SolverConfig(dim=2, nx=nx, ny=ny, nz=1, order=order, visc="Euler", bc_x=1, bc_y=1, dt=dt, gamma=gam,
+                       R=1.0, dx=dx, dy=dy, dz=None, boundary=bnd, **kw)
+    return cfg, qj
+
+
+OS_RULES = {"x_lo": "fixed", "x_hi": "zero_gradient", "y_lo": "slip_wall", "y_hi": "fixed"}
+WALLS = {"x_lo": "slip_wall", "x_hi": "slip_wall", "y_lo": "slip_wall", "y_hi": "zero_gradient"}
+DUCT_CASES = [
+    ("os_slau6_hybrid_rk3", OS_RULES, dict(order=6, scheme="SLAU", tvd="hybrid", slau="HRSLAU2", rk=3)),
+    ("os_hybrid6_rk3", OS_RULES, dict(order=6, scheme="Hybrid", tvd="hybrid", rk=3)),
+    ("walls_keep6_rk4", WALLS, dict(order=6, scheme="KEEP", rk=4)),
+    ("walls_slau4_tvd_rk3", WALLS, dict(order=4, scheme="SLAU", tvd="tvd", slau="SLAU", rk=3)),
+    ("os_keep4_rk4", OS_RULES, dict(order=4, scheme="KEEP", rk=4)),
+    ("os_slau2_rk3", OS_RULES, dict(order=2, scheme="SLAU", rk=3)),
+]
+
+
+@pytest.mark.parametrize("name,rules,kw", DUCT_CASES, ids=[c[0] for c in DUCT_CASES])
+def test_xy_boundaries_bitexact_vs_oracle(name, rules, kw, cuda_device):
+    cfg, qj = duct(41, 23, rules=rules, **kw)
+    s = Solver(cfg, cuda_device)
+    s.set_state(qj)
+    r_gpu = s.rhs()
+    s.step(6)
+    q_gpu = s.get_state()
+    s.close()
+    np.testing.assert_array_equal(r_gpu, oracle.rhs(cfg, qj))
+    np.testing.assert_array_equal(q_gpu, oracle.step(cfg, qj, 6))
+
+
+def test_xy_fill_matches_oracle(cuda_device):
+    """oux_fill_ghosts with the OS rule set: every boundary cell, corners included."""
+    cfg, qj = duct(33, 17, order=6, rules=OS_RULES, scheme="SLAU")
+    rng = np.random.default_rng(5)
+    q = np.asfortranarray(qj * (1.0 + 0.01 * rng.standard_normal(qj.shape)))
+    s = Solver(cfg, cuda_device)
+    s.set_state(q)
+    s.fill_ghosts()
+    out = s.get_state()
+    s.close()
+    np.testing.assert_array_equal(out, oracle.fill_ghosts(cfg, q))
+
+
+def test_xy_mixed_close_to_fp64(cuda_device):
+    """The mixed form with non-periodic x and y (KEEP-4, RK4, walls and fixed faces):
+    relative L2 against FP64 within the mixed form's bound for switch-free schemes."""
+    import dataclasses
+    cfg, qj = duct(41, 23, order=4, rules=OS_RULES, scheme="KEEP", rk=4)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = Solver(dataclasses.replace(cfg, precision=prec), cuda_device)
+        s.set_state(qj)
+        s.step(20)
+        out[prec] = s.get_state()
+        s.close()
+    for l in range(4):
+        a, b = out["mixed"][:, l], out["fp64"][:, l]
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-5, l
+
+
+def test_reflected_oblique_shock_vs_shock_relations(tmp_path, cuda_device):
+    """ouxsbli/tests/test_os.py with its settings: M0 2, p_tot 100 kPa, T_tot 295 K,
+    incident shock 37.2 deg, 257 x 129 nodes on 5 x 2 mm, dt 3 ns, 0.1 ms in one
+    output interval.  Pre-shock region (left 10 %, upper half) against the free
+    stream, post-reflection region (right 10 %, lower third) against the state
+    behind the reflected shock; each mean within 3 %, and |v| / u3 < 3 %."""
+    import oblique_shock as osk
+    from ouxsbli_b200 import Case
+    from ouxsbli_b200.output import read_vtr
+    wd = tmp_path / "os"
+    R, gamma, M0, p_tot, T_tot = 287.03, 1.4, 2.0, 100.0e3, 295.0
+    beta, dt, endT = math.pi * 37.2 / 180.0, 3.0e-9, 0.1e-3
+    case = Case(source="2D_solver/OS", workdir=str(wd), scheme="slau", accuracy=6, visc="euler", tvd="hybrid",
+                nx=257, ny=129, Lx=5.0e-3, Ly=2.0e-3, gamma=gamma, Pr=0.72, R=R, M0=M0, p_tot=p_tot, T_tot=T_tot,
+                beta=beta, dt=dt, np=1, nt=int(endT / dt))
+    case.build()
+    case.run(nranks=2, device=cuda_device)
+    x, y, z, f = read_vtr(sorted((wd / "data").glob("Q*.vtr"))[-1])
+    ni, nj = x.size, y.size
+    rho = f["rho"].reshape(nj, ni).astype(float)
+    p = f["p"].reshape(nj, ni).astype(float)
+    vel = f["velocity"].reshape(nj, ni, 3).astype(float)
+    u, v = vel[..., 0], vel[..., 1]
+    rho1, u1, p1 = osk.free_stream(M0, p_tot, T_tot, gamma, R)
+    rho3, ux3, _, p3, _ = osk.reflected_state(M0, p_tot, T_tot, beta, gamma, R)
+    pre = (slice(nj // 2, None), slice(None, ni // 10))
+    post = (slice(None, nj // 3), slice(9 * ni // 10, None))
+
+    def close(a, b, label):
+        assert abs(a - b) / abs(b) < 0.03, (label, a, b)
+
+    close(rho[pre].mean(), rho1, "pre rho")
+    close(u[pre].mean(), u1, "pre u")
+    close(p[pre].mean(), p1, "pre p")
+    close(rho[post].mean(), rho3, "post rho")
+    close(u[post].mean(), ux3, "post u")
+    close(p[post].mean(), p3, "post p")
+    assert abs(v[post].mean()) / ux3 < 0.03, v[post].mean()

@@ -185,3 +185,54 @@ class TestSodExact:
         assert abs(u.max() - 0.92745) < 5e-5       # the star velocity
         # mass conservation: integral of rho over [0, 1] equals the initial one
         assert abs(np.trapezoid(rho, x) - 0.5625) < 2e-3
+
+
+class TestObliqueShock:
+    def test_weak_angles_of_the_reflection_case(self):
+        """M = 2, theta = 8 deg: weak incident angle 37.2 deg; the reflected shock at the
+        downstream Mach number turns the flow back at 44.1 deg (the angles the
+        reference's reflected-shock case and its test use)."""
+        import math
+        from oblique_shock import deflection, free_stream, shock, weak_beta
+        b = weak_beta(2.0, math.radians(8.0))
+        assert abs(math.degrees(b) - 37.21) < 0.01
+        assert abs(math.degrees(deflection(2.0, b)) - 8.0) < 1e-9
+        rho1, U1, p1 = free_stream(2.0, 100e3, 295.0, 1.4, 287.03)
+        rho2, U2, p2, th = shock(rho1, U1, p1, math.radians(37.2), 1.4)
+        M2 = U2 / math.sqrt(1.4 * p2 / rho2)
+        assert abs(math.degrees(weak_beta(M2, th)) - 44.1) < 0.1
+
+    def test_normal_shock_table_values(self):
+        """Normal shock at Mn = 2 (NACA 1135 table): p2/p1 = 4.5, rho2/rho1 = 2.6667, Mn2 = 0.5774."""
+        from oblique_shock import normal_jump
+        pr, rr, mn2 = normal_jump(2.0)
+        assert abs(pr - 4.5) < 1e-12 and abs(rr - 8.0 / 3.0) < 1e-12 and abs(mn2 - 0.57735) < 1e-5
+
+
+class TestBoundaryRules:
+    """The oracle's boundary-cell fill for non-periodic x and y (the OS rule set)."""
+
+    def test_rules_and_corners(self):
+        from oracle import oracle
+        from ouxsbli_b200.solver import SolverConfig
+        nx, ny = 9, 7
+        rng = np.random.default_rng(3)
+        q = np.asfortranarray(rng.uniform(1.0, 2.0, (nx, 4, ny)))
+        top = rng.uniform(3.0, 4.0, (4, nx))
+        inflow = rng.uniform(5.0, 6.0, (4, ny))
+        cfg = SolverConfig(dim=2, nx=nx, ny=ny, nz=1, order=6, visc="Euler", bc_x=1, bc_y=1,
+                           dx=np.ones(nx - 1), dy=np.ones(ny - 1), dz=None,
+                           boundary={"x_lo": ("fixed", inflow), "x_hi": "zero_gradient",
+                                     "y_lo": "slip_wall", "y_hi": ("fixed", top)})
+        out = oracle.fill_ghosts(cfg, q)
+        np.testing.assert_array_equal(out[1:-1, :, 1:-1], q[1:-1, :, 1:-1])   # interior untouched
+        for i in range(1, nx - 1):
+            np.testing.assert_array_equal(out[i, :, -1], top[:, i])
+            np.testing.assert_array_equal(out[i, :, 0], q[i, :, 1] * np.array([1, 1, -1, 1]))
+        for j in range(ny):
+            np.testing.assert_array_equal(out[0, :, j], inflow[:, j])
+        for j in range(1, ny - 1):
+            np.testing.assert_array_equal(out[-1, :, j], q[-2, :, j])
+        # corners at x high: the zero-gradient copy of the y-boundary cell beside them
+        np.testing.assert_array_equal(out[-1, :, 0], q[-2, :, 1] * np.array([1, 1, -1, 1]))
+        np.testing.assert_array_equal(out[-1, :, -1], top[:, -2])
