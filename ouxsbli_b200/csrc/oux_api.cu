@@ -497,12 +497,15 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   return OUX_OK;
 }
 
+// Ghost / boundary fill of a full FP64 state, or (T = float) of the mixed form's
+// stage increments over h->Q.
 template <class T>
 int ghost(oux_handle* h, T* Q, cudaStream_t s) {
   const Geo& G = h->G;
   int64_t n = (int64_t)G.nx * G.ny * G.nz;
   Timed tm(h, KK_GHOST, s);
-  k_ghost<T><<<grid_for(n / 4 + 1, 256), 256, 0, s>>>(Q, G, h->nv);
+  const double* Qn = sizeof(T) < sizeof(double) ? h->Q : nullptr;
+  k_ghost<T><<<grid_for(n / 4 + 1, 256), 256, 0, s>>>(Q, G, h->nv, Qn);
   h->launches++;
   return OUX_OK;
 }

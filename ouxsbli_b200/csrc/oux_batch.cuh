@@ -226,7 +226,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, batch_minb(DIM)) k_batch_step(B
       case PH_GHOST_QN: {
         const int64_t c1 = batch_end(c0, bi.count, B.chunk, ghost_cells(G));
         if (ph.kind == PH_GHOST_QS) {
-          for (int64_t t = c0 + tid; t < c1; t += BATCH_THREADS) ghost_cell<T>(A.Qs, G, DIM + 2, t);
+          for (int64_t t = c0 + tid; t < c1; t += BATCH_THREADS)
+            ghost_cell<T>(A.Qs, G, DIM + 2, t, sizeof(T) < sizeof(double) ? A.Qn : nullptr);
         } else {
           for (int64_t t = c0 + tid; t < c1; t += BATCH_THREADS) ghost_cell<double>(A.Qn, G, DIM + 2, t);
         }

@@ -352,23 +352,24 @@ __host__ __device__ inline int64_t ghost_cells(const Geo& G) {
   return (int64_t)gz * G.ny * G.nx + (int64_t)Nz * (2 * gy) * G.nx + (int64_t)Nz * Ny * (2 * G.gx);
 }
 
-// Apply face f's rule to the neighbour values v (in place); pos: position along the
-// face (j for x faces, i for y faces).  INCR: v are mixed-form stage increments.
-template <class T, bool INCR>
-__device__ __forceinline__ void bc_rule(const Geo& G, int f, int pos, int nv, T (&v)[5]) {
+// Apply face f's rule to the neighbour state v (in place); pos: position along the
+// face (j for x faces, i for y faces).
+__device__ __forceinline__ void bc_rule(const Geo& G, int f, int pos, int nv, double (&v)[5]) {
   const int kind = (G.bkind >> (4 * f)) & 15;
   if (kind == 1) {  // slip wall: normal momentum (rho u for x faces, rho v for y faces) negated
     const int n = f < 2 ? 1 : 2;
     v[n] = -v[n];
   } else if (kind == 2) {  // fixed
     const int len = f < 2 ? G.ny : G.nx;
-    for (int l = 0; l < nv; ++l) v[l] = INCR ? T(0) : (T)G.bfix[f][(int64_t)l * len + pos];
+    for (int l = 0; l < nv; ++l) v[l] = G.bfix[f][(int64_t)l * len + pos];
   }
 }
 
+// Qn: null for a full state Q; in the mixed form Q holds FP32 stage increments over
+// the FP64 state Qn, and a boundary rule is applied to Qn + Q (the increment stored
+// is the rule's state minus Qn), so it acts as on a full state.
 template <class T>
-__device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t) {
-  constexpr bool INCR = sizeof(T) < sizeof(double);  // mixed form: Q holds stage increments
+__device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t, const double* Qn = nullptr) {
   const int g = G.g, gx = G.gx, gy = G.gy;
   const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
   const int gz = (G.dim == 3) ? 2 * g : 0;
@@ -399,7 +400,13 @@ __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t
     for (int l = 0; l < nv; ++l) Q[o + l * G.vs] = Q[s + l * G.vs];
     return;
   }
-  T v[5];
+  double v[5];
+  auto load = [&](int64_t s) {
+    for (int l = 0; l < nv; ++l) {
+      const int64_t q = s + l * G.vs;
+      v[l] = Qn ? Qn[q] + (double)Q[q] : (double)Q[q];
+    }
+  };
   const int sk = (G.dim == 3) ? (k - g + Nz) % Nz + g : 0;
   if (xb) {
     // x face: the neighbour column's value in this row -- a periodic image of an
@@ -407,32 +414,32 @@ __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t
     const int fx = i == 0 ? 0 : 1, in = i == 0 ? 1 : G.nx - 2;
     if (G.bcy && (j == 0 || j == G.ny - 1)) {
       const int fy = j == 0 ? 2 : 3, jn = j == 0 ? 1 : G.ny - 2;
-      const int64_t s = G.at(in, jn, sk);
-      for (int l = 0; l < nv; ++l) v[l] = Q[s + l * G.vs];
-      bc_rule<T, INCR>(G, fy, in, nv, v);
+      load(G.at(in, jn, sk));
+      bc_rule(G, fy, in, nv, v);
     } else {
       const int sj = G.bcy ? j : (j - gy + Ny) % Ny + gy;
-      const int64_t s = G.at(in, sj, sk);
-      for (int l = 0; l < nv; ++l) v[l] = Q[s + l * G.vs];
+      load(G.at(in, sj, sk));
     }
-    bc_rule<T, INCR>(G, fx, j, nv, v);
+    bc_rule(G, fx, j, nv, v);
   } else {
     // y face of an interior column (or a periodic-x ghost column's image)
     const int fy = j == 0 ? 2 : 3, jn = j == 0 ? 1 : G.ny - 2;
     const int si = G.bcx ? i : (i - gx + Nx) % Nx + gx;
-    const int64_t s = G.at(si, jn, sk);
-    for (int l = 0; l < nv; ++l) v[l] = Q[s + l * G.vs];
-    bc_rule<T, INCR>(G, fy, i, nv, v);
+    load(G.at(si, jn, sk));
+    bc_rule(G, fy, i, nv, v);
   }
-  for (int l = 0; l < nv; ++l) Q[o + l * G.vs] = v[l];
+  for (int l = 0; l < nv; ++l) {
+    const int64_t q = o + l * G.vs;
+    Q[q] = Qn ? (T)(v[l] - Qn[q]) : (T)v[l];
+  }
 }
 
 template <class T>
-__global__ void k_ghost(T* Q, Geo G, int nv) {
+__global__ void k_ghost(T* Q, Geo G, int nv, const double* Qn) {
   const int64_t tot = ghost_cells(G);
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
        t += (int64_t)gridDim.x * blockDim.x)
-    ghost_cell<T>(Q, G, nv, t);
+    ghost_cell<T>(Q, G, nv, t, Qn);
 }
 
 }  // namespace oux
