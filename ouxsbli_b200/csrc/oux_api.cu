@@ -51,6 +51,10 @@ int validate(const oux_config* c, std::string& why) {
     return OUX_E_INVALID;
   }
   if ((int64_t)c->nx * c->ny * nzc > (int64_t)1 << 34) { why = "grid too large"; return OUX_E_INVALID; }
+  if ((int64_t)c->nx * c->ny > ((int64_t)1 << 31) - 256 || nzc > 65535) {
+    why = "grid too large (an x-y plane must hold fewer than 2^31 - 256 points, nz at most 65535)";
+    return OUX_E_INVALID;
+  }
   if (c->scheme < 0 || c->scheme > 3) { why = "unknown scheme"; return OUX_E_INVALID; }
   if (c->dim == 2 && c->scheme == OUX_ROE) { why = "the 2D solver has no Roe scheme"; return OUX_E_INVALID; }
   if (c->visc < 0 || c->visc > 2) { why = "unknown visc"; return OUX_E_INVALID; }
@@ -440,33 +444,33 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   bool visc = c.visc != OUX_EULER;
   {
     Timed tm(h, KK_PRIM, s);
-    const int gb = grid_for(ncell, 256);
+    const dim3 gb = plane_grid(G);
     if constexpr (sizeof(T) < sizeof(double)) {
       // mixed form: Q^(s) = Q^n + FP32 increment (no increment for the first stage)
       const float* dQ = std::is_same<TS, double>::value ? nullptr : reinterpret_cast<const float*>(src);
       if (G.dim == 3) {
-        if (visc) k_prim_mx<3, true><<<gb, 256, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
-        else k_prim_mx<3, false><<<gb, 256, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
+        if (visc) k_prim_mx<3, true><<<gb, PLANE_THREADS, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
+        else k_prim_mx<3, false><<<gb, PLANE_THREADS, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
       } else {
-        if (visc) k_prim_mx<2, true><<<gb, 256, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
-        else k_prim_mx<2, false><<<gb, 256, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
+        if (visc) k_prim_mx<2, true><<<gb, PLANE_THREADS, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
+        else k_prim_mx<2, false><<<gb, PLANE_THREADS, 0, s>>>(h->Q, dQ, G, h->Wf, h->M.jac, h->K);
       }
     } else {
       if (G.dim == 3) {
-        if (visc) k_prim<3, true, TS, T><<<gb, 256, 0, s>>>(src, G, W, h->M.jac, h->K);
-        else k_prim<3, false, TS, T><<<gb, 256, 0, s>>>(src, G, W, h->M.jac, h->K);
+        if (visc) k_prim<3, true, TS, T><<<gb, PLANE_THREADS, 0, s>>>(src, G, W, h->M.jac, h->K);
+        else k_prim<3, false, TS, T><<<gb, PLANE_THREADS, 0, s>>>(src, G, W, h->M.jac, h->K);
       } else {
-        if (visc) k_prim<2, true, TS, T><<<gb, 256, 0, s>>>(src, G, W, h->M.jac, h->K);
-        else k_prim<2, false, TS, T><<<gb, 256, 0, s>>>(src, G, W, h->M.jac, h->K);
+        if (visc) k_prim<2, true, TS, T><<<gb, PLANE_THREADS, 0, s>>>(src, G, W, h->M.jac, h->K);
+        else k_prim<2, false, TS, T><<<gb, PLANE_THREADS, 0, s>>>(src, G, W, h->M.jac, h->K);
       }
     }
   }
   h->launches++;
   if (c.scheme != OUX_KEEP) {  // Ducros sensor
     Timed tm(h, KK_SENSOR, s);
-    const int gb = grid_for(ncell, 256);
-    if (G.dim == 3) k_sensor<3, T><<<gb, 256, 0, s>>>(G, W, h->M);
-    else k_sensor<2, T><<<gb, 256, 0, s>>>(G, W, h->M);
+    const dim3 gb = plane_grid(G);
+    if (G.dim == 3) k_sensor<3, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
+    else k_sensor<2, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
     h->launches++;
   }
   if (h->les) {

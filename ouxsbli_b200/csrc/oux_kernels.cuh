@@ -78,15 +78,34 @@ __device__ __forceinline__ T ldro(const T* p) {
   else return *p;
 }
 
+// Padded cell (i, j, k) of a flat index t (x fastest over nx, then ny, then nz).
+__device__ __forceinline__ void cell_of(const Geo& G, int64_t t, int& i, int& j, int& k) {
+  i = (int)(t % G.nx);
+  const int64_t r = t / G.nx;
+  j = (int)(r % G.ny);
+  k = (int)(r / G.ny);
+}
+
+// Plane-flattened launch of a per-cell kernel: blockIdx.y is the z plane, and a
+// block's 256 threads cover 256 consecutive cells of the plane (x fastest), so the
+// cell follows from one 32-bit division per thread.
+constexpr int PLANE_THREADS = 256;
+__device__ __forceinline__ bool plane_cell(const Geo& G, int& i, int& j, int& k) {
+  const int t = blockIdx.x * PLANE_THREADS + threadIdx.x;
+  if (t >= G.nx * G.ny) return false;
+  j = t / G.nx;
+  i = t - j * G.nx;
+  k = blockIdx.y;
+  return true;
+}
+inline dim3 plane_grid(const Geo& G) {
+  return dim3((unsigned)((G.nx * G.ny + PLANE_THREADS - 1) / PLANE_THREADS), (unsigned)G.nz, 1);
+}
+
 // ---- prim: src/calc_physical_quantities.f90:60-116 (3D), :7-57 (2D) -------
-// One padded cell t (x fastest over nx, then ny, then nz).
 template <int DIM, bool VISC, class TS, class T, bool RO = false>
 __device__ __forceinline__ void prim_cell(const TS* Q, const Geo& G, const Fields<T>& W, const double* jac,
-                                          const PhysConst& K, int64_t t) {
-  int i = (int)(t % G.nx);
-  int64_t r = t / G.nx;
-  int j = (int)(r % G.ny);
-  int k = (int)(r / G.ny);
+                                          const PhysConst& K, int i, int j, int k) {
   int64_t o = G.at(i, j, k);
   T Jv = (T)ldro<RO>(jac + (int64_t)j * G.nx + i);
   T q1 = (T)ldro<RO>(Q + o);
@@ -109,13 +128,19 @@ __device__ __forceinline__ void prim_cell(const TS* Q, const Geo& G, const Field
   if constexpr (VISC) W.mu[o] = T(K.sutherland) / (temp + T(111)) * (temp * sqrt(temp));
 }
 
+template <int DIM, bool VISC, class TS, class T, bool RO = false>
+__device__ __forceinline__ void prim_cell(const TS* Q, const Geo& G, const Fields<T>& W, const double* jac,
+                                          const PhysConst& K, int64_t t) {
+  int i, j, k;
+  cell_of(G, t, i, j, k);
+  prim_cell<DIM, VISC, TS, T, RO>(Q, G, W, jac, K, i, j, k);
+}
+
 template <int DIM, bool VISC, class TS, class T>
-__global__ void k_prim(const TS* __restrict__ Q, Geo G, Fields<T> W, const double* __restrict__ jac,
-                       PhysConst K) {
-  int64_t n = (int64_t)G.nx * G.ny * G.nz;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x)
-    prim_cell<DIM, VISC, TS, T, true>(Q, G, W, jac, K, t);
+__global__ void __launch_bounds__(PLANE_THREADS) k_prim(const TS* __restrict__ Q, Geo G, Fields<T> W,
+                                                        const double* __restrict__ jac, PhysConst K) {
+  int i, j, k;
+  if (plane_cell(G, i, j, k)) prim_cell<DIM, VISC, TS, T, true>(Q, G, W, jac, K, i, j, k);
 }
 
 // ---- mixed-form primitives: Q = Q^n (FP64) + dQ (FP32 stage increment, may be
@@ -124,11 +149,7 @@ __global__ void k_prim(const TS* __restrict__ Q, Geo G, Fields<T> W, const doubl
 template <int DIM, bool VISC, bool RO = false>
 __device__ __forceinline__ void prim_mx_cell(const double* Qn, const float* dQ, const Geo& G,
                                              const Fields<float>& W, const double* jac, const PhysConst& K,
-                                             int64_t t) {
-  int i = (int)(t % G.nx);
-  int64_t r = t / G.nx;
-  int j = (int)(r % G.ny);
-  int k = (int)(r / G.ny);
+                                             int i, int j, int k) {
   int64_t o = G.at(i, j, k);
   double q[5];
 #pragma unroll
@@ -151,23 +172,28 @@ __device__ __forceinline__ void prim_mx_cell(const double* Qn, const float* dQ, 
   if constexpr (VISC) W.mu[o] = (float)(K.sutherland / (temp + 111.0) * (temp * sqrt(temp)));
 }
 
+template <int DIM, bool VISC, bool RO = false>
+__device__ __forceinline__ void prim_mx_cell(const double* Qn, const float* dQ, const Geo& G,
+                                             const Fields<float>& W, const double* jac, const PhysConst& K,
+                                             int64_t t) {
+  int i, j, k;
+  cell_of(G, t, i, j, k);
+  prim_mx_cell<DIM, VISC, RO>(Qn, dQ, G, W, jac, K, i, j, k);
+}
+
 template <int DIM, bool VISC>
-__global__ void k_prim_mx(const double* __restrict__ Qn, const float* __restrict__ dQ, Geo G, Fields<float> W,
-                          const double* __restrict__ jac, PhysConst K) {
-  int64_t n = (int64_t)G.nx * G.ny * G.nz;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x)
-    prim_mx_cell<DIM, VISC, true>(Qn, dQ, G, W, jac, K, t);
+__global__ void __launch_bounds__(PLANE_THREADS) k_prim_mx(const double* __restrict__ Qn,
+                                                           const float* __restrict__ dQ, Geo G, Fields<float> W,
+                                                           const double* __restrict__ jac, PhysConst K) {
+  int i, j, k;
+  if (plane_cell(G, i, j, k)) prim_mx_cell<DIM, VISC, true>(Qn, dQ, G, W, jac, K, i, j, k);
 }
 
 // ---- Ducros sensor: calc_Ducros (3D_solver/src/calc_hybrid.f90:11-72; 2D twin
 // :11-55) on cells 1..n-2, with the reference's copies to the outer faces.
 template <int DIM, class T, bool RO = false>
-__device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, const Metrics& M, int64_t t) {
-  const int i = (int)(t % G.nx);
-  const int64_t r = t / G.nx;
-  const int j = (int)(r % G.ny);
-  const int k = (int)(r / G.ny);
+__device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, const Metrics& M, int i, int j,
+                                            int k) {
   if (i < 1 || i > G.nx - 2 || j < 1 || j > G.ny - 2) return;
   if (DIM == 3 && (k < 1 || k > G.nz - 2)) return;
   const int64_t o = G.at(i, j, k);
@@ -212,12 +238,17 @@ __device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, co
   }
 }
 
+template <int DIM, class T, bool RO = false>
+__device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, const Metrics& M, int64_t t) {
+  int i, j, k;
+  cell_of(G, t, i, j, k);
+  sensor_cell<DIM, T, RO>(G, W, M, i, j, k);
+}
+
 template <int DIM, class T>
-__global__ void k_sensor(Geo G, Fields<T> W, Metrics M) {
-  int64_t n = (int64_t)G.nx * G.ny * G.nz;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x)
-    sensor_cell<DIM, T, false>(G, W, M, t);
+__global__ void __launch_bounds__(PLANE_THREADS) k_sensor(Geo G, Fields<T> W, Metrics M) {
+  int i, j, k;
+  if (plane_cell(G, i, j, k)) sensor_cell<DIM, T, false>(G, W, M, i, j, k);
 }
 
 // ---- SMS sub-grid model: 3D_solver/src/calc_les.f90:30-125 -------------------
