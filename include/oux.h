@@ -76,15 +76,15 @@ typedef struct oux_config {
   int32_t tvd;          /* enum oux_tvd */
   int32_t slau;         /* enum oux_slau_variant */
   int32_t rk;           /* 3 (TVD-RK3) or 4 (classical RK4) */
-  int32_t bc_x, bc_y, bc_z; /* 0 = periodic.  bc_x = 1 (2D Euler): non-periodic x -- every x
+  int32_t bc_x, bc_y, bc_z; /* 0 = periodic.  bc_x = 1 (2D): non-periodic x -- every x
                                face with the order lowered next to the boundary, as the
                                reference's calc_{slau,keep,hybrid}_x boundary kernels do
                                (2D_solver/src/calc_*_kernel.f90.fypp), and one boundary
                                cell on each side, zero-gradient unless oux_set_boundary
                                gives its face another rule (2D_solver/ST/set.f90 set_bc).
-                               bc_y = 1 (2D Euler, with bc_x = 1): the same for y
-                               (calc_*_y), as the BC_X = BC_Y = True cases build them
-                               (2D_solver/OS).  bc_z must be 0. */
+                               bc_y = 1 (2D): the same for y (calc_*_y), as the
+                               BC_X = BC_Y = True cases build them (2D_solver/OS, BL).
+                               Euler or NS; bc_z must be 0. */
   int32_t precision;    /* enum oux_precision */
   double gamma, R, Pr, Prt, threshold, dt;
   const double *dx, *dy, *dz; /* host arrays, n-1 entries each (dz unused in 2D) */
@@ -140,6 +140,10 @@ int oux_unpack_state(const oux_handle* h, const void* dev_layout_host, double* r
  * every row (x faces) or column (y faces) from the adjacent interior cell:
  *   ZERO_GRADIENT  the neighbour's Q/J (the default of every non-periodic face)
  *   SLIP_WALL      the neighbour's Q/J with the normal momentum negated
+ *   NOSLIP_WALL    the neighbour's density and pressure with zero momentum:
+ *                  p_wall = (gamma-1) (E - (m1^2 + m2^2) / (2 rho)) of the neighbour's
+ *                  Q/J, E_wall = p_wall / (gamma-1) (the wall rows of
+ *                  2D_solver/ST/set.f90 and 2D_solver/BL0/set.f90)
  *   FIXED          caller values: fixed_dev holds nv x len doubles of Q/J, variable-
  *                  major ([l * len + pos]; len = ny for x faces, nx for y faces),
  *                  device memory owned by the caller and read at every fill until
@@ -150,7 +154,7 @@ int oux_unpack_state(const oux_handle* h, const void* dev_layout_host, double* r
  * 2D_solver/OS/set.f90).  The face's direction must be non-periodic.  Set rules
  * before oux_batch_create when the handle joins a batch. */
 enum oux_face { OUX_FACE_X_LO = 0, OUX_FACE_X_HI = 1, OUX_FACE_Y_LO = 2, OUX_FACE_Y_HI = 3 };
-enum oux_bc_kind { OUX_BC_ZERO_GRADIENT = 0, OUX_BC_SLIP_WALL = 1, OUX_BC_FIXED = 2 };
+enum oux_bc_kind { OUX_BC_ZERO_GRADIENT = 0, OUX_BC_SLIP_WALL = 1, OUX_BC_FIXED = 2, OUX_BC_NOSLIP_WALL = 3 };
 int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fixed_dev);
 
 /* --- hot path ----------------------------------------------------------- */

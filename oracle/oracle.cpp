@@ -54,7 +54,7 @@ typedef struct orc_config {
   double gamma, R, Pr, Prt, threshold, dt;
   int bc_y;           // 0 periodic; 1 non-periodic y (2D, with bc_x = 1)
   int bkind[4];       // boundary-cell rule of the faces x lo, x hi, y lo, y hi:
-                      // 0 zero gradient, 1 slip wall, 2 fixed values
+                      // 0 zero gradient, 1 slip wall, 2 fixed values, 3 no-slip wall
   const double* bfix[4];  // fixed values of Q/J, nv x (ny for x faces, nx for y faces), variable-major
 } orc_config;
 
@@ -1275,7 +1275,8 @@ void residual(Ctx& C, double coef, std::vector<double>& Rout) {
 // adjacent interior cell by the face's rule -- what a case's set_bc does
 // (2D_solver/OS/set.f90:50-90: y rows first for every column, then x columns for every
 // row; 2D_solver/ST/set.f90: zero-gradient x).  Rules: 0 copy, 1 copy with the normal
-// momentum negated, 2 the given values.
+// momentum negated, 2 the given values, 3 no-slip wall (the neighbour's density and
+// pressure, zero momentum).
 void bc_rule(const Ctx& C, int f, int pos, double* v) {  // pos: 1-based j (x faces) / i (y faces)
   int kind = C.c.bkind[f];
   if (kind == 1) {
@@ -1284,6 +1285,11 @@ void bc_rule(const Ctx& C, int f, int pos, double* v) {  // pos: 1-based j (x fa
   } else if (kind == 2) {
     int len = f < 2 ? C.ny : C.nx;
     for (int l = 0; l < C.nv; ++l) v[l] = C.c.bfix[f][(size_t)l * len + (pos - 1)];
+  } else if (kind == 3) {  // no-slip wall: 2D_solver/ST/set.f90, 2D_solver/BL0/set.f90 wall rows
+    double p_wall = C.K.gamma_1 * (v[3] - 0.5 * (v[1] * v[1] + v[2] * v[2]) / v[0]);
+    v[1] = 0.0;
+    v[2] = 0.0;
+    v[3] = p_wall * C.K.over_gamma_1;
   }
 }
 

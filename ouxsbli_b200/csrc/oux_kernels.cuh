@@ -34,6 +34,7 @@ struct Geo {
                               // faces 0..3: x low, x high, y low, y high
   int64_t sx, plane, vs;      // row stride, plane stride, variable stride (elements)
   const double* bfix[4];      // OUX_BC_FIXED faces: nv x (ny for x faces, nx for y faces) values of Q/J
+  double gamma_1, over_gamma_1;  // gamma - 1 and 1 / (gamma - 1), for the no-slip wall rule
   __host__ __device__ int64_t at(int i, int j, int k) const { return (int64_t)k * plane + (int64_t)j * sx + i; }
 };
 
@@ -369,7 +370,9 @@ __global__ void k_mut_edges(Geo G, Fields<T> W) {
 // case's set_bc (2D_solver/ST/set.f90, 2D_solver/OS/set.f90:50-90):
 //   OUX_BC_ZERO_GRADIENT  copy of the neighbour
 //   OUX_BC_SLIP_WALL      copy with the normal momentum negated
-//   OUX_BC_FIXED          caller-given Q/J values (stage increments of the mixed form: 0)
+//   OUX_BC_FIXED          caller-given Q/J values
+//   OUX_BC_NOSLIP_WALL    the neighbour's density and pressure, zero momentum (the
+//                         wall rows of 2D_solver/ST/set.f90 and 2D_solver/BL0/set.f90)
 // With both x and y non-periodic the y faces are set first for every column and the
 // x faces after them for every row (2D_solver/OS/set.f90 order), so a corner takes
 // its x rule applied to the y-boundary value next to it.  Every value is computed
@@ -393,6 +396,11 @@ __device__ __forceinline__ void bc_rule(const Geo& G, int f, int pos, int nv, do
   } else if (kind == 2) {  // fixed
     const int len = f < 2 ? G.ny : G.nx;
     for (int l = 0; l < nv; ++l) v[l] = G.bfix[f][(int64_t)l * len + pos];
+  } else if (kind == 3) {  // no-slip wall (2D): p_wall from the neighbour, momenta 0
+    const double p_wall = G.gamma_1 * (v[3] - 0.5 * (v[1] * v[1] + v[2] * v[2]) / v[0]);
+    v[1] = 0.0;
+    v[2] = 0.0;
+    v[3] = p_wall * G.over_gamma_1;
   }
 }
 

@@ -614,9 +614,18 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[ca], (T)invd[ca][ci[ca]]);
         tile[TF_D3 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[cb], (T)invd[cb][ci[cb]]);
       } else {
+        // 2D: only where the stencil stays inside the grid; the other cells lie
+        // outside the 4th-order guard of calc_Ev4 / calc_Fv4, whose 2nd-order
+        // fallback does not read these values (non-periodic edges, order 2 grids)
         const int n = DIR, t = 1 - DIR;
-        tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[t], o, stv[t], (T)invd[t][ci[t]]);
-        tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[t], (T)invd[t][ci[t]]);
+        constexpr int HD = SIXTH ? 3 : 2;
+        if (ci[t] >= HD && ci[t] + HD < (t == 0 ? G.nx : G.ny)) {
+          tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[t], o, stv[t], (T)invd[t][ci[t]]);
+          tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[t], (T)invd[t][ci[t]]);
+        } else {
+          tile[TF_D0 * NC + c] = T(0);
+          tile[TF_D2 * NC + c] = T(0);
+        }
       }
     }
   }

@@ -33,11 +33,11 @@ class SolverConfig:
     slau: str = "HRSLAU2"          # SLAU_VARIANT
     rk: int = 3
     precision: str = "fp64"        # fp64 | mixed (FP32 stage states/fluxes, FP64 Q^n + accumulation)
-    bc_x: int = 0                  # 0 periodic; 1 non-periodic x (boundary flux kernels, boundary cells; 2D Euler)
-    bc_y: int = 0                  # the same for y (2D Euler, with bc_x = 1)
+    bc_x: int = 0                  # 0 periodic; 1 non-periodic x (boundary flux kernels, boundary cells; 2D)
+    bc_y: int = 0                  # the same for y (2D)
     # rules of the non-periodic faces ("x_lo", "x_hi", "y_lo", "y_hi"): "zero_gradient"
-    # (the default), "slip_wall" or ("fixed", values (nv, ny) for x faces / (nv, nx) for
-    # y faces, of Q/J)
+    # (the default), "slip_wall", "noslip_wall" or ("fixed", values (nv, ny) for x faces /
+    # (nv, nx) for y faces, of Q/J)
     boundary: dict = field(default=None, repr=False)
     gamma: float = 1.4
     R: float = 287.03

@@ -47,7 +47,8 @@ def create(cfg):
     (dict(nx=6), "too small"),
     (dict(bc_x=1), "non-periodic x"),
     (dict(bc_x=2), "boundaries"),
-    (dict(dim=2, nz=1, bc_x=1, visc="NS"), "2D Euler"),
+    (dict(dim=2, nz=1, order=2, ny=3, dy=np.full(2, 0.1), bc_y=1), "ny >= 4"),
+    (dict(bc_y=1), "2D solves"),
     (dict(rk=2), "rk"),
     (dict(dim=2, nz=1, scheme="Roe"), "Roe"),
     (dict(visc="NS", visc_order=2), "calc_Ev2_in"),
@@ -98,3 +99,22 @@ def test_pack_unpack_roundtrip_host():
     i, j, k, l = 4, 7, 3, 2
     assert dev[l * lay.var_stride + k * lay.plane_stride + j * lay.row_stride + i] == ref[i, l, j, k]
     _lib.LIB.oux_destroy(h)
+
+
+def test_set_boundary_checks_without_a_device():
+    """oux_set_boundary validates on the host: the face's direction must be
+    non-periodic, the rule known, and a fixed rule needs its values."""
+    n = 12
+    d = np.full(n - 1, 0.1)
+    cfg = SolverConfig(dim=2, nx=n, ny=n, nz=1, order=4, visc="NS", bc_y=1, dx=d, dy=d, dz=None, dt=1e-4)
+    rc, h = create(cfg)
+    assert rc == 0
+    L = _lib.LIB
+    assert L.oux_set_boundary(h, _lib.FACES["x_lo"], 0, None) == _lib.OUX_E_INVALID  # x is periodic
+    assert "periodic" in L.oux_last_error().decode()
+    assert L.oux_set_boundary(h, _lib.FACES["y_lo"], 9, None) == _lib.OUX_E_INVALID
+    assert L.oux_set_boundary(h, _lib.FACES["y_hi"], _lib.BC_KINDS["fixed"], None) == _lib.OUX_E_INVALID
+    assert L.oux_set_boundary(h, 7, 0, None) == _lib.OUX_E_INVALID
+    assert L.oux_set_boundary(h, _lib.FACES["y_lo"], _lib.BC_KINDS["noslip_wall"], None) == 0
+    assert L.oux_set_boundary(h, _lib.FACES["y_hi"], _lib.BC_KINDS["slip_wall"], None) == 0
+    L.oux_destroy(h)
