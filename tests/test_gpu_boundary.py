@@ -315,7 +315,11 @@ def test_viscous_walls_bitexact_vs_oracle(name, rules, bc_x, kw, cuda_device):
     s.step(6)
     q_gpu = s.get_state()
     s.close()
-    np.testing.assert_array_equal(r_gpu, oracle.rhs(cfg, qj))
+    # residual of the updated cells: with a periodic x the ghost columns are refilled
+    # from their images after each stage (the oracle, like the reference, updates them
+    # first)
+    xs = slice(cfg.g - 1, -(cfg.g - 1)) if not bc_x and cfg.g > 1 else slice(None)
+    np.testing.assert_array_equal(r_gpu[xs], oracle.rhs(cfg, qj)[xs])
     np.testing.assert_array_equal(q_gpu, oracle.step(cfg, qj, 6))
 
 
