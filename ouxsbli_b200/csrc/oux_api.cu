@@ -494,6 +494,7 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   } else {
     rc = launch_sweeps_t<T>(G.dim, c.order, h->vk, h->les, -1, A, s);
   }
+  if (rc == 2) return fail(OUX_E_INVALID, "no sweep kernel is built for this configuration");
   if (rc) return fail(OUX_E_CUDA, std::string("sweep launch: ") + cudaGetErrorString(cudaGetLastError()));
   h->launches += G.dim;
   return OUX_OK;

@@ -9,7 +9,7 @@ int batch_launch_mx_o2(int dim, int vk, bool les, const BatchArgs<float>& B, int
   if (dim == D && vk == V && les == L) return konly ? batch_launch_t<D, 2, V, L, float, true>(B, bps, nsm, grid, s, dry) \
                  : batch_launch_t<D, 2, V, L, float, false>(B, bps, nsm, grid, s, dry);
   OUX_CASE(3, VK_EULER, false) OUX_CASE(3, VK_GV2, false) OUX_CASE(3, VK_GV2, true)
-  OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_GV2, false)
+  OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_GV2, false) OUX_CASE(2, VK_2D4, false)
 #undef OUX_CASE
   return 2;
 }

@@ -10,7 +10,7 @@ int launch_sweeps_mx_o2(int dim, int vk, bool les, int dir, const StepArgs<float
     return dir < 0 ? launch_stage_sweeps<D, 2, V, L, float>(A, s)                            \
                    : launch_stage_sweep_dir<D, 2, V, L, float>(A, dir, s);
   OUX_CASE(3, VK_EULER, false) OUX_CASE(3, VK_GV2, false) OUX_CASE(3, VK_GV2, true)
-  OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_GV2, false)
+  OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_GV2, false) OUX_CASE(2, VK_2D4, false)
 #undef OUX_CASE
   return 2;
 }
