@@ -98,7 +98,10 @@ class Case:
                 glob[k] = v
         ic_type = glob.pop("ic_type", None)
         if ic_type == 3:
-            raise RuntimeError("RiemannIC needs a non-periodic (wall / inflow) case, which is not built")
+            if not case.bc_x or case.dim != 2:
+                raise RuntimeError("RiemannIC needs a case with a non-periodic x (2D_solver/ST)")
+            glob["riemann"] = {k: glob.pop(k) for k in ("rho_l", "u_l", "p_l", "rho_r", "u_r", "p_r", "x0_frac")
+                               if k in glob}
         if ic_type == 2 and "Ma" in glob:
             glob["M0"] = glob.pop("Ma")
         if ic_type == 1:
@@ -127,6 +130,18 @@ class Case:
         p = dict(self.globals)
         p["order"] = int(self.config["ORDER"])
         p, xc, yc, zc, dx, dy, dz, Q = build_initial(self._case, p)
+        if "riemann" in p:
+            # RiemannIC (ouxsbli/ic.py): the left state at x < x0_frac * Lx, the right
+            # state from there on, uniform in y
+            r = p["riemann"]
+            gam = p["gamma"]
+            left = xc < r.get("x0_frac", 0.5) * (xc[-1] - xc[0]) + xc[0]
+            for side, m in (("l", left), ("r", ~left)):
+                rho, u, pr = r.get("rho_" + side, 1.0), r.get("u_" + side, 0.0), r.get("p_" + side, 1.0)
+                Q[m, 0] = rho
+                Q[m, 1] = rho * u
+                Q[m, 2] = 0.0
+                Q[m, 3] = pr / (gam - 1.0) + 0.5 * rho * u * u
         if "uniform" in p:
             u = p["uniform"]
             Q[:] = 0.0

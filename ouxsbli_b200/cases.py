@@ -202,8 +202,8 @@ def _st_derived(p: dict) -> dict:
     p["p0"] = p["rho0"] * p["R"] * p["T0"]
     p["rho1"] = 0.125 * p["rho0"]
     p["p1"] = 0.1 * p["p0"]
-    p["Lx"] = p["Re"] * p["mu0"] / math.sqrt(p["rho0"] * p["p0"])
-    p["Ly"] = 0.1 * p["Lx"]
+    p.setdefault("Lx", p["Re"] * p["mu0"] / math.sqrt(p["rho0"] * p["p0"]))
+    p.setdefault("Ly", 0.1 * p["Lx"])
     c0 = math.sqrt(p["p0"] / p["rho0"])
     if p.get("dt") is None:
         p["dt"] = p["CFL"] * p["Lx"] / (float(p["nx"] - 1) * c0)

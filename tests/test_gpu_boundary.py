@@ -104,6 +104,30 @@ def test_shock_tube_vs_exact_sod(tmp_path, cuda_device):
     assert l1_rho < 0.01 and l1_p < 0.01, (l1_rho, l1_p)
 
 
+def test_riemann_ic_sod_vs_exact(tmp_path, cuda_device):
+    """RiemannIC (ouxsbli/ic.py) on the shock tube: Sod's states in units with
+    rho_l = p_l = 1 on a unit tube (SLAU-6, TVD hybrid, RK3, 513 nodes) to t = 0.2,
+    against the exact solution: relative L1 of density and pressure < 1 %."""
+    import sod_exact
+    from ouxsbli_b200 import Case
+    from ouxsbli_b200.ic import RiemannIC
+    from ouxsbli_b200.output import read_vtr
+    wd = tmp_path / "rie"
+    dt = 0.3 / 512 / 1.5
+    nt = int(round(0.2 / dt))
+    case = Case(source="2D_solver/ST", workdir=str(wd), ic=RiemannIC(), visc="euler", tvd="hybrid", scheme="slau",
+                accuracy=6, rk="tvd_rk3", nx=513, ny=7, Lx=1.0, Ly=0.1, dt=dt, nt=nt, np=1)
+    case.build()
+    case.run(device=cuda_device)
+    x, y, z, f = read_vtr(sorted((wd / "data").glob("Q*.vtr"))[-1])
+    rho = f["rho"].reshape(y.size, x.size)[3].astype(float)
+    p = f["p"].reshape(y.size, x.size)[3].astype(float)
+    rho_ex, _, p_ex = sod_exact.solve(x.astype(float), nt * dt, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1, gamma=1.4, x0=0.5)
+    l1_rho = np.mean(np.abs(rho - rho_ex)) / np.mean(rho_ex)
+    l1_p = np.mean(np.abs(p - p_ex)) / np.mean(p_ex)
+    assert l1_rho < 0.01 and l1_p < 0.01, (l1_rho, l1_p)
+
+
 def test_boundary_mixed_close_to_fp64(cuda_device):
     """The mixed form with a non-periodic x: smooth flow (KEEP-4, RK4), relative L2
     against FP64 within the mixed form's bound for switch-free schemes (1e-5)."""

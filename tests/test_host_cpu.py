@@ -85,6 +85,17 @@ class TestCaseConfig:
         with pytest.raises(RuntimeError):
             Case("3D_solver/ETGV", tmp_path / "rie", ic=RiemannIC()).build()
 
+    def test_riemann_ic_on_the_shock_tube(self, tmp_path):
+        """RiemannIC on a case with a non-periodic x: the left state up to x0 * Lx."""
+        c = Case("2D_solver/ST", tmp_path / "st", ic=RiemannIC(rho_l=2.0, p_l=3.0, x0=0.25), visc="euler",
+                 nx=41, ny=7, Lx=1.0, Ly=0.1, dt=1e-3, nt=1, np=1)
+        c._setup()
+        p, xc, yc, zc, dx, dy, dz, Q = c._initial()
+        assert p["Lx"] == 1.0
+        left = xc < 0.25
+        assert np.all(Q[left, 0] == 2.0) and np.all(Q[~left, 0] == 0.125)
+        assert np.allclose(Q[left, 3], 3.0 / 0.4) and np.allclose(Q[~left, 3], 0.1 / 0.4)
+
     def test_ic_bc_specs(self):
         assert ic_to_params(TaylorGreenIC(Ma=0.2))["Ma"] == 0.2
         assert ic_to_params({"type": "uniform", "rho": 2.0})["rho0"] == 2.0
