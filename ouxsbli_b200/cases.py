@@ -239,6 +239,76 @@ def _st_init(p: dict, x, y, z=None) -> np.ndarray:
 
 
 # ---------------------------------------------------------------------------
+# Kelvin-Helmholtz instability: 3D_solver/KHI (mod_globals.f90, set.f90 set_init):
+# a supersonic stream (T2, 3 c2) in 0.25 L <= y <= 0.75 L inside a Mach-2 stream
+# (T1), equal pressure, perturbed by v = amp u1 sin(2 pi x / Lx), w = amp u1 sin(2 pi z / Lz).
+# ---------------------------------------------------------------------------
+def _khi_derived(p: dict) -> dict:
+    p = dict(p)
+    g, R = p["gamma"], p["R"]
+    p["rho1"] = p["p"] / (R * p["T1"])
+    p["u1"] = 2.0 * math.sqrt(g * R * p["T1"])
+    p["rho2"] = p["p"] / (R * p["T2"])
+    p["u2"] = 3.0 * math.sqrt(g * R * p["T2"])
+    if p.get("dt") is None:
+        p["dt"] = p["CFL"] * p["Lx"] / (float(p["nx"] - 1) * abs(p["u1"]))
+    p.setdefault("endT", 10.0 * p["Lx"] / p["u2"])
+    if p.get("nt") is None:
+        p["nt"] = int(p["endT"] / (float(p["np"]) * p["dt"]))
+    return p
+
+
+def _khi_init(p: dict, x, y, z) -> np.ndarray:
+    """set_init on the interior cells (offset g), then the periodic fill."""
+    g = p["order"] // 2
+    gam = p["gamma"]
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    v = p["amp"] * p["u1"] * np.sin(2.0 * math.pi * X / p["Lx"])
+    w = p["amp"] * p["u1"] * np.sin(2.0 * math.pi * Z / p["Lz"])
+    outer = (Y > 0.75 * p["Lx"]) | (Y < 0.25 * p["Lx"])
+    rho = np.where(outer, p["rho1"], p["rho2"])
+    u = np.where(outer, p["u1"], p["u2"])
+    Q = np.zeros((x.size, 5, y.size, z.size), order="F")
+    Q[:, 0] = rho
+    Q[:, 1] = rho * u
+    Q[:, 2] = rho * v
+    Q[:, 3] = rho * w
+    Q[:, 4] = p["p"] / (gam - 1.0) + 0.5 * rho * (u ** 2 + v ** 2 + w ** 2)
+    fill_periodic(Q, g)
+    return Q
+
+
+# ---------------------------------------------------------------------------
+# Double shear layer: 2D_solver/DSL (mod_globals.f90, set.f90 set_init): two tanh
+# shear layers at y = pi/2 and 3 pi/2 on [0, 2 pi)^2 with a sinusoidal v
+# perturbation; set_init writes every point, ghosts included.
+# ---------------------------------------------------------------------------
+def _dsl_derived(p: dict) -> dict:
+    p = dict(p)
+    p.setdefault("Lx", 2.0 * math.pi)
+    p.setdefault("Ly", 2.0 * math.pi)
+    p["d1"] = math.pi / 15.0 if p.get("d1") is None else p["d1"]
+    if p.get("nt") is None:
+        p["nt"] = int(p["endT"] / (float(p["np"]) * p["dt"]))
+    return p
+
+
+def _dsl_init(p: dict, x, y, z=None) -> np.ndarray:
+    gam, rho0, u0, M0, d1, d2 = p["gamma"], p["rho0"], p["u0"], p["M0"], p["d1"], p["d2"]
+    pr = rho0 * u0 ** 2 / (gam * M0 ** 2)
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    lower = Y <= math.pi
+    ru = np.where(lower, rho0 * u0 * np.tanh((Y - 0.5 * math.pi) / d1), rho0 * u0 * np.tanh((1.5 * math.pi - Y) / d1))
+    rv = rho0 * u0 * d2 * np.sin(X)
+    Q = np.zeros((x.size, 4, y.size), order="F")
+    Q[:, 0] = rho0
+    Q[:, 1] = ru
+    Q[:, 2] = rv
+    Q[:, 3] = pr / (gam - 1.0) + 0.5 * (ru ** 2 + rv ** 2) / rho0
+    return Q
+
+
+# ---------------------------------------------------------------------------
 # Reflection of an oblique shock from a slip wall: 2D_solver/OS (mod_globals.f90,
 # set.f90).  Supersonic inflow at x low, zero-gradient outflow at x high, a slip wall
 # at y low and, at y high, the free stream up to 0.1 Lx and the state behind an
@@ -348,6 +418,23 @@ CASES: dict[str, CaseDef] = {
         _st_init, _st_derived,
         "Inviscid shock tube, Sod problem (2D_solver/ST)",
         grid=_st_grid, bc_x=True),
+    "KHI": CaseDef(
+        "KHI", 3,
+        dict(VISC="Euler", SCHEME="KEEP", ORDER=6, TVD="none", SLAU_VARIANT="HRSLAU2", RK=3,
+             BC_X=False, BC_Y=False, BC_Z=False, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=130, ny=130, nz=130, Lx=5.0e-3, Ly=5.0e-3, Lz=5.0e-3, gamma=1.4, Pr=0.71, Prt=0.9, R=287.15,
+             p=2.72e3, T1=162.7908, T2=104.6303, amp=0.05, CFL=0.05, np=100, dt=None, nt=None,
+             threshold=0.9),
+        _khi_init, _khi_derived,
+        "Kelvin-Helmholtz instability of a supersonic shear layer (3D_solver/KHI)"),
+    "DSL": CaseDef(
+        "DSL", 2,
+        dict(VISC="Euler", SCHEME="KEEP", ORDER=6, TVD="none", SLAU_VARIANT="HRSLAU2", RK=4,
+             BC_X=False, BC_Y=False, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=513, ny=513, gamma=1.4, Pr=0.71, Prt=0.9, R=287.03, M0=0.1, rho0=1.0, u0=1.0, d1=None,
+             d2=0.05, dt=0.25 * 0.25e-3, endT=8.0, np=10, nt=None, threshold=0.4),
+        _dsl_init, _dsl_derived,
+        "Double shear layer (2D_solver/DSL)"),
     "OS": CaseDef(
         "OS", 2,
         dict(VISC="Euler", SCHEME="SLAU", ORDER=6, TVD="hybrid", SLAU_VARIANT="HRSLAU2", RK=3,

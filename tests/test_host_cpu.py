@@ -289,3 +289,16 @@ class TestKnownAnswerHelpersAgainstReferenceUtils:
         assert math.isclose(rho3, o["reflected"][0], rel_tol=1e-12)
         assert math.isclose(p3, o["reflected"][3], rel_tol=1e-12)
         assert abs(U3 - o["reflected"][1]) / o["reflected"][1] < 0.03
+
+
+def test_every_case_builds_its_initial_field(tmp_path):
+    """Each case's defaults (scaled down) give a finite initial field of the right shape."""
+    from ouxsbli_b200.cases import CASES
+    small = {3: dict(nx=14, ny=14, nz=14), 2: dict(nx=22, ny=22)}
+    for name, case in CASES.items():
+        src = f"{case.dim}D_solver/{name}"
+        c = Case(src, tmp_path / name, nt=1, np=1, **small[case.dim])
+        c._setup()
+        p, xc, yc, zc, dx, dy, dz, Q = c._initial()
+        nv = case.dim + 2
+        assert Q.shape[1] == nv and np.isfinite(Q).all() and (Q[:, 0] > 0).all(), name
