@@ -84,7 +84,11 @@ typedef struct oux_config {
                                gives its face another rule (2D_solver/ST/set.f90 set_bc).
                                bc_y = 1 (2D): the same for y (calc_*_y), as the
                                BC_X = BC_Y = True cases build them (2D_solver/OS, BL).
-                               Euler or NS; bc_z must be 0. */
+                               Euler or NS.  bc_z = 2 (3D, not LES): a z slab of a
+                               larger grid (COMMZ, 3D_solver/src/calc_para.f90:343-384):
+                               its g ghost planes at each z end are written by the
+                               caller's halo exchange (oux_halo_pack / _unpack) after
+                               every stage, not by the periodic fill. */
   int32_t precision;    /* enum oux_precision */
   double gamma, R, Pr, Prt, threshold, dt;
   const double *dx, *dy, *dz; /* host arrays, n-1 entries each (dz unused in 2D) */
@@ -132,6 +136,23 @@ int oux_get_state_async(oux_handle* h, double* host_qj, void* stream);
 /* Pure host converters between the reference order and the device layout. */
 int oux_pack_state(const oux_handle* h, const double* ref_qj, void* dev_layout_host);
 int oux_unpack_state(const oux_handle* h, const void* dev_layout_host, double* ref_qj);
+
+/* --- stages and halo planes (z slabs, bc_z = 2) ----------------------------- */
+/* One RK stage (0..2 for RK3, 0..3 for RK4) of a time step with the ghost /
+ * boundary fill of the array it writes; oux_step(h, 1) is the stages in order.
+ * A z slab exchanges halos between stages, as the reference's COMMZ path does
+ * after each stage (3D_solver/src/calc_time_dev.f90.fypp:465-498, calc_para.f90:
+ * 343-384): oux_halo_pack copies the g lowest and g highest interior planes of
+ * every variable of the array the stage wrote into lo_dev / hi_dev ([nv][g][plane],
+ * oux_halo_bytes each; elements FP64, or FP32 stage increments in the mixed form);
+ * the caller sends lo to the rank below and hi to the rank above (periodic in
+ * rank), and oux_halo_unpack writes the buffer received from the rank below (its
+ * hi) into the lower ghost planes and the one from the rank above (its lo) into
+ * the upper ones. */
+int oux_stage(oux_handle* h, int32_t stage, void* stream);
+int oux_halo_bytes(const oux_handle* h, int32_t stage, size_t* bytes);
+int oux_halo_pack(oux_handle* h, int32_t stage, void* lo_dev, void* hi_dev, void* stream);
+int oux_halo_unpack(oux_handle* h, int32_t stage, const void* lo_dev, const void* hi_dev, void* stream);
 
 /* --- boundary cells of non-periodic directions --------------------------- */
 /* Replaces the case's own set_bc subroutine (2D_solver/OS/set.f90:50-90,

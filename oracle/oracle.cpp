@@ -56,6 +56,7 @@ typedef struct orc_config {
   int bkind[4];       // boundary-cell rule of the faces x lo, x hi, y lo, y hi:
                       // 0 zero gradient, 1 slip wall, 2 fixed values, 3 no-slip wall
   const double* bfix[4];  // fixed values of Q/J, nv x (ny for x faces, nx for y faces), variable-major
+  int bc_z;           // 0 periodic; 2 z slab: the z ghost planes are left to the halo exchange
 } orc_config;
 
 }  // extern "C"
@@ -1308,6 +1309,8 @@ void fill_ghosts(const Ctx& C, double* Q) {
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
+        // z slab (COMMZ, calc_para.f90:343-384): z ghost planes come from the neighbours
+        if (C.c.dim == 3 && C.c.bc_z == 2 && (k <= g || k > nz - g)) continue;
         bool xb = C.c.bc_x && (i == 1 || i == nx), yb = C.c.bc_y && (j == 1 || j == ny);
         int kk = C.c.dim == 3 ? wrap(k, g, Nz) : 1;
         double v[5];
@@ -1382,63 +1385,72 @@ inline size_t qup(const Ctx& C, int i, int l, int j, int k) {  // cell (i+1, j+1
   return C.qidx(i + 1, l + 1, j + 1, C.c.dim == 3 ? k + 1 : 1);
 }
 
-// One time step: 3D_solver/src/calc_time_dev.f90.fypp:81-101 (RK3), :264-287 (RK4)
-void one_step(Solver& S, double* QJ) {
-  Ctx& C = S.C;
+// Stage st of one time step: 3D_solver/src/calc_time_dev.f90.fypp:81-101 (RK3),
+// :264-287 (RK4).  QJ holds Q^n (the last stage writes Q^{n+1} into it), QJ2 the
+// stage state and Rs the RK4 accumulator, all kept by the caller between stages.
+void one_stage(Ctx& C, std::vector<double>& R, double* QJ, double* QJ2, double* Rs, int st) {
   int nv = C.nv;
   if (C.c.rk == 3) {
-    calc_efg(C, QJ);
-    residual(C, 1.0, S.R);
-    for_update(C, [&](int i, int j, int k) {
-      for (int l = 0; l < nv; ++l) S.QJ2[qup(C, i, l, j, k)] = QJ[qup(C, i, l, j, k)] - S.R[ridx(C, i, l, j, k)];
-    });
-    fill_ghosts(C, S.QJ2.data());
-    calc_efg(C, S.QJ2.data());
-    residual(C, 0.25, S.R);
-    for_update(C, [&](int i, int j, int k) {
-      for (int l = 0; l < nv; ++l) {
-        size_t q = qup(C, i, l, j, k);
-        S.QJ2[q] = (0.75 * QJ[q] + 0.25 * S.QJ2[q] - S.R[ridx(C, i, l, j, k)]) * 1.0;
-      }
-    });
-    fill_ghosts(C, S.QJ2.data());
-    calc_efg(C, S.QJ2.data());
-    residual(C, 2.0, S.R);
-    for_update(C, [&](int i, int j, int k) {
-      for (int l = 0; l < nv; ++l) {
-        size_t q = qup(C, i, l, j, k);
-        QJ[q] = (2.0 * S.QJ2[q] + 1.0 * QJ[q] - S.R[ridx(C, i, l, j, k)]) * one_third;
-      }
-    });
-    fill_ghosts(C, QJ);
+    if (st == 0) {
+      calc_efg(C, QJ);
+      residual(C, 1.0, R);
+      for_update(C, [&](int i, int j, int k) {
+        for (int l = 0; l < nv; ++l) QJ2[qup(C, i, l, j, k)] = QJ[qup(C, i, l, j, k)] - R[ridx(C, i, l, j, k)];
+      });
+      fill_ghosts(C, QJ2);
+    } else if (st == 1) {
+      calc_efg(C, QJ2);
+      residual(C, 0.25, R);
+      for_update(C, [&](int i, int j, int k) {
+        for (int l = 0; l < nv; ++l) {
+          size_t q = qup(C, i, l, j, k);
+          QJ2[q] = (0.75 * QJ[q] + 0.25 * QJ2[q] - R[ridx(C, i, l, j, k)]) * 1.0;
+        }
+      });
+      fill_ghosts(C, QJ2);
+    } else {
+      calc_efg(C, QJ2);
+      residual(C, 2.0, R);
+      for_update(C, [&](int i, int j, int k) {
+        for (int l = 0; l < nv; ++l) {
+          size_t q = qup(C, i, l, j, k);
+          QJ[q] = (2.0 * QJ2[q] + 1.0 * QJ[q] - R[ridx(C, i, l, j, k)]) * one_third;
+        }
+      });
+      fill_ghosts(C, QJ);
+    }
   } else {
     const double c1[3] = {0.5, 0.5, 1.0}, c2[3] = {1.0, 2.0, 2.0};
-    const double* src = QJ;
-    for (int s = 0; s < 3; ++s) {
-      calc_efg(C, src);
-      residual(C, 1.0, S.R);
+    if (st < 3) {
+      calc_efg(C, st == 0 ? QJ : QJ2);
+      residual(C, 1.0, R);
       for_update(C, [&](int i, int j, int k) {
         for (int l = 0; l < nv; ++l) {
           size_t q = qup(C, i, l, j, k), r = ridx(C, i, l, j, k);
-          S.QJ2[q] = QJ[q] - c1[s] * S.R[r];
-          S.Rs[r] = S.Rs[r] + c2[s] * S.R[r];
+          QJ2[q] = QJ[q] - c1[st] * R[r];
+          Rs[r] = Rs[r] + c2[st] * R[r];
         }
       });
-      fill_ghosts(C, S.QJ2.data());
-      src = S.QJ2.data();
+      fill_ghosts(C, QJ2);
+    } else {
+      calc_efg(C, QJ2);
+      residual(C, 1.0, R);
+      for_update(C, [&](int i, int j, int k) {
+        for (int l = 0; l < nv; ++l) {
+          size_t q = qup(C, i, l, j, k), r = ridx(C, i, l, j, k);
+          double Rl = Rs[r] + R[r];
+          QJ[q] = QJ[q] - Rl * one_sixth;
+          Rs[r] = 0.0;
+        }
+      });
+      fill_ghosts(C, QJ);
     }
-    calc_efg(C, S.QJ2.data());
-    residual(C, 1.0, S.R);
-    for_update(C, [&](int i, int j, int k) {
-      for (int l = 0; l < nv; ++l) {
-        size_t q = qup(C, i, l, j, k), r = ridx(C, i, l, j, k);
-        double Rl = S.Rs[r] + S.R[r];
-        QJ[q] = QJ[q] - Rl * one_sixth;
-        S.Rs[r] = 0.0;
-      }
-    });
-    fill_ghosts(C, QJ);
   }
+}
+
+void one_step(Solver& S, double* QJ) {
+  const int nst = S.C.c.rk == 3 ? 3 : 4;
+  for (int st = 0; st < nst; ++st) one_stage(S.C, S.R, QJ, S.QJ2.data(), S.Rs.data(), st);
 }
 
 }  // namespace
@@ -1453,6 +1465,18 @@ int orc_step(const orc_config* cfg, const double* dx, const double* dy, const do
   S.QJ2.assign(QJ, QJ + S.C.w.Q.size());
   S.Rs.assign((size_t)(S.C.nx - 2) * S.C.nv * (S.C.ny - 2) * (cfg->dim == 3 ? S.C.nz - 2 : 1), 0.0);
   for (int n = 0; n < nsteps; ++n) one_step(S, QJ);
+  return 0;
+}
+
+// One RK stage on caller-kept arrays (a z slab's stepping between halo exchanges):
+// QJ = Q^n (Q^{n+1} after the last stage), QJ2 = the stage state (same layout),
+// Rs = the RK4 accumulator ((nx-2, nv, ny-2, nz-2), zero at the start of a step).
+int orc_stage(const orc_config* cfg, const double* dx, const double* dy, const double* dz, double* QJ,
+              double* QJ2, double* Rs, int stage) {
+  Ctx C;
+  init_ctx(C, cfg, dx, dy, dz);
+  std::vector<double> R;
+  one_stage(C, R, QJ, QJ2, Rs, stage);
   return 0;
 }
 

@@ -40,7 +40,7 @@ class _Cfg(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("dim", "nx", "ny", "nz", "order", "scheme", "visc", "visc_order",
                                        "visc_stencil", "tvd", "slau", "rk", "bc_x")] + \
                [(n, C.c_double) for n in ("gamma", "R", "Pr", "Prt", "threshold", "dt")] + \
-               [("bc_y", C.c_int), ("bkind", C.c_int * 4), ("bfix", C.POINTER(C.c_double) * 4)]
+               [("bc_y", C.c_int), ("bkind", C.c_int * 4), ("bfix", C.POINTER(C.c_double) * 4), ("bc_z", C.c_int)]
 
 
 _lib = None
@@ -58,6 +58,7 @@ def lib() -> C.CDLL:
         _lib.orc_fields.argtypes = [cp, dp, dp, dp, dp, dp]
         _lib.orc_jacobian.argtypes = [cp, dp, dp, dp, dp]
         _lib.orc_fill_ghosts.argtypes = [cp, dp]
+        _lib.orc_stage.argtypes = [cp, dp, dp, dp, dp, dp, dp, C.c_int]
         _lib.orc_diag_f32.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                       C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), dp]
     return _lib
@@ -82,6 +83,7 @@ def make_cfg(cfg) -> _Cfg:
     c.rk = cfg.rk
     c.bc_x = getattr(cfg, "bc_x", 0)
     c.bc_y = getattr(cfg, "bc_y", 0)
+    c.bc_z = getattr(cfg, "bc_z", 0)
     c._keep = []
     rules = cfg.boundary_rules() if hasattr(cfg, "boundary_rules") else []
     for face, kind, vals in rules:
@@ -134,6 +136,35 @@ def fields(cfg, qj: np.ndarray) -> dict:
     names = ["rho", "u", "v", "w", "p", "T", "mu", "sensor", "mut", "qc2"]
     shp = (cfg.nx, cfg.ny, cfg.nz) if cfg.dim == 3 else (cfg.nx, cfg.ny)
     return {nm: out[i * n:(i + 1) * n].reshape(shp, order="F") for i, nm in enumerate(names)}
+
+
+class Stepper:
+    """Stage-by-stage stepping of one state (orc_stage), for z slabs that exchange
+    halo planes between stages.  q (Q^n) and q2 (the stage state) are Fortran-order
+    arrays in the reference layout; rs is the RK4 accumulator."""
+
+    def __init__(self, cfg, qj: np.ndarray):
+        self.cfg = cfg
+        self.c = make_cfg(cfg)
+        self.dx, self.dy, self.dz = _axes(cfg)
+        self.q = np.asfortranarray(qj, dtype=np.float64).copy(order="F")
+        self.q2 = self.q.copy(order="F")
+        nv = cfg.dim + 2
+        shape = (cfg.nx - 2, nv, cfg.ny - 2, cfg.nz - 2) if cfg.dim == 3 else (cfg.nx - 2, nv, cfg.ny - 2)
+        self.rs = np.zeros(shape, order="F")
+
+    @property
+    def stages(self) -> int:
+        return 3 if self.cfg.rk == 3 else 4
+
+    def written(self, stage: int) -> np.ndarray:
+        """The array stage `stage` writes (Q^{n+1} after the last stage)."""
+        return self.q if stage == self.stages - 1 else self.q2
+
+    def stage(self, st: int) -> None:
+        rc = lib().orc_stage(C.byref(self.c), _ptr(self.dx), _ptr(self.dy), _ptr(self.dz), _ptr(self.q),
+                             _ptr(self.q2), _ptr(self.rs), int(st))
+        assert rc == 0
 
 
 def fill_ghosts(cfg, qj: np.ndarray) -> np.ndarray:

@@ -35,7 +35,8 @@ FAULT_TIMEOUT = 4
 SYMBOLS = [
     "oux_create", "oux_destroy", "oux_last_error", "oux_abi_version", "oux_state_bytes",
     "oux_scratch_bytes", "oux_layout_of", "oux_bind", "oux_set_state", "oux_get_state",
-    "oux_pack_state", "oux_unpack_state", "oux_set_boundary", "oux_fill_ghosts", "oux_rhs", "oux_step", "oux_get_state_async",
+    "oux_pack_state", "oux_unpack_state", "oux_set_boundary", "oux_fill_ghosts", "oux_rhs",
+    "oux_stage", "oux_halo_bytes", "oux_halo_pack", "oux_halo_unpack", "oux_step", "oux_get_state_async",
     "oux_diagnostics", "oux_check_state", "oux_status", "oux_profile", "oux_profile_read",
     "oux_host_ref_diagnostics", "oux_launch_count", "oux_rhs_noalloc",
     "oux_batch_create", "oux_batch_workspace_bytes", "oux_batch_bind", "oux_batch_step",
@@ -102,6 +103,10 @@ def _load() -> C.CDLL:
         "oux_pack_state": (C.c_int, [vp, dp, vp]),
         "oux_unpack_state": (C.c_int, [vp, vp, dp]),
         "oux_set_boundary": (C.c_int, [vp, C.c_int32, C.c_int32, vp]),
+        "oux_stage": (C.c_int, [vp, C.c_int32, vp]),
+        "oux_halo_bytes": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_size_t)]),
+        "oux_halo_pack": (C.c_int, [vp, C.c_int32, vp, vp, vp]),
+        "oux_halo_unpack": (C.c_int, [vp, C.c_int32, vp, vp, vp]),
         "oux_fill_ghosts": (C.c_int, [vp, vp]),
         "oux_rhs": (C.c_int, [vp, vp, vp]),
         "oux_step": (C.c_int, [vp, i32, vp]),

@@ -62,9 +62,18 @@ int validate(const oux_config* c, std::string& why) {
   if (c->tvd < 0 || c->tvd > 2) { why = "unknown tvd mode"; return OUX_E_INVALID; }
   if (c->slau < 0 || c->slau > 1) { why = "unknown SLAU variant"; return OUX_E_INVALID; }
   if (c->rk != 3 && c->rk != 4) { why = "rk must be 3 or 4"; return OUX_E_INVALID; }
-  if ((c->dim == 3 && c->bc_z) || c->bc_x < 0 || c->bc_x > 1 || c->bc_y < 0 || c->bc_y > 1) {
-    why = "boundaries: bc_z = 0 (periodic); bc_x, bc_y = 0 (periodic) or 1 (non-periodic, 2D Euler)";
+  if ((c->dim == 3 && c->bc_z != 0 && c->bc_z != 2) || c->bc_x < 0 || c->bc_x > 1 || c->bc_y < 0 ||
+      c->bc_y > 1) {
+    why = "boundaries: bc_z = 0 (periodic) or 2 (z-slab, halo planes from neighbours); bc_x, bc_y = 0 "
+          "(periodic) or 1 (non-periodic, 2D)";
     return OUX_E_INVALID;
+  }
+  if (c->dim == 3 && c->bc_z == 2) {
+    if (c->visc == OUX_LES) {
+      why = "z slabs (bc_z = 2): the SGS viscosity's edge layers wrap z, so LES runs are not built as slabs";
+      return OUX_E_INVALID;
+    }
+    if (c->nz < 3 * g) { why = "z slab (bc_z = 2) needs at least g interior planes (nz >= 3g)"; return OUX_E_INVALID; }
   }
   if ((c->bc_x == 1 || c->bc_y == 1) && c->dim != 2) {
     why = "non-periodic x / y (bc_x = 1, bc_y = 1) is built for 2D solves";
@@ -179,6 +188,7 @@ Geo make_geo(const oux_config& c) {
   G.gx = c.bc_x ? 1 : G.g;
   G.bcy = c.bc_y;
   G.gy = c.bc_y ? 1 : G.g;
+  G.bcz = c.dim == 3 ? c.bc_z : 0;
   G.bkind = 0;  // zero-gradient boundary cells until oux_set_boundary says otherwise
   for (int f = 0; f < 4; ++f) G.bfix[f] = nullptr;
   G.gamma_1 = c.gamma - 1.0;  // mod_constant.f90.fypp gamma_1, over_gamma_1
@@ -513,41 +523,70 @@ int ghost(oux_handle* h, T* Q, cudaStream_t s) {
   return OUX_OK;
 }
 
-// nsteps time steps with compute type T (double: plain FP64 form; float: mixed form)
+// Stage st (0-based) of one time step with compute type T (double: plain FP64 form;
+// float: mixed form), followed by the ghost / boundary fill of the array it wrote.
 template <class T>
-int run_steps(oux_handle* h, int nsteps, cudaStream_t s) {
+int run_stage_n(oux_handle* h, int st, cudaStream_t s) {
   double* Qn = h->Q;
   T* Qs = reinterpret_cast<T*>(h->Qs);
-  for (int n = 0; n < nsteps; ++n) {
-    StepArgs<T> A = base_args<T>(h);
-    int rc;
-    if (h->cfg.rk == 3) {
-      // calc_time_dev.f90.fypp:81-101
+  StepArgs<T> A = base_args<T>(h);
+  int rc;
+  if (h->cfg.rk == 3) {
+    // calc_time_dev.f90.fypp:81-101
+    if (st == 0) {
       A.mode = CM_RK3_1; A.coef = 1.0;
       if ((rc = run_stage<T, double>(h, Qn, A, s))) return rc;
       ghost<T>(h, Qs, s);
+    } else if (st == 1) {
       A.mode = CM_RK3_2; A.coef = 0.25; A.c1 = 0.75; A.c2 = 0.25; A.c4 = 1.0;
       if ((rc = run_stage<T, T>(h, Qs, A, s))) return rc;
       ghost<T>(h, Qs, s);
+    } else {
       A.mode = CM_RK3_3; A.coef = 2.0; A.c1 = 2.0; A.c2 = 1.0; A.c4 = 1.0 / 3.0;
       if ((rc = run_stage<T, T>(h, Qs, A, s))) return rc;
       ghost<double>(h, Qn, s);
+    }
+  } else {
+    // calc_time_dev.f90.fypp:264-287
+    const double c1[3] = {0.5, 0.5, 1.0}, c2[3] = {1.0, 2.0, 2.0};
+    if (st < 3) {
+      A.mode = CM_RK4_S; A.coef = 1.0; A.c1 = c1[st]; A.c2 = c2[st];
+      if (st == 0) rc = run_stage<T, double>(h, Qn, A, s);
+      else rc = run_stage<T, T>(h, Qs, A, s);
+      if (rc) return rc;
+      ghost<T>(h, Qs, s);
     } else {
-      // calc_time_dev.f90.fypp:264-287
-      const double c1[3] = {0.5, 0.5, 1.0}, c2[3] = {1.0, 2.0, 2.0};
-      for (int st = 0; st < 3; ++st) {
-        A.mode = CM_RK4_S; A.coef = 1.0; A.c1 = c1[st]; A.c2 = c2[st];
-        if (st == 0) rc = run_stage<T, double>(h, Qn, A, s);
-        else rc = run_stage<T, T>(h, Qs, A, s);
-        if (rc) return rc;
-        ghost<T>(h, Qs, s);
-      }
       A.mode = CM_RK4_4; A.coef = 1.0;
       if ((rc = run_stage<T, T>(h, Qs, A, s))) return rc;
       ghost<double>(h, Qn, s);
     }
   }
   return OUX_OK;
+}
+
+// nsteps time steps
+template <class T>
+int run_steps(oux_handle* h, int nsteps, cudaStream_t s) {
+  const int nst = h->cfg.rk == 3 ? 3 : 4;
+  for (int n = 0; n < nsteps; ++n)
+    for (int st = 0; st < nst; ++st) {
+      int rc = run_stage_n<T>(h, st, s);
+      if (rc) return rc;
+    }
+  return OUX_OK;
+}
+
+// The array stage st writes (Q^n after the last stage, else the stage state) and
+// its element size.
+void stage_array(oux_handle* h, int st, unsigned char** base, size_t* elem) {
+  const int nst = h->cfg.rk == 3 ? 3 : 4;
+  if (st == nst - 1) {
+    *base = reinterpret_cast<unsigned char*>(h->Q);
+    *elem = sizeof(double);
+  } else {
+    *base = reinterpret_cast<unsigned char*>(h->Qs);
+    *elem = h->mixed ? sizeof(float) : sizeof(double);
+  }
 }
 
 // ---- allocation-free residual (oux_rhs_noalloc) ------------------------------------
@@ -826,6 +865,70 @@ int oux_fill_ghosts(oux_handle* h, void* stream) {
   ghost<double>(h, h->Q, (cudaStream_t)stream);
   OUX_CUDA(cudaGetLastError());
   return OUX_OK;
+}
+
+int oux_stage(oux_handle* h, int32_t stage, void* stream) {
+  if (!h) return fail(OUX_E_INVALID, "null handle");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  const int nst = h->cfg.rk == 3 ? 3 : 4;
+  if (stage < 0 || stage >= nst) return fail(OUX_E_INVALID, "stage out of range (0..2 for RK3, 0..3 for RK4)");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = h->mixed ? run_stage_n<float>(h, stage, s) : run_stage_n<double>(h, stage, s);
+  if (rc) return rc;
+  OUX_CUDA(cudaGetLastError());
+  return OUX_OK;
+}
+
+int oux_halo_bytes(const oux_handle* h, int32_t stage, size_t* bytes) {
+  if (!h || !bytes) return fail(OUX_E_INVALID, "null argument");
+  const int nst = h->cfg.rk == 3 ? 3 : 4;
+  if (stage < 0 || stage >= nst) return fail(OUX_E_INVALID, "stage out of range");
+  size_t elem = stage == nst - 1 ? sizeof(double) : (h->mixed ? sizeof(float) : sizeof(double));
+  *bytes = (size_t)h->nv * h->G.g * h->G.plane * elem;
+  return OUX_OK;
+}
+
+// g planes of every variable of the array `stage` writes, between the state and a
+// packed buffer [nv][g][plane]: pack (to_buf) copies planes k0..k0+g-1 into buf,
+// unpack copies buf into them.
+static int halo_copy(oux_handle* h, int stage, int k0, void* buf, bool to_buf, cudaStream_t s) {
+  unsigned char* base;
+  size_t elem;
+  stage_array(h, stage, &base, &elem);
+  const Geo& G = h->G;
+  const size_t chunk = (size_t)G.g * G.plane * elem;
+  for (int l = 0; l < h->nv; ++l) {
+    unsigned char* st = base + ((size_t)l * G.vs + (size_t)k0 * G.plane) * elem;
+    unsigned char* bf = static_cast<unsigned char*>(buf) + (size_t)l * chunk;
+    OUX_CUDA(cudaMemcpyAsync(to_buf ? bf : st, to_buf ? st : bf, chunk, cudaMemcpyDeviceToDevice, s));
+  }
+  return OUX_OK;
+}
+
+int oux_halo_pack(oux_handle* h, int32_t stage, void* lo_dev, void* hi_dev, void* stream) {
+  if (!h || !lo_dev || !hi_dev) return fail(OUX_E_INVALID, "null argument");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  if (h->G.dim != 3 || h->G.bcz != 2) return fail(OUX_E_INVALID, "halo exchange needs a z slab (bc_z = 2)");
+  const int nst = h->cfg.rk == 3 ? 3 : 4;
+  if (stage < 0 || stage >= nst) return fail(OUX_E_INVALID, "stage out of range");
+  const int g = h->G.g, nz = h->G.nz;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = halo_copy(h, stage, g, lo_dev, true, s);  // lowest interior planes -> the rank below
+  if (!rc) rc = halo_copy(h, stage, nz - 2 * g, hi_dev, true, s);  // highest -> the rank above
+  return rc;
+}
+
+int oux_halo_unpack(oux_handle* h, int32_t stage, const void* lo_dev, const void* hi_dev, void* stream) {
+  if (!h || !lo_dev || !hi_dev) return fail(OUX_E_INVALID, "null argument");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  if (h->G.dim != 3 || h->G.bcz != 2) return fail(OUX_E_INVALID, "halo exchange needs a z slab (bc_z = 2)");
+  const int nst = h->cfg.rk == 3 ? 3 : 4;
+  if (stage < 0 || stage >= nst) return fail(OUX_E_INVALID, "stage out of range");
+  const int g = h->G.g, nz = h->G.nz;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = halo_copy(h, stage, 0, const_cast<void*>(lo_dev), false, s);  // from the rank below
+  if (!rc) rc = halo_copy(h, stage, nz - g, const_cast<void*>(hi_dev), false, s);  // from the rank above
+  return rc;
 }
 
 int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fixed_dev) {

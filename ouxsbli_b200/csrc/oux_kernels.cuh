@@ -30,6 +30,7 @@ struct Geo {
   int dim, nx, ny, nz, g;     // padded extents, ghost width
   int gx, bcx;                // x ghost width of the cell ranges (g, or 1 for a non-periodic x), bc_x
   int gy, bcy;                // the same for y
+  int bcz;                    // 2: z slab, the z ghost planes come from the neighbouring slabs
   int bkind;                  // boundary-cell rule of face f (enum oux_bc_kind) in bits 4f..4f+3;
                               // faces 0..3: x low, x high, y low, y high
   int64_t sx, plane, vs;      // row stride, plane stride, variable stride (elements)
@@ -379,10 +380,11 @@ __global__ void k_mut_edges(Geo G, Fields<T> W) {
 // from interior cells only, so the cells can be filled in any order.
 // The three groups enumerate z-ghost planes, y-ghost rows of interior planes and
 // x-ghost cells of interior rows without touching interior cells.
+// A z slab (bcz = 2) leaves its z ghost planes to the halo exchange.
 __host__ __device__ inline int64_t ghost_cells(const Geo& G) {
   const int g = G.g, gy = G.gy;
   const int Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
-  const int gz = (G.dim == 3) ? 2 * g : 0;
+  const int gz = (G.dim == 3 && G.bcz != 2) ? 2 * g : 0;
   return (int64_t)gz * G.ny * G.nx + (int64_t)Nz * (2 * gy) * G.nx + (int64_t)Nz * Ny * (2 * G.gx);
 }
 
@@ -411,7 +413,7 @@ template <class T>
 __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t, const double* Qn = nullptr) {
   const int g = G.g, gx = G.gx, gy = G.gy;
   const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
-  const int gz = (G.dim == 3) ? 2 * g : 0;
+  const int gz = (G.dim == 3 && G.bcz != 2) ? 2 * g : 0;
   int64_t nA = (int64_t)gz * G.ny * G.nx;            // z ghost planes
   int64_t nB = (int64_t)Nz * (2 * gy) * G.nx;        // y ghost rows
   int zo = (G.dim == 3) ? g : 0;

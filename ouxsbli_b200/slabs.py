@@ -1,0 +1,179 @@
+"""Z-slab decomposition of one 3D solve over ranks: the reference's COMMZ path
+(3D_solver/src/calc_para.f90:343-384, exchanged after every RK stage in
+3D_solver/src/calc_time_dev.f90.fypp:465-498).
+
+The global grid's Nz interior planes are split evenly over `world` ranks. Each rank
+holds its Nz / world planes plus g ghost planes at each z end (`bc_z = 2`: the library
+leaves those planes to the caller). After every stage the rank sends the g lowest
+interior planes of the array the stage wrote to the rank below and the g highest to
+the rank above (periodic in rank), and writes what it receives into its ghost
+planes. x and y stay periodic within the slab.
+
+Two exchanges are provided: `halo_exchange` over a torch.distributed process group
+(NCCL between GPUs, gloo for host tensors), and `LocalSlabs`, which runs all slabs
+of a grid in one process on one device and exchanges by device copies, one slab
+after the other (no kernel waits on another slab's).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+import torch
+import torch.distributed as dist
+
+from ._lib import LIB, check
+from .solver import Solver, SolverConfig
+
+# message tags: a rank's highest planes go up (received as the lower halo), its
+# lowest planes go down (received as the upper halo)
+TAG_UP, TAG_DOWN = 1, 2
+
+
+def slab_bounds(nz: int, g: int, rank: int, world: int) -> tuple[int, int]:
+    """(k0, nz_local): the slab's first global plane (ghosts included) and its plane count."""
+    Nz = nz - 2 * g
+    if world < 1 or Nz % world:
+        raise ValueError(f"{Nz} interior z planes do not split evenly over {world} ranks")
+    n = Nz // world
+    if n < g:
+        raise ValueError(f"a slab of {n} planes is thinner than the halo ({g} planes)")
+    return rank * n, n + 2 * g
+
+
+def slab_config(cfg: SolverConfig, rank: int, world: int) -> tuple[SolverConfig, int]:
+    """The rank's local configuration (bc_z = 2, its z spacings) and its k0."""
+    if cfg.dim != 3:
+        raise ValueError("z slabs need a 3D configuration")
+    k0, n = slab_bounds(cfg.nz, cfg.g, rank, world)
+    dz = np.asarray(cfg.dz, dtype=np.float64)[k0:k0 + n - 1].copy()
+    return dataclasses.replace(cfg, nz=n, dz=dz, bc_z=2), k0
+
+
+def slab_state(qj: np.ndarray, cfg: SolverConfig, rank: int, world: int) -> np.ndarray:
+    """The rank's part of a global state in the reference layout QJ(nx, nv, ny, nz)."""
+    k0, n = slab_bounds(cfg.nz, cfg.g, rank, world)
+    return np.asfortranarray(qj[:, :, :, k0:k0 + n])
+
+
+def halo_exchange(send_lo: torch.Tensor, send_hi: torch.Tensor, recv_lo: torch.Tensor, recv_hi: torch.Tensor,
+                  rank: int, world: int, group=None) -> None:
+    """Send `send_lo` down and `send_hi` up; receive the lower halo from below into
+    `recv_lo` and the upper halo from above into `recv_hi` (periodic in rank).
+
+    Sends and receives are posted in the same order on every rank (up first, then
+    down) and tagged, so two ranks that are each other's upper and lower neighbour
+    match them correctly."""
+    if world == 1:
+        recv_lo.copy_(send_hi)
+        recv_hi.copy_(send_lo)
+        return
+    up, down = (rank + 1) % world, (rank - 1) % world
+    ops = [dist.P2POp(dist.isend, send_hi, up, group, TAG_UP),
+           dist.P2POp(dist.irecv, recv_lo, down, group, TAG_UP),
+           dist.P2POp(dist.isend, send_lo, down, group, TAG_DOWN),
+           dist.P2POp(dist.irecv, recv_hi, up, group, TAG_DOWN)]
+    for req in dist.batch_isend_irecv(ops):
+        req.wait()
+
+
+class SlabSolver:
+    """One rank's slab of a global 3D solve, driven stage by stage with halo exchanges."""
+
+    def __init__(self, cfg: SolverConfig, rank: int, world: int, device, group=None):
+        self.global_cfg = cfg
+        self.rank, self.world, self.group = rank, world, group
+        self.cfg, self.k0 = slab_config(cfg, rank, world)
+        self.solver = Solver(self.cfg, device)
+        self.device = self.solver.device
+        self.stages = 3 if cfg.rk == 3 else 4
+        nbytes = max(self._halo_bytes(st) for st in range(self.stages))
+        self.bufs = [torch.empty(nbytes, dtype=torch.uint8, device=self.device) for _ in range(4)]
+
+    def _halo_bytes(self, stage: int) -> int:
+        b = C.c_size_t()
+        check(LIB.oux_halo_bytes(self.solver._h, stage, C.byref(b)))
+        return b.value
+
+    def set_global_state(self, qj: np.ndarray) -> None:
+        self.solver.set_state(slab_state(qj, self.global_cfg, self.rank, self.world))
+
+    def get_state(self) -> np.ndarray:
+        return self.solver.get_state()
+
+    # the three steps of one stage, split so that a group of slabs in one process can
+    # interleave them
+    def run_stage(self, st: int) -> None:
+        with torch.cuda.device(self.device):
+            check(LIB.oux_stage(self.solver._h, st, self.solver._s()))
+
+    def pack(self, st: int) -> tuple[torch.Tensor, torch.Tensor]:
+        n = self._halo_bytes(st)
+        lo, hi = self.bufs[0][:n], self.bufs[1][:n]
+        with torch.cuda.device(self.device):
+            check(LIB.oux_halo_pack(self.solver._h, st, C.c_void_p(lo.data_ptr()), C.c_void_p(hi.data_ptr()),
+                                    self.solver._s()))
+        return lo, hi
+
+    def recv_buffers(self, st: int) -> tuple[torch.Tensor, torch.Tensor]:
+        n = self._halo_bytes(st)
+        return self.bufs[2][:n], self.bufs[3][:n]
+
+    def unpack(self, st: int) -> None:
+        lo, hi = self.recv_buffers(st)
+        with torch.cuda.device(self.device):
+            check(LIB.oux_halo_unpack(self.solver._h, st, C.c_void_p(lo.data_ptr()), C.c_void_p(hi.data_ptr()),
+                                      self.solver._s()))
+
+    def step(self, nsteps: int = 1) -> None:
+        """nsteps time steps, exchanging halos with the neighbouring ranks after each stage."""
+        for _ in range(nsteps):
+            for st in range(self.stages):
+                self.run_stage(st)
+                send_lo, send_hi = self.pack(st)
+                recv_lo, recv_hi = self.recv_buffers(st)
+                halo_exchange(send_lo, send_hi, recv_lo, recv_hi, self.rank, self.world, self.group)
+                self.unpack(st)
+
+    def close(self) -> None:
+        self.solver.close()
+
+
+class LocalSlabs:
+    """All `world` slabs of a global 3D solve in one process on one device: the
+    decomposition without a process group (halo exchange by device copies)."""
+
+    def __init__(self, cfg: SolverConfig, world: int, device="cuda:0"):
+        self.cfg = cfg
+        self.world = world
+        self.slabs = [SlabSolver(cfg, r, world, device) for r in range(world)]
+
+    def set_state(self, qj: np.ndarray) -> None:
+        for s in self.slabs:
+            s.set_global_state(qj)
+
+    def step(self, nsteps: int = 1) -> None:
+        W = self.world
+        for _ in range(nsteps):
+            for st in range(self.slabs[0].stages):
+                for s in self.slabs:
+                    s.run_stage(st)
+                sent = [s.pack(st) for s in self.slabs]
+                for r, s in enumerate(self.slabs):
+                    recv_lo, recv_hi = s.recv_buffers(st)
+                    recv_lo.copy_(sent[(r - 1) % W][1])  # the highest planes of the slab below
+                    recv_hi.copy_(sent[(r + 1) % W][0])  # the lowest planes of the slab above
+                for s in self.slabs:
+                    s.unpack(st)
+
+    def get_state(self) -> np.ndarray:
+        """The global state reassembled (ghost planes from the first and last slab)."""
+        g = self.cfg.g
+        parts = [s.get_state() for s in self.slabs]
+        inner = [p[:, :, :, g:-g] for p in parts]
+        return np.asfortranarray(np.concatenate([parts[0][:, :, :, :g], *inner, parts[-1][:, :, :, -g:]], axis=3))
+
+    def close(self) -> None:
+        for s in self.slabs:
+            s.close()

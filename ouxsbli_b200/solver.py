@@ -35,6 +35,7 @@ class SolverConfig:
     precision: str = "fp64"        # fp64 | mixed (FP32 stage states/fluxes, FP64 Q^n + accumulation)
     bc_x: int = 0                  # 0 periodic; 1 non-periodic x (boundary flux kernels, boundary cells; 2D)
     bc_y: int = 0                  # the same for y (2D)
+    bc_z: int = 0                  # 0 periodic; 2 z slab of a larger grid (ghost planes from halo exchange)
     # rules of the non-periodic faces ("x_lo", "x_hi", "y_lo", "y_hi"): "zero_gradient"
     # (the default), "slip_wall", "noslip_wall" or ("fixed", values (nv, ny) for x faces /
     # (nv, nx) for y faces, of Q/J)
@@ -102,7 +103,7 @@ class SolverConfig:
         c.rk = self.rk
         c.bc_x = self.bc_x
         c.bc_y = self.bc_y
-        c.bc_z = 0
+        c.bc_z = self.bc_z if self.dim == 3 else 0
         c.precision = _lib.PRECISION[self.precision]
         c.gamma, c.R, c.Pr, c.Prt, c.threshold, c.dt = (self.gamma, self.R, self.Pr, self.Prt,
                                                          self.threshold, self.dt)
