@@ -186,6 +186,7 @@ def test_z_slabs_match_the_undivided_solve(world, rk, precision, cuda_device):
     rounding differs from the undivided mixed run (relative L2 <= 1e-6)."""
     import dataclasses
     from ouxsbli_b200.slabs import LocalSlabs
+    from ouxsbli_b200.solver import Solver, SolverConfig
     from ouxsbli_b200.cases import CASES, build_initial
     from ouxsbli_b200.grid import jacobian, to_qj
     p = dict(CASES["NSTGV"].params)
