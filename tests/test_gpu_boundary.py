@@ -388,3 +388,36 @@ def test_shear_decay_between_noslip_walls(order, visc_order, scheme, cuda_device
     ratio = amplitude(q) / amplitude(qj)
     expect = math.exp(-nu * math.pi ** 2 * nsteps * cfg.dt / H ** 2)
     assert abs(ratio / expect - 1.0) < 2e-3, (ratio, expect)
+
+
+def test_walled_members_in_one_batch_bitexact(cuda_device):
+    """Batched steps (one persistent kernel over all members) with non-periodic members
+    beside a periodic one: every member bit-identical to its single-solve run."""
+    from helpers import vortex2d
+    from ouxsbli_b200.batch import Batch
+    euler = [duct(33, 17, order=4, rules=OS_RULES, scheme="SLAU", tvd="hybrid", rk=3),
+             duct(41, 23, order=4, rules=WALLS, scheme="KEEP", rk=3),
+             vortex2d(36, order=4, beta=2.0, mach=0.4, scheme="KEEP", visc="Euler", rk=3)]
+    viscous = [wall_channel(24, 21, order=4, visc_order=4, rules=CHANNEL, scheme="KEEP", rk=4)[:2],
+               wall_channel(16, 25, order=4, visc_order=4, rules=BL_RULES, bc_x=1, scheme="SLAU", rk=4)[:2]]
+    for cases in (euler, viscous):
+        ref = []
+        for cfg, qj in cases:
+            s = Solver(cfg, cuda_device)
+            s.set_state(qj)
+            s.step(5)
+            ref.append(s.get_state())
+            s.close()
+        solvers = []
+        for cfg, qj in cases:
+            s = Solver(cfg, cuda_device)
+            s.set_state(qj)
+            solvers.append(s)
+        b = Batch(solvers)
+        b.step(5)
+        assert b.status() == 0
+        for s, r in zip(solvers, ref):
+            np.testing.assert_array_equal(s.get_state(), r)
+        b.close()
+        for s in solvers:
+            s.close()
