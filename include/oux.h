@@ -170,13 +170,33 @@ int oux_halo_unpack(oux_handle* h, int32_t stage, const void* lo_dev, const void
  *                  device memory owned by the caller and read at every fill until
  *                  the face is set again.  In the mixed form the stage increments
  *                  of FIXED cells are 0 (Q^n holds the values).
- * y faces are applied first over every column, then x faces over every row, so a
- * corner takes its x rule applied to the y-boundary cell next to it (the order of
- * 2D_solver/OS/set.f90).  The face's direction must be non-periodic.  Set rules
- * before oux_batch_create when the handle joins a batch. */
+ * By default y faces are applied first over every column, then x faces over every
+ * row, so a corner takes its x rule applied to the y-boundary cell next to it (the
+ * order of 2D_solver/OS/set.f90; oux_set_boundary_order reverses it).  The face's
+ * direction must be non-periodic.  Set rules before oux_batch_create when the
+ * handle joins a batch. */
 enum oux_face { OUX_FACE_X_LO = 0, OUX_FACE_X_HI = 1, OUX_FACE_Y_LO = 2, OUX_FACE_Y_HI = 3 };
-enum oux_bc_kind { OUX_BC_ZERO_GRADIENT = 0, OUX_BC_SLIP_WALL = 1, OUX_BC_FIXED = 2, OUX_BC_NOSLIP_WALL = 3 };
+enum oux_bc_kind { OUX_BC_ZERO_GRADIENT = 0, OUX_BC_SLIP_WALL = 1, OUX_BC_FIXED = 2, OUX_BC_NOSLIP_WALL = 3,
+                   OUX_BC_FARFIELD = 4 };
 int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fixed_dev);
+/* FARFIELD (x high or y high): the boundary state from the Riemann invariants along
+ * the outward normal, R+ = u_n + 2c/(gamma-1) of the neighbour and R- = u_normal -
+ * 2 c_inf/(gamma-1) of the far field; u_n = (R+ + R-)/2, c = (gamma-1)(R+ - R-)/4,
+ * rho = rho_inf (c / c_inf)^(2/(gamma-1)), p = rho c^2 / gamma, tangential velocity
+ * u_tangential (the top row of 2D_solver/BL0/set.f90). */
+int oux_set_boundary_farfield(oux_handle* h, int32_t face, double rho_inf, double u_tangential,
+                              double u_normal, double c_inf);
+/* A rule per position along the face: kinds_dev holds one enum oux_bc_kind per
+ * boundary cell (ny for x faces, nx for y faces), device memory owned by the caller
+ * and read at every fill; FIXED positions take the face's values of
+ * oux_set_boundary, FARFIELD positions its far-field state.  NULL restores the
+ * face's single rule.  (2D_solver/BL0/set.f90: a slip-like copy ahead of the plate,
+ * a no-slip wall along it.) */
+int oux_set_boundary_cells(oux_handle* h, int32_t face, const int8_t* kinds_dev);
+/* y_last = 1: the y faces are applied after the x faces, so a corner takes its y
+ * rule of the x-boundary value beside it (2D_solver/BL0/set.f90); 0 (default): the
+ * reverse (2D_solver/OS/set.f90). */
+int oux_set_boundary_order(oux_handle* h, int32_t y_last);
 
 /* --- hot path ----------------------------------------------------------- */
 /* Ghost / boundary-cell fill: periodic images, set_bc_cyclic{2,4,6}

@@ -57,6 +57,9 @@ typedef struct orc_config {
                       // 0 zero gradient, 1 slip wall, 2 fixed values, 3 no-slip wall
   const double* bfix[4];  // fixed values of Q/J, nv x (ny for x faces, nx for y faces), variable-major
   int bc_z;           // 0 periodic; 2 z slab: the z ghost planes are left to the halo exchange
+  int ylast;          // 1: y faces applied after x faces (corners take their y rule)
+  const signed char* bkinds[4];  // per-position rule of a face, or null
+  double bpar[4][4];  // far-field state of a face: rho, tangential velocity, normal velocity, c
 } orc_config;
 
 }  // extern "C"
@@ -1278,8 +1281,10 @@ void residual(Ctx& C, double coef, std::vector<double>& Rout) {
 // row; 2D_solver/ST/set.f90: zero-gradient x).  Rules: 0 copy, 1 copy with the normal
 // momentum negated, 2 the given values, 3 no-slip wall (the neighbour's density and
 // pressure, zero momentum).
-void bc_rule(const Ctx& C, int f, int pos, double* v) {  // pos: 1-based j (x faces) / i (y faces)
-  int kind = C.c.bkind[f];
+// pos: 1-based j (x faces) / i (y faces); (bi, bj), (ni, nj): 1-based boundary cell and
+// neighbour, for the Jacobian of the far-field rule
+void bc_rule(const Ctx& C, int f, int pos, double* v, int bi, int bj, int ni, int nj) {
+  int kind = C.c.bkinds[f] ? (int)C.c.bkinds[f][pos - 1] : C.c.bkind[f];
   if (kind == 1) {
     int n = f < 2 ? 1 : 2;
     v[n] = -v[n];
@@ -1291,6 +1296,25 @@ void bc_rule(const Ctx& C, int f, int pos, double* v) {  // pos: 1-based j (x fa
     v[1] = 0.0;
     v[2] = 0.0;
     v[3] = p_wall * C.K.over_gamma_1;
+  } else if (kind == 4) {  // far field: Riemann invariants, the top row of 2D_solver/BL0/set.f90
+    const double* P = C.c.bpar[f];
+    const int n = f < 2 ? 1 : 2, t = 3 - n;
+    const double Jn = C.g.jac[(size_t)(nj - 1) * C.nx + (ni - 1)];
+    const double Jt = 1.0 / C.g.jac[(size_t)(bj - 1) * C.nx + (bi - 1)];
+    const double pin = C.K.gamma_1 * (v[3] - 0.5 * (v[1] * v[1] + v[2] * v[2]) / v[0]) * Jn;
+    const double rhoin = v[0] * Jn;
+    const double cin = std::sqrt(C.K.gamma * pin / rhoin);
+    const double vin = v[n] / v[0];
+    const double Rp = vin + 2.0 * cin * C.K.over_gamma_1;
+    const double Rm = P[2] - 2.0 * P[3] * C.K.over_gamma_1;
+    const double vb = 0.5 * (Rp + Rm);
+    const double cb = 0.25 * C.K.gamma_1 * (Rp - Rm);
+    const double rhob = std::pow(cb * (1.0 / P[3]), 2.0 * C.K.over_gamma_1) * P[0];
+    const double pb = (rhob * (cb * cb)) * (1.0 / C.K.gamma);
+    v[0] = rhob * Jt;
+    v[t] = rhob * P[1] * Jt;
+    v[n] = rhob * vb * Jt;
+    v[3] = (pb * C.K.over_gamma_1 + 0.5 * rhob * (P[1] * P[1] + vb * vb)) * Jt;
   }
 }
 
@@ -1319,22 +1343,26 @@ void fill_ghosts(const Ctx& C, double* Q) {
           if (ii == i && jj == j && kk == k) continue;
           for (int l = 1; l <= nv; ++l) Q[C.qidx(i, l, j, k)] = Q[C.qidx(ii, l, jj, kk)];
           continue;
+        } else if (xb && yb) {  // corner: the rule applied last, to the other one's boundary value
+          int in = i == 1 ? 2 : nx - 1, jn = j == 1 ? 2 : ny - 1;
+          for (int l = 1; l <= nv; ++l) v[l - 1] = Q[C.qidx(in, l, jn, kk)];
+          if (!C.c.ylast) {
+            bc_rule(C, j == 1 ? 2 : 3, in, v, in, j, in, jn);
+            bc_rule(C, i == 1 ? 0 : 1, j, v, i, j, in, j);
+          } else {
+            bc_rule(C, i == 1 ? 0 : 1, jn, v, i, jn, in, jn);
+            bc_rule(C, j == 1 ? 2 : 3, i, v, i, j, i, jn);
+          }
         } else if (xb) {
           int in = i == 1 ? 2 : nx - 1;
-          if (yb) {
-            int jn = j == 1 ? 2 : ny - 1;
-            for (int l = 1; l <= nv; ++l) v[l - 1] = Q[C.qidx(in, l, jn, kk)];
-            bc_rule(C, j == 1 ? 2 : 3, in, v);
-          } else {
-            int jj = C.c.bc_y ? j : wrap(j, gy, Ny);
-            for (int l = 1; l <= nv; ++l) v[l - 1] = Q[C.qidx(in, l, jj, kk)];
-          }
-          bc_rule(C, i == 1 ? 0 : 1, j, v);
+          int jj = C.c.bc_y ? j : wrap(j, gy, Ny);
+          for (int l = 1; l <= nv; ++l) v[l - 1] = Q[C.qidx(in, l, jj, kk)];
+          bc_rule(C, i == 1 ? 0 : 1, j, v, i, jj, in, jj);
         } else {
           int jn = j == 1 ? 2 : ny - 1;
           int ii = C.c.bc_x ? i : wrap(i, gx, Nx);
           for (int l = 1; l <= nv; ++l) v[l - 1] = Q[C.qidx(ii, l, jn, kk)];
-          bc_rule(C, j == 1 ? 2 : 3, i, v);
+          bc_rule(C, j == 1 ? 2 : 3, i, v, ii, j, ii, jn);
         }
         for (int l = 1; l <= nv; ++l) Q[C.qidx(i, l, j, k)] = v[l - 1];
       }

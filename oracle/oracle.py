@@ -40,7 +40,8 @@ class _Cfg(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("dim", "nx", "ny", "nz", "order", "scheme", "visc", "visc_order",
                                        "visc_stencil", "tvd", "slau", "rk", "bc_x")] + \
                [(n, C.c_double) for n in ("gamma", "R", "Pr", "Prt", "threshold", "dt")] + \
-               [("bc_y", C.c_int), ("bkind", C.c_int * 4), ("bfix", C.POINTER(C.c_double) * 4), ("bc_z", C.c_int)]
+               [("bc_y", C.c_int), ("bkind", C.c_int * 4), ("bfix", C.POINTER(C.c_double) * 4), ("bc_z", C.c_int),
+                ("ylast", C.c_int), ("bkinds", C.POINTER(C.c_int8) * 4), ("bpar", (C.c_double * 4) * 4)]
 
 
 _lib = None
@@ -86,11 +87,19 @@ def make_cfg(cfg) -> _Cfg:
     c.bc_z = getattr(cfg, "bc_z", 0)
     c._keep = []
     rules = cfg.boundary_rules() if hasattr(cfg, "boundary_rules") else []
-    for face, kind, vals in rules:
-        c.bkind[face] = kind
-        if vals is not None:
-            c._keep.append(vals)
-            c.bfix[face] = _ptr(vals)
+    for r in rules:
+        face = r["face"]
+        c.bkind[face] = r["kind"]
+        if r["fixed"] is not None:
+            c._keep.append(r["fixed"])
+            c.bfix[face] = _ptr(r["fixed"])
+        if r["farfield"] is not None:
+            for q in range(4):
+                c.bpar[face][q] = r["farfield"][q]
+        if r["cells"] is not None:
+            c._keep.append(r["cells"])
+            c.bkinds[face] = r["cells"].ctypes.data_as(C.POINTER(C.c_int8))
+    c.ylast = 1 if getattr(cfg, "boundary_order", "x_last") == "y_last" else 0
     c.gamma, c.R, c.Pr, c.Prt, c.threshold, c.dt = cfg.gamma, cfg.R, cfg.Pr, cfg.Prt, cfg.threshold, cfg.dt
     return c
 

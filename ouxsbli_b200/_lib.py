@@ -36,7 +36,8 @@ SYMBOLS = [
     "oux_create", "oux_destroy", "oux_last_error", "oux_abi_version", "oux_state_bytes",
     "oux_scratch_bytes", "oux_layout_of", "oux_bind", "oux_set_state", "oux_get_state",
     "oux_pack_state", "oux_unpack_state", "oux_set_boundary", "oux_fill_ghosts", "oux_rhs",
-    "oux_stage", "oux_halo_bytes", "oux_halo_pack", "oux_halo_unpack", "oux_step", "oux_get_state_async",
+    "oux_stage", "oux_halo_bytes", "oux_halo_pack", "oux_halo_unpack",
+    "oux_set_boundary_farfield", "oux_set_boundary_cells", "oux_set_boundary_order", "oux_step", "oux_get_state_async",
     "oux_diagnostics", "oux_check_state", "oux_status", "oux_profile", "oux_profile_read",
     "oux_host_ref_diagnostics", "oux_launch_count", "oux_rhs_noalloc",
     "oux_batch_create", "oux_batch_workspace_bytes", "oux_batch_bind", "oux_batch_step",
@@ -44,7 +45,7 @@ SYMBOLS = [
 ]
 NOALLOC_SCRATCH_BYTES = 32 << 20  # OUX_NOALLOC_SCRATCH_BYTES
 FACES = {"x_lo": 0, "x_hi": 1, "y_lo": 2, "y_hi": 3}                  # enum oux_face
-BC_KINDS = {"zero_gradient": 0, "slip_wall": 1, "fixed": 2, "noslip_wall": 3}  # enum oux_bc_kind
+BC_KINDS = {"zero_gradient": 0, "slip_wall": 1, "fixed": 2, "noslip_wall": 3, "farfield": 4}  # enum oux_bc_kind
 
 
 class OuxConfig(C.Structure):
@@ -103,6 +104,9 @@ def _load() -> C.CDLL:
         "oux_pack_state": (C.c_int, [vp, dp, vp]),
         "oux_unpack_state": (C.c_int, [vp, vp, dp]),
         "oux_set_boundary": (C.c_int, [vp, C.c_int32, C.c_int32, vp]),
+        "oux_set_boundary_farfield": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]),
+        "oux_set_boundary_cells": (C.c_int, [vp, C.c_int32, vp]),
+        "oux_set_boundary_order": (C.c_int, [vp, C.c_int32]),
         "oux_stage": (C.c_int, [vp, C.c_int32, vp]),
         "oux_halo_bytes": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_size_t)]),
         "oux_halo_pack": (C.c_int, [vp, C.c_int32, vp, vp, vp]),

@@ -124,7 +124,8 @@ class Case:
             gamma=p["gamma"], R=p["R"], Pr=p.get("Pr", 0.71), Prt=p.get("Prt", 0.9),
             threshold=p.get("threshold", 0.4), dt=p["dt"], dx=dx, dy=dy, dz=dz,
             bc_x=1 if c.get("BC_X") else 0, bc_y=1 if c.get("BC_Y") else 0,
-            boundary=self._case.boundary(p, jacobian(dx, dy, None)) if self._case.boundary else None)
+            boundary=self._case.boundary(p, jacobian(dx, dy, None)) if self._case.boundary else None,
+            boundary_order=self._case.boundary_order)
 
     def _initial(self):
         p = dict(self.globals)

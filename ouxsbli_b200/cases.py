@@ -36,6 +36,7 @@ class CaseDef:
     bc_x: bool = False        # the case's x boundaries are non-periodic (BC_X = True)
     bc_y: bool = False        # the case's y boundaries are non-periodic (BC_Y = True)
     boundary: Callable = None  # (params, J) -> rules of the non-periodic faces (SolverConfig.boundary)
+    boundary_order: str = "x_last"  # which rules the corners take last (SolverConfig.boundary_order)
 
 
 # ---------------------------------------------------------------------------
@@ -382,6 +383,76 @@ def _os_boundary(p: dict, J: np.ndarray) -> dict:
     return {"x_lo": ("fixed", inflow), "x_hi": "zero_gradient", "y_lo": "slip_wall", "y_hi": ("fixed", top)}
 
 
+# ---------------------------------------------------------------------------
+# Laminar boundary layer on a flat plate at Mach 2: 2D_solver/BL0 (mod_globals.f90,
+# set.f90).  Inflow at x low, zero gradient at x high; along y low a copy of the
+# neighbour ahead of the plate (the first nx/10 columns) and an adiabatic no-slip
+# wall after; a characteristic far field at y high; corners take their y rule (the
+# y rows are written after the x columns).
+# ---------------------------------------------------------------------------
+def _bl_derived(p: dict) -> dict:
+    p = dict(p)
+    g, R, M0 = p["gamma"], p["R"], p["M0"]
+    p.setdefault("Lx", 80.0 * p["blt"])
+    p.setdefault("Ly", 5.0 * p["blt"])
+    f = 1.0 + 0.5 * (g - 1.0) * M0 ** 2
+    p["p0"] = p["p_tot"] / f ** (g / (g - 1.0))
+    p["T0"] = p["T_tot"] / f
+    p["rho0"] = p["p0"] / (R * p["T0"])
+    p["u0"] = M0 * math.sqrt(g * R * p["T0"])
+    p["Cp"] = g * R / (g - 1.0)
+    p["Taw"] = p["T0"] * (1.0 + p["rf"] * 0.5 * (g - 1.0) * M0 ** 2)
+    # set_bc's inflow / far-field temperature and density (equal to T0, rho0 up to rounding)
+    p["T_bc"] = p["Taw"] - p["rf"] * p["u0"] ** 2 / (2.0 * p["Cp"])
+    p["rho_bc"] = p["p0"] / (R * p["T_bc"])
+    p["c_bc"] = math.sqrt(g * p["p0"] / p["rho_bc"])
+    if p.get("nt") is None:
+        p["nt"] = int(p["endT"] / (float(p["np"]) * p["dt"]))
+    return p
+
+
+def _bl_grid(p: dict):
+    """set_grid: uniform x nodes from 0; y nodes refined at the wall up to 3 blt
+    (dy = min(1, max(0.07, j / 128)) dx), then stretched by up to 1.75 dx."""
+    nx, ny, blt = p["nx"], p["ny"], p["blt"]
+    dx1 = p["Lx"] / (nx - 1)
+    dy1 = dx1
+    x = np.zeros(nx)
+    dx = np.full(nx - 1, dx1)
+    for i in range(nx - 1):
+        x[i + 1] = x[i] + dx[i]
+    y = np.zeros(ny)
+    dy = np.zeros(ny - 1)
+    ny_b = 0
+    for j in range(1, ny):  # Fortran j = 1 .. ny-1
+        if y[j - 1] <= 3.0 * blt:
+            dy[j - 1] = min(1.0, max(0.07, float(j) / 128.0)) * dy1
+            ny_b = j
+        else:
+            dy[j - 1] = dy1 * (1.0 + 0.75 * float(j - ny_b) / float(ny - ny_b))
+        y[j] = y[j - 1] + dy[j - 1]
+    return x, dx, y, dy
+
+
+def _bl_init(p: dict, x, y, z=None) -> np.ndarray:
+    nx, ny, gam = x.size, y.size, p["gamma"]
+    Q = np.zeros((nx, 4, ny), order="F")
+    Q[:, 0] = p["rho0"]
+    Q[:, 1] = p["rho0"] * p["u0"]
+    Q[:, 3] = p["p0"] / (gam - 1.0) + 0.5 * p["rho0"] * p["u0"] ** 2
+    return Q
+
+
+def _bl_boundary(p: dict, J: np.ndarray) -> dict:
+    nx, ny = J.shape
+    gam, rho, u0 = p["gamma"], p["rho_bc"], p["u0"]
+    free = np.array([rho, rho * u0, 0.0, p["p0"] / (gam - 1.0) + 0.5 * rho * u0 ** 2])
+    inflow = free[:, None] * (1.0 / J[0, :])[None, :]
+    return {"x_lo": ("fixed", inflow), "x_hi": "zero_gradient",
+            "y_lo": ("split", nx // 10 - 1, "zero_gradient", "noslip_wall"),
+            "y_hi": ("farfield", rho, u0, 0.0, p["c_bc"])}
+
+
 CASES: dict[str, CaseDef] = {
     "NSTGV": CaseDef(
         "NSTGV", 3,
@@ -435,6 +506,15 @@ CASES: dict[str, CaseDef] = {
              d2=0.05, dt=0.25 * 0.25e-3, endT=8.0, np=10, nt=None, threshold=0.4),
         _dsl_init, _dsl_derived,
         "Double shear layer (2D_solver/DSL)"),
+    "BL0": CaseDef(
+        "BL0", 2,
+        dict(VISC="NS", SCHEME="SLAU", ORDER=2, VISC_ORDER=2, TVD="none", SLAU_VARIANT="HRSLAU2", RK=3,
+             BC_X=True, BC_Y=True, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=1025, ny=129, blt=0.5e-3, endT=0.4e-3, np=40, dt=3.0e-9, nt=None, R=287.03, gamma=1.4, Pr=0.72,
+             Prt=0.9, M0=2.0, p_tot=100.0e3, T_tot=295.0, rf=0.89, threshold=0.4),
+        _bl_init, _bl_derived,
+        "Laminar boundary layer on a flat plate at Mach 2 (2D_solver/BL0)",
+        grid=_bl_grid, bc_x=True, bc_y=True, boundary=_bl_boundary, boundary_order="y_last"),
     "OS": CaseDef(
         "OS", 2,
         dict(VISC="Euler", SCHEME="SLAU", ORDER=6, TVD="hybrid", SLAU_VARIANT="HRSLAU2", RK=3,

@@ -191,8 +191,16 @@ Geo make_geo(const oux_config& c) {
   G.bcz = c.dim == 3 ? c.bc_z : 0;
   G.bkind = 0;  // zero-gradient boundary cells until oux_set_boundary says otherwise
   for (int f = 0; f < 4; ++f) G.bfix[f] = nullptr;
-  G.gamma_1 = c.gamma - 1.0;  // mod_constant.f90.fypp gamma_1, over_gamma_1
+  G.gamma_1 = c.gamma - 1.0;  // mod_constant.f90.fypp gamma_1, over_gamma_1, over_gamma
   G.over_gamma_1 = 1.0 / (c.gamma - 1.0);
+  G.gamma = c.gamma;
+  G.over_gamma = 1.0 / c.gamma;
+  for (int f = 0; f < 4; ++f) {
+    G.bkinds[f] = nullptr;
+    for (int q = 0; q < 4; ++q) G.bpar[f][q] = 0.0;
+  }
+  G.ylast = 0;
+  G.bjac = nullptr;
   G.sx = round_up(c.nx, 4);
   G.plane = G.sx * c.ny;
   G.vs = round_up(G.plane * G.nz, 32);
@@ -395,6 +403,7 @@ void carve(oux_handle* h) {
   h->M.inv_dy = take(h->inv_dy);
   h->M.inv_dz = take(h->inv_dz);
   h->M.jac = take(h->jac);
+  h->G.bjac = h->M.jac;
   if (h->cfg.dim == 3) {
     h->M.dtdxdy = take(h->dtdxdy);
     h->M.dtdydz = take(h->dtdydz);
@@ -934,7 +943,8 @@ int oux_halo_unpack(oux_handle* h, int32_t stage, const void* lo_dev, const void
 int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fixed_dev) {
   if (!h) return fail(OUX_E_INVALID, "null handle");
   if (face < 0 || face > 3) return fail(OUX_E_INVALID, "face must be 0..3 (x low, x high, y low, y high)");
-  if (kind < OUX_BC_ZERO_GRADIENT || kind > OUX_BC_NOSLIP_WALL) return fail(OUX_E_INVALID, "unknown boundary rule");
+  if (kind < OUX_BC_ZERO_GRADIENT || kind > OUX_BC_NOSLIP_WALL)
+    return fail(OUX_E_INVALID, "unknown boundary rule (far-field faces: oux_set_boundary_farfield)");
   if (!(face < 2 ? h->G.bcx : h->G.bcy))
     return fail(OUX_E_INVALID, "the face's direction is periodic (set bc_x / bc_y = 1)");
   if (kind == OUX_BC_FIXED && !fixed_dev) return fail(OUX_E_INVALID, "a fixed rule needs its device values");
@@ -942,6 +952,37 @@ int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fi
     return fail(OUX_E_INVALID, "fixed values must be 8-byte aligned");
   h->G.bkind = (h->G.bkind & ~(15 << (4 * face))) | (kind << (4 * face));
   h->G.bfix[face] = kind == OUX_BC_FIXED ? fixed_dev : nullptr;
+  return OUX_OK;
+}
+
+int oux_set_boundary_farfield(oux_handle* h, int32_t face, double rho_inf, double u_tangential,
+                              double u_normal, double c_inf) {
+  if (!h) return fail(OUX_E_INVALID, "null handle");
+  if (face != OUX_FACE_X_HI && face != OUX_FACE_Y_HI)
+    return fail(OUX_E_INVALID, "the far-field rule is built for the high faces (x high, y high)");
+  if (!(face < 2 ? h->G.bcx : h->G.bcy))
+    return fail(OUX_E_INVALID, "the face's direction is periodic (set bc_x / bc_y = 1)");
+  if (!(rho_inf > 0.0) || !(c_inf > 0.0)) return fail(OUX_E_INVALID, "far field needs rho > 0 and c > 0");
+  h->G.bkind = (h->G.bkind & ~(15 << (4 * face))) | (OUX_BC_FARFIELD << (4 * face));
+  h->G.bpar[face][0] = rho_inf;
+  h->G.bpar[face][1] = u_tangential;
+  h->G.bpar[face][2] = u_normal;
+  h->G.bpar[face][3] = c_inf;
+  return OUX_OK;
+}
+
+int oux_set_boundary_cells(oux_handle* h, int32_t face, const int8_t* kinds_dev) {
+  if (!h) return fail(OUX_E_INVALID, "null handle");
+  if (face < 0 || face > 3) return fail(OUX_E_INVALID, "face must be 0..3 (x low, x high, y low, y high)");
+  if (kinds_dev && !(face < 2 ? h->G.bcx : h->G.bcy))
+    return fail(OUX_E_INVALID, "the face's direction is periodic (set bc_x / bc_y = 1)");
+  h->G.bkinds[face] = reinterpret_cast<const signed char*>(kinds_dev);
+  return OUX_OK;
+}
+
+int oux_set_boundary_order(oux_handle* h, int32_t y_last) {
+  if (!h) return fail(OUX_E_INVALID, "null handle");
+  h->G.ylast = y_last ? 1 : 0;
   return OUX_OK;
 }
 

@@ -35,7 +35,12 @@ struct Geo {
                               // faces 0..3: x low, x high, y low, y high
   int64_t sx, plane, vs;      // row stride, plane stride, variable stride (elements)
   const double* bfix[4];      // OUX_BC_FIXED faces: nv x (ny for x faces, nx for y faces) values of Q/J
-  double gamma_1, over_gamma_1;  // gamma - 1 and 1 / (gamma - 1), for the no-slip wall rule
+  double gamma_1, over_gamma_1;  // gamma - 1 and 1 / (gamma - 1), for the wall and far-field rules
+  double gamma, over_gamma;
+  const signed char* bkinds[4];  // per-position rule of a face (overrides its kind), or null
+  double bpar[4][4];          // far-field state of a face: rho, tangential and normal velocity, c
+  int ylast;                  // 1: y faces applied after x faces (corners take their y rule)
+  const double* bjac;         // J(nx, ny), for the far-field rule
   __host__ __device__ int64_t at(int i, int j, int k) const { return (int64_t)k * plane + (int64_t)j * sx + i; }
 };
 
@@ -374,6 +379,12 @@ __global__ void k_mut_edges(Geo G, Fields<T> W) {
 //   OUX_BC_FIXED          caller-given Q/J values
 //   OUX_BC_NOSLIP_WALL    the neighbour's density and pressure, zero momentum (the
 //                         wall rows of 2D_solver/ST/set.f90 and 2D_solver/BL0/set.f90)
+//   OUX_BC_FARFIELD       (high faces) the boundary state from the Riemann invariants
+//                         of the neighbour and of a far-field state (the top row of
+//                         2D_solver/BL0/set.f90)
+// A face may carry a rule per position (bkinds).  By default y faces are applied
+// first and x faces last (2D_solver/OS/set.f90), so a corner takes its x rule of the
+// y-boundary value beside it; with ylast the order is reversed (2D_solver/BL0/set.f90).
 // With both x and y non-periodic the y faces are set first for every column and the
 // x faces after them for every row (2D_solver/OS/set.f90 order), so a corner takes
 // its x rule applied to the y-boundary value next to it.  Every value is computed
@@ -389,9 +400,11 @@ __host__ __device__ inline int64_t ghost_cells(const Geo& G) {
 }
 
 // Apply face f's rule to the neighbour state v (in place); pos: position along the
-// face (j for x faces, i for y faces).
-__device__ __forceinline__ void bc_rule(const Geo& G, int f, int pos, int nv, double (&v)[5]) {
-  const int kind = (G.bkind >> (4 * f)) & 15;
+// face (j for x faces, i for y faces); jb / jn: the J(nx, ny) offsets of the boundary
+// cell and of its neighbour.
+__device__ __forceinline__ void bc_rule(const Geo& G, int f, int pos, int nv, double (&v)[5], int64_t jb,
+                                        int64_t jn) {
+  const int kind = G.bkinds[f] ? (int)G.bkinds[f][pos] : (G.bkind >> (4 * f)) & 15;
   if (kind == 1) {  // slip wall: normal momentum (rho u for x faces, rho v for y faces) negated
     const int n = f < 2 ? 1 : 2;
     v[n] = -v[n];
@@ -403,6 +416,24 @@ __device__ __forceinline__ void bc_rule(const Geo& G, int f, int pos, int nv, do
     v[1] = 0.0;
     v[2] = 0.0;
     v[3] = p_wall * G.over_gamma_1;
+  } else if (kind == 4) {  // far field (2D, high faces): Riemann invariants along the normal
+    const double* P = G.bpar[f];
+    const int n = f < 2 ? 1 : 2, t = 3 - n;
+    const double Jn = G.bjac[jn], Jt = 1.0 / G.bjac[jb];
+    const double pin = G.gamma_1 * (v[3] - 0.5 * (v[1] * v[1] + v[2] * v[2]) / v[0]) * Jn;
+    const double rhoin = v[0] * Jn;
+    const double cin = sqrt(G.gamma * pin / rhoin);
+    const double vin = v[n] / v[0];
+    const double Rp = vin + 2.0 * cin * G.over_gamma_1;
+    const double Rm = P[2] - 2.0 * P[3] * G.over_gamma_1;
+    const double vb = 0.5 * (Rp + Rm);
+    const double cb = 0.25 * G.gamma_1 * (Rp - Rm);
+    const double rhob = pow(cb * (1.0 / P[3]), 2.0 * G.over_gamma_1) * P[0];
+    const double pb = (rhob * (cb * cb)) * G.over_gamma;
+    v[0] = rhob * Jt;
+    v[t] = rhob * P[1] * Jt;
+    v[n] = rhob * vb * Jt;
+    v[3] = (pb * G.over_gamma_1 + 0.5 * rhob * (P[1] * P[1] + vb * vb)) * Jt;
   }
 }
 
@@ -449,25 +480,32 @@ __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t
     }
   };
   const int sk = (G.dim == 3) ? (k - g + Nz) % Nz + g : 0;
-  if (xb) {
-    // x face: the neighbour column's value in this row -- a periodic image of an
-    // interior row, or (non-periodic y) that column's y-boundary value
+  const int64_t nx = G.nx;
+  if (xb && yb) {
+    // corner: the rule applied last, to the other direction's boundary value beside it
     const int fx = i == 0 ? 0 : 1, in = i == 0 ? 1 : G.nx - 2;
-    if (G.bcy && (j == 0 || j == G.ny - 1)) {
-      const int fy = j == 0 ? 2 : 3, jn = j == 0 ? 1 : G.ny - 2;
-      load(G.at(in, jn, sk));
-      bc_rule(G, fy, in, nv, v);
+    const int fy = j == 0 ? 2 : 3, jn = j == 0 ? 1 : G.ny - 2;
+    load(G.at(in, jn, sk));
+    if (!G.ylast) {
+      bc_rule(G, fy, in, nv, v, j * nx + in, jn * nx + in);
+      bc_rule(G, fx, j, nv, v, j * nx + i, j * nx + in);
     } else {
-      const int sj = G.bcy ? j : (j - gy + Ny) % Ny + gy;
-      load(G.at(in, sj, sk));
+      bc_rule(G, fx, jn, nv, v, jn * nx + i, jn * nx + in);
+      bc_rule(G, fy, i, nv, v, j * nx + i, jn * nx + i);
     }
-    bc_rule(G, fx, j, nv, v);
+  } else if (xb) {
+    // x face: the neighbour column's value in this row (a periodic image of an
+    // interior row when y is periodic)
+    const int fx = i == 0 ? 0 : 1, in = i == 0 ? 1 : G.nx - 2;
+    const int sj = G.bcy ? j : (j - gy + Ny) % Ny + gy;
+    load(G.at(in, sj, sk));
+    bc_rule(G, fx, j, nv, v, sj * nx + i, sj * nx + in);
   } else {
     // y face of an interior column (or a periodic-x ghost column's image)
     const int fy = j == 0 ? 2 : 3, jn = j == 0 ? 1 : G.ny - 2;
     const int si = G.bcx ? i : (i - gx + Nx) % Nx + gx;
     load(G.at(si, jn, sk));
-    bc_rule(G, fy, i, nv, v);
+    bc_rule(G, fy, i, nv, v, j * nx + si, jn * nx + si);
   }
   for (int l = 0; l < nv; ++l) {
     const int64_t q = o + l * G.vs;

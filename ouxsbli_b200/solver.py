@@ -40,6 +40,7 @@ class SolverConfig:
     # (the default), "slip_wall", "noslip_wall" or ("fixed", values (nv, ny) for x faces /
     # (nv, nx) for y faces, of Q/J)
     boundary: dict = field(default=None, repr=False)
+    boundary_order: str = "x_last"   # x_last: corners take their x rule (OS); y_last: their y rule (BL0)
     gamma: float = 1.4
     R: float = 287.03
     Pr: float = 0.71
@@ -64,22 +65,40 @@ class SolverConfig:
         n = (self.nx - 2 * gx) * (self.ny - 2 * gy)
         return n * (self.nz - 2 * g if self.dim == 3 else 1)
 
-    def boundary_rules(self) -> list[tuple[int, int, np.ndarray | None]]:
-        """(face, kind, fixed values as a C-contiguous (nv, len) array or None) per given face."""
+    def boundary_rules(self) -> list[dict]:
+        """The non-periodic faces' rules, normalised: per given face a dict with
+        face, kind, fixed ((nv, len) values or None), farfield ((rho, u_t, u_n, c) or
+        None) and cells (int8 kind per position or None).
+
+        Rule forms: "zero_gradient", "slip_wall", "noslip_wall"; ("fixed", values of
+        shape (nv, ny) for x faces / (nv, nx) for y faces, of Q/J); ("farfield", rho,
+        u_tangential, u_normal, c) on a high face; ("split", at, rule_lo, rule_hi):
+        positions below `at` follow rule_lo, the others rule_hi (two of the plain
+        names)."""
         out = []
         for name, rule in (self.boundary or {}).items():
             face = _lib.FACES[name]
-            if isinstance(rule, str):
-                out.append((face, _lib.BC_KINDS[rule], None))
-                continue
-            kind, vals = rule
-            if kind != "fixed":
-                raise ValueError(f"unknown boundary rule {rule!r}")
             n = self.ny if face < 2 else self.nx
-            v = np.ascontiguousarray(vals, dtype=np.float64)
-            if v.shape != (self.nv, n):
-                raise ValueError(f"fixed values of face {name} must have shape {(self.nv, n)}, got {v.shape}")
-            out.append((face, _lib.BC_KINDS["fixed"], v))
+            r = {"face": face, "kind": None, "fixed": None, "farfield": None, "cells": None}
+            if isinstance(rule, str):
+                r["kind"] = _lib.BC_KINDS[rule]
+            elif rule[0] == "fixed":
+                v = np.ascontiguousarray(rule[1], dtype=np.float64)
+                if v.shape != (self.nv, n):
+                    raise ValueError(f"fixed values of face {name} must have shape {(self.nv, n)}, got {v.shape}")
+                r["kind"], r["fixed"] = _lib.BC_KINDS["fixed"], v
+            elif rule[0] == "farfield":
+                if face not in (_lib.FACES["x_hi"], _lib.FACES["y_hi"]):
+                    raise ValueError("the far-field rule is built for the high faces")
+                r["kind"], r["farfield"] = _lib.BC_KINDS["farfield"], tuple(float(x) for x in rule[1:5])
+            elif rule[0] == "split":
+                at, lo, hi = int(rule[1]), _lib.BC_KINDS[rule[2]], _lib.BC_KINDS[rule[3]]
+                cells = np.full(n, hi, dtype=np.int8)
+                cells[:max(0, min(at, n))] = lo
+                r["kind"], r["cells"] = hi, cells
+            else:
+                raise ValueError(f"unknown boundary rule {rule!r}")
+            out.append(r)
         return out
 
     def to_c(self) -> tuple[OuxConfig, list]:
@@ -141,14 +160,23 @@ class Solver:
         lay = _lib.OuxLayout()
         check(LIB.oux_layout_of(self._h, C.byref(lay)))
         self.layout = lay
-        self._bfix = {}  # device copies of fixed boundary values (the library reads them every fill)
-        for face, kind, vals in cfg.boundary_rules():
-            ptr = None
-            if vals is not None:
-                t = torch.from_numpy(vals.ravel()).to(self.device)
-                self._bfix[face] = t
-                ptr = C.c_void_p(t.data_ptr())
-            check(LIB.oux_set_boundary(self._h, face, kind, ptr))
+        self._bfix = {}  # device copies of boundary values / kinds (the library reads them every fill)
+        for r in cfg.boundary_rules():
+            face = r["face"]
+            if r["farfield"] is not None:
+                check(LIB.oux_set_boundary_farfield(self._h, face, *r["farfield"]))
+            else:
+                ptr = None
+                if r["fixed"] is not None:
+                    t = torch.from_numpy(r["fixed"].ravel()).to(self.device)
+                    self._bfix[face] = t
+                    ptr = C.c_void_p(t.data_ptr())
+                check(LIB.oux_set_boundary(self._h, face, r["kind"], ptr))
+            if r["cells"] is not None:
+                t = torch.from_numpy(r["cells"]).to(self.device)
+                self._bfix[("cells", face)] = t
+                check(LIB.oux_set_boundary_cells(self._h, face, C.c_void_p(t.data_ptr())))
+        check(LIB.oux_set_boundary_order(self._h, 1 if cfg.boundary_order == "y_last" else 0))
 
     # -- lifetime --
     def close(self) -> None:

@@ -421,3 +421,18 @@ def test_walled_members_in_one_batch_bitexact(cuda_device):
         b.close()
         for s in solvers:
             s.close()
+
+
+def test_bl0_case_matches_oracle(tmp_path, cuda_device):
+    """The BL0 case (inflow, split bottom face with a no-slip plate, characteristic far
+    field on top, y-last corners; NS SLAU-2 with the Gaitonde-Visbal stencil) through
+    Case.run, 5 steps, against the oracle. The far-field rule evaluates pow (libm on
+    the host, CUDA on the device), so the states agree to rounding, not bit for bit."""
+    from ouxsbli_b200 import Case
+    c = Case("2D_solver/BL0", tmp_path / "bl0", nx=65, ny=33, nt=5, np=1)
+    c.build()
+    c.run(device=cuda_device)
+    p, xc, yc, zc, dx, dy, dz, Q = c._initial()
+    cfg = c._solver_config(p, dx, dy, dz)
+    want = oracle.step(cfg, to_qj(Q, jacobian(dx, dy, None)), 5)
+    np.testing.assert_allclose(c.solver.get_state(), want, rtol=1e-12, atol=0)

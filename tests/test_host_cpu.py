@@ -302,3 +302,44 @@ def test_every_case_builds_its_initial_field(tmp_path):
         p, xc, yc, zc, dx, dy, dz, Q = c._initial()
         nv = case.dim + 2
         assert Q.shape[1] == nv and np.isfinite(Q).all() and (Q[:, 0] > 0).all(), name
+
+
+def test_oracle_farfield_and_split_rules():
+    """The oracle's far-field rule (Riemann invariants, the top row of
+    2D_solver/BL0/set.f90) and a split face against numpy restatements."""
+    from oracle import oracle
+    from ouxsbli_b200.grid import jacobian
+    from ouxsbli_b200.solver import SolverConfig
+    nx, ny, g1 = 10, 8, 0.4
+    rng = np.random.default_rng(11)
+    dx, dy = rng.uniform(0.8, 1.2, nx - 1), rng.uniform(0.8, 1.2, ny - 1)
+    J = jacobian(dx, dy, None)
+    rho = rng.uniform(1.0, 1.2, (nx, ny))
+    u, v = rng.uniform(1.5, 2.0, (nx, ny)), rng.uniform(-0.1, 0.1, (nx, ny))
+    p = rng.uniform(0.7, 0.8, (nx, ny))
+    q = np.zeros((nx, 4, ny), order="F")
+    q[:, 0], q[:, 1], q[:, 2] = rho / J, rho * u / J, rho * v / J
+    q[:, 3] = (p / g1 + 0.5 * rho * (u * u + v * v)) / J
+    far = (1.1, 1.9, 0.0, 0.9)
+    cfg = SolverConfig(dim=2, nx=nx, ny=ny, nz=1, order=2, visc="Euler", bc_x=1, bc_y=1, dx=dx, dy=dy, dz=None,
+                       gamma=1.4, boundary={"y_hi": ("farfield",) + far,
+                                            "y_lo": ("split", 4, "zero_gradient", "noslip_wall")},
+                       boundary_order="y_last")
+    out = oracle.fill_ghosts(cfg, q)
+    for i in range(1, nx - 1):
+        Jn, Jb = J[i, ny - 2], J[i, ny - 1]
+        qn = q[i, :, ny - 2]
+        pin = g1 * (qn[3] - 0.5 * (qn[1] ** 2 + qn[2] ** 2) / qn[0]) * Jn
+        cin = np.sqrt(1.4 * pin / (qn[0] * Jn))
+        Rp, Rm = qn[2] / qn[0] + 2 * cin / g1, far[2] - 2 * far[3] / g1
+        vb, cb = 0.5 * (Rp + Rm), 0.25 * g1 * (Rp - Rm)
+        rb = (cb / far[3]) ** (2 / g1) * far[0]
+        pb = rb * cb * cb / 1.4
+        want = np.array([rb, rb * far[1], rb * vb, pb / g1 + 0.5 * rb * (far[1] ** 2 + vb ** 2)]) / Jb
+        np.testing.assert_allclose(out[i, :, ny - 1], want, rtol=1e-13)
+        qw = q[i, :, 1]
+        if i < 4:
+            np.testing.assert_array_equal(out[i, :, 0], qw)
+        else:
+            pw = g1 * (qw[3] - 0.5 * (qw[1] ** 2 + qw[2] ** 2) / qw[0])
+            np.testing.assert_allclose(out[i, :, 0], [qw[0], 0.0, 0.0, pw / g1], rtol=1e-15)
