@@ -436,3 +436,44 @@ def test_bl0_case_matches_oracle(tmp_path, cuda_device):
     cfg = c._solver_config(p, dx, dy, dz)
     want = oracle.step(cfg, to_qj(Q, jacobian(dx, dy, None)), 5)
     np.testing.assert_allclose(c.solver.get_state(), want, rtol=1e-12, atol=0)
+
+
+def test_bl0_flat_plate_skin_friction(tmp_path, cuda_device):
+    """BL0 at its own settings (Mach 2, 1025 x 129 nodes, 0.4 ms = 5 flow-through
+    times): the laminar boundary layer on the adiabatic plate. Skin friction from the
+    discrete wall shear (face-averaged Sutherland mu times the wall-face velocity
+    gradient) against the plate's similarity law: Cf sqrt(Re_x) constant downstream
+    (spread < 3 %) and within 8 % of the Eckert reference-temperature value
+    0.664 sqrt(C*), C* = rho* mu* / (rho_e mu_e) at T* = Te (1 + 0.032 M^2 +
+    0.58 (Tw / Te - 1)), Tw = Te (1 + sqrt(Pr) (gamma - 1) / 2 M^2)."""
+    from ouxsbli_b200 import Case
+    c = Case("2D_solver/BL0", tmp_path / "bl0", np=1, nt=133333)
+    c.build()
+    c.run(device=cuda_device)
+    p, xc, yc, zc, dx, dy, dz, Q = c._initial()
+    q = c.solver.get_state()
+    J = jacobian(dx, dy, None)
+    g, R, M0 = p["gamma"], p["R"], p["M0"]
+    rho = q[:, 0] * J
+    u = q[:, 1] / q[:, 0]
+    v = q[:, 2] / q[:, 0]
+    pr = (g - 1.0) * (q[:, 3] * J - 0.5 * rho * (u * u + v * v))
+    T = pr / (rho * R)
+
+    def mu(t):
+        return 1.716e-5 * 384.2 * 273.2 ** -1.5 / (t + 111.0) * t ** 1.5
+
+    Te, rho_e, u_e = p["T0"], p["rho0"], p["u0"]
+    x_le = xc[p["nx"] // 10 - 1]
+    vals = []
+    for frac in np.linspace(0.45, 0.95, 6):
+        i = int(frac * (p["nx"] - 1))
+        tau = 0.5 * (mu(T[i, 0]) + mu(T[i, 1])) * (u[i, 1] - u[i, 0]) / (yc[1] - yc[0])
+        rex = rho_e * u_e * (xc[i] - x_le) / mu(Te)
+        vals.append(tau / (0.5 * rho_e * u_e ** 2) * math.sqrt(rex))
+    vals = np.array(vals)
+    Tw = Te * (1.0 + math.sqrt(p["Pr"]) * 0.5 * (g - 1.0) * M0 ** 2)
+    Ts = Te * (1.0 + 0.032 * M0 ** 2 + 0.58 * (Tw / Te - 1.0))
+    eckert = 0.664 * math.sqrt(mu(Ts) / mu(Te) * Te / Ts)
+    assert vals.max() / vals.min() - 1.0 < 0.03, vals
+    assert abs(vals.mean() / eckert - 1.0) < 0.08, (vals, eckert)
