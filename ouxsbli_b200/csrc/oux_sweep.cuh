@@ -839,15 +839,20 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   }
 }
 
+// Threads of a k_sweep block (1D): the tile shape rounded up to whole warps.  For the
+// x sweep (33 x 4 face threads) the 28 extra threads load tile cells only, so the
+// 38 x 4 tile loads in one pass.
+template <int DIR> __host__ __device__ constexpr int sweep_threads() {
+  return (SweepShape<DIR>::TX * SweepShape<DIR>::TY + 31) / 32 * 32;
+}
+
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
-__global__ void __launch_bounds__(SweepShape<DIR>::TX * SweepShape<DIR>::TY,
-                                  DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
+__global__ void __launch_bounds__(sweep_threads<DIR>(), DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
 k_sweep(StepArgs<T> A, int last) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int TX = SweepShape<DIR>::TX, TY = SweepShape<DIR>::TY;
   // coherent loads: measured as fast as the read-only path for y/z and faster for x
   sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>()>(
-      A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.y * TX + threadIdx.x, TX * TY);
+      A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.x, sweep_threads<DIR>());
 }
 
 }  // namespace oux
