@@ -43,10 +43,12 @@ enum PhaseKind {
 
 constexpr int BATCH_MAX_PHASES = 40;
 constexpr int BATCH_THREADS = 288;   // 32 x 9: the y/z sweep tile shape
-constexpr int BATCH_ROWS_X = 8;      // x-sweep tile 33 x 8 (264 of the 288 threads)
+constexpr int BATCH_ROWS_X = 7;      // x-sweep tile 33 x 7 (231 of the 288 threads): its 38 x 7 cells
+                                      // load in one pass of the block
 constexpr int BATCH_ROWS_YZ = 8;     // y/z-sweep tile 32 x (8 + 1)
 static_assert(32 * (BATCH_ROWS_YZ + 1) == BATCH_THREADS, "y/z tile shape must fill the batch block");
 static_assert(33 * BATCH_ROWS_X <= BATCH_THREADS, "x tile shape must fit the batch block");
+static_assert(38 * BATCH_ROWS_X <= BATCH_THREADS, "the x tile should load in one pass");
 #ifndef OUX_BATCH_SPIN_LIMIT
 #define OUX_BATCH_SPIN_LIMIT (1 << 22)  // polls of >= 64 ns each: a few seconds at most
 #endif
