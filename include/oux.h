@@ -71,7 +71,7 @@ typedef struct oux_config {
   int32_t order;        /* convective order 2, 4, 6 */
   int32_t scheme;       /* enum oux_scheme */
   int32_t visc;         /* enum oux_visc */
-  int32_t visc_order;   /* 2, 4, 6 (defaults to order when 0) */
+  int32_t visc_order;   /* 2, 4, 6; 0: the order in 3D, 4 (order >= 4) or 2 in 2D */
   int32_t visc_stencil; /* enum oux_visc_stencil (ME4 only with visc_order 6) */
   int32_t tvd;          /* enum oux_tvd */
   int32_t slau;         /* enum oux_slau_variant */

@@ -1554,10 +1554,11 @@ int orc_jacobian(const orc_config* cfg, const double* dx, const double* dy, cons
   return 0;
 }
 
-int orc_fill_ghosts(const orc_config* cfg, double* QJ) {
+// Ghost / boundary-cell fill of QJ (the grid's spacings give the Jacobian the
+// far-field rule reads).
+int orc_fill_ghosts(const orc_config* cfg, const double* dx, const double* dy, const double* dz, double* QJ) {
   Ctx C;
-  C.c = *cfg; C.nx = cfg->nx; C.ny = cfg->ny; C.nz = cfg->dim == 3 ? cfg->nz : 1;
-  C.nv = cfg->dim + 2;
+  init_ctx(C, cfg, dx, dy, dz);
   fill_ghosts(C, QJ);
   return 0;
 }

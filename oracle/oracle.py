@@ -58,7 +58,7 @@ def lib() -> C.CDLL:
         _lib.orc_rhs.argtypes = [cp, dp, dp, dp, dp, dp]
         _lib.orc_fields.argtypes = [cp, dp, dp, dp, dp, dp]
         _lib.orc_jacobian.argtypes = [cp, dp, dp, dp, dp]
-        _lib.orc_fill_ghosts.argtypes = [cp, dp]
+        _lib.orc_fill_ghosts.argtypes = [cp, dp, dp, dp, dp]
         _lib.orc_stage.argtypes = [cp, dp, dp, dp, dp, dp, dp, C.c_int]
         _lib.orc_diag_f32.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                       C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), dp]
@@ -77,7 +77,8 @@ def make_cfg(cfg) -> _Cfg:
     c.order = cfg.order
     c.scheme = SCHEMES[cfg.scheme]
     c.visc = VISC[cfg.visc]
-    c.visc_order = cfg.visc_order or cfg.order
+    # unset: the order in 3D, 4 if the order is at least 4 else 2 in 2D (as the library)
+    c.visc_order = cfg.visc_order or (cfg.order if cfg.dim == 3 else (4 if cfg.order >= 4 else 2))
     c.visc_stencil = STENCILS[cfg.visc_stencil]
     c.tvd = TVD[cfg.tvd]
     c.slau = SLAU_VARIANTS[cfg.slau]
@@ -181,7 +182,8 @@ def fill_ghosts(cfg, qj: np.ndarray) -> np.ndarray:
     boundary-cell rules of the non-periodic faces)."""
     q = np.asfortranarray(qj, dtype=np.float64).copy(order="F")
     c = make_cfg(cfg)
-    assert lib().orc_fill_ghosts(C.byref(c), _ptr(q)) == 0
+    dx, dy, dz = _axes(cfg)
+    assert lib().orc_fill_ghosts(C.byref(c), _ptr(dx), _ptr(dy), _ptr(dz), _ptr(q)) == 0
     return q
 
 

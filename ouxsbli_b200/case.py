@@ -107,8 +107,8 @@ class Case:
         if ic_type == 1:
             glob["uniform"] = {k: glob.pop(k) for k in ("rho0", "u0", "v0", "w0", "p0") if k in glob}
         for key in ("BC_X", "BC_Y", "BC_Z", "RESCALE", "COMMZ"):
-            if (key == "BC_X" and case.bc_x) or (key == "BC_Y" and case.bc_y):
-                continue  # built: non-periodic x / y (2D Euler, the case's boundary-cell rules)
+            if (key == "BC_X" and (case.bc_x or case.x_periodic_copy)) or (key == "BC_Y" and case.bc_y):
+                continue  # built: non-periodic x / y (2D, the case's boundary-cell rules)
             if config.get(key):
                 raise RuntimeError(f"{key}=True needs wall/inflow or multi-rank code paths, which are not built "
                                    "(only fully periodic rectilinear cases)")
@@ -123,7 +123,7 @@ class Case:
             visc_stencil=c.get("VISC_STENCIL", "Central"), tvd=c["TVD"], slau=c["SLAU_VARIANT"], rk=int(c["RK"]),
             gamma=p["gamma"], R=p["R"], Pr=p.get("Pr", 0.71), Prt=p.get("Prt", 0.9),
             threshold=p.get("threshold", 0.4), dt=p["dt"], dx=dx, dy=dy, dz=dz,
-            bc_x=1 if c.get("BC_X") else 0, bc_y=1 if c.get("BC_Y") else 0,
+            bc_x=1 if c.get("BC_X") and not self._case.x_periodic_copy else 0, bc_y=1 if c.get("BC_Y") else 0,
             boundary=self._case.boundary(p, jacobian(dx, dy, None)) if self._case.boundary else None,
             boundary_order=self._case.boundary_order)
 

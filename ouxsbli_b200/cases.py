@@ -37,6 +37,7 @@ class CaseDef:
     bc_y: bool = False        # the case's y boundaries are non-periodic (BC_Y = True)
     boundary: Callable = None  # (params, J) -> rules of the non-periodic faces (SolverConfig.boundary)
     boundary_order: str = "x_last"  # which rules the corners take last (SolverConfig.boundary_order)
+    x_periodic_copy: bool = False  # BC_X = True, but set_bc copies the x ghosts periodically: periodic x
 
 
 # ---------------------------------------------------------------------------
@@ -453,6 +454,65 @@ def _bl_boundary(p: dict, J: np.ndarray) -> dict:
             "y_hi": ("farfield", rho, u0, 0.0, p["c_bc"])}
 
 
+# ---------------------------------------------------------------------------
+# Temporally developing boundary layer on a wall: 2D_solver/SBLI (mod_globals.f90,
+# set.f90, src/set_init_common.f90 set_init_tbl, src/set_compressible_bl.f90).  Its
+# set_bc copies the x ghosts periodically (the x flux kernels are the boundary
+# versions, which only change faces of ghost cells), a no-slip wall at y low and the
+# free stream at y high.  The initial field is a compressible laminar layer of 99 %
+# thickness blt.
+# ---------------------------------------------------------------------------
+def _sbli_derived(p: dict) -> dict:
+    p = dict(p)
+    p.setdefault("Lx", 100.0 * p["blt"])
+    p.setdefault("Ly", 5.0 * p["blt"])
+    p = _bl_derived(p)
+    return p
+
+
+def _sbli_grid(p: dict):
+    """set_grid: the flat-plate grid, x shifted by -70 blt."""
+    x, dx, y, dy = _bl_grid(p)
+    return x - 70.0 * p["blt"], dx, y, dy
+
+
+def _sbli_init(p: dict, x, y, z=None) -> np.ndarray:
+    """set_init_tbl: the profile in every column, then the wall row of the no-slip rule."""
+    from .blasius import compressible_profile
+    gam, R = p["gamma"], p["R"]
+    og1 = 1.0 / (gam - 1.0)
+    mu0 = sutherland_mu(p["T0"])
+    rho, u, v, T = compressible_profile(y, p["blt"], p["u0"], p["T0"], p["p0"], R, p["Cp"], p["rf"], p["Taw"], mu0)
+    Q = np.zeros((x.size, 4, y.size), order="F")
+    q1 = p["p0"] / (R * T)
+    Q[:, 0] = q1
+    Q[:, 1] = q1 * u
+    Q[:, 2] = q1 * v
+    Q[:, 3] = p["p0"] * og1 + 0.5 * (Q[:, 1] ** 2 + Q[:, 2] ** 2) / Q[:, 0]
+    Q[:, 0, 0] = Q[:, 0, 1]
+    Q[:, 1, 0] = 0.0
+    Q[:, 2, 0] = 0.0
+    p_wall = (gam - 1.0) * (Q[1, 3, 1] - 0.5 * (Q[1, 1, 1] ** 2 + Q[1, 2, 1] ** 2) / Q[1, 0, 1])
+    Q[:, 3, 0] = p_wall * og1
+    g = p["order"] // 2  # the x ghosts are periodic images (set_bc's x copies)
+    N = x.size - 2 * g
+    for i in list(range(g)) + list(range(x.size - g, x.size)):
+        Q[i] = Q[g + (i - g) % N]
+    return Q
+
+
+def _sbli_boundary(p: dict, J: np.ndarray) -> dict:
+    nx, ny = J.shape
+    gam, rho, u0 = p["gamma"], p["rho_bc"], p["u0"]
+    top = np.empty((4, nx))
+    top[0] = rho
+    top[1] = rho * u0
+    top[2] = 0.0
+    top[3] = p["p0"] * (1.0 / (gam - 1.0)) + 0.5 * rho * u0 ** 2
+    top = top * (1.0 / J[:, ny - 1])[None, :]
+    return {"y_lo": "noslip_wall", "y_hi": ("fixed", top)}
+
+
 CASES: dict[str, CaseDef] = {
     "NSTGV": CaseDef(
         "NSTGV", 3,
@@ -515,6 +575,16 @@ CASES: dict[str, CaseDef] = {
         _bl_init, _bl_derived,
         "Laminar boundary layer on a flat plate at Mach 2 (2D_solver/BL0)",
         grid=_bl_grid, bc_x=True, bc_y=True, boundary=_bl_boundary, boundary_order="y_last"),
+    "SBLI": CaseDef(
+        "SBLI", 2,
+        dict(VISC="NS", SCHEME="SLAU", ORDER=6, TVD="hybrid", SLAU_VARIANT="HRSLAU2", RK=3,
+             BC_X=True, BC_Y=True, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=1025, ny=257, blt=0.8e-3, endT=0.1e-3, np=10, dt=3.0e-9, nt=None, R=287.03, gamma=1.4, Pr=0.72,
+             Prt=0.9, M0=2.0, p_tot=100.0e3, T_tot=295.0, rf=0.89, threshold=0.4),
+        _sbli_init, _sbli_derived,
+        "Temporally developing laminar boundary layer on a wall (2D_solver/SBLI)",
+        grid=_sbli_grid, bc_x=False, bc_y=True, boundary=_sbli_boundary, boundary_order="y_last",
+        x_periodic_copy=True),
     "OS": CaseDef(
         "OS", 2,
         dict(VISC="Euler", SCHEME="SLAU", ORDER=6, TVD="hybrid", SLAU_VARIANT="HRSLAU2", RK=3,

@@ -94,7 +94,9 @@ int validate(const oux_config* c, std::string& why) {
 // calc_flux_base.f90.fypp:161-177 (3D) and 2D_solver/src/calc_flux_base.f90.fypp:108-132.
 int visc_kind(const oux_config* c, std::string& why) {
   if (c->visc == OUX_EULER) return VK_EULER;
-  int vo = c->visc_order ? c->visc_order : c->order;
+  // unset visc_order: the order in 3D (calc_visc_high.f90.fypp:2-4), 4 if the order
+  // is at least 4 else 2 in 2D (2D_solver/src/calc_flux_base.f90.fypp:2-4)
+  int vo = c->visc_order ? c->visc_order : (c->dim == 2 ? (c->order >= 4 ? 4 : 2) : c->order);
   if (c->dim == 2) {
     // calc_Ev4 / calc_Fv4 guard their 4th-order stencil by absolute indices, so
     // any convective order works (2D_solver/BL: ORDER 2, VISC_ORDER 4)

@@ -477,3 +477,16 @@ def test_bl0_flat_plate_skin_friction(tmp_path, cuda_device):
     eckert = 0.664 * math.sqrt(mu(Ts) / mu(Te) * Te / Ts)
     assert vals.max() / vals.min() - 1.0 < 0.03, vals
     assert abs(vals.mean() / eckert - 1.0) < 0.08, (vals, eckert)
+
+
+def test_sbli_case_matches_oracle(tmp_path, cuda_device):
+    """2D_solver/SBLI through Case.run (periodic x, no-slip wall and fixed free stream
+    in y, NS SLAU-6 with the 2D 4th-order viscous stencil, the compressible laminar
+    initial layer), 5 steps, against the oracle: bit-identical."""
+    from ouxsbli_b200 import Case
+    c = Case("2D_solver/SBLI", tmp_path / "sbli", nx=70, ny=41, nt=5, np=1)
+    c.build()
+    c.run(device=cuda_device)
+    p, xc, yc, zc, dx, dy, dz, Q = c._initial()
+    cfg = c._solver_config(p, dx, dy, dz)
+    np.testing.assert_array_equal(c.solver.get_state(), oracle.step(cfg, to_qj(Q, jacobian(dx, dy, None)), 5))

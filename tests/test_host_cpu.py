@@ -343,3 +343,22 @@ def test_oracle_farfield_and_split_rules():
         else:
             pw = g1 * (qw[3] - 0.5 * (qw[1] ** 2 + qw[2] ** 2) / qw[0])
             np.testing.assert_allclose(out[i, :, 0], [qw[0], 0.0, 0.0, pw / g1], rtol=1e-15)
+
+
+def test_blasius_solution_and_compressible_layer():
+    """The Blasius solution (f''(0) = 0.332057, f'(4.91) = 0.99) and the compressible
+    layer built on it: no-slip at the wall, the free stream at the edge, adiabatic
+    wall temperature."""
+    from ouxsbli_b200.blasius import blasius, compressible_profile
+    eta, f, fp, fpp0 = blasius()
+    assert abs(fpp0 - 0.332057) < 2e-6
+    assert abs(np.interp(4.91, eta, fp) - 0.99) < 1e-4
+    y = np.linspace(0.0, 3e-3, 61)
+    T0, u0, p0, R, g, rf = 163.9, 513.25, 12780.0, 287.03, 1.4, 0.89
+    Cp = g * R / (g - 1.0)
+    Taw = T0 * (1.0 + rf * 0.2 * 4.0)
+    rho, u, v, T = compressible_profile(y, 0.8e-3, u0, T0, p0, R, Cp, rf, Taw, 1.1e-5)
+    assert u[0] == 0.0 and v[0] == 0.0 and abs(T[0] - Taw) < 1e-9
+    assert abs(u[-1] - u0) < 1e-6 * u0 and abs(T[-1] - (Taw - rf * u0 ** 2 / (2 * Cp))) < 1e-6
+    i99 = np.searchsorted(u, 0.99 * u0)
+    assert abs(y[i99] - 0.8e-3) < 2 * (y[1] - y[0])
