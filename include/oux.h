@@ -84,11 +84,13 @@ typedef struct oux_config {
                                gives its face another rule (2D_solver/ST/set.f90 set_bc).
                                bc_y = 1 (2D): the same for y (calc_*_y), as the
                                BC_X = BC_Y = True cases build them (2D_solver/OS, BL).
-                               Euler or NS.  bc_z = 2 (3D, not LES): a z slab of a
+                               Euler or NS.  3D non-periodic x / y / z (bc_z = 1) are
+                               built for order 2 Euler (3D_solver/STZ), one boundary
+                               cell a side.  bc_z = 2, 3, 4 (3D, not LES): a z slab of a
                                larger grid (COMMZ, 3D_solver/src/calc_para.f90:343-384):
-                               its g ghost planes at each z end are written by the
-                               caller's halo exchange (oux_halo_pack / _unpack) after
-                               every stage, not by the periodic fill. */
+                               its g ghost planes at the halo ends (enum oux_bc_z) are
+                               written by the caller's halo exchange (oux_halo_pack /
+                               _unpack) after every stage, not by the fill. */
   int32_t precision;    /* enum oux_precision */
   double gamma, R, Pr, Prt, threshold, dt;
   const double *dx, *dy, *dz; /* host arrays, n-1 entries each (dz unused in 2D) */
@@ -157,8 +159,9 @@ int oux_halo_unpack(oux_handle* h, int32_t stage, const void* lo_dev, const void
 /* --- boundary cells of non-periodic directions --------------------------- */
 /* Replaces the case's own set_bc subroutine (2D_solver/OS/set.f90:50-90,
  * 2D_solver/ST/set.f90 set_bc), which the reference compiles into each case.
- * Faces: x low, x high, y low, y high.  Rules, applied to the one boundary cell of
- * every row (x faces) or column (y faces) from the adjacent interior cell:
+ * Faces: x low, x high, y low, y high (z low, z high in 3D).  Rules, applied to the
+ * one boundary cell of every row (x faces) or column (y faces) from the adjacent
+ * interior cell (3D: every line of cells normal to the face):
  *   ZERO_GRADIENT  the neighbour's Q/J (the default of every non-periodic face)
  *   SLIP_WALL      the neighbour's Q/J with the normal momentum negated
  *   NOSLIP_WALL    the neighbour's density and pressure with zero momentum:
@@ -166,16 +169,24 @@ int oux_halo_unpack(oux_handle* h, int32_t stage, const void* lo_dev, const void
  *                  Q/J, E_wall = p_wall / (gamma-1) (the wall rows of
  *                  2D_solver/ST/set.f90 and 2D_solver/BL0/set.f90)
  *   FIXED          caller values: fixed_dev holds nv x len doubles of Q/J, variable-
- *                  major ([l * len + pos]; len = ny for x faces, nx for y faces),
+ *                  major ([l * len + pos]; len = ny for x faces, nx for y faces;
+ *                  3D: pos = j + ny k, i + nx k, i + nx j for x, y, z faces),
  *                  device memory owned by the caller and read at every fill until
  *                  the face is set again.  In the mixed form the stage increments
  *                  of FIXED cells are 0 (Q^n holds the values).
  * By default y faces are applied first over every column, then x faces over every
  * row, so a corner takes its x rule applied to the y-boundary cell next to it (the
- * order of 2D_solver/OS/set.f90; oux_set_boundary_order reverses it).  The face's
+ * order of 2D_solver/OS/set.f90; oux_set_boundary_order reverses it).  In 3D the
+ * x, y and z faces are applied in that order (3D_solver/STZ/set.f90).  The face's
  * direction must be non-periodic.  Set rules before oux_batch_create when the
  * handle joins a batch. */
-enum oux_face { OUX_FACE_X_LO = 0, OUX_FACE_X_HI = 1, OUX_FACE_Y_LO = 2, OUX_FACE_Y_HI = 3 };
+enum oux_face { OUX_FACE_X_LO = 0, OUX_FACE_X_HI = 1, OUX_FACE_Y_LO = 2, OUX_FACE_Y_HI = 3,
+                OUX_FACE_Z_LO = 4, OUX_FACE_Z_HI = 5 };
+/* bc_z (3D): periodic, non-periodic, or a z slab of a larger grid whose ghost planes
+ * at both ends / the upper end only / the lower end only come from the halo exchange
+ * (the other end being the grid's boundary, with the rules of its face). */
+enum oux_bc_z { OUX_Z_PERIODIC = 0, OUX_Z_WALLS = 1, OUX_Z_SLAB = 2, OUX_Z_SLAB_LO_WALL = 3,
+                OUX_Z_SLAB_HI_WALL = 4 };
 enum oux_bc_kind { OUX_BC_ZERO_GRADIENT = 0, OUX_BC_SLIP_WALL = 1, OUX_BC_FIXED = 2, OUX_BC_NOSLIP_WALL = 3,
                    OUX_BC_FARFIELD = 4 };
 int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fixed_dev);

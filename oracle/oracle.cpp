@@ -56,10 +56,13 @@ typedef struct orc_config {
   int bkind[4];       // boundary-cell rule of the faces x lo, x hi, y lo, y hi:
                       // 0 zero gradient, 1 slip wall, 2 fixed values, 3 no-slip wall
   const double* bfix[4];  // fixed values of Q/J, nv x (ny for x faces, nx for y faces), variable-major
-  int bc_z;           // 0 periodic; 2 z slab: the z ghost planes are left to the halo exchange
+  int bc_z;           // 0 periodic; 1 non-periodic; z slab whose ghost planes at both ends (2), the
+                      // upper end (3) or the lower end (4) are left to the halo exchange
   int ylast;          // 1: y faces applied after x faces (corners take their y rule)
   const signed char* bkinds[4];  // per-position rule of a face, or null
   double bpar[4][4];  // far-field state of a face: rho, tangential velocity, normal velocity, c
+  int bkindz[2];      // 3D: rules of the faces z lo, z hi
+  const double* bfix3[6];  // 3D: fixed values of the faces x lo .. z hi (pos j+ny k, i+nx k, i+nx j)
 } orc_config;
 
 }  // extern "C"
@@ -1318,7 +1321,71 @@ void bc_rule(const Ctx& C, int f, int pos, double* v, int bi, int bj, int ni, in
   }
 }
 
+// 3D with non-periodic directions (order 2, one boundary cell a side): the x, y and
+// z faces' rules in that order (3D_solver/STZ/set.f90 set_bc), each applied to the
+// value the previous ones left beside it.
+void fill_ghosts_3d_bnd(const Ctx& C, double* Q) {
+  const int n[3] = {C.nx, C.ny, C.nz}, g = C.c.order / 2, nv = C.nv;
+  const int bz = C.c.bc_z;
+  const bool per[3] = {!C.c.bc_x, !C.c.bc_y, bz == 0};
+  const bool blo[3] = {(bool)C.c.bc_x, (bool)C.c.bc_y, bz == 1 || bz == 3};
+  const bool bhi[3] = {(bool)C.c.bc_x, (bool)C.c.bc_y, bz == 1 || bz == 4};
+  const bool halo_lo = bz == 2 || bz == 4, halo_hi = bz == 2 || bz == 3;
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < n[2]; ++k)
+    for (int j = 0; j < n[1]; ++j)
+      for (int i = 0; i < n[0]; ++i) {
+        if ((halo_lo && k < g) || (halo_hi && k >= n[2] - g)) continue;
+        const int c[3] = {i, j, k};
+        int src[3], cur[3];
+        bool bnd[3], inside = true;
+        for (int a = 0; a < 3; ++a) {
+          src[a] = c[a];
+          bnd[a] = false;
+          if (per[a]) {
+            if (c[a] < g || c[a] >= n[a] - g) {
+              src[a] = (c[a] - g + (n[a] - 2 * g)) % (n[a] - 2 * g) + g;
+              inside = false;
+            }
+          } else if ((c[a] == 0 && blo[a]) || (c[a] == n[a] - 1 && bhi[a])) {
+            bnd[a] = true;
+            src[a] = c[a] == 0 ? 1 : n[a] - 2;
+            inside = false;
+          }
+          cur[a] = src[a];
+        }
+        if (inside) continue;
+        double v[5];
+        for (int l = 0; l < nv; ++l) v[l] = Q[C.qidx(src[0] + 1, l + 1, src[1] + 1, src[2] + 1)];
+        for (int a = 0; a < 3; ++a) {
+          if (!bnd[a]) continue;
+          cur[a] = c[a];
+          const int f = 2 * a + (c[a] == 0 ? 0 : 1);
+          const int kind = f < 4 ? C.c.bkind[f] : C.c.bkindz[f - 4];
+          if (kind == 1) {
+            v[1 + a] = -v[1 + a];
+          } else if (kind == 2) {
+            const size_t pos = a == 0 ? cur[1] + (size_t)n[1] * cur[2]
+                                      : (a == 1 ? cur[0] + (size_t)n[0] * cur[2] : cur[0] + (size_t)n[0] * cur[1]);
+            const size_t len = a == 0 ? (size_t)n[1] * n[2] : (a == 1 ? (size_t)n[0] * n[2] : (size_t)n[0] * n[1]);
+            for (int l = 0; l < nv; ++l) v[l] = C.c.bfix3[f][l * len + pos];
+          } else if (kind == 3) {
+            double p_wall = C.K.gamma_1 * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / v[0]);
+            v[1] = 0.0;
+            v[2] = 0.0;
+            v[3] = 0.0;
+            v[4] = p_wall * C.K.over_gamma_1;
+          }
+        }
+        for (int l = 0; l < nv; ++l) Q[C.qidx(i + 1, l + 1, j + 1, k + 1)] = v[l];
+      }
+}
+
 void fill_ghosts(const Ctx& C, double* Q) {
+  if (C.c.dim == 3 && (C.c.bc_x || C.c.bc_y || C.c.bc_z == 1 || C.c.bc_z == 3 || C.c.bc_z == 4)) {
+    fill_ghosts_3d_bnd(C, Q);
+    return;
+  }
   int nx = C.nx, ny = C.ny, nz = C.nz, nv = C.nv, g = C.c.order / 2;
   int gx = C.c.bc_x ? 1 : g, gy = C.c.bc_y ? 1 : g;
   int Nx = nx - 2 * gx, Ny = ny - 2 * gy, Nz = nz - 2 * g;

@@ -41,7 +41,8 @@ class _Cfg(C.Structure):
                                        "visc_stencil", "tvd", "slau", "rk", "bc_x")] + \
                [(n, C.c_double) for n in ("gamma", "R", "Pr", "Prt", "threshold", "dt")] + \
                [("bc_y", C.c_int), ("bkind", C.c_int * 4), ("bfix", C.POINTER(C.c_double) * 4), ("bc_z", C.c_int),
-                ("ylast", C.c_int), ("bkinds", C.POINTER(C.c_int8) * 4), ("bpar", (C.c_double * 4) * 4)]
+                ("ylast", C.c_int), ("bkinds", C.POINTER(C.c_int8) * 4), ("bpar", (C.c_double * 4) * 4),
+                ("bkindz", C.c_int * 2), ("bfix3", C.POINTER(C.c_double) * 6)]
 
 
 _lib = None
@@ -90,10 +91,16 @@ def make_cfg(cfg) -> _Cfg:
     rules = cfg.boundary_rules() if hasattr(cfg, "boundary_rules") else []
     for r in rules:
         face = r["face"]
-        c.bkind[face] = r["kind"]
+        if face < 4:
+            c.bkind[face] = r["kind"]
+        else:
+            c.bkindz[face - 4] = r["kind"]
         if r["fixed"] is not None:
             c._keep.append(r["fixed"])
-            c.bfix[face] = _ptr(r["fixed"])
+            if cfg.dim == 3:
+                c.bfix3[face] = _ptr(r["fixed"])
+            else:
+                c.bfix[face] = _ptr(r["fixed"])
         if r["farfield"] is not None:
             for q in range(4):
                 c.bpar[face][q] = r["farfield"][q]

@@ -44,7 +44,7 @@ SYMBOLS = [
     "oux_batch_status", "oux_batch_info", "oux_batch_destroy",
 ]
 NOALLOC_SCRATCH_BYTES = 32 << 20  # OUX_NOALLOC_SCRATCH_BYTES
-FACES = {"x_lo": 0, "x_hi": 1, "y_lo": 2, "y_hi": 3}                  # enum oux_face
+FACES = {"x_lo": 0, "x_hi": 1, "y_lo": 2, "y_hi": 3, "z_lo": 4, "z_hi": 5}  # enum oux_face
 BC_KINDS = {"zero_gradient": 0, "slip_wall": 1, "fixed": 2, "noslip_wall": 3, "farfield": 4}  # enum oux_bc_kind
 
 

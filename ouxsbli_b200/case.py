@@ -107,8 +107,9 @@ class Case:
         if ic_type == 1:
             glob["uniform"] = {k: glob.pop(k) for k in ("rho0", "u0", "v0", "w0", "p0") if k in glob}
         for key in ("BC_X", "BC_Y", "BC_Z", "RESCALE", "COMMZ"):
-            if (key == "BC_X" and (case.bc_x or case.x_periodic_copy)) or (key == "BC_Y" and case.bc_y):
-                continue  # built: non-periodic x / y (2D, the case's boundary-cell rules)
+            if (key == "BC_X" and (case.bc_x or case.x_periodic_copy)) or (key == "BC_Y" and case.bc_y) or \
+                    (key == "BC_Z" and case.bc_z) or (key == "COMMZ" and case.slabs):
+                continue  # built: the case's boundary-cell rules, its z slabs
             if config.get(key):
                 raise RuntimeError(f"{key}=True needs wall/inflow or multi-rank code paths, which are not built "
                                    "(only fully periodic rectilinear cases)")
@@ -118,12 +119,15 @@ class Case:
         from .solver import SolverConfig
         c = self.config
         return SolverConfig(
-            dim=self._case.dim, nx=p["nx"], ny=p["ny"], nz=p.get("nz", 1) if self._case.dim == 3 else 1,
+            dim=self._case.dim, nx=p["nx"], ny=p["ny"],
+            nz=p.get("nz_grid", p.get("nz", 1)) if self._case.dim == 3 else 1,
             order=int(c["ORDER"]), scheme=c["SCHEME"], visc=c["VISC"], visc_order=int(c.get("VISC_ORDER", 0) or 0),
             visc_stencil=c.get("VISC_STENCIL", "Central"), tvd=c["TVD"], slau=c["SLAU_VARIANT"], rk=int(c["RK"]),
             gamma=p["gamma"], R=p["R"], Pr=p.get("Pr", 0.71), Prt=p.get("Prt", 0.9),
             threshold=p.get("threshold", 0.4), dt=p["dt"], dx=dx, dy=dy, dz=dz,
-            bc_x=1 if c.get("BC_X") and not self._case.x_periodic_copy else 0, bc_y=1 if c.get("BC_Y") else 0,
+            bc_x=1 if (c.get("BC_X") or self._case.bc_x) and not self._case.x_periodic_copy else 0,
+            bc_y=1 if (c.get("BC_Y") or self._case.bc_y) else 0,
+            bc_z=1 if self._case.dim == 3 and (c.get("BC_Z") or self._case.bc_z) else 0,
             boundary=self._case.boundary(p, jacobian(dx, dy, None)) if self._case.boundary else None,
             boundary_order=self._case.boundary_order)
 
@@ -189,7 +193,7 @@ class Case:
         J = jacobian(dx, dy, dz if dim == 3 else None)
         nv = dim + 2
         if self.config.get("RESTART"):
-            shape = (p["nx"], nv, p["ny"], p["nz"]) if dim == 3 else (p["nx"], nv, p["ny"])
+            shape = (p["nx"], nv, p["ny"], p.get("nz_grid", p["nz"])) if dim == 3 else (p["nx"], nv, p["ny"])
             Q = read_restart(self.workdir / "recal" / "Q00001.dat", shape)
         qj = to_qj(Q, J)
         cfg = self._solver_config(p, dx, dy, dz)
@@ -216,7 +220,12 @@ class Case:
             with open(data / "diagnostics_fp64.d", "a") as fh:
                 fh.write(f"{t:.16e} {d[0]:.16e} {d[1]:.16e} {d[2]:.16e}\n")
 
-        s = Solver(cfg, device)
+        if self.config.get("COMMZ") and self._case.slabs:
+            # the reference's z slabs, in one process on one GPU (ouxsbli_b200.slabs)
+            from .slabs import LocalSlabs
+            s = LocalSlabs(cfg, int(p.get("slabs", self._case.slabs)), device)
+        else:
+            s = Solver(cfg, device)
         self.solver = s
         s.set_state(qj)
         output(0, qj, s)

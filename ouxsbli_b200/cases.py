@@ -38,6 +38,8 @@ class CaseDef:
     boundary: Callable = None  # (params, J) -> rules of the non-periodic faces (SolverConfig.boundary)
     boundary_order: str = "x_last"  # which rules the corners take last (SolverConfig.boundary_order)
     x_periodic_copy: bool = False  # BC_X = True, but set_bc copies the x ghosts periodically: periodic x
+    bc_z: bool = False        # 3D: the case's z boundaries are non-periodic (BC_Z = True)
+    slabs: int = 0            # COMMZ: the number of z slabs the reference's run splits the grid into
 
 
 # ---------------------------------------------------------------------------
@@ -513,6 +515,53 @@ def _sbli_boundary(p: dict, J: np.ndarray) -> dict:
     return {"y_lo": "noslip_wall", "y_hi": ("fixed", top)}
 
 
+# ---------------------------------------------------------------------------
+# Shock tube along z over two z slabs (COMMZ): 3D_solver/STZ (mod_globals.f90,
+# set.f90).  Order-2 SLAU, slip walls in x and y (the mirrored ghost cells of its
+# set_bc), zero gradient at the two z ends of the grid; the lower slab starts in the
+# left state, the upper one in the right state.  `nz` is a slab's plane count (its
+# interior + one ghost plane each end), as in the reference, whose four MPI ranks
+# hold two z slabs.
+# ---------------------------------------------------------------------------
+def _stz_derived(p: dict) -> dict:
+    p = dict(p)
+    p["nz_grid"] = p["slabs"] * (p["nz"] - 2) + 2  # planes of the whole grid
+    if p.get("dt") is None:
+        p["dt"] = p["CFL"] * p["Lz"] / (float(p["nz"] - 1) * math.sqrt(p["p_L"] / p["rho_L"]))
+    if p.get("nt") is None:
+        p["nt"] = int(p["endT"] / (float(p["np"]) * p["dt"]))
+    return p
+
+
+def _stz_grid(p: dict):
+    """set_grid: uniform cell centres, one ghost a side; z over all slabs."""
+    def axis(n, L):
+        d = L / (n - 2)
+        return d * (np.arange(n) - 0.5), np.full(n - 1, d)  # first interior centre at d / 2
+    nint = p["nz"] - 2
+    x, dx = axis(p["nx"], p["Lx"])
+    y, dy = axis(p["ny"], p["Ly"])
+    z, dz = axis(p["slabs"] * nint + 2, p["Lz"])
+    return x, dx, y, dy, z, dz
+
+
+def _stz_init(p: dict, x, y, z) -> np.ndarray:
+    """set_init: the left state in the first slab's planes (ghost included), the right
+    state in the second's."""
+    gam = p["gamma"]
+    nx, ny, nz = x.size, y.size, z.size
+    Q = np.zeros((nx, 5, ny, nz), order="F")
+    left = np.arange(nz) < p["nz"] - 1
+    Q[:, 0] = np.where(left, p["rho_L"], p["rho_R"])[None, None, :]
+    Q[:, 4] = np.where(left, p["p_L"], p["p_R"])[None, None, :] / (gam - 1.0)
+    return Q
+
+
+def _stz_boundary(p: dict, J) -> dict:
+    return {"x_lo": "slip_wall", "x_hi": "slip_wall", "y_lo": "slip_wall", "y_hi": "slip_wall",
+            "z_lo": "zero_gradient", "z_hi": "zero_gradient"}
+
+
 CASES: dict[str, CaseDef] = {
     "NSTGV": CaseDef(
         "NSTGV", 3,
@@ -531,6 +580,16 @@ CASES: dict[str, CaseDef] = {
              M0=0.4, RHO0=1.0, threshold=0.4),
         _etgv_init, _etgv_derived,
         "Inviscid Taylor-Green vortex (3D_solver/ETGV)"),
+    "STZ": CaseDef(
+        "STZ", 3,
+        dict(VISC="Euler", SCHEME="SLAU", ORDER=2, TVD="tvd", SLAU_VARIANT="SLAU", RK=3,
+             BC_X=False, BC_Y=False, BC_Z=True, RESCALE=False, COMMZ=True, RESTART=False),
+        dict(nx=6, ny=6, nz=513, slabs=2, Lx=0.1, Ly=0.1, Lz=1.0, gamma=1.4, Pr=0.71, Prt=0.9, R=287.03,
+             rho_L=1.0, p_L=1.0, rho_R=0.125, p_R=0.1, CFL=0.01, endT=0.1, np=50, dt=None, nt=None,
+             threshold=0.4),
+        _stz_init, _stz_derived,
+        "Shock tube along z over two z slabs (3D_solver/STZ)",
+        grid=_stz_grid, bc_x=True, bc_y=True, boundary=_stz_boundary, bc_z=True, slabs=2),
     "EVC": CaseDef(
         "EVC", 2,
         dict(VISC="Euler", SCHEME="KEEP", ORDER=6, TVD="none", SLAU_VARIANT="HRSLAU2", RK=4,
@@ -605,9 +664,12 @@ def build_initial(case: CaseDef, params: dict):
     if case.derived:
         p = case.derived(p)
     if case.dim == 3:
-        xc, dx = cyclic_axis(p["nx"], p["Lx"], order)
-        yc, dy = cyclic_axis(p["ny"], p["Ly"], order)
-        zc, dz = cyclic_axis(p["nz"], p["Lz"], order)
+        if case.grid is not None:
+            xc, dx, yc, dy, zc, dz = case.grid(p)
+        else:
+            xc, dx = cyclic_axis(p["nx"], p["Lx"], order)
+            yc, dy = cyclic_axis(p["ny"], p["Ly"], order)
+            zc, dz = cyclic_axis(p["nz"], p["Lz"], order)
         Q = case.init(p, xc, yc, zc)
     else:
         if case.grid is not None:

@@ -62,21 +62,22 @@ int validate(const oux_config* c, std::string& why) {
   if (c->tvd < 0 || c->tvd > 2) { why = "unknown tvd mode"; return OUX_E_INVALID; }
   if (c->slau < 0 || c->slau > 1) { why = "unknown SLAU variant"; return OUX_E_INVALID; }
   if (c->rk != 3 && c->rk != 4) { why = "rk must be 3 or 4"; return OUX_E_INVALID; }
-  if ((c->dim == 3 && c->bc_z != 0 && c->bc_z != 2) || c->bc_x < 0 || c->bc_x > 1 || c->bc_y < 0 ||
+  if ((c->dim == 3 && (c->bc_z < 0 || c->bc_z > 4)) || c->bc_x < 0 || c->bc_x > 1 || c->bc_y < 0 ||
       c->bc_y > 1) {
-    why = "boundaries: bc_z = 0 (periodic) or 2 (z-slab, halo planes from neighbours); bc_x, bc_y = 0 "
-          "(periodic) or 1 (non-periodic, 2D)";
+    why = "boundaries: bc_x, bc_y = 0 (periodic) or 1 (non-periodic); bc_z = 0 (periodic), 1 (non-periodic) "
+          "or a z slab (2: halo planes at both ends, 3: at the upper end, 4: at the lower end)";
     return OUX_E_INVALID;
   }
-  if (c->dim == 3 && c->bc_z == 2) {
+  if (c->dim == 3 && c->bc_z >= 2) {
     if (c->visc == OUX_LES) {
-      why = "z slabs (bc_z = 2): the SGS viscosity's edge layers wrap z, so LES runs are not built as slabs";
+      why = "z slabs (bc_z >= 2): the SGS viscosity's edge layers wrap z, so LES runs are not built as slabs";
       return OUX_E_INVALID;
     }
-    if (c->nz < 3 * g) { why = "z slab (bc_z = 2) needs at least g interior planes (nz >= 3g)"; return OUX_E_INVALID; }
+    if (c->nz < 3 * g) { why = "z slab (bc_z >= 2) needs at least g interior planes (nz >= 3g)"; return OUX_E_INVALID; }
   }
-  if ((c->bc_x == 1 || c->bc_y == 1) && c->dim != 2) {
-    why = "non-periodic x / y (bc_x = 1, bc_y = 1) is built for 2D solves";
+  if (c->dim == 3 && (c->bc_x == 1 || c->bc_y == 1 || c->bc_z == 1 || c->bc_z == 3 || c->bc_z == 4) &&
+      (c->order != 2 || c->visc != OUX_EULER)) {
+    why = "3D non-periodic boundaries are built for order 2 Euler solves (3D_solver/STZ)";
     return OUX_E_INVALID;
   }
   if (c->bc_y == 1 && c->ny < 4) { why = "non-periodic y (bc_y = 1) needs ny >= 4"; return OUX_E_INVALID; }
@@ -203,6 +204,7 @@ Geo make_geo(const oux_config& c) {
   }
   G.ylast = 0;
   G.bjac = nullptr;
+  for (int f = 0; f < 6; ++f) G.bfix3[f] = nullptr;
   G.sx = round_up(c.nx, 4);
   G.plane = G.sx * c.ny;
   G.vs = round_up(G.plane * G.nz, 32);
@@ -919,7 +921,7 @@ static int halo_copy(oux_handle* h, int stage, int k0, void* buf, bool to_buf, c
 int oux_halo_pack(oux_handle* h, int32_t stage, void* lo_dev, void* hi_dev, void* stream) {
   if (!h || !lo_dev || !hi_dev) return fail(OUX_E_INVALID, "null argument");
   if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
-  if (h->G.dim != 3 || h->G.bcz != 2) return fail(OUX_E_INVALID, "halo exchange needs a z slab (bc_z = 2)");
+  if (h->G.dim != 3 || h->G.bcz < 2) return fail(OUX_E_INVALID, "halo exchange needs a z slab (bc_z >= 2)");
   const int nst = h->cfg.rk == 3 ? 3 : 4;
   if (stage < 0 || stage >= nst) return fail(OUX_E_INVALID, "stage out of range");
   const int g = h->G.g, nz = h->G.nz;
@@ -932,28 +934,36 @@ int oux_halo_pack(oux_handle* h, int32_t stage, void* lo_dev, void* hi_dev, void
 int oux_halo_unpack(oux_handle* h, int32_t stage, const void* lo_dev, const void* hi_dev, void* stream) {
   if (!h || !lo_dev || !hi_dev) return fail(OUX_E_INVALID, "null argument");
   if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
-  if (h->G.dim != 3 || h->G.bcz != 2) return fail(OUX_E_INVALID, "halo exchange needs a z slab (bc_z = 2)");
+  if (h->G.dim != 3 || h->G.bcz < 2) return fail(OUX_E_INVALID, "halo exchange needs a z slab (bc_z >= 2)");
   const int nst = h->cfg.rk == 3 ? 3 : 4;
   if (stage < 0 || stage >= nst) return fail(OUX_E_INVALID, "stage out of range");
   const int g = h->G.g, nz = h->G.nz;
   cudaStream_t s = (cudaStream_t)stream;
-  int rc = halo_copy(h, stage, 0, const_cast<void*>(lo_dev), false, s);  // from the rank below
-  if (!rc) rc = halo_copy(h, stage, nz - g, const_cast<void*>(hi_dev), false, s);  // from the rank above
+  // only the halo ends: a slab end on the grid's boundary keeps its boundary cells
+  int rc = OUX_OK;
+  if (!z_fill_lo(h->G)) rc = halo_copy(h, stage, 0, const_cast<void*>(lo_dev), false, s);  // from below
+  if (!rc && !z_fill_hi(h->G)) rc = halo_copy(h, stage, nz - g, const_cast<void*>(hi_dev), false, s);  // above
   return rc;
 }
 
 int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fixed_dev) {
   if (!h) return fail(OUX_E_INVALID, "null handle");
-  if (face < 0 || face > 3) return fail(OUX_E_INVALID, "face must be 0..3 (x low, x high, y low, y high)");
+  const int nfaces = h->G.dim == 3 ? 6 : 4;
+  if (face < 0 || face >= nfaces)
+    return fail(OUX_E_INVALID, "face must be 0..3 (x low, x high, y low, y high), 4..5 (z low, z high) in 3D");
   if (kind < OUX_BC_ZERO_GRADIENT || kind > OUX_BC_NOSLIP_WALL)
     return fail(OUX_E_INVALID, "unknown boundary rule (far-field faces: oux_set_boundary_farfield)");
-  if (!(face < 2 ? h->G.bcx : h->G.bcy))
-    return fail(OUX_E_INVALID, "the face's direction is periodic (set bc_x / bc_y = 1)");
+  bool open;
+  if (face < 2) open = h->G.bcx;
+  else if (face < 4) open = h->G.bcy;
+  else open = face == 4 ? z_bnd_lo(h->G) : z_bnd_hi(h->G);
+  if (!open) return fail(OUX_E_INVALID, "the face is periodic or a slab's halo end");
   if (kind == OUX_BC_FIXED && !fixed_dev) return fail(OUX_E_INVALID, "a fixed rule needs its device values");
   if (kind == OUX_BC_FIXED && (reinterpret_cast<uintptr_t>(fixed_dev) & 7))
     return fail(OUX_E_INVALID, "fixed values must be 8-byte aligned");
   h->G.bkind = (h->G.bkind & ~(15 << (4 * face))) | (kind << (4 * face));
-  h->G.bfix[face] = kind == OUX_BC_FIXED ? fixed_dev : nullptr;
+  if (h->G.dim == 3) h->G.bfix3[face] = kind == OUX_BC_FIXED ? fixed_dev : nullptr;
+  else h->G.bfix[face] = kind == OUX_BC_FIXED ? fixed_dev : nullptr;
   return OUX_OK;
 }
 

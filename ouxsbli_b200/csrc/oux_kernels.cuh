@@ -30,7 +30,9 @@ struct Geo {
   int dim, nx, ny, nz, g;     // padded extents, ghost width
   int gx, bcx;                // x ghost width of the cell ranges (g, or 1 for a non-periodic x), bc_x
   int gy, bcy;                // the same for y
-  int bcz;                    // 2: z slab, the z ghost planes come from the neighbouring slabs
+  int bcz;                    // enum oux_bc_z: 0 periodic; 1 non-periodic (both ends); slabs whose
+                              // z ghost planes come from the neighbours: 2 both ends, 3 / 4 the
+                              // upper / lower end only (the other end is the grid's boundary)
   int bkind;                  // boundary-cell rule of face f (enum oux_bc_kind) in bits 4f..4f+3;
                               // faces 0..3: x low, x high, y low, y high
   int64_t sx, plane, vs;      // row stride, plane stride, variable stride (elements)
@@ -41,6 +43,7 @@ struct Geo {
   double bpar[4][4];          // far-field state of a face: rho, tangential and normal velocity, c
   int ylast;                  // 1: y faces applied after x faces (corners take their y rule)
   const double* bjac;         // J(nx, ny), for the far-field rule
+  const double* bfix3[6];     // 3D: fixed values of the faces x lo .. z hi
   __host__ __device__ int64_t at(int i, int j, int k) const { return (int64_t)k * plane + (int64_t)j * sx + i; }
 };
 
@@ -391,11 +394,17 @@ __global__ void k_mut_edges(Geo G, Fields<T> W) {
 // from interior cells only, so the cells can be filled in any order.
 // The three groups enumerate z-ghost planes, y-ghost rows of interior planes and
 // x-ghost cells of interior rows without touching interior cells.
-// A z slab (bcz = 2) leaves its z ghost planes to the halo exchange.
+// z ends whose ghost planes the fill writes (the others come from the halo exchange)
+__host__ __device__ inline bool z_fill_lo(const Geo& G) { return G.bcz == 0 || G.bcz == 1 || G.bcz == 3; }
+__host__ __device__ inline bool z_fill_hi(const Geo& G) { return G.bcz == 0 || G.bcz == 1 || G.bcz == 4; }
+__host__ __device__ inline bool z_bnd_lo(const Geo& G) { return G.bcz == 1 || G.bcz == 3; }
+__host__ __device__ inline bool z_bnd_hi(const Geo& G) { return G.bcz == 1 || G.bcz == 4; }
+
+// A z slab leaves the ghost planes of its halo ends to the halo exchange.
 __host__ __device__ inline int64_t ghost_cells(const Geo& G) {
   const int g = G.g, gy = G.gy;
   const int Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
-  const int gz = (G.dim == 3 && G.bcz != 2) ? 2 * g : 0;
+  const int gz = (G.dim == 3) ? g * ((int)z_fill_lo(G) + (int)z_fill_hi(G)) : 0;
   return (int64_t)gz * G.ny * G.nx + (int64_t)Nz * (2 * gy) * G.nx + (int64_t)Nz * Ny * (2 * G.gx);
 }
 
@@ -437,6 +446,68 @@ __device__ __forceinline__ void bc_rule(const Geo& G, int f, int pos, int nv, do
   }
 }
 
+// 3D grids with non-periodic directions (order 2: one boundary cell a side): the
+// rules of the x, y and z faces applied in that order, each to the value the
+// previous ones left beside it (2D_solver-style zero gradient / slip / no-slip /
+// fixed values; the order of 3D_solver/STZ/set.f90 set_bc).  Periodic directions
+// take their images; the ghost planes of a slab's halo ends are not enumerated.
+// Faces 4 / 5 are z low / high; fixed values are indexed by the face's position
+// (x faces j + ny k, y faces i + nx k, z faces i + nx j).
+template <class T>
+__device__ __forceinline__ void ghost_cell_3d_bnd(T* Q, const Geo& G, int nv, int i, int j, int k,
+                                                  const double* Qn) {
+  const int n[3] = {G.nx, G.ny, G.nz};
+  const int c[3] = {i, j, k};
+  const bool per[3] = {!G.bcx, !G.bcy, G.bcz == 0};
+  const bool blo[3] = {(bool)G.bcx, (bool)G.bcy, z_bnd_lo(G)};
+  const bool bhi[3] = {(bool)G.bcx, (bool)G.bcy, z_bnd_hi(G)};
+  int src[3], cur[3];
+  bool bnd[3];
+  for (int a = 0; a < 3; ++a) {
+    const int g = G.g;
+    src[a] = c[a];
+    bnd[a] = false;
+    if (per[a]) {
+      if (c[a] < g || c[a] >= n[a] - g) src[a] = (c[a] - g + (n[a] - 2 * g)) % (n[a] - 2 * g) + g;
+    } else if ((c[a] == 0 && blo[a]) || (c[a] == n[a] - 1 && bhi[a])) {
+      bnd[a] = true;
+      src[a] = c[a] == 0 ? 1 : n[a] - 2;
+    }
+    cur[a] = src[a];
+  }
+  double v[5];
+  const int64_t s = G.at(src[0], src[1], src[2]);
+  for (int l = 0; l < nv; ++l) {
+    const int64_t q = s + l * G.vs;
+    v[l] = Qn ? Qn[q] + (double)Q[q] : (double)Q[q];
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (!bnd[a]) continue;
+    cur[a] = c[a];
+    const int f = 2 * a + (c[a] == 0 ? 0 : 1);
+    const int kind = (G.bkind >> (4 * f)) & 15;
+    if (kind == 1) {  // slip wall: the normal momentum negated
+      v[1 + a] = -v[1 + a];
+    } else if (kind == 2) {  // fixed values of the face position
+      const int64_t pos = a == 0 ? cur[1] + (int64_t)G.ny * cur[2]
+                                 : (a == 1 ? cur[0] + (int64_t)G.nx * cur[2] : cur[0] + (int64_t)G.nx * cur[1]);
+      const int64_t len = a == 0 ? (int64_t)G.ny * G.nz : (a == 1 ? (int64_t)G.nx * G.nz : (int64_t)G.nx * G.ny);
+      for (int l = 0; l < nv; ++l) v[l] = G.bfix3[f][l * len + pos];
+    } else if (kind == 3) {  // no-slip wall: the neighbour's density and pressure, zero momentum
+      const double p_wall = G.gamma_1 * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / v[0]);
+      v[1] = 0.0;
+      v[2] = 0.0;
+      v[3] = 0.0;
+      v[4] = p_wall * G.over_gamma_1;
+    }
+  }
+  const int64_t o = G.at(i, j, k);
+  for (int l = 0; l < nv; ++l) {
+    const int64_t q = o + l * G.vs;
+    Q[q] = Qn ? (T)(v[l] - Qn[q]) : (T)v[l];
+  }
+}
+
 // Qn: null for a full state Q; in the mixed form Q holds FP32 stage increments over
 // the FP64 state Qn, and a boundary rule is applied to Qn + Q (the increment stored
 // is the rule's state minus Qn), so it acts as on a full state.
@@ -444,14 +515,15 @@ template <class T>
 __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t, const double* Qn = nullptr) {
   const int g = G.g, gx = G.gx, gy = G.gy;
   const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
-  const int gz = (G.dim == 3 && G.bcz != 2) ? 2 * g : 0;
+  const int glo = (G.dim == 3 && z_fill_lo(G)) ? g : 0, ghi = (G.dim == 3 && z_fill_hi(G)) ? g : 0;
+  const int gz = glo + ghi;
   int64_t nA = (int64_t)gz * G.ny * G.nx;            // z ghost planes
   int64_t nB = (int64_t)Nz * (2 * gy) * G.nx;        // y ghost rows
   int zo = (G.dim == 3) ? g : 0;
   int i, j, k;
   if (t < nA) {
     i = (int)(t % G.nx); int64_t r = t / G.nx; j = (int)(r % G.ny); int kk = (int)(r / G.ny);
-    k = kk < g ? kk : G.nz - 2 * g + kk;
+    k = kk < glo ? kk : G.nz - gz + kk;
   } else if (t < nA + nB) {
     int64_t s = t - nA;
     i = (int)(s % G.nx); int64_t r = s / G.nx; int jj = (int)(r % (2 * gy)); k = (int)(r / (2 * gy)) + zo;
@@ -462,6 +534,10 @@ __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t
     i = ii < gx ? ii : G.nx - 2 * gx + ii;
   }
   const int64_t o = G.at(i, j, k);
+  if (G.dim == 3 && (G.bcx || G.bcy || z_bnd_lo(G) || z_bnd_hi(G))) {
+    ghost_cell_3d_bnd<T>(Q, G, nv, i, j, k, Qn);
+    return;
+  }
   const bool xb = G.bcx && (i == 0 || i == G.nx - 1);  // x boundary cell
   const bool yb = G.bcy && (j == 0 || j == G.ny - 1);  // y boundary cell
   if (!xb && !yb) {  // periodic images only

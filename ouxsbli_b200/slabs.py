@@ -42,13 +42,44 @@ def slab_bounds(nz: int, g: int, rank: int, world: int) -> tuple[int, int]:
     return rank * n, n + 2 * g
 
 
+def slab_bc_z(periodic: bool, rank: int, world: int) -> int:
+    """The slab's bc_z (enum oux_bc_z): halo planes at both ends, or, on a grid with a
+    non-periodic z, the grid's boundary at the first slab's lower / the last slab's
+    upper end."""
+    if periodic:
+        return 2
+    if world == 1:
+        return 1
+    if rank == 0:
+        return 3
+    return 4 if rank == world - 1 else 2
+
+
 def slab_config(cfg: SolverConfig, rank: int, world: int) -> tuple[SolverConfig, int]:
-    """The rank's local configuration (bc_z = 2, its z spacings) and its k0."""
+    """The rank's local configuration (its bc_z, z spacings and boundary rules) and its k0."""
     if cfg.dim != 3:
         raise ValueError("z slabs need a 3D configuration")
+    if cfg.bc_z not in (0, 1):
+        raise ValueError("split a periodic (bc_z = 0) or non-periodic (bc_z = 1) grid")
     k0, n = slab_bounds(cfg.nz, cfg.g, rank, world)
     dz = np.asarray(cfg.dz, dtype=np.float64)[k0:k0 + n - 1].copy()
-    return dataclasses.replace(cfg, nz=n, dz=dz, bc_z=2), k0
+    bc_z = slab_bc_z(cfg.bc_z == 0, rank, world)
+    boundary = None
+    if cfg.boundary:
+        boundary = {}
+        for face, rule in cfg.boundary.items():
+            if face == "z_lo" and bc_z not in (1, 3):
+                continue
+            if face == "z_hi" and bc_z not in (1, 4):
+                continue
+            if not isinstance(rule, str) and rule[0] == "fixed" and face in ("x_lo", "x_hi", "y_lo", "y_hi"):
+                # 3D fixed values are indexed (l, k, position in the plane): keep the slab's planes
+                v = np.asarray(rule[1])
+                other = cfg.ny if face.startswith("x") else cfg.nx
+                v = v.reshape(v.shape[0], cfg.nz, other)[:, k0:k0 + n].reshape(v.shape[0], -1)
+                rule = ("fixed", v)
+            boundary[face] = rule
+    return dataclasses.replace(cfg, nz=n, dz=dz, bc_z=bc_z, boundary=boundary), k0
 
 
 def slab_state(qj: np.ndarray, cfg: SolverConfig, rank: int, world: int) -> np.ndarray:
@@ -58,24 +89,33 @@ def slab_state(qj: np.ndarray, cfg: SolverConfig, rank: int, world: int) -> np.n
 
 
 def halo_exchange(send_lo: torch.Tensor, send_hi: torch.Tensor, recv_lo: torch.Tensor, recv_hi: torch.Tensor,
-                  rank: int, world: int, group=None) -> None:
+                  rank: int, world: int, group=None, periodic: bool = True) -> None:
     """Send `send_lo` down and `send_hi` up; receive the lower halo from below into
-    `recv_lo` and the upper halo from above into `recv_hi` (periodic in rank).
+    `recv_lo` and the upper halo from above into `recv_hi` (periodic in rank; with a
+    non-periodic z the first rank has no rank below and the last none above).
 
     Sends and receives are posted in the same order on every rank (up first, then
     down) and tagged, so two ranks that are each other's upper and lower neighbour
     match them correctly."""
     if world == 1:
-        recv_lo.copy_(send_hi)
-        recv_hi.copy_(send_lo)
+        if periodic:
+            recv_lo.copy_(send_hi)
+            recv_hi.copy_(send_lo)
         return
     up, down = (rank + 1) % world, (rank - 1) % world
-    ops = [dist.P2POp(dist.isend, send_hi, up, group, TAG_UP),
-           dist.P2POp(dist.irecv, recv_lo, down, group, TAG_UP),
-           dist.P2POp(dist.isend, send_lo, down, group, TAG_DOWN),
-           dist.P2POp(dist.irecv, recv_hi, up, group, TAG_DOWN)]
-    for req in dist.batch_isend_irecv(ops):
-        req.wait()
+    has_up = periodic or rank < world - 1
+    has_down = periodic or rank > 0
+    ops = []
+    if has_up:
+        ops.append(dist.P2POp(dist.isend, send_hi, up, group, TAG_UP))
+    if has_down:
+        ops.append(dist.P2POp(dist.irecv, recv_lo, down, group, TAG_UP))
+        ops.append(dist.P2POp(dist.isend, send_lo, down, group, TAG_DOWN))
+    if has_up:
+        ops.append(dist.P2POp(dist.irecv, recv_hi, up, group, TAG_DOWN))
+    if ops:
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
 
 
 class SlabSolver:
@@ -133,7 +173,8 @@ class SlabSolver:
                 self.run_stage(st)
                 send_lo, send_hi = self.pack(st)
                 recv_lo, recv_hi = self.recv_buffers(st)
-                halo_exchange(send_lo, send_hi, recv_lo, recv_hi, self.rank, self.world, self.group)
+                halo_exchange(send_lo, send_hi, recv_lo, recv_hi, self.rank, self.world, self.group,
+                              periodic=self.global_cfg.bc_z == 0)
                 self.unpack(st)
 
     def close(self) -> None:
@@ -160,10 +201,13 @@ class LocalSlabs:
                 for s in self.slabs:
                     s.run_stage(st)
                 sent = [s.pack(st) for s in self.slabs]
+                periodic = self.cfg.bc_z == 0
                 for r, s in enumerate(self.slabs):
                     recv_lo, recv_hi = s.recv_buffers(st)
-                    recv_lo.copy_(sent[(r - 1) % W][1])  # the highest planes of the slab below
-                    recv_hi.copy_(sent[(r + 1) % W][0])  # the lowest planes of the slab above
+                    if periodic or r > 0:
+                        recv_lo.copy_(sent[(r - 1) % W][1])  # the highest planes of the slab below
+                    if periodic or r < W - 1:
+                        recv_hi.copy_(sent[(r + 1) % W][0])  # the lowest planes of the slab above
                 for s in self.slabs:
                     s.unpack(st)
 
@@ -173,6 +217,19 @@ class LocalSlabs:
         parts = [s.get_state() for s in self.slabs]
         inner = [p[:, :, :, g:-g] for p in parts]
         return np.asfortranarray(np.concatenate([parts[0][:, :, :, :g], *inner, parts[-1][:, :, :, -g:]], axis=3))
+
+    def check_state(self) -> int:
+        """The OR of the slabs' fault bits (NaN / non-positive density or pressure)."""
+        bits = 0
+        for s in self.slabs:
+            bits |= s.solver.check_state()
+        return bits
+
+    def diagnostics(self) -> tuple[float, float, float]:
+        """KE, entropy and enstrophy averaged over the whole grid (the slabs hold equal
+        numbers of cells)."""
+        d = np.array([s.solver.diagnostics() for s in self.slabs])
+        return tuple(float(x) for x in d.mean(axis=0))
 
     def close(self) -> None:
         for s in self.slabs:

@@ -35,7 +35,7 @@ class SolverConfig:
     precision: str = "fp64"        # fp64 | mixed (FP32 stage states/fluxes, FP64 Q^n + accumulation)
     bc_x: int = 0                  # 0 periodic; 1 non-periodic x (boundary flux kernels, boundary cells; 2D)
     bc_y: int = 0                  # the same for y (2D)
-    bc_z: int = 0                  # 0 periodic; 2 z slab of a larger grid (ghost planes from halo exchange)
+    bc_z: int = 0                  # 0 periodic; 1 non-periodic; 2-4 z slab of a larger grid (enum oux_bc_z)
     # rules of the non-periodic faces ("x_lo", "x_hi", "y_lo", "y_hi"): "zero_gradient"
     # (the default), "slip_wall", "noslip_wall" or ("fixed", values (nv, ny) for x faces /
     # (nv, nx) for y faces, of Q/J)
@@ -78,7 +78,10 @@ class SolverConfig:
         out = []
         for name, rule in (self.boundary or {}).items():
             face = _lib.FACES[name]
-            n = self.ny if face < 2 else self.nx
+            if self.dim == 3:
+                n = (self.ny * self.nz, self.nx * self.nz, self.nx * self.ny)[face // 2]
+            else:
+                n = self.ny if face < 2 else self.nx
             r = {"face": face, "kind": None, "fixed": None, "farfield": None, "cells": None}
             if isinstance(rule, str):
                 r["kind"] = _lib.BC_KINDS[rule]

@@ -214,3 +214,42 @@ def test_z_slabs_match_the_undivided_solve(world, rk, precision, cuda_device):
     else:
         for l in range(5):
             assert np.linalg.norm(a[:, l] - b[:, l]) / np.linalg.norm(b[:, l]) <= 1e-6, l
+
+
+@pytest.mark.parametrize("slabs", [2, 4])
+def test_stz_slabs_with_walls_match_the_oracle(slabs, tmp_path, cuda_device):
+    """3D_solver/STZ through Case.run: the grid in z slabs (the first and last with
+    the grid's zero-gradient ends, the inner ones exchanging halos) with slip walls in
+    x and y, 6 steps, against the oracle on the undivided grid: bit-identical."""
+    from ouxsbli_b200 import Case
+    from ouxsbli_b200.grid import jacobian, to_qj
+    c = Case("3D_solver/STZ", tmp_path / "stz", nz=33, nt=6, np=1, slabs=slabs)
+    c.build()
+    c.run(device=cuda_device)
+    p, xc, yc, zc, dx, dy, dz, Q = c._initial()
+    cfg = c._solver_config(p, dx, dy, dz)
+    np.testing.assert_array_equal(c.solver.get_state(), oracle.step(cfg, to_qj(Q, jacobian(dx, dy, dz)), 6))
+
+
+def test_stz_shock_tube_along_z_vs_exact_sod(tmp_path, cuda_device):
+    """3D_solver/STZ at its own settings (two slabs of 511 interior planes, SLAU1 /
+    TVD minmod order 2, 50 x 102 steps to t = 0.0996): the profile along z against
+    the exact Sod solution, relative L1 of density and pressure < 1 %."""
+    import sod_exact
+    from ouxsbli_b200 import Case
+    from ouxsbli_b200.grid import jacobian
+    c = Case("3D_solver/STZ", tmp_path / "stz")
+    c.build()
+    c.run(device=cuda_device)
+    p, xc, yc, zc, dx, dy, dz, Q = c._initial()
+    q = c.solver.get_state()
+    J = jacobian(dx, dy, dz)
+    rho = q[2, 0, 2] * J[2, 2]
+    w = q[2, 3, 2] / q[2, 0, 2]
+    pr = 0.4 * (q[2, 4, 2] * J[2, 2] - 0.5 * rho * w * w)
+    t = p["nt"] * p["np"] * p["dt"]
+    z = zc[1:-1]
+    re, _, pe = sod_exact.solve(z, t, p["rho_L"], 0.0, p["p_L"], p["rho_R"], 0.0, p["p_R"], gamma=1.4, x0=0.5)
+    l1_rho = np.mean(np.abs(rho[1:-1] - re)) / np.mean(re)
+    l1_p = np.mean(np.abs(pr[1:-1] - pe)) / np.mean(pe)
+    assert l1_rho < 0.01 and l1_p < 0.01, (l1_rho, l1_p)
