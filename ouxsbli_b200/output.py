@@ -153,11 +153,15 @@ class HistoryWriter:
         if step == 0:
             self.ke0, self.s0 = np.float32(ke), np.float32(ent)
         ke32, s32 = np.float32(ke), np.float32(ent)
+        # a flow that starts at rest has ke0 = 0: the ratio is written as the reference
+        # writes it, Infinity / NaN
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ds = np.float32((self.s0 - s32) / self.s0)
+            kr = np.float32(ke32 / self.ke0)
         with open(self.dir / "entropy.d", "a") as f:
-            f.write(fortran_e(float(np.float32(t))) + fortran_e(float(np.float32((self.s0 - s32) / self.s0))) + "\n")
+            f.write(fortran_e(float(np.float32(t))) + fortran_e(float(ds)) + "\n")
         with open(self.dir / "kinetic_energy.d", "a") as f:
-            f.write(fortran_e(float(np.float32(t))) + fortran_e(float(ke32)) +
-                    fortran_e(float(np.float32(ke32 / self.ke0))) + "\n")
+            f.write(fortran_e(float(np.float32(t))) + fortran_e(float(ke32)) + fortran_e(float(kr)) + "\n")
 
 
 def write_restart(path, q: np.ndarray) -> None:
