@@ -195,6 +195,7 @@ int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fi
  * 2 c_inf/(gamma-1) of the far field; u_n = (R+ + R-)/2, c = (gamma-1)(R+ - R-)/4,
  * rho = rho_inf (c / c_inf)^(2/(gamma-1)), p = rho c^2 / gamma, tangential velocity
  * u_tangential (the top row of 2D_solver/BL0/set.f90). */
+/* (2D solves.) */
 int oux_set_boundary_farfield(oux_handle* h, int32_t face, double rho_inf, double u_tangential,
                               double u_normal, double c_inf);
 /* A rule per position along the face: kinds_dev holds one enum oux_bc_kind per
@@ -202,7 +203,7 @@ int oux_set_boundary_farfield(oux_handle* h, int32_t face, double rho_inf, doubl
  * and read at every fill; FIXED positions take the face's values of
  * oux_set_boundary, FARFIELD positions its far-field state.  NULL restores the
  * face's single rule.  (2D_solver/BL0/set.f90: a slip-like copy ahead of the plate,
- * a no-slip wall along it.) */
+ * a no-slip wall along it.)  2D solves. */
 int oux_set_boundary_cells(oux_handle* h, int32_t face, const int8_t* kinds_dev);
 /* y_last = 1: the y faces are applied after the x faces, so a corner takes its y
  * rule of the x-boundary value beside it (2D_solver/BL0/set.f90); 0 (default): the

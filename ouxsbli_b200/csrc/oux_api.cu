@@ -970,6 +970,7 @@ int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fi
 int oux_set_boundary_farfield(oux_handle* h, int32_t face, double rho_inf, double u_tangential,
                               double u_normal, double c_inf) {
   if (!h) return fail(OUX_E_INVALID, "null handle");
+  if (h->G.dim != 2) return fail(OUX_E_INVALID, "the far-field rule is built for 2D solves");
   if (face != OUX_FACE_X_HI && face != OUX_FACE_Y_HI)
     return fail(OUX_E_INVALID, "the far-field rule is built for the high faces (x high, y high)");
   if (!(face < 2 ? h->G.bcx : h->G.bcy))
@@ -985,6 +986,7 @@ int oux_set_boundary_farfield(oux_handle* h, int32_t face, double rho_inf, doubl
 
 int oux_set_boundary_cells(oux_handle* h, int32_t face, const int8_t* kinds_dev) {
   if (!h) return fail(OUX_E_INVALID, "null handle");
+  if (h->G.dim != 2) return fail(OUX_E_INVALID, "per-position rules are built for 2D solves");
   if (face < 0 || face > 3) return fail(OUX_E_INVALID, "face must be 0..3 (x low, x high, y low, y high)");
   if (kinds_dev && !(face < 2 ? h->G.bcx : h->G.bcy))
     return fail(OUX_E_INVALID, "the face's direction is periodic (set bc_x / bc_y = 1)");
