@@ -578,7 +578,11 @@ def main():
                                         "mean of the 3 RK3 stages)",
                 "traffic_source": "ncu dram__bytes_read+write of one stage-1 z-sweep launch at 160^3 "
                                   "(bytes per interior cell), scaled by cells",
-                "limiter": "latency: long-scoreboard stalls at 2 resident blocks/SM (ncu, profiles/)",
+                "limiter": "FP64 issue and latency: long-scoreboard stalls at 2 resident blocks/SM (ncu, profiles/)",
+                # the FP64 pipe of the sweeps (ncu --set full captures at 160^3, summarised in profiles/)
+                "fp64_pipe_pct_of_peak_ncu": {"sweep_z": 30.8, "sweep_x": 40.4,
+                                              "source": "profiles/sweep_z_tgv160_hybrid6_ns_fp64.md, "
+                                                        "profiles/sweep_x_tgv160_hybrid6_ns_fp64.md"},
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "dominant_kernel": dom, "per_kernel": per_kernel,
                 "step": {"achieved": step_achieved, "frac": step_achieved / peak,
