@@ -639,12 +639,18 @@ void calc_conv(Ctx& C) {
         if (C.c.dim == 2) F[3] = F[4];
         for (int l = 0; l < C.nv; ++l) C.w.F[C.fidx(l + 1, i - 1, j, C.c.dim == 3 ? k - 1 : 1)] = F[l];
       }
+  // z faces: k in io+1..nz-(io+1), or every face 1..nz-1 with a non-periodic z (the
+  // 3D boundary kernels calc_*_z, 3D_solver/src/calc_slau_kernel.f90.fypp)
+  const bool zb = C.c.dim == 3 && C.c.bc_z == 1;
+  const int k0 = zb ? 1 : io + 1, k1 = zb ? nz - 1 : nz - (io + 1);
   if (C.c.dim == 3)
 #pragma omp parallel for schedule(static) private(F)
-    for (int k = io + 1; k <= nz - (io + 1); ++k)
+    for (int k = k0; k <= k1; ++k)
       for (int j = 2; j <= ny - 1; ++j)
         for (int i = 2; i <= nx - 1; ++i) {
-          conv_face(C, 2, i, j, k, F, ord);
+          int o = ord;
+          if (zb) o = (ord == 6 && 3 <= k && k <= nz - 3) ? 6 : (ord >= 4 && 2 <= k && k <= nz - 2) ? 4 : 2;
+          conv_face(C, 2, i, j, k, F, o);
           for (int l = 0; l < 5; ++l) C.w.G[C.gidx(l + 1, i - 1, j - 1, k)] = F[l];
         }
 }

@@ -76,8 +76,12 @@ int validate(const oux_config* c, std::string& why) {
     if (c->nz < 3 * g) { why = "z slab (bc_z >= 2) needs at least g interior planes (nz >= 3g)"; return OUX_E_INVALID; }
   }
   if (c->dim == 3 && (c->bc_x == 1 || c->bc_y == 1 || c->bc_z == 1 || c->bc_z == 3 || c->bc_z == 4) &&
-      (c->order != 2 || c->visc != OUX_EULER)) {
-    why = "3D non-periodic boundaries are built for order 2 Euler solves (3D_solver/STZ)";
+      c->visc != OUX_EULER) {
+    why = "3D non-periodic boundaries are built for Euler solves (no 3D viscous boundary stencils)";
+    return OUX_E_INVALID;
+  }
+  if (c->dim == 3 && (c->bc_z == 3 || c->bc_z == 4) && c->order != 2) {
+    why = "a z slab with a boundary end (bc_z = 3, 4) is built for order 2";
     return OUX_E_INVALID;
   }
   if (c->bc_y == 1 && c->ny < 4) { why = "non-periodic y (bc_y = 1) needs ny >= 4"; return OUX_E_INVALID; }
@@ -192,6 +196,7 @@ Geo make_geo(const oux_config& c) {
   G.bcy = c.bc_y;
   G.gy = c.bc_y ? 1 : G.g;
   G.bcz = c.dim == 3 ? c.bc_z : 0;
+  G.gz = (G.bcz == 1 || G.bcz == 3 || G.bcz == 4) ? 1 : G.g;
   G.bkind = 0;  // zero-gradient boundary cells until oux_set_boundary says otherwise
   for (int f = 0; f < 4; ++f) G.bfix[f] = nullptr;
   G.gamma_1 = c.gamma - 1.0;  // mod_constant.f90.fypp gamma_1, over_gamma_1, over_gamma
@@ -353,14 +358,15 @@ __global__ void k_diag_final(const double* partials, int nb, double inv_n, doubl
 __global__ void k_check(const double* __restrict__ Q, Geo G, const double* __restrict__ jac, double gamma_1,
                         int* status) {
   const int g = G.g;
-  const int Nx = G.nx - 2 * G.gx, Ny = G.ny - 2 * G.gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
+  const int Nx = G.nx - 2 * G.gx, Ny = G.ny - 2 * G.gy, Nz = (G.dim == 3) ? G.nz - 2 * G.gz : 1;
   int64_t n = (int64_t)Nx * Ny * Nz;
   int bits = 0;
+  (void)g;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
     int i = (int)(t % Nx) + G.gx;
     int64_t r = t / Nx;
     int j = (int)(r % Ny) + G.gy;
-    int k = (G.dim == 3) ? (int)(r / Ny) + g : 0;
+    int k = (G.dim == 3) ? (int)(r / Ny) + G.gz : 0;
     int64_t o = G.at(i, j, k);
     double Jv = jac[(int64_t)j * G.nx + i];
     double q1 = Q[o], rho = Jv * q1;

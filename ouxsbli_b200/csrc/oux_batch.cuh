@@ -104,7 +104,7 @@ __host__ __device__ constexpr size_t batch_smem() {
 template <int DIR>
 __host__ __device__ inline void sweep_grid(const Geo& G, int n[3]) {
   const int g = G.g;
-  const int Nx = G.nx - 2 * G.gx, Ny = G.ny - 2 * G.gy, Nz = G.dim == 3 ? G.nz - 2 * g : 1;
+  const int Nx = G.nx - 2 * G.gx, Ny = G.ny - 2 * G.gy, Nz = G.dim == 3 ? G.nz - 2 * G.gz : 1;
   if (DIR == 0) { n[0] = (Nx + 31) / 32; n[1] = (Ny + BATCH_ROWS_X - 1) / BATCH_ROWS_X; n[2] = Nz; }
   else if (DIR == 1) { n[0] = (Nx + 31) / 32; n[1] = (Ny + BATCH_ROWS_YZ - 1) / BATCH_ROWS_YZ; n[2] = Nz; }
   else { n[0] = (Nx + 31) / 32; n[1] = (Nz + BATCH_ROWS_YZ - 1) / BATCH_ROWS_YZ; n[2] = Ny; }

@@ -30,6 +30,7 @@ struct Geo {
   int dim, nx, ny, nz, g;     // padded extents, ghost width
   int gx, bcx;                // x ghost width of the cell ranges (g, or 1 for a non-periodic x), bc_x
   int gy, bcy;                // the same for y
+  int gz;                     // z ghost width of the cell ranges (g, or 1 for a non-periodic z)
   int bcz;                    // enum oux_bc_z: 0 periodic; 1 non-periodic (both ends); slabs whose
                               // z ghost planes come from the neighbours: 2 both ends, 3 / 4 the
                               // upper / lower end only (the other end is the grid's boundary)
@@ -402,9 +403,9 @@ __host__ __device__ inline bool z_bnd_hi(const Geo& G) { return G.bcz == 1 || G.
 
 // A z slab leaves the ghost planes of its halo ends to the halo exchange.
 __host__ __device__ inline int64_t ghost_cells(const Geo& G) {
-  const int g = G.g, gy = G.gy;
-  const int Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
-  const int gz = (G.dim == 3) ? g * ((int)z_fill_lo(G) + (int)z_fill_hi(G)) : 0;
+  const int gy = G.gy;
+  const int Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * G.gz : 1;
+  const int gz = (G.dim == 3) ? G.gz * ((int)z_fill_lo(G) + (int)z_fill_hi(G)) : 0;
   return (int64_t)gz * G.ny * G.nx + (int64_t)Nz * (2 * gy) * G.nx + (int64_t)Nz * Ny * (2 * G.gx);
 }
 
@@ -514,12 +515,12 @@ __device__ __forceinline__ void ghost_cell_3d_bnd(T* Q, const Geo& G, int nv, in
 template <class T>
 __device__ __forceinline__ void ghost_cell(T* Q, const Geo& G, int nv, int64_t t, const double* Qn = nullptr) {
   const int g = G.g, gx = G.gx, gy = G.gy;
-  const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * g : 1;
-  const int glo = (G.dim == 3 && z_fill_lo(G)) ? g : 0, ghi = (G.dim == 3 && z_fill_hi(G)) ? g : 0;
+  const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * gy, Nz = (G.dim == 3) ? G.nz - 2 * G.gz : 1;
+  const int glo = (G.dim == 3 && z_fill_lo(G)) ? G.gz : 0, ghi = (G.dim == 3 && z_fill_hi(G)) ? G.gz : 0;
   const int gz = glo + ghi;
   int64_t nA = (int64_t)gz * G.ny * G.nx;            // z ghost planes
   int64_t nB = (int64_t)Nz * (2 * gy) * G.nx;        // y ghost rows
-  int zo = (G.dim == 3) ? g : 0;
+  int zo = (G.dim == 3) ? G.gz : 0;
   int i, j, k;
   if (t < nA) {
     i = (int)(t % G.nx); int64_t r = t / G.nx; j = (int)(r % G.ny); int kk = (int)(r / G.ny);

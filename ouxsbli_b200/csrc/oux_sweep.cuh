@@ -516,22 +516,23 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   const Geo& G = A.G;
   const int g = G.g, gx = G.gx, gy = G.gy;  // gx / gy: 1 with a non-periodic x / y
   const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * gy;
-  const int Nz = (DIM == 3) ? G.nz - 2 * g : 1;
+  const int gz = G.gz;                        // 1 with a non-periodic z
+  const int Nz = (DIM == 3) ? G.nz - 2 * gz : 1;
   const bool act = tid < TX * TY;  // thread owns a face / cell slot of the tile shape
   const int tx = tid % TX, ty = tid / TX;
   const int nthr = nthr_all;
   // block origin (first owned cell) in padded coordinates
   int bx0, by0, bz0;
   if constexpr (DIR == 0) {
-    bx0 = gx + 32 * b0; by0 = gy + ROWS * b1; bz0 = (DIM == 3) ? g + b2 : 0;
+    bx0 = gx + 32 * b0; by0 = gy + ROWS * b1; bz0 = (DIM == 3) ? gz + b2 : 0;
   } else if constexpr (DIR == 1) {
-    bx0 = gx + 32 * b0; by0 = gy + ROWS * b1; bz0 = (DIM == 3) ? g + b2 : 0;
+    bx0 = gx + 32 * b0; by0 = gy + ROWS * b1; bz0 = (DIM == 3) ? gz + b2 : 0;
   } else {
-    bx0 = gx + 32 * b0; bz0 = g + ROWS * b1; by0 = gy + b2;
+    bx0 = gx + 32 * b0; bz0 = gz + ROWS * b1; by0 = gy + b2;
   }
   const int64_t stv[3] = {1, G.sx, G.plane};
   const int nsweep = DIR == 0 ? G.nx : (DIR == 1 ? G.ny : G.nz);
-  const int ext[3] = {gx + Nx, gy + Ny, g + Nz};
+  const int ext[3] = {gx + Nx, gy + Ny, gz + Nz};
 
   // ---- operand prefetch (y/z sweeps): the thread that owns a cell copies it ----
   constexpr bool PF_ON = PF > 0 && DIR != 0;
@@ -647,7 +648,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       rowok = fc[0] < ext[0];
     }
     const int f = fc[DIR];
-    const bool valid = act && rowok && f >= (DIR == 0 ? gx : DIR == 1 ? gy : g) - 1 && f <= ext[DIR] - 1;
+    const bool valid = act && rowok && f >= (DIR == 0 ? gx : DIR == 1 ? gy : gz) - 1 && f <= ext[DIR] - 1;
     if (valid) {
       T F[5];
       // tile position of cell f + off is base + (2 + off) * step
@@ -656,15 +657,16 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       auto sc = [&](int field, int m) -> T { return tile[field * NC + cb + m * step]; };
       T fd = T(0);
       if (!KONLY && A.scheme != 0) fd = T(0.5) * (st0(TF_SEN, 2) + st0(TF_SEN, 3));
-      if constexpr (DIM == 2) {
-        // non-periodic x / y: every face, the stencil order lowered next to the
+      if constexpr (DIM == 2 || VK == VK_EULER) {
+        // non-periodic x / y (/ z): every face, the stencil order lowered next to the
         // boundary as the reference's boundary kernels do (2D_solver/src/calc_{slau,
-        // keep,hybrid}_kernel.f90.fypp, calc_*_x and calc_*_y): 6th for
-        // 2 <= f <= n-4, 4th for 1 <= f <= n-3, else 2nd / first order (f: 0-based
-        // left cell of the face)
+        // keep,hybrid}_kernel.f90.fypp, calc_*_x and calc_*_y; 3D_solver/src/calc_*
+        // _kernel.f90.fypp): 6th for 2 <= f <= n-4, 4th for 1 <= f <= n-3, else 2nd /
+        // first order (f: 0-based left cell of the face).  3D walls are Euler only.
         int lo = ORDER;
-        const int nn = DIR == 0 ? G.nx : G.ny;
-        if (DIR == 0 ? G.bcx : G.bcy)
+        const int nn = DIR == 0 ? G.nx : (DIR == 1 ? G.ny : G.nz);
+        const bool nonper = DIR == 0 ? (bool)G.bcx : (DIR == 1 ? (bool)G.bcy : G.bcz == 1);
+        if (nonper)
           lo = (ORDER == 6 && f >= 2 && f <= nn - 4) ? 6 : (ORDER >= 4 && f >= 1 && f <= nn - 3) ? 4 : 2;
         if (lo == ORDER) {
           conv_flux<ORDER, KONLY>(A, sc, fd, DIR, F);

@@ -62,8 +62,9 @@ class SolverConfig:
     def interior_cells(self) -> int:
         g = self.g
         gx, gy = (1 if self.bc_x else g), (1 if self.bc_y else g)
+        gz = 1 if self.bc_z in (1, 3, 4) else g
         n = (self.nx - 2 * gx) * (self.ny - 2 * gy)
-        return n * (self.nz - 2 * g if self.dim == 3 else 1)
+        return n * (self.nz - 2 * gz if self.dim == 3 else 1)
 
     def boundary_rules(self) -> list[dict]:
         """The non-periodic faces' rules, normalised: per given face a dict with
