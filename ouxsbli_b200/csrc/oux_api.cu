@@ -46,7 +46,12 @@ int validate(const oux_config* c, std::string& why) {
   if (c->order != 2 && c->order != 4 && c->order != 6) { why = "order must be 2, 4 or 6"; return OUX_E_INVALID; }
   int g = c->order / 2;
   int nzc = c->dim == 3 ? c->nz : 1;
-  if (c->nx < 2 * g + 1 || c->ny < 2 * g + 1 || (c->dim == 3 && c->nz < 2 * g + 1) || c->nx < 4) {
+  // a periodic axis keeps g ghost cells a side, a non-periodic one a single boundary
+  // cell (and at least two interior cells for the boundary faces' fallback stencils)
+  auto too_small = [&](int n, bool nonper) { return nonper ? n < 4 : n < 2 * g + 1; };
+  const bool zb = c->dim == 3 && (c->bc_z == 1 || c->bc_z == 3 || c->bc_z == 4);
+  if (too_small(c->nx, c->bc_x == 1) || too_small(c->ny, c->bc_y == 1) ||
+      (c->dim == 3 && too_small(c->nz, zb)) || c->nx < 4) {
     why = "grid too small for the stencil (need at least 1 interior cell per axis)";
     return OUX_E_INVALID;
   }
