@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--mixed-check-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy check (the north star's 1000)")
+    ap.add_argument("--commz", action="store_true",
+                    help="split the one grid into z slabs over the ranks (halo exchange after every stage; "
+                         "strong scaling) instead of running independent replicas")
     ap.add_argument("--workload", default="tgv256", choices=["tgv256", "large512"],
                     help="large512: FP64 vs mixed on the 512^3 ME4 supersonic TGV (opt-in, minutes)")
     ap.add_argument("--large-steps", type=int, default=2000)
@@ -371,12 +374,62 @@ def run_large(args):
     return 0
 
 
+def run_commz(args):
+    """The --n^3 workload split into z slabs over the torchrun ranks (one slab per GPU,
+    halo exchange over NCCL after every stage, ouxsbli_b200.slabs): whole-grid
+    cell-steps per second of the slowest rank, strong scaling."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from ouxsbli_b200.replicas import max_over_ranks
+    from ouxsbli_b200.slabs import SlabSolver
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    group = None
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    cfg, qj = workload(args.n, args.scheme, args.visc)
+    slab = SlabSolver(cfg, rank, world, dev, group)
+    slab.set_global_state(qj)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    slab.step(args.warmup)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    slab.step(args.steps)
+    e1.record(stream)
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1), dev)
+    cells = cfg.interior_cells()
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": cells * args.steps / (ms / 1e3) / 1e6, "unit": METRIC,
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic TGV initial field)",
+                          "config": config_json(args, cfg) | {"parallelism": f"{world} z slabs (COMMZ)"},
+                          "gpu_launches": None}))
+    slab.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "large512":
         return run_large(args)
+    if args.commz:
+        return run_commz(args)
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
