@@ -1046,6 +1046,88 @@ void visc_face_gv2(const Ctx& C, int dir, int i, int j, int k, double out[4]) {
   out[3] = les ? (vw + Hsgs) : vw;
 }
 
+// 2nd-order fallback of the high-order viscous kernels outside their guard
+// (Navier-Stokes), written per direction as the reference writes it:
+// calc_Ev (3D_solver/src/calc_visc_high.f90.fypp:194-260), calc_Fv (:432-497),
+// calc_Gv (:674-739).  Returns the 4 subtracted terms like visc_face_high.
+void visc_face_fb3(const Ctx& C, int dir, int i, int j, int k, double out[4]) {
+  Prim P{C};
+  const Consts& K = C.K;
+  const double dxi = C.g.xix[i - 1], dyj = C.g.etay[j - 1], dzk = C.g.zetaz[k - 1];
+  // 0.25 (m1 (-a(-) + a(0) - a2(-) + a2(0)) + m2 (-a(0) + a(+) - a2(0) + a2(+))) d, the
+  // tangential derivative of field `a` (a2: the face's second cell) along `t`
+  auto tder = [&](int comp, int t, int i2, int j2, int k2, double m1, double m2, double d) {
+    int di = t == 0, dj = t == 1, dk = t == 2;
+    auto a = [&](int ii, int jj, int kk) { return P.vel(comp, ii, jj, kk); };
+    return 0.25 * (m1 * (-a(i - di, j - dj, k - dk) + a(i, j, k) - a(i2 - di, j2 - dj, k2 - dk) + a(i2, j2, k2)) +
+                   m2 * (-a(i, j, k) + a(i + di, j + dj, k + dk) - a(i2, j2, k2) + a(i2 + di, j2 + dj, k2 + dk))) *
+           d;
+  };
+  auto mavg = [&](int t, int i2, int j2, int k2, double& m1, double& m2) {
+    int di = t == 0, dj = t == 1, dk = t == 2;
+    m1 = 0.25 * (P.mu(i - di, j - dj, k - dk) + P.mu(i, j, k) + P.mu(i2 - di, j2 - dj, k2 - dk) + P.mu(i2, j2, k2));
+    m2 = 0.25 * (P.mu(i, j, k) + P.mu(i + di, j + dj, k + dk) + P.mu(i2, j2, k2) + P.mu(i2 + di, j2 + dj, k2 + dk));
+  };
+  if (dir == 0) {
+    const int i2 = i + 1;
+    double mx = 0.5 * (P.mu(i, j, k) + P.mu(i2, j, k));
+    double kTx = K.Cp_over_Pr * mx * (-P.T(i, j, k) + P.T(i2, j, k)) * dxi;
+    double m1, m2;
+    mavg(1, i2, j, k, m1, m2);
+    double muy = tder(0, 1, i2, j, k, m1, m2, dyj), mvy = tder(1, 1, i2, j, k, m1, m2, dyj);
+    mavg(2, i2, j, k, m1, m2);
+    double muz = tder(0, 2, i2, j, k, m1, m2, dzk), mwz = tder(2, 2, i2, j, k, m1, m2, dzk);
+    double mux = mx * (-P.u(i, j, k) + P.u(i2, j, k)) * dxi;
+    double mvx = mx * (-P.v(i, j, k) + P.v(i2, j, k)) * dxi;
+    double mwx = mx * (-P.w(i, j, k) + P.w(i2, j, k)) * dxi;
+    double txx = two_third * (2.0 * mux - mvy - mwz);
+    double txy = muy + mvx;
+    double txz = mwx + muz;
+    double utxx = 0.5 * (P.u(i, j, k) + P.u(i2, j, k)) * txx;
+    double vtxy = 0.5 * (P.v(i, j, k) + P.v(i2, j, k)) * txy;
+    double wtxz = 0.5 * (P.w(i, j, k) + P.w(i2, j, k)) * txz;
+    out[0] = txx; out[1] = txy; out[2] = txz; out[3] = utxx + vtxy + wtxz + kTx;
+  } else if (dir == 1) {
+    const int j2 = j + 1;
+    double my = 0.5 * (P.mu(i, j, k) + P.mu(i, j2, k));
+    double kTy = K.Cp_over_Pr * my * (-P.T(i, j, k) + P.T(i, j2, k)) * dyj;
+    double m1, m2;
+    mavg(0, i, j2, k, m1, m2);
+    double mux = tder(0, 0, i, j2, k, m1, m2, dxi), mvx = tder(1, 0, i, j2, k, m1, m2, dxi);
+    mavg(2, i, j2, k, m1, m2);
+    double mvz = tder(1, 2, i, j2, k, m1, m2, dzk), mwz = tder(2, 2, i, j2, k, m1, m2, dzk);
+    double muy = my * (-P.u(i, j, k) + P.u(i, j2, k)) * dyj;
+    double mvy = my * (-P.v(i, j, k) + P.v(i, j2, k)) * dyj;
+    double mwy = my * (-P.w(i, j, k) + P.w(i, j2, k)) * dyj;
+    double tyx = muy + mvx;
+    double tyy = two_third * (2.0 * mvy - mwz - mux);
+    double tyz = mvz + mwy;
+    double utyx = 0.5 * (P.u(i, j, k) + P.u(i, j2, k)) * tyx;
+    double vtyy = 0.5 * (P.v(i, j, k) + P.v(i, j2, k)) * tyy;
+    double wtyz = 0.5 * (P.w(i, j, k) + P.w(i, j2, k)) * tyz;
+    out[0] = tyx; out[1] = tyy; out[2] = tyz; out[3] = utyx + vtyy + wtyz + kTy;
+  } else {
+    const int k2 = k + 1;
+    double m1, m2;
+    mavg(0, i, j, k2, m1, m2);
+    double mux = tder(0, 0, i, j, k2, m1, m2, dxi), mwx = tder(2, 0, i, j, k2, m1, m2, dxi);
+    mavg(1, i, j, k2, m1, m2);
+    double mvy = tder(1, 1, i, j, k2, m1, m2, dyj), mwy = tder(2, 1, i, j, k2, m1, m2, dyj);
+    double mz = 0.5 * (P.mu(i, j, k) + P.mu(i, j, k2));
+    double kTz = K.Cp_over_Pr * mz * (-P.T(i, j, k) + P.T(i, j, k2)) * dzk;
+    double muz = mz * (-P.u(i, j, k) + P.u(i, j, k2)) * dzk;
+    double mvz = mz * (-P.v(i, j, k) + P.v(i, j, k2)) * dzk;
+    double mwz = mz * (-P.w(i, j, k) + P.w(i, j, k2)) * dzk;
+    double tzx = mwx + muz;
+    double tzy = mvz + mwy;
+    double tzz = two_third * (2.0 * mwz - mux - mvy);
+    double utzx = 0.5 * (P.u(i, j, k) + P.u(i, j, k2)) * tzx;
+    double vtzy = 0.5 * (P.v(i, j, k) + P.v(i, j, k2)) * tzy;
+    double wtzz = 0.5 * (P.w(i, j, k) + P.w(i, j, k2)) * tzz;
+    out[0] = tzx; out[1] = tzy; out[2] = tzz; out[3] = utzx + vtzy + wtzz + kTz;
+  }
+}
+
 void calc_visc3(Ctx& C) {
   int nx = C.nx, ny = C.ny, nz = C.nz;
   double o[4];
@@ -1074,6 +1156,32 @@ void calc_visc3(Ctx& C) {
   if (vo == 4) { a0 = 2; a1 = 2; b0 = 3; b1 = 2; }
   else if (me4) { a0 = 3; a1 = 3; b0 = 3; b1 = 2; }
   else { a0 = 3; a1 = 3; b0 = 4; b1 = 3; }
+  const bool walls = C.c.bc_x || C.c.bc_y || C.c.bc_z == 1 || C.c.bc_z == 3 || C.c.bc_z == 4;
+  if (walls) {
+    // every face of the kernels' launch ranges, the guard choosing the stencil
+    // (calc_visc_high.f90.fypp: Ev i 1..nx-1, j 2..ny-1, k 2..nz-1, and alike)
+    auto face = [&](int dir, int i, int j, int k, double o4[4]) {
+      const int c[3] = {i, j, k}, n[3] = {nx, ny, nz};
+      bool in = true;
+      for (int a = 0; a < 3; ++a)
+        in = in && (a == dir ? (a0 <= c[a] && c[a] <= n[a] - a1) : (b0 <= c[a] && c[a] <= n[a] - b1));
+      if (in) visc_face_high(C, dir, i, j, k, o4);
+      else visc_face_fb3(C, dir, i, j, k, o4);
+    };
+#pragma omp parallel for schedule(static) private(o)
+    for (int k = 2; k <= nz - 1; ++k)
+      for (int j = 2; j <= ny - 1; ++j)
+        for (int i = 1; i <= nx - 1; ++i) { face(0, i, j, k, o); apply(&C.w.E[C.eidx(1, i, j - 1, k - 1)], o); }
+#pragma omp parallel for schedule(static) private(o)
+    for (int k = 2; k <= nz - 1; ++k)
+      for (int j = 1; j <= ny - 1; ++j)
+        for (int i = 2; i <= nx - 1; ++i) { face(1, i, j, k, o); apply(&C.w.F[C.fidx(1, i - 1, j, k - 1)], o); }
+#pragma omp parallel for schedule(static) private(o)
+    for (int k = 1; k <= nz - 1; ++k)
+      for (int j = 2; j <= ny - 1; ++j)
+        for (int i = 2; i <= nx - 1; ++i) { face(2, i, j, k, o); apply(&C.w.G[C.gidx(1, i - 1, j - 1, k)], o); }
+    return;
+  }
 #pragma omp parallel for schedule(static) private(o)
   for (int k = b0; k <= nz - b1; ++k)
     for (int j = b0; j <= ny - b1; ++j)

@@ -81,8 +81,9 @@ int validate(const oux_config* c, std::string& why) {
     if (c->nz < 3 * g) { why = "z slab (bc_z >= 2) needs at least g interior planes (nz >= 3g)"; return OUX_E_INVALID; }
   }
   if (c->dim == 3 && (c->bc_x == 1 || c->bc_y == 1 || c->bc_z == 1 || c->bc_z == 3 || c->bc_z == 4) &&
-      c->visc != OUX_EULER) {
-    why = "3D non-periodic boundaries are built for Euler solves (no 3D viscous boundary stencils)";
+      c->visc == OUX_LES) {
+    why = "3D non-periodic boundaries are built for Euler and Navier-Stokes solves (not LES: the SGS "
+          "viscosity's boundary values are not built)";
     return OUX_E_INVALID;
   }
   if (c->dim == 3 && (c->bc_z == 3 || c->bc_z == 4) && c->order != 2) {
@@ -102,7 +103,26 @@ int validate(const oux_config* c, std::string& why) {
 
 // Viscous kernel family the reference selects for (dim, order, visc_order, stencil):
 // calc_flux_base.f90.fypp:161-177 (3D) and 2D_solver/src/calc_flux_base.f90.fypp:108-132.
+int visc_kind_base(const oux_config* c, std::string& why);
+
+// 3D Navier-Stokes grids with a non-periodic direction take the walled variants
+// (order fallback of the convective faces, 2nd-order fallback of the viscous faces
+// outside the high-order guard); at order 2 neither applies and the periodic
+// kernels serve unchanged.
 int visc_kind(const oux_config* c, std::string& why) {
+  const int vk = visc_kind_base(c, why);
+  const bool walls = c->dim == 3 && (c->bc_x == 1 || c->bc_y == 1 || c->bc_z == 1 || c->bc_z == 3 || c->bc_z == 4);
+  if (vk <= VK_EULER || !walls || c->order == 2) return vk;
+  switch (vk) {
+    case VK_C6: return VK_C6W;
+    case VK_C4: return VK_C4W;
+    case VK_ME4: return VK_ME4W;
+    case VK_GV2: return VK_GV2W;
+    default: return vk;
+  }
+}
+
+int visc_kind_base(const oux_config* c, std::string& why) {
   if (c->visc == OUX_EULER) return VK_EULER;
   // unset visc_order: the order in 3D (calc_visc_high.f90.fypp:2-4), 4 if the order
   // is at least 4 else 2 in 2D (2D_solver/src/calc_flux_base.f90.fypp:2-4)

@@ -222,6 +222,8 @@ int oux_batch_create(oux_handle* const* members, int32_t n, const oux_batch_tuni
   if (t.mode != OUX_BATCH_PERSISTENT && t.mode != OUX_BATCH_GRAPH) return fail(OUX_E_INVALID, "unknown batch mode");
   if (t.mode == OUX_BATCH_GRAPH) t.use_graph = 1;
   oux_handle* h0 = members[0];
+  if (h0 && vk_wall(h0->vk))
+    return fail(OUX_E_INVALID, "batches of 3D Navier-Stokes solves with non-periodic boundaries are not built");
   for (int i = 0; i < n; ++i) {
     const oux_handle* h = members[i];
     if (!h) return fail(OUX_E_INVALID, "null member");

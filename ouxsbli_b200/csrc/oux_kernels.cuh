@@ -12,7 +12,15 @@
 
 namespace oux {
 
-enum ViscKind { VK_EULER = 0, VK_C6 = 1, VK_C4 = 2, VK_ME4 = 3, VK_GV2 = 4, VK_2D4 = 5 };
+enum ViscKind { VK_EULER = 0, VK_C6 = 1, VK_C4 = 2, VK_ME4 = 3, VK_GV2 = 4, VK_2D4 = 5,
+                // 3D Navier-Stokes grids with a non-periodic direction: the same stencils
+                // with the convective order lowered next to a boundary and the viscous
+                // faces outside the high-order guard on the 2nd-order fallback
+                VK_C6W = 6, VK_C4W = 7, VK_ME4W = 8, VK_GV2W = 9 };
+__host__ __device__ constexpr int vk_base(int vk) {
+  return vk == VK_C6W ? VK_C6 : vk == VK_C4W ? VK_C4 : vk == VK_ME4W ? VK_ME4 : vk == VK_GV2W ? VK_GV2 : vk;
+}
+__host__ __device__ constexpr bool vk_wall(int vk) { return vk >= VK_C6W; }
 // Stage combinations of 3D_solver/src/calc_steps.f90 with Qn = the FP64 state
 // Q^n and Qs = the stage state (FP64 in the plain form, FP32 in the mixed form);
 // all arithmetic of the combinations is FP64.

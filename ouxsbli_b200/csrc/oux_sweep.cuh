@@ -482,6 +482,59 @@ __device__ __forceinline__ void visc_2d4(const StepArgs<T>& A, const Acc& s, int
   out[3] = wu + wv + kT;
 }
 
+// ---- 3D 2nd-order fallback of the high-order viscous faces (Navier-Stokes) -------
+// The branch of calc_Ev / calc_Fv / calc_Gv taken outside their high-order guard
+// (3D_solver/src/calc_visc_high.f90.fypp:194-260, 432-497, 674-739): face viscosity
+// and normal derivatives from the face's two cells; tangential derivatives from the
+// two cell pairs on either side weighted by their 4-point viscosity averages.
+// D[c][a] is mu * d(velocity c) / d(axis a) as the reference names them (mux, mvy ...).
+template <class T>
+__device__ __forceinline__ void visc_fb3(const StepArgs<T>& A, int nd, int64_t o, const int64_t st[3],
+                                         const T invs[3], T out[4]) {
+  const Fields<T>& W = A.W;
+  const T* vel[3] = {W.u, W.v, W.w};
+  const int64_t o2 = o + st[nd];
+  const T inv = invs[nd];
+  const T mn = T(0.5) * (W.mu[o] + W.mu[o2]);
+  const T kT = T(A.K.Cp_over_Pr) * mn * (-W.T_[o] + W.T_[o2]) * inv;
+  T D[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) D[c][nd] = mn * (-vel[c][o] + vel[c][o2]) * inv;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (a == nd) continue;
+    const int64_t s = st[a];
+    const T m1 = T(0.25) * (W.mu[o - s] + W.mu[o] + W.mu[o2 - s] + W.mu[o2]);
+    const T m2 = T(0.25) * (W.mu[o] + W.mu[o + s] + W.mu[o2] + W.mu[o2 + s]);
+    auto tder = [&](const T* q) {
+      return T(0.25) * (m1 * (-q[o - s] + q[o] - q[o2 - s] + q[o2]) + m2 * (-q[o] + q[o + s] - q[o2] + q[o2 + s])) *
+             invs[a];
+    };
+    D[nd][a] = tder(vel[nd]);  // normal velocity along the tangent (cross stress)
+    D[a][a] = tder(vel[a]);    // tangential velocity along itself (normal stress)
+  }
+  const T two3 = T(2.0 / 3.0);
+  T t[3];
+  if (nd == 0) {
+    t[0] = two3 * (T(2) * D[0][0] - D[1][1] - D[2][2]);  // txx
+    t[1] = D[0][1] + D[1][0];                             // txy = muy + mvx
+    t[2] = D[2][0] + D[0][2];                             // txz = mwx + muz
+  } else if (nd == 1) {
+    t[0] = D[0][1] + D[1][0];                             // tyx = muy + mvx
+    t[1] = two3 * (T(2) * D[1][1] - D[2][2] - D[0][0]);  // tyy
+    t[2] = D[1][2] + D[2][1];                             // tyz = mvz + mwy
+  } else {
+    t[0] = D[2][0] + D[0][2];                             // tzx = mwx + muz
+    t[1] = D[1][2] + D[2][1];                             // tzy = mvz + mwy
+    t[2] = two3 * (T(2) * D[2][2] - D[0][0] - D[1][1]);  // tzz
+  }
+  T e = T(0.5) * (vel[0][o] + vel[0][o2]) * t[0];
+  e = e + T(0.5) * (vel[1][o] + vel[1][o2]) * t[1];
+  e = e + T(0.5) * (vel[2][o] + vel[2][o2]) * t[2];
+  out[0] = t[0]; out[1] = t[1]; out[2] = t[2];
+  out[3] = e + kT;
+}
+
 }  // namespace oux
 
 namespace oux {
@@ -509,8 +562,10 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   constexpr int TL = tile_len<ORDER, DIR, ROWS>();
   constexpr int NC = tile_cells<ORDER, DIR, ROWS>();
   constexpr int TX = SweepShape<DIR, ROWS>::TX, TY = SweepShape<DIR, ROWS>::TY;
-  constexpr bool HIGH = (VK == VK_C6 || VK == VK_C4 || VK == VK_ME4 || VK == VK_2D4);
-  constexpr bool SIXTH = (VK == VK_C6);
+  constexpr int VB = vk_base(VK);      // stencil family
+  constexpr bool WALL = vk_wall(VK);   // 3D viscous grid with a non-periodic direction
+  constexpr bool HIGH = (VB == VK_C6 || VB == VK_C4 || VB == VK_ME4 || VB == VK_2D4);
+  constexpr bool SIXTH = (VB == VK_C6);
   T* tile = reinterpret_cast<T*>(smraw);
   double* Fs = reinterpret_cast<double*>(smraw + sizeof(T) * TF_COUNT * NC);
   const Geo& G = A.G;
@@ -610,10 +665,19 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       if constexpr (DIM == 3) {
         const int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
         const int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
-        tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[a1], o, stv[a1], (T)invd[a1][ci[a1]]);
-        tile[TF_D1 * NC + c] = node_d<SIXTH, RO>(vel[a2], o, stv[a2], (T)invd[a2][ci[a2]]);
-        tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[ca], (T)invd[ca][ci[ca]]);
-        tile[TF_D3 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[cb], (T)invd[cb][ci[cb]]);
+        // with a non-periodic direction, only where the stencil stays inside the grid:
+        // the other cells lie outside the high-order guard, whose 2nd-order fallback
+        // does not read these values
+        constexpr int HD = SIXTH ? 3 : 2;
+        const int na[3] = {G.nx, G.ny, G.nz};
+        auto nd = [&](const T* f, int ax) -> T {
+          if (WALL && !(ci[ax] >= HD && ci[ax] + HD < na[ax])) return T(0);
+          return node_d<SIXTH, RO>(f, o, stv[ax], (T)invd[ax][ci[ax]]);
+        };
+        tile[TF_D0 * NC + c] = nd(vel[a1], a1);
+        tile[TF_D1 * NC + c] = nd(vel[a2], a2);
+        tile[TF_D2 * NC + c] = nd(vel[n], ca);
+        tile[TF_D3 * NC + c] = nd(vel[n], cb);
       } else {
         // 2D: only where the stencil stays inside the grid; the other cells lie
         // outside the 4th-order guard of calc_Ev4 / calc_Fv4, whose 2nd-order
@@ -657,12 +721,13 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       auto sc = [&](int field, int m) -> T { return tile[field * NC + cb + m * step]; };
       T fd = T(0);
       if (!KONLY && A.scheme != 0) fd = T(0.5) * (st0(TF_SEN, 2) + st0(TF_SEN, 3));
-      if constexpr (DIM == 2 || VK == VK_EULER) {
+      if constexpr (DIM == 2 || VK == VK_EULER || WALL) {
         // non-periodic x / y (/ z): every face, the stencil order lowered next to the
         // boundary as the reference's boundary kernels do (2D_solver/src/calc_{slau,
         // keep,hybrid}_kernel.f90.fypp, calc_*_x and calc_*_y; 3D_solver/src/calc_*
         // _kernel.f90.fypp): 6th for 2 <= f <= n-4, 4th for 1 <= f <= n-3, else 2nd /
-        // first order (f: 0-based left cell of the face).  3D walls are Euler only.
+        // first order (f: 0-based left cell of the face).  Compiled out of the periodic
+        // 3D viscous sweeps (their walled variants carry it).
         int lo = ORDER;
         const int nn = DIR == 0 ? G.nx : (DIR == 1 ? G.ny : G.nz);
         const bool nonper = DIR == 0 ? (bool)G.bcx : (DIR == 1 ? (bool)G.bcy : G.bcz == 1);
@@ -684,7 +749,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         T vo[4];
         const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
         const T inv = (T)invd[DIR][f];
-        if constexpr (VK == VK_GV2) {
+        if constexpr (VB == VK_GV2) {
           const int64_t o = G.at(fc[0], fc[1], DIM == 3 ? fc[2] : 0);
           T invs[3] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]], DIM == 3 ? (T)A.M.inv_dz[fc[2]] : T(0)};
           visc_gv2<DIM, LES, RO>(A, DIR, o, stv, invs, vo);
@@ -700,10 +765,31 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
           auto sv = [&](int field, int m) -> T { return tile[field * NC + base + m * step]; };
           visc_2d4(A, sv, DIR, inner, o, stv, invs, vo);
         } else {
-          constexpr int off0 = (VK == VK_C4) ? -1 : -2;
+          constexpr int off0 = (VB == VK_C4) ? -1 : -2;
           const int vb = base + (2 + off0) * step;
           auto sv = [&](int field, int m) -> T { return tile[field * NC + vb + m * step]; };
-          visc_high<VK, LES>(A, sv, DIR, inv, vo);
+          if constexpr (WALL) {
+            // high-order guard of calc_{E,F,G}v (calc_visc_high.f90.fypp:114/139/169,
+            // 350/376/406, 592/618/648), 0-based: C4 faces 1..n-3 and transverse cells
+            // 2..n-3, ME4 faces 2..n-4 and cells 2..n-3, C6 faces 2..n-4 and cells 3..n-4
+            static_assert(!LES, "walled viscous sweeps are Navier-Stokes only");
+            constexpr int FA = (VB == VK_C4) ? 1 : 2, TA = (VB == VK_C6) ? 3 : 2;
+            const int na[3] = {G.nx, G.ny, G.nz};
+            bool inner = f >= FA && f <= na[DIR] - 2 - FA;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+              if (a != DIR) inner = inner && fc[a] >= TA && fc[a] <= na[a] - 1 - TA;
+            if (inner) {
+              visc_high<VB, LES>(A, sv, DIR, inv, vo);
+            } else {
+              const int64_t o = G.at(fc[0], fc[1], fc[2]);
+              T invs[3] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]], (T)A.M.inv_dz[fc[2]]};
+              invs[DIR] = inv;
+              visc_fb3(A, DIR, o, stv, invs, vo);
+            }
+          } else {
+            visc_high<VB, LES>(A, sv, DIR, inv, vo);
+          }
         }
         if constexpr (DIM == 3) {
           F[1] = F[1] - vo[0]; F[2] = F[2] - vo[1]; F[3] = F[3] - vo[2]; F[4] = F[4] - vo[3];
