@@ -190,15 +190,19 @@ enum oux_face { OUX_FACE_X_LO = 0, OUX_FACE_X_HI = 1, OUX_FACE_Y_LO = 2, OUX_FAC
  * (the other end being the grid's boundary, with the rules of its face). */
 enum oux_bc_z { OUX_Z_PERIODIC = 0, OUX_Z_WALLS = 1, OUX_Z_SLAB = 2, OUX_Z_SLAB_LO_WALL = 3,
                 OUX_Z_SLAB_HI_WALL = 4 };
+/* NEUMANN: the neighbour's primitive state (rho, velocity, p) carried through the
+ * two cells' Jacobians, Q/J(b) = Q(n) / J(b) (3D_solver/src/set_bc_tbl_sbli.f90
+ * set_bc_Neumann_tbl_top_down, the TBL / SBLI top); ZERO_GRADIENT copies Q/J. */
 enum oux_bc_kind { OUX_BC_ZERO_GRADIENT = 0, OUX_BC_SLIP_WALL = 1, OUX_BC_FIXED = 2, OUX_BC_NOSLIP_WALL = 3,
-                   OUX_BC_FARFIELD = 4 };
+                   OUX_BC_FARFIELD = 4, OUX_BC_NEUMANN = 5 };
 int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fixed_dev);
 /* FARFIELD (x high or y high): the boundary state from the Riemann invariants along
  * the outward normal, R+ = u_n + 2c/(gamma-1) of the neighbour and R- = u_normal -
  * 2 c_inf/(gamma-1) of the far field; u_n = (R+ + R-)/2, c = (gamma-1)(R+ - R-)/4,
  * rho = rho_inf (c / c_inf)^(2/(gamma-1)), p = rho c^2 / gamma, tangential velocity
- * u_tangential (the top row of 2D_solver/BL0/set.f90). */
-/* (2D solves.) */
+ * u_tangential (the top row of 2D_solver/BL0/set.f90).  In 3D the tangential
+ * velocity is the first tangential axis's (u on y high, v on x high) and the other is
+ * 0 (3D_solver/src/set_bc_tbl_sbli.f90 set_bc_Riemann_tbl_top_down). */
 int oux_set_boundary_farfield(oux_handle* h, int32_t face, double rho_inf, double u_tangential,
                               double u_normal, double c_inf);
 /* A rule per position along the face: kinds_dev holds one enum oux_bc_kind per

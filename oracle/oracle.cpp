@@ -1432,6 +1432,16 @@ void bc_rule(const Ctx& C, int f, int pos, double* v, int bi, int bj, int ni, in
     v[t] = rhob * P[1] * Jt;
     v[n] = rhob * vb * Jt;
     v[3] = (pb * C.K.over_gamma_1 + 0.5 * rhob * (P[1] * P[1] + vb * vb)) * Jt;
+  } else if (kind == 5) {  // Neumann: 3D_solver/src/set_bc_tbl_sbli.f90:6-36 without w
+    const double Jn = C.g.jac[(size_t)(nj - 1) * C.nx + (ni - 1)];
+    const double Jt = 1.0 / C.g.jac[(size_t)(bj - 1) * C.nx + (bi - 1)];
+    const double over_QJ1 = 1.0 / v[0];
+    const double rhob = v[0] * Jn, ub = v[1] * over_QJ1, vb = v[2] * over_QJ1;
+    const double pb = C.K.gamma_1 * (v[3] * Jn - 0.5 * rhob * (ub * ub + vb * vb));
+    v[0] = rhob * Jt;
+    v[1] = rhob * ub * Jt;
+    v[2] = rhob * vb * Jt;
+    v[3] = (pb * C.K.over_gamma_1 + 0.5 * rhob * (ub * ub + vb * vb)) * Jt;
   }
 }
 
@@ -1489,6 +1499,44 @@ void fill_ghosts_3d_bnd(const Ctx& C, double* Q) {
             v[2] = 0.0;
             v[3] = 0.0;
             v[4] = p_wall * C.K.over_gamma_1;
+          } else if (kind == 4 || kind == 5) {
+            // Jacobian(i, j) of the boundary cell and of the cell its value came from
+            const int bi = cur[0], bj = cur[1];
+            const int ni = a == 0 ? src[0] : cur[0], nj = a == 1 ? src[1] : cur[1];
+            const double Jn = C.g.jac[(size_t)nj * C.nx + ni];
+            const double Jt = 1.0 / C.g.jac[(size_t)bj * C.nx + bi];
+            if (kind == 4) {
+              // 3D_solver/src/set_bc_tbl_sbli.f90:38-76 (set_bc_Riemann_tbl_top_down) on y
+              // high; on x high the same along x with v the far field's tangential velocity
+              const double* P = C.c.bpar[f];
+              const int nn = 1 + a, t1 = a == 0 ? 2 : 1, t2 = 3;
+              double pin = C.K.gamma_1 * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / v[0]) * Jn;
+              double rhoin = v[0] * Jn;
+              double cin = std::sqrt(C.K.gamma * pin / rhoin);
+              double vin = v[nn] / v[0];
+              double Rp = vin + 2.0 * cin * C.K.over_gamma_1;
+              double Rm = P[2] - 2.0 * P[3] * C.K.over_gamma_1;
+              double vb = 0.5 * (Rp + Rm);
+              double cb = 0.25 * C.K.gamma_1 * (Rp - Rm);
+              double rhob = std::pow(cb * (1.0 / P[3]), 2.0 * C.K.over_gamma_1) * P[0];
+              double pb = (rhob * (cb * cb)) * (1.0 / C.K.gamma);
+              v[0] = rhob * Jt;
+              v[t1] = rhob * P[1] * Jt;
+              v[nn] = rhob * vb * Jt;
+              v[t2] = 0.0;
+              v[4] = (pb * C.K.over_gamma_1 + 0.5 * rhob * (P[1] * P[1] + vb * vb)) * Jt;
+            } else {
+              // 3D_solver/src/set_bc_tbl_sbli.f90:6-36 (set_bc_Neumann_tbl_top_down)
+              double over_QJ1 = 1.0 / v[0];
+              double rhob = v[0] * Jn;
+              double ub = v[1] * over_QJ1, vb = v[2] * over_QJ1, wb = v[3] * over_QJ1;
+              double pb = C.K.gamma_1 * (v[4] * Jn - 0.5 * rhob * (ub * ub + vb * vb + wb * wb));
+              v[0] = rhob * Jt;
+              v[1] = rhob * ub * Jt;
+              v[2] = rhob * vb * Jt;
+              v[3] = rhob * wb * Jt;
+              v[4] = (pb * C.K.over_gamma_1 + 0.5 * rhob * (ub * ub + vb * vb + wb * wb)) * Jt;
+            }
           }
         }
         for (int l = 0; l < nv; ++l) Q[C.qidx(i + 1, l + 1, j + 1, k + 1)] = v[l];

@@ -45,7 +45,8 @@ SYMBOLS = [
 ]
 NOALLOC_SCRATCH_BYTES = 32 << 20  # OUX_NOALLOC_SCRATCH_BYTES
 FACES = {"x_lo": 0, "x_hi": 1, "y_lo": 2, "y_hi": 3, "z_lo": 4, "z_hi": 5}  # enum oux_face
-BC_KINDS = {"zero_gradient": 0, "slip_wall": 1, "fixed": 2, "noslip_wall": 3, "farfield": 4}  # enum oux_bc_kind
+BC_KINDS = {"zero_gradient": 0, "slip_wall": 1, "fixed": 2, "noslip_wall": 3, "farfield": 4,
+            "neumann": 5}  # enum oux_bc_kind
 
 
 class OuxConfig(C.Structure):

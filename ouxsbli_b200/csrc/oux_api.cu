@@ -982,7 +982,7 @@ int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fi
   const int nfaces = h->G.dim == 3 ? 6 : 4;
   if (face < 0 || face >= nfaces)
     return fail(OUX_E_INVALID, "face must be 0..3 (x low, x high, y low, y high), 4..5 (z low, z high) in 3D");
-  if (kind < OUX_BC_ZERO_GRADIENT || kind > OUX_BC_NOSLIP_WALL)
+  if (kind < OUX_BC_ZERO_GRADIENT || kind > OUX_BC_NEUMANN || kind == OUX_BC_FARFIELD)
     return fail(OUX_E_INVALID, "unknown boundary rule (far-field faces: oux_set_boundary_farfield)");
   bool open;
   if (face < 2) open = h->G.bcx;
@@ -1001,7 +1001,6 @@ int oux_set_boundary(oux_handle* h, int32_t face, int32_t kind, const double* fi
 int oux_set_boundary_farfield(oux_handle* h, int32_t face, double rho_inf, double u_tangential,
                               double u_normal, double c_inf) {
   if (!h) return fail(OUX_E_INVALID, "null handle");
-  if (h->G.dim != 2) return fail(OUX_E_INVALID, "the far-field rule is built for 2D solves");
   if (face != OUX_FACE_X_HI && face != OUX_FACE_Y_HI)
     return fail(OUX_E_INVALID, "the far-field rule is built for the high faces (x high, y high)");
   if (!(face < 2 ? h->G.bcx : h->G.bcy))

@@ -43,7 +43,7 @@ struct Geo {
                               // z ghost planes come from the neighbours: 2 both ends, 3 / 4 the
                               // upper / lower end only (the other end is the grid's boundary)
   int bkind;                  // boundary-cell rule of face f (enum oux_bc_kind) in bits 4f..4f+3;
-                              // faces 0..3: x low, x high, y low, y high
+                              // faces 0..5: x low, x high, y low, y high, z low, z high
   int64_t sx, plane, vs;      // row stride, plane stride, variable stride (elements)
   const double* bfix[4];      // OUX_BC_FIXED faces: nv x (ny for x faces, nx for y faces) values of Q/J
   double gamma_1, over_gamma_1;  // gamma - 1 and 1 / (gamma - 1), for the wall and far-field rules
@@ -51,7 +51,7 @@ struct Geo {
   const signed char* bkinds[4];  // per-position rule of a face (overrides its kind), or null
   double bpar[4][4];          // far-field state of a face: rho, tangential and normal velocity, c
   int ylast;                  // 1: y faces applied after x faces (corners take their y rule)
-  const double* bjac;         // J(nx, ny), for the far-field rule
+  const double* bjac;         // J(nx, ny), for the far-field and Neumann rules
   const double* bfix3[6];     // 3D: fixed values of the faces x lo .. z hi
   __host__ __device__ int64_t at(int i, int j, int k) const { return (int64_t)k * plane + (int64_t)j * sx + i; }
 };
@@ -393,7 +393,9 @@ __global__ void k_mut_edges(Geo G, Fields<T> W) {
 //                         wall rows of 2D_solver/ST/set.f90 and 2D_solver/BL0/set.f90)
 //   OUX_BC_FARFIELD       (high faces) the boundary state from the Riemann invariants
 //                         of the neighbour and of a far-field state (the top row of
-//                         2D_solver/BL0/set.f90)
+//                         2D_solver/BL0/set.f90; 3D: 3D_solver/src/set_bc_tbl_sbli.f90)
+//   OUX_BC_NEUMANN        the neighbour's primitive state through the two cells'
+//                         Jacobians (3D_solver/src/set_bc_tbl_sbli.f90:6-36)
 // A face may carry a rule per position (bkinds).  By default y faces are applied
 // first and x faces last (2D_solver/OS/set.f90), so a corner takes its x rule of the
 // y-boundary value beside it; with ylast the order is reversed (2D_solver/BL0/set.f90).
@@ -452,6 +454,15 @@ __device__ __forceinline__ void bc_rule(const Geo& G, int f, int pos, int nv, do
     v[t] = rhob * P[1] * Jt;
     v[n] = rhob * vb * Jt;
     v[3] = (pb * G.over_gamma_1 + 0.5 * rhob * (P[1] * P[1] + vb * vb)) * Jt;
+  } else if (kind == 5) {  // Neumann: the neighbour's primitive state through the two cells' Jacobians
+    const double Jn = G.bjac[jn], Jt = 1.0 / G.bjac[jb];
+    const double o1 = 1.0 / v[0];
+    const double rhob = v[0] * Jn, ub = v[1] * o1, vb = v[2] * o1;
+    const double pb = G.gamma_1 * (v[3] * Jn - 0.5 * rhob * (ub * ub + vb * vb));
+    v[0] = rhob * Jt;
+    v[1] = rhob * ub * Jt;
+    v[2] = rhob * vb * Jt;
+    v[3] = (pb * G.over_gamma_1 + 0.5 * rhob * (ub * ub + vb * vb)) * Jt;
   }
 }
 
@@ -508,6 +519,44 @@ __device__ __forceinline__ void ghost_cell_3d_bnd(T* Q, const Geo& G, int nv, in
       v[2] = 0.0;
       v[3] = 0.0;
       v[4] = p_wall * G.over_gamma_1;
+    } else if (kind == 4 || kind == 5) {
+      // the x-y Jacobian table (uniform z) at the boundary cell and at the cell its
+      // value came from (3D_solver/src/set_bc_tbl_sbli.f90: Jacobian(i,ny), (i,ny-1))
+      int nb[2] = {cur[0], cur[1]};
+      if (a < 2) nb[a] = src[a];
+      const double Jn = G.bjac[(int64_t)nb[1] * G.nx + nb[0]];
+      const double Jt = 1.0 / G.bjac[(int64_t)cur[1] * G.nx + cur[0]];
+      if (kind == 4) {
+        // far field (x / y high; set_bc_Riemann_tbl_top_down, :38-76): Riemann invariants
+        // along the normal, the first tangential velocity the far field's, the second 0
+        const double* P = G.bpar[f];
+        const int n = 1 + a, t1 = a == 0 ? 2 : 1, t2 = 3;
+        const double pin = G.gamma_1 * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / v[0]) * Jn;
+        const double rhoin = v[0] * Jn;
+        const double cin = sqrt(G.gamma * pin / rhoin);
+        const double vin = v[n] / v[0];
+        const double Rp = vin + 2.0 * cin * G.over_gamma_1;
+        const double Rm = P[2] - 2.0 * P[3] * G.over_gamma_1;
+        const double vb = 0.5 * (Rp + Rm);
+        const double cb = 0.25 * G.gamma_1 * (Rp - Rm);
+        const double rhob = pow(cb * (1.0 / P[3]), 2.0 * G.over_gamma_1) * P[0];
+        const double pb = (rhob * (cb * cb)) * G.over_gamma;
+        v[0] = rhob * Jt;
+        v[t1] = rhob * P[1] * Jt;
+        v[n] = rhob * vb * Jt;
+        v[t2] = 0.0;
+        v[4] = (pb * G.over_gamma_1 + 0.5 * rhob * (P[1] * P[1] + vb * vb)) * Jt;
+      } else {
+        // Neumann (set_bc_Neumann_tbl_top_down, :6-36): the neighbour's primitive state
+        const double o1 = 1.0 / v[0];
+        const double rhob = v[0] * Jn, ub = v[1] * o1, vb = v[2] * o1, wb = v[3] * o1;
+        const double pb = G.gamma_1 * (v[4] * Jn - 0.5 * rhob * (ub * ub + vb * vb + wb * wb));
+        v[0] = rhob * Jt;
+        v[1] = rhob * ub * Jt;
+        v[2] = rhob * vb * Jt;
+        v[3] = rhob * wb * Jt;
+        v[4] = (pb * G.over_gamma_1 + 0.5 * rhob * (ub * ub + vb * vb + wb * wb)) * Jt;
+      }
     }
   }
   const int64_t o = G.at(i, j, k);

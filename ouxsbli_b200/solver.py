@@ -33,12 +33,12 @@ class SolverConfig:
     slau: str = "HRSLAU2"          # SLAU_VARIANT
     rk: int = 3
     precision: str = "fp64"        # fp64 | mixed (FP32 stage states/fluxes, FP64 Q^n + accumulation)
-    bc_x: int = 0                  # 0 periodic; 1 non-periodic x (boundary flux kernels, boundary cells; 2D)
-    bc_y: int = 0                  # the same for y (2D)
+    bc_x: int = 0                  # 0 periodic; 1 non-periodic x (boundary flux kernels, boundary cells)
+    bc_y: int = 0                  # the same for y
     bc_z: int = 0                  # 0 periodic; 1 non-periodic; 2-4 z slab of a larger grid (enum oux_bc_z)
-    # rules of the non-periodic faces ("x_lo", "x_hi", "y_lo", "y_hi"): "zero_gradient"
-    # (the default), "slip_wall", "noslip_wall" or ("fixed", values (nv, ny) for x faces /
-    # (nv, nx) for y faces, of Q/J)
+    # rules of the non-periodic faces ("x_lo", "x_hi", "y_lo", "y_hi", "z_lo", "z_hi"):
+    # "zero_gradient" (the default), "slip_wall", "noslip_wall", "neumann" or the forms
+    # boundary_rules() lists (fixed values, far field, a split face)
     boundary: dict = field(default=None, repr=False)
     boundary_order: str = "x_last"   # x_last: corners take their x rule (OS); y_last: their y rule (BL0)
     gamma: float = 1.4
@@ -71,7 +71,7 @@ class SolverConfig:
         face, kind, fixed ((nv, len) values or None), farfield ((rho, u_t, u_n, c) or
         None) and cells (int8 kind per position or None).
 
-        Rule forms: "zero_gradient", "slip_wall", "noslip_wall"; ("fixed", values of
+        Rule forms: "zero_gradient", "slip_wall", "noslip_wall", "neumann"; ("fixed", values of
         shape (nv, ny) for x faces / (nv, nx) for y faces, of Q/J); ("farfield", rho,
         u_tangential, u_normal, c) on a high face; ("split", at, rule_lo, rule_hi):
         positions below `at` follow rule_lo, the others rule_hi (two of the plain

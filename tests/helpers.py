@@ -1,6 +1,8 @@
 """Workload builders shared by the tests (initial fields, configurations)."""
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 from ouxsbli_b200.cases import CASES, build_initial, isentropic_vortex
@@ -76,3 +78,58 @@ def diagnostics_numpy(cfg, qj):
     om = [d6(W, 1) - d6(V, 2), d6(U, 2) - d6(W, 0), d6(V, 0) - d6(U, 1)]
     ens = np.mean(0.5 * f["rho"][sl] * sum(o[sl] ** 2 for o in om))
     return float(ke), float(ent), float(ens)
+
+
+# ---- 3D viscous boxes with walls ----------------------------------------------------
+H, R, GAMMA, T0, RHO0 = 1.0e-3, 287.03, 1.4, 300.0, 1.2
+
+
+def _axis(n_int, L, order, nonper):
+    """(n, coordinates, spacings) of an axis: one boundary cell a side or g ghost cells."""
+    if nonper:
+        n = n_int + 2
+        d = np.full(n - 1, L / (n - 1))
+        return n, np.concatenate([[0.0], np.cumsum(d)]), d
+    n = n_int + 2 * (order // 2)
+    x, d = cyclic_axis(n, L, order)
+    return n, x, d
+
+
+def wall_box(nx_int, ny, nz_int, order, rules, bc_x=0, bc_z=0, U=5.0, perturb=True, plate=False, **kw):
+    """A 3D viscous (Sutherland, air) shear flow over a y range of 1 mm with walls at
+    y = 0 (and y = H), periodic or non-periodic in x and z: u = U sin(pi y / H)
+    (channel) or U sin(pi y / 2H) (plate: u = U at the top), plus a 3D perturbation."""
+    g = order // 2
+    Lx, Lz = 0.5e-3, 0.4e-3
+    nx, x, dx = _axis(nx_int, Lx, order, bc_x)
+    nz, z, dz = _axis(nz_int, Lz, order, bc_z)
+    dy = np.full(ny - 1, H / (ny - 1))
+    y = np.concatenate([[0.0], np.cumsum(dy)])
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    sy = np.sin(math.pi * Y / H)
+    rho = np.full_like(X, RHO0)
+    u = U * (np.sin(0.5 * math.pi * Y / H) if plate else sy)
+    v = np.zeros_like(X)
+    w = np.zeros_like(X)
+    if perturb:
+        rho = rho * (1.0 + 0.02 * np.sin(2 * math.pi * X / Lx) * np.cos(2 * math.pi * Z / Lz) * sy)
+        v = 0.3 * U * np.sin(2 * math.pi * X / Lx) * sy ** 2
+        w = 0.2 * U * np.sin(2 * math.pi * Z / Lz) * np.cos(2 * math.pi * X / Lx) * sy
+    p = np.full_like(X, RHO0 * R * T0) * (1.0 + (0.01 * np.cos(2 * math.pi * Z / Lz) if perturb else 0.0))
+    Q = np.zeros((nx, 5, ny, nz), order="F")
+    Q[:, 0], Q[:, 1], Q[:, 2], Q[:, 3] = rho, rho * u, rho * v, rho * w
+    Q[:, 4] = p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    # periodic directions: ghost cells are exact images of the interior
+    if not bc_x:
+        N = nx - 2 * g
+        for i in list(range(g)) + list(range(nx - g, nx)):
+            Q[i] = Q[g + (i - g) % N]
+    if not bc_z:
+        N = nz - 2 * g
+        for k in list(range(g)) + list(range(nz - g, nz)):
+            Q[:, :, :, k] = Q[:, :, :, g + (k - g) % N]
+    qj = to_qj(Q, jacobian(dx, dy, dz))
+    dt = 0.4 * min(dx.min(), dy.min(), dz.min()) / (U + math.sqrt(GAMMA * R * T0))
+    cfg = SolverConfig(dim=3, nx=nx, ny=ny, nz=nz, order=order, visc="NS", bc_x=bc_x, bc_y=1, bc_z=bc_z, dt=dt,
+                       gamma=GAMMA, R=R, Pr=0.72, dx=dx, dy=dy, dz=dz, boundary=rules, **kw)
+    return cfg, qj, y

@@ -138,8 +138,9 @@ def test_set_boundary_checks_without_a_device():
 
 
 def test_3d_boundary_setters_without_a_device():
-    """3D order-2 boundaries: z faces open only on non-periodic ends; the 2D-only rules
-    (far field, per-position kinds) are refused."""
+    """3D order-2 boundaries: z faces open only on non-periodic ends; the far field on
+    a non-periodic high face and the Neumann rule are taken, far field through its own
+    setter only; per-position kinds (2D only) are refused."""
     n = 10
     d = np.full(n - 1, 0.1)
     cfg = SolverConfig(dim=3, nx=n, ny=n, nz=n, order=2, visc="Euler", bc_x=1, bc_z=3, dx=d, dy=d, dz=d, dt=1e-4)
@@ -150,6 +151,11 @@ def test_3d_boundary_setters_without_a_device():
     assert L.oux_set_boundary(h, _lib.FACES["z_hi"], 0, None) == _lib.OUX_E_INVALID       # a halo end
     assert L.oux_set_boundary(h, _lib.FACES["y_lo"], 0, None) == _lib.OUX_E_INVALID       # periodic y
     assert L.oux_set_boundary(h, _lib.FACES["x_hi"], _lib.BC_KINDS["noslip_wall"], None) == 0
-    assert L.oux_set_boundary_farfield(h, _lib.FACES["x_hi"], 1.0, 1.0, 0.0, 1.0) == _lib.OUX_E_INVALID
+    assert L.oux_set_boundary_farfield(h, _lib.FACES["x_hi"], 1.0, 1.0, 0.0, 1.0) == 0
+    assert L.oux_set_boundary_farfield(h, _lib.FACES["x_lo"], 1.0, 1.0, 0.0, 1.0) == _lib.OUX_E_INVALID
+    assert L.oux_set_boundary_farfield(h, _lib.FACES["y_hi"], 1.0, 1.0, 0.0, 1.0) == _lib.OUX_E_INVALID
+    assert L.oux_set_boundary(h, _lib.FACES["x_hi"], _lib.BC_KINDS["farfield"], None) == _lib.OUX_E_INVALID
+    assert L.oux_set_boundary(h, _lib.FACES["x_lo"], _lib.BC_KINDS["neumann"], None) == 0
+    assert L.oux_set_boundary(h, _lib.FACES["x_lo"], 6, None) == _lib.OUX_E_INVALID
     assert L.oux_set_boundary_cells(h, _lib.FACES["x_lo"], None) == _lib.OUX_E_INVALID
     L.oux_destroy(h)

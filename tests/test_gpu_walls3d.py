@@ -7,62 +7,9 @@ import math
 import numpy as np
 import pytest
 
+from helpers import GAMMA, H, R, RHO0, T0, wall_box
 from oracle import oracle
-from ouxsbli_b200.grid import cyclic_axis, jacobian, to_qj
-from ouxsbli_b200.solver import Solver, SolverConfig
-
-H, R, GAMMA, T0, RHO0 = 1.0e-3, 287.03, 1.4, 300.0, 1.2
-
-
-def _axis(n_int, L, order, nonper):
-    """(n, coordinates, spacings) of an axis: one boundary cell a side or g ghost cells."""
-    if nonper:
-        n = n_int + 2
-        d = np.full(n - 1, L / (n - 1))
-        return n, np.concatenate([[0.0], np.cumsum(d)]), d
-    n = n_int + 2 * (order // 2)
-    x, d = cyclic_axis(n, L, order)
-    return n, x, d
-
-
-def wall_box(nx_int, ny, nz_int, order, rules, bc_x=0, bc_z=0, U=5.0, perturb=True, **kw):
-    """A viscous (Sutherland, air) shear flow between y walls 1 mm apart, periodic or
-    non-periodic in x and z: u = U sin(pi y / H) plus a 3D perturbation."""
-    g = order // 2
-    Lx, Lz = 0.5e-3, 0.4e-3
-    nx, x, dx = _axis(nx_int, Lx, order, bc_x)
-    nz, z, dz = _axis(nz_int, Lz, order, bc_z)
-    dy = np.full(ny - 1, H / (ny - 1))
-    y = np.concatenate([[0.0], np.cumsum(dy)])
-    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
-    sy = np.sin(math.pi * Y / H)
-    rho = np.full_like(X, RHO0)
-    u = U * sy
-    v = np.zeros_like(X)
-    w = np.zeros_like(X)
-    if perturb:
-        rho = rho * (1.0 + 0.02 * np.sin(2 * math.pi * X / Lx) * np.cos(2 * math.pi * Z / Lz) * sy)
-        v = 0.3 * U * np.sin(2 * math.pi * X / Lx) * sy ** 2
-        w = 0.2 * U * np.sin(2 * math.pi * Z / Lz) * np.cos(2 * math.pi * X / Lx) * sy
-    p = np.full_like(X, RHO0 * R * T0) * (1.0 + (0.01 * np.cos(2 * math.pi * Z / Lz) if perturb else 0.0))
-    Q = np.zeros((nx, 5, ny, nz), order="F")
-    Q[:, 0], Q[:, 1], Q[:, 2], Q[:, 3] = rho, rho * u, rho * v, rho * w
-    Q[:, 4] = p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
-    # periodic directions: ghost cells are exact images of the interior
-    if not bc_x:
-        N = nx - 2 * g
-        for i in list(range(g)) + list(range(nx - g, nx)):
-            Q[i] = Q[g + (i - g) % N]
-    if not bc_z:
-        N = nz - 2 * g
-        for k in list(range(g)) + list(range(nz - g, nz)):
-            Q[:, :, :, k] = Q[:, :, :, g + (k - g) % N]
-    qj = to_qj(Q, jacobian(dx, dy, dz))
-    dt = 0.4 * min(dx.min(), dy.min(), dz.min()) / (U + math.sqrt(GAMMA * R * T0))
-    cfg = SolverConfig(dim=3, nx=nx, ny=ny, nz=nz, order=order, visc="NS", bc_x=bc_x, bc_y=1, bc_z=bc_z, dt=dt,
-                       gamma=GAMMA, R=R, Pr=0.72, dx=dx, dy=dy, dz=dz, boundary=rules, **kw)
-    return cfg, qj, y
-
+from ouxsbli_b200.solver import Solver
 
 CHANNEL = {"y_lo": "noslip_wall", "y_hi": "noslip_wall"}
 # a flat-plate-like box: zero-gradient in / outflow, no-slip floor, zero-gradient top
@@ -153,3 +100,33 @@ def test_3d_shear_decay_between_noslip_walls(order, vo, stencil, cuda_device):
     ratio = amplitude(q) / amplitude(qj)
     expect = math.exp(-nu * math.pi ** 2 * nsteps * cfg.dt / H ** 2)
     assert abs(ratio / expect - 1.0) < 2e-3, (ratio, expect)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("top", ["neumann", "farfield"])
+def test_3d_tbl_top_rules_vs_oracle(top, cuda_device):
+    """The TBL / SBLI top boundary (3D_solver/src/set_bc_tbl_sbli.f90) over a no-slip
+    floor with zero-gradient x ends (NS SLAU-6 / Central-6, RK3, u = U at the top):
+    with the Neumann top, residual and state after 4 steps bit-identical to the oracle;
+    with the far-field top, whose rule calls pow (libm on the host, CUDA on the
+    device), equal to rounding (1e-12 of each variable's largest value)."""
+    c0 = math.sqrt(GAMMA * R * T0)
+    rule = "neumann" if top == "neumann" else ("farfield", RHO0, 5.0, 0.0, c0)
+    rules = {**PLATE, "y_hi": rule}
+    cfg, qj, _ = wall_box(14, 16, 10, 6, rules, bc_x=1, bc_z=0, plate=True, scheme="SLAU", rk=3, tvd="hybrid")
+    s = Solver(cfg, cuda_device)
+    s.set_state(qj)
+    r = s.rhs()
+    s.step(4)
+    q = s.get_state()
+    s.close()
+    zs = slice(cfg.g - 1, -(cfg.g - 1))  # updated cells of the periodic z
+    r_want, q_want = oracle.rhs(cfg, qj), oracle.step(cfg, qj, 4)
+    if top == "neumann":
+        np.testing.assert_array_equal(r[..., zs], r_want[..., zs])
+        np.testing.assert_array_equal(q, q_want)
+    else:
+        for l in range(5):
+            np.testing.assert_allclose(r[:, l, :, zs], r_want[:, l, :, zs], rtol=0,
+                                       atol=1e-12 * np.abs(r_want[:, l, :, zs]).max())
+            np.testing.assert_allclose(q[:, l], q_want[:, l], rtol=0, atol=1e-12 * np.abs(q_want[:, l]).max())

@@ -362,3 +362,41 @@ def test_blasius_solution_and_compressible_layer():
     assert abs(u[-1] - u0) < 1e-6 * u0 and abs(T[-1] - (Taw - rf * u0 ** 2 / (2 * Cp))) < 1e-6
     i99 = np.searchsorted(u, 0.99 * u0)
     assert abs(y[i99] - 0.8e-3) < 2 * (y[1] - y[0])
+
+
+def test_3d_tbl_top_rules_of_the_oracle():
+    """The oracle's TBL / SBLI top rules (3D_solver/src/set_bc_tbl_sbli.f90) on a 3D
+    plate box: the Neumann top carries the neighbour's primitive state (rho, u, v, w,
+    p) into the top cells; the far-field top keeps the neighbour's outgoing invariant
+    v + 2c/(gamma-1), the far field's incoming one v - 2c/(gamma-1) and entropy
+    p / rho^gamma, with u = u_inf and w = 0."""
+    from helpers import GAMMA, R, RHO0, T0, wall_box
+    from oracle import oracle
+    from ouxsbli_b200.grid import jacobian
+    c0, U = math.sqrt(GAMMA * R * T0), 5.0
+    g1 = GAMMA - 1.0
+    for top in ("neumann", ("farfield", RHO0, U, 0.0, c0)):
+        rules = {"x_lo": "zero_gradient", "x_hi": "zero_gradient", "y_lo": "noslip_wall", "y_hi": top}
+        cfg, qj, _ = wall_box(10, 12, 6, 6, rules, bc_x=1, plate=True, U=U)
+        q = oracle.fill_ghosts(cfg, qj)
+        J = jacobian(cfg.dx, cfg.dy, cfg.dz)
+        g = cfg.g
+        prim = []
+        for j in (cfg.ny - 1, cfg.ny - 2):  # the top cells and their neighbours
+            a = q[1:-1, :, j, g:-g]
+            Jj = J[1:-1, j][:, None]
+            rho = a[:, 0] * Jj
+            u, v, w = a[:, 1] / a[:, 0], a[:, 2] / a[:, 0], a[:, 3] / a[:, 0]
+            p = g1 * (a[:, 4] * Jj - 0.5 * rho * (u * u + v * v + w * w))
+            prim.append((rho, u, v, w, p))
+        (rb, ub, vb, wb, pb), (rn, un, vn, wn, pn) = prim
+        if top == "neumann":
+            for b, n in zip((rb, ub, vb, wb, pb), (rn, un, vn, wn, pn)):
+                np.testing.assert_allclose(b, n, rtol=1e-13, atol=1e-13 * np.abs(n).max())
+        else:
+            cb, cn = np.sqrt(GAMMA * pb / rb), np.sqrt(GAMMA * pn / rn)
+            np.testing.assert_allclose(vb + 2 * cb / g1, vn + 2 * cn / g1, rtol=1e-12)
+            np.testing.assert_allclose(vb - 2 * cb / g1, -2 * c0 / g1, rtol=1e-12)
+            np.testing.assert_allclose(pb / rb ** GAMMA, (RHO0 * c0 ** 2 / GAMMA) / RHO0 ** GAMMA, rtol=1e-12)
+            np.testing.assert_allclose(ub, U, rtol=1e-13)
+            assert np.all(wb == 0.0)
