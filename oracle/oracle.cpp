@@ -751,6 +751,41 @@ void calc_mut(Ctx& C) {  // :96-125 plus set_bc_mut_common (set_bc_common.f90:29
                                                         C.g.etay[j - 1], C.g.zetaz[k - 1], q, C.K);
       }
   std::vector<double>* arrs[2] = {&C.w.mut, &C.w.qc2};
+  const bool walls = C.c.bc_x || C.c.bc_y || C.c.bc_z == 1;
+  if (walls) {
+    // a non-periodic face takes its neighbour's value, 0 on a no-slip wall (set_bc_mut
+    // of 3D_solver/TBL/set.f90 and SBLI/set.f90: wall 0, top and outlet copies); a
+    // periodic one its image at distance n-2 as set_bc_mut_common does; x faces for
+    // the interior rows, then y faces, then z faces over everything before them
+    const bool per[3] = {!C.c.bc_x, !C.c.bc_y, C.c.bc_z == 0};
+    const int n[3] = {nx, ny, nz};
+    auto kind = [&](int f) { return f < 4 ? C.c.bkind[f] : C.c.bkindz[f - 4]; };
+    for (auto* ap : arrs) {
+      std::vector<double>& a = *ap;
+      for (int ax = 0; ax < 3; ++ax)
+        for (int side = 0; side < 2; ++side) {
+          const int c = side ? n[ax] : 1;
+          const int s = per[ax] ? (side ? 2 : n[ax] - 1) : (side ? n[ax] - 1 : 2);
+          const bool zero = !per[ax] && kind(2 * ax + side) == 3;
+          // the other two axes: interior cells for x, all cells of the earlier axes after
+          const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+          for (int q2 = 1; q2 <= n[o2]; ++q2)
+            for (int q1 = 1; q1 <= n[o1]; ++q1) {
+              // x: rows j, k interior; y: i all, k interior; z: everything
+              int idx[3];
+              idx[ax] = c; idx[o1] = q1; idx[o2] = q2;
+              bool in = true;
+              if (ax == 0) in = idx[1] >= 2 && idx[1] <= ny - 1 && idx[2] >= 2 && idx[2] <= nz - 1;
+              if (ax == 1) in = idx[2] >= 2 && idx[2] <= nz - 1;
+              if (!in) continue;
+              int sidx[3] = {idx[0], idx[1], idx[2]};
+              sidx[ax] = s;
+              a[C.sidx(idx[0], idx[1], idx[2])] = zero ? 0.0 : a[C.sidx(sidx[0], sidx[1], sidx[2])];
+            }
+        }
+    }
+    return;
+  }
   for (auto* ap : arrs) {
     std::vector<double>& a = *ap;
     for (int k = 2; k <= nz - 1; ++k)
@@ -1046,8 +1081,9 @@ void visc_face_gv2(const Ctx& C, int dir, int i, int j, int k, double out[4]) {
   out[3] = les ? (vw + Hsgs) : vw;
 }
 
-// 2nd-order fallback of the high-order viscous kernels outside their guard
-// (Navier-Stokes), written per direction as the reference writes it:
+// 2nd-order fallback of the high-order viscous kernels outside their guard, written
+// per direction as the reference writes it (LES: the SGS stresses added after the
+// work terms, and the SGS enthalpy flux):
 // calc_Ev (3D_solver/src/calc_visc_high.f90.fypp:194-260), calc_Fv (:432-497),
 // calc_Gv (:674-739).  Returns the 4 subtracted terms like visc_face_high.
 void visc_face_fb3(const Ctx& C, int dir, int i, int j, int k, double out[4]) {
@@ -1068,6 +1104,16 @@ void visc_face_fb3(const Ctx& C, int dir, int i, int j, int k, double out[4]) {
     m1 = 0.25 * (P.mu(i - di, j - dj, k - dk) + P.mu(i, j, k) + P.mu(i2 - di, j2 - dj, k2 - dk) + P.mu(i2, j2, k2));
     m2 = 0.25 * (P.mu(i, j, k) + P.mu(i + di, j + dj, k + dk) + P.mu(i2, j2, k2) + P.mu(i2 + di, j2 + dj, k2 + dk));
   };
+  auto mavg_sgs = [&](int t, int i2, int j2, int k2, double& m1, double& m2) {
+    int di = t == 0, dj = t == 1, dk = t == 2;
+    m1 = 0.25 * (P.mut(i - di, j - dj, k - dk) + P.mut(i, j, k) + P.mut(i2 - di, j2 - dj, k2 - dk) + P.mut(i2, j2, k2));
+    m2 = 0.25 * (P.mut(i, j, k) + P.mut(i + di, j + dj, k + dk) + P.mut(i2, j2, k2) + P.mut(i2 + di, j2 + dj, k2 + dk));
+  };
+  const bool les = C.c.visc == ORC_LES;
+  auto Hs = [&](int ii, int jj, int kk) {
+    double u = P.u(ii, jj, kk), v = P.v(ii, jj, kk), w = P.w(ii, jj, kk);
+    return K.Cp * P.T(ii, jj, kk) + 0.5 * (u * u + v * v + w * w) + P.qc2(ii, jj, kk);
+  };
   if (dir == 0) {
     const int i2 = i + 1;
     double mx = 0.5 * (P.mu(i, j, k) + P.mu(i2, j, k));
@@ -1086,7 +1132,23 @@ void visc_face_fb3(const Ctx& C, int dir, int i, int j, int k, double out[4]) {
     double utxx = 0.5 * (P.u(i, j, k) + P.u(i2, j, k)) * txx;
     double vtxy = 0.5 * (P.v(i, j, k) + P.v(i2, j, k)) * txy;
     double wtxz = 0.5 * (P.w(i, j, k) + P.w(i2, j, k)) * txz;
+    double Hsgs = 0.0;
+    if (les) {
+      double mxsgs = 0.5 * (P.mut(i, j, k) + P.mut(i2, j, k));
+      mavg_sgs(1, i2, j, k, m1, m2);
+      double muysgs = tder(0, 1, i2, j, k, m1, m2, dyj), mvysgs = tder(1, 1, i2, j, k, m1, m2, dyj);
+      mavg_sgs(2, i2, j, k, m1, m2);
+      double muzsgs = tder(0, 2, i2, j, k, m1, m2, dzk), mwzsgs = tder(2, 2, i2, j, k, m1, m2, dzk);
+      double muxsgs = mxsgs * (-P.u(i, j, k) + P.u(i2, j, k)) * dxi;
+      double mvxsgs = mxsgs * (-P.v(i, j, k) + P.v(i2, j, k)) * dxi;
+      double mwxsgs = mxsgs * (-P.w(i, j, k) + P.w(i2, j, k)) * dxi;
+      txx = txx + two_third * (2.0 * muxsgs - mvysgs - mwzsgs);
+      txy = txy + muysgs + mvxsgs;
+      txz = txz + mwxsgs + muzsgs;
+      Hsgs = -mxsgs * (-Hs(i, j, k) + Hs(i2, j, k)) * dxi / K.Prt;
+    }
     out[0] = txx; out[1] = txy; out[2] = txz; out[3] = utxx + vtxy + wtxz + kTx;
+    if (les) out[3] = out[3] + Hsgs;
   } else if (dir == 1) {
     const int j2 = j + 1;
     double my = 0.5 * (P.mu(i, j, k) + P.mu(i, j2, k));
@@ -1105,7 +1167,23 @@ void visc_face_fb3(const Ctx& C, int dir, int i, int j, int k, double out[4]) {
     double utyx = 0.5 * (P.u(i, j, k) + P.u(i, j2, k)) * tyx;
     double vtyy = 0.5 * (P.v(i, j, k) + P.v(i, j2, k)) * tyy;
     double wtyz = 0.5 * (P.w(i, j, k) + P.w(i, j2, k)) * tyz;
+    double Hsgs = 0.0;
+    if (les) {
+      double mysgs = 0.5 * (P.mut(i, j, k) + P.mut(i, j2, k));
+      mavg_sgs(0, i, j2, k, m1, m2);
+      double muxsgs = tder(0, 0, i, j2, k, m1, m2, dxi), mvxsgs = tder(1, 0, i, j2, k, m1, m2, dxi);
+      mavg_sgs(2, i, j2, k, m1, m2);
+      double mvzsgs = tder(1, 2, i, j2, k, m1, m2, dzk), mwzsgs = tder(2, 2, i, j2, k, m1, m2, dzk);
+      double muysgs = mysgs * (-P.u(i, j, k) + P.u(i, j2, k)) * dyj;
+      double mvysgs = mysgs * (-P.v(i, j, k) + P.v(i, j2, k)) * dyj;
+      double mwysgs = mysgs * (-P.w(i, j, k) + P.w(i, j2, k)) * dyj;
+      tyx = tyx + muysgs + mvxsgs;
+      tyy = tyy + two_third * (2.0 * mvysgs - mwzsgs - muxsgs);
+      tyz = tyz + mvzsgs + mwysgs;
+      Hsgs = -mysgs * (-Hs(i, j, k) + Hs(i, j2, k)) * dyj / K.Prt;
+    }
     out[0] = tyx; out[1] = tyy; out[2] = tyz; out[3] = utyx + vtyy + wtyz + kTy;
+    if (les) out[3] = out[3] + Hsgs;
   } else {
     const int k2 = k + 1;
     double m1, m2;
@@ -1124,7 +1202,23 @@ void visc_face_fb3(const Ctx& C, int dir, int i, int j, int k, double out[4]) {
     double utzx = 0.5 * (P.u(i, j, k) + P.u(i, j, k2)) * tzx;
     double vtzy = 0.5 * (P.v(i, j, k) + P.v(i, j, k2)) * tzy;
     double wtzz = 0.5 * (P.w(i, j, k) + P.w(i, j, k2)) * tzz;
+    double Hsgs = 0.0;
+    if (les) {
+      mavg_sgs(0, i, j, k2, m1, m2);
+      double muxsgs = tder(0, 0, i, j, k2, m1, m2, dxi), mwxsgs = tder(2, 0, i, j, k2, m1, m2, dxi);
+      mavg_sgs(1, i, j, k2, m1, m2);
+      double mvysgs = tder(1, 1, i, j, k2, m1, m2, dyj), mwysgs = tder(2, 1, i, j, k2, m1, m2, dyj);
+      double mzsgs = 0.5 * (P.mut(i, j, k) + P.mut(i, j, k2));
+      double muzsgs = mzsgs * (-P.u(i, j, k) + P.u(i, j, k2)) * dzk;
+      double mvzsgs = mzsgs * (-P.v(i, j, k) + P.v(i, j, k2)) * dzk;
+      double mwzsgs = mzsgs * (-P.w(i, j, k) + P.w(i, j, k2)) * dzk;
+      tzx = tzx + mwxsgs + muzsgs;
+      tzy = tzy + mvzsgs + mwysgs;
+      tzz = tzz + two_third * (2.0 * mwzsgs - muxsgs - mvysgs);
+      Hsgs = -mzsgs * (-Hs(i, j, k) + Hs(i, j, k2)) * dzk / K.Prt;
+    }
     out[0] = tzx; out[1] = tzy; out[2] = tzz; out[3] = utzx + vtzy + wtzz + kTz;
+    if (les) out[3] = out[3] + Hsgs;
   }
 }
 

@@ -80,12 +80,6 @@ int validate(const oux_config* c, std::string& why) {
     }
     if (c->nz < 3 * g) { why = "z slab (bc_z >= 2) needs at least g interior planes (nz >= 3g)"; return OUX_E_INVALID; }
   }
-  if (c->dim == 3 && (c->bc_x == 1 || c->bc_y == 1 || c->bc_z == 1 || c->bc_z == 3 || c->bc_z == 4) &&
-      c->visc == OUX_LES) {
-    why = "3D non-periodic boundaries are built for Euler and Navier-Stokes solves (not LES: the SGS "
-          "viscosity's boundary values are not built)";
-    return OUX_E_INVALID;
-  }
   if (c->dim == 3 && (c->bc_z == 3 || c->bc_z == 4) && c->order != 2) {
     why = "a z slab with a boundary end (bc_z = 3, 4) is built for order 2";
     return OUX_E_INVALID;

@@ -356,21 +356,37 @@ __global__ void k_mut(Geo G, Fields<T> W, Metrics M, PhysConst K) {
 }
 
 // set_bc_mut_common (3D_solver/src/set_bc_common.f90:296-335): one ghost layer,
-// images taken at distance n-2 (the reference's composite copy order).
+// images taken at distance n-2 (the reference's composite copy order).  On a
+// non-periodic face the boundary cell takes its neighbour's value, or 0 on a no-slip
+// wall (set_bc_mut of 3D_solver/TBL/set.f90 and SBLI/set.f90: wall 0, top and
+// outlet copies).  Applying the faces one after the other, x, y, z, as those routines
+// do, gives the same as this per-cell rule: 0 if the cell lies on a no-slip face,
+// else the value of its source cell in every edge direction at once.
 template <class T>
 __device__ __forceinline__ void mut_edge_cell(const Geo& G, const Fields<T>& W, int64_t t) {
-  int i = (int)(t % G.nx);
-  int64_t r = t / G.nx;
-  int j = (int)(r % G.ny);
-  int k = (int)(r / G.ny);
-  bool edge = (i == 0 || i == G.nx - 1 || j == 0 || j == G.ny - 1 || k == 0 || k == G.nz - 1);
+  const int c[3] = {(int)(t % G.nx), (int)((t / G.nx) % G.ny), (int)(t / ((int64_t)G.nx * G.ny))};
+  const int n[3] = {G.nx, G.ny, G.nz};
+  const bool per[3] = {!G.bcx, !G.bcy, G.bcz == 0};
+  int s[3];
+  bool edge = false, zero = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    s[a] = c[a];
+    const bool lo = c[a] == 0, hi = c[a] == n[a] - 1;
+    if (!lo && !hi) continue;
+    edge = true;
+    if (per[a]) {
+      s[a] = lo ? n[a] - 2 : 1;
+    } else {
+      s[a] = lo ? 1 : n[a] - 2;
+      const int f = 2 * a + (hi ? 1 : 0);
+      if (((G.bkind >> (4 * f)) & 15) == 3) zero = true;
+    }
+  }
   if (!edge) return;
-  int si = i == 0 ? G.nx - 2 : (i == G.nx - 1 ? 1 : i);
-  int sj = j == 0 ? G.ny - 2 : (j == G.ny - 1 ? 1 : j);
-  int sk = k == 0 ? G.nz - 2 : (k == G.nz - 1 ? 1 : k);
-  int64_t o = G.at(i, j, k), s = G.at(si, sj, sk);
-  W.mut[o] = W.mut[s];
-  W.qc2[o] = W.qc2[s];
+  const int64_t o = G.at(c[0], c[1], c[2]), src = G.at(s[0], s[1], s[2]);
+  W.mut[o] = zero ? T(0) : W.mut[src];
+  W.qc2[o] = zero ? T(0) : W.qc2[src];
 }
 
 template <class T>

@@ -487,8 +487,10 @@ __device__ __forceinline__ void visc_2d4(const StepArgs<T>& A, const Acc& s, int
 // (3D_solver/src/calc_visc_high.f90.fypp:194-260, 432-497, 674-739): face viscosity
 // and normal derivatives from the face's two cells; tangential derivatives from the
 // two cell pairs on either side weighted by their 4-point viscosity averages.
-// D[c][a] is mu * d(velocity c) / d(axis a) as the reference names them (mux, mvy ...).
-template <class T>
+// D[c][a] is mu * d(velocity c) / d(axis a) as the reference names them (mux, mvy ...);
+// LES adds the same stresses with the SGS viscosity (Ds, muxsgs ...) after the work
+// terms, and the SGS enthalpy flux.
+template <bool LES, class T>
 __device__ __forceinline__ void visc_fb3(const StepArgs<T>& A, int nd, int64_t o, const int64_t st[3],
                                          const T invs[3], T out[4]) {
   const Fields<T>& W = A.W;
@@ -497,42 +499,75 @@ __device__ __forceinline__ void visc_fb3(const StepArgs<T>& A, int nd, int64_t o
   const T inv = invs[nd];
   const T mn = T(0.5) * (W.mu[o] + W.mu[o2]);
   const T kT = T(A.K.Cp_over_Pr) * mn * (-W.T_[o] + W.T_[o2]) * inv;
-  T D[3][3];
+  // mu * derivatives with viscosity field m (mu, or mut for the SGS part)
+  auto derivs = [&](const T* m, T D[3][3]) {
+    const T mf = T(0.5) * (m[o] + m[o2]);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) D[c][nd] = mn * (-vel[c][o] + vel[c][o2]) * inv;
+    for (int a = 0; a < 3; ++a) {
+      if (a == nd) continue;
+      const int64_t s = st[a];
+      const T m1 = T(0.25) * (m[o - s] + m[o] + m[o2 - s] + m[o2]);
+      const T m2 = T(0.25) * (m[o] + m[o + s] + m[o2] + m[o2 + s]);
+      auto tder = [&](const T* q) {
+        return T(0.25) * (m1 * (-q[o - s] + q[o] - q[o2 - s] + q[o2]) + m2 * (-q[o] + q[o + s] - q[o2] + q[o2 + s])) *
+               invs[a];
+      };
+      D[nd][a] = tder(vel[nd]);  // normal velocity along the tangent (cross stress)
+      D[a][a] = tder(vel[a]);    // tangential velocity along itself (normal stress)
+    }
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    if (a == nd) continue;
-    const int64_t s = st[a];
-    const T m1 = T(0.25) * (W.mu[o - s] + W.mu[o] + W.mu[o2 - s] + W.mu[o2]);
-    const T m2 = T(0.25) * (W.mu[o] + W.mu[o + s] + W.mu[o2] + W.mu[o2 + s]);
-    auto tder = [&](const T* q) {
-      return T(0.25) * (m1 * (-q[o - s] + q[o] - q[o2 - s] + q[o2]) + m2 * (-q[o] + q[o + s] - q[o2] + q[o2 + s])) *
-             invs[a];
-    };
-    D[nd][a] = tder(vel[nd]);  // normal velocity along the tangent (cross stress)
-    D[a][a] = tder(vel[a]);    // tangential velocity along itself (normal stress)
-  }
+    for (int c = 0; c < 3; ++c) D[c][nd] = mf * (-vel[c][o] + vel[c][o2]) * inv;
+  };
   const T two3 = T(2.0 / 3.0);
-  T t[3];
+  // the stresses of the face in the reference's operand order; `t` starts from base
+  auto stresses = [&](const T D[3][3], const T base[3], T t[3]) {
+    if (nd == 0) {
+      t[0] = base[0] + two3 * (T(2) * D[0][0] - D[1][1] - D[2][2]);  // txx
+      t[1] = base[1] + D[0][1] + D[1][0];                             // txy: muy + mvx
+      t[2] = base[2] + D[2][0] + D[0][2];                             // txz: mwx + muz
+    } else if (nd == 1) {
+      t[0] = base[0] + D[0][1] + D[1][0];                             // tyx: muy + mvx
+      t[1] = base[1] + two3 * (T(2) * D[1][1] - D[2][2] - D[0][0]);  // tyy
+      t[2] = base[2] + D[1][2] + D[2][1];                             // tyz: mvz + mwy
+    } else {
+      t[0] = base[0] + D[2][0] + D[0][2];                             // tzx: mwx + muz
+      t[1] = base[1] + D[1][2] + D[2][1];                             // tzy: mvz + mwy
+      t[2] = base[2] + two3 * (T(2) * D[2][2] - D[0][0] - D[1][1]);  // tzz
+    }
+  };
+  T D[3][3], t[3];
+  derivs(W.mu, D);
   if (nd == 0) {
-    t[0] = two3 * (T(2) * D[0][0] - D[1][1] - D[2][2]);  // txx
-    t[1] = D[0][1] + D[1][0];                             // txy = muy + mvx
-    t[2] = D[2][0] + D[0][2];                             // txz = mwx + muz
+    t[0] = two3 * (T(2) * D[0][0] - D[1][1] - D[2][2]);
+    t[1] = D[0][1] + D[1][0];
+    t[2] = D[2][0] + D[0][2];
   } else if (nd == 1) {
-    t[0] = D[0][1] + D[1][0];                             // tyx = muy + mvx
-    t[1] = two3 * (T(2) * D[1][1] - D[2][2] - D[0][0]);  // tyy
-    t[2] = D[1][2] + D[2][1];                             // tyz = mvz + mwy
+    t[0] = D[0][1] + D[1][0];
+    t[1] = two3 * (T(2) * D[1][1] - D[2][2] - D[0][0]);
+    t[2] = D[1][2] + D[2][1];
   } else {
-    t[0] = D[2][0] + D[0][2];                             // tzx = mwx + muz
-    t[1] = D[1][2] + D[2][1];                             // tzy = mvz + mwy
-    t[2] = two3 * (T(2) * D[2][2] - D[0][0] - D[1][1]);  // tzz
+    t[0] = D[2][0] + D[0][2];
+    t[1] = D[1][2] + D[2][1];
+    t[2] = two3 * (T(2) * D[2][2] - D[0][0] - D[1][1]);
   }
   T e = T(0.5) * (vel[0][o] + vel[0][o2]) * t[0];
   e = e + T(0.5) * (vel[1][o] + vel[1][o2]) * t[1];
   e = e + T(0.5) * (vel[2][o] + vel[2][o2]) * t[2];
+  e = e + kT;
+  if constexpr (LES) {
+    T Ds[3][3], ts[3];
+    derivs(W.mut, Ds);
+    stresses(Ds, t, ts);
+    t[0] = ts[0]; t[1] = ts[1]; t[2] = ts[2];
+    auto Hf = [&](int64_t q) {
+      const T uu = W.u[q], vv = W.v[q], ww = W.w[q];
+      return T(A.K.Cp) * W.T_[q] + T(0.5) * (uu * uu + vv * vv + ww * ww) + W.qc2[q];
+    };
+    const T msf = T(0.5) * (W.mut[o] + W.mut[o2]);
+    e = e + -msf * (-Hf(o) + Hf(o2)) * inv / T(A.K.Prt);
+  }
   out[0] = t[0]; out[1] = t[1]; out[2] = t[2];
-  out[3] = e + kT;
+  out[3] = e;
 }
 
 }  // namespace oux
@@ -772,7 +807,6 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
             // high-order guard of calc_{E,F,G}v (calc_visc_high.f90.fypp:114/139/169,
             // 350/376/406, 592/618/648), 0-based: C4 faces 1..n-3 and transverse cells
             // 2..n-3, ME4 faces 2..n-4 and cells 2..n-3, C6 faces 2..n-4 and cells 3..n-4
-            static_assert(!LES, "walled viscous sweeps are Navier-Stokes only");
             constexpr int FA = (VB == VK_C4) ? 1 : 2, TA = (VB == VK_C6) ? 3 : 2;
             const int na[3] = {G.nx, G.ny, G.nz};
             bool inner = f >= FA && f <= na[DIR] - 2 - FA;
@@ -785,7 +819,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
               const int64_t o = G.at(fc[0], fc[1], fc[2]);
               T invs[3] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]], (T)A.M.inv_dz[fc[2]]};
               invs[DIR] = inv;
-              visc_fb3(A, DIR, o, stv, invs, vo);
+              visc_fb3<LES>(A, DIR, o, stv, invs, vo);
             }
           } else {
             visc_high<VB, LES>(A, sv, DIR, inv, vo);

@@ -8,7 +8,7 @@ int launch_sweeps_fp64_o4(int dim, int vk, bool les, const StepArgs<double>& A, 
 #define OUX_CASE(D, V, L) \
   if (dim == D && vk == V && les == L) return launch_stage_sweeps<D, 4, V, L, double>(A, s);
   OUX_CASE(3, VK_EULER, false) OUX_CASE(3, VK_C4, false) OUX_CASE(3, VK_GV2, false)
-  OUX_CASE(3, VK_C4W, false) OUX_CASE(3, VK_GV2W, false)
+  OUX_CASE(3, VK_C4W, false) OUX_CASE(3, VK_GV2W, false) OUX_CASE(3, VK_C4W, true) OUX_CASE(3, VK_GV2W, true)
   OUX_CASE(3, VK_C4, true) OUX_CASE(3, VK_GV2, true)
   OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_2D4, false) OUX_CASE(2, VK_GV2, false)
 #undef OUX_CASE
@@ -19,7 +19,7 @@ int launch_sweep_dir_fp64_o4(int dim, int vk, bool les, int dir, const StepArgs<
 #define OUX_CASE(D, V, L) \
   if (dim == D && vk == V && les == L) return launch_stage_sweep_dir<D, 4, V, L, double>(A, dir, s);
   OUX_CASE(3, VK_EULER, false) OUX_CASE(3, VK_C4, false) OUX_CASE(3, VK_GV2, false)
-  OUX_CASE(3, VK_C4W, false) OUX_CASE(3, VK_GV2W, false)
+  OUX_CASE(3, VK_C4W, false) OUX_CASE(3, VK_GV2W, false) OUX_CASE(3, VK_C4W, true) OUX_CASE(3, VK_GV2W, true)
   OUX_CASE(3, VK_C4, true) OUX_CASE(3, VK_GV2, true)
   OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_2D4, false) OUX_CASE(2, VK_GV2, false)
 #undef OUX_CASE

@@ -9,6 +9,7 @@ int launch_sweeps_fp64_o6(int dim, int vk, bool les, const StepArgs<double>& A, 
   if (dim == D && vk == V && les == L) return launch_stage_sweeps<D, 6, V, L, double>(A, s);
   OUX_CASE(3, VK_EULER, false) OUX_CASE(3, VK_C6, false) OUX_CASE(3, VK_C4, false) OUX_CASE(3, VK_ME4, false)
   OUX_CASE(3, VK_C6W, false) OUX_CASE(3, VK_C4W, false) OUX_CASE(3, VK_ME4W, false)
+  OUX_CASE(3, VK_C6W, true) OUX_CASE(3, VK_C4W, true) OUX_CASE(3, VK_ME4W, true)
   OUX_CASE(3, VK_C6, true) OUX_CASE(3, VK_C4, true) OUX_CASE(3, VK_ME4, true)
   OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_2D4, false) OUX_CASE(2, VK_GV2, false)
 #undef OUX_CASE
@@ -20,6 +21,7 @@ int launch_sweep_dir_fp64_o6(int dim, int vk, bool les, int dir, const StepArgs<
   if (dim == D && vk == V && les == L) return launch_stage_sweep_dir<D, 6, V, L, double>(A, dir, s);
   OUX_CASE(3, VK_EULER, false) OUX_CASE(3, VK_C6, false) OUX_CASE(3, VK_C4, false) OUX_CASE(3, VK_ME4, false)
   OUX_CASE(3, VK_C6W, false) OUX_CASE(3, VK_C4W, false) OUX_CASE(3, VK_ME4W, false)
+  OUX_CASE(3, VK_C6W, true) OUX_CASE(3, VK_C4W, true) OUX_CASE(3, VK_ME4W, true)
   OUX_CASE(3, VK_C6, true) OUX_CASE(3, VK_C4, true) OUX_CASE(3, VK_ME4, true)
   OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_2D4, false) OUX_CASE(2, VK_GV2, false)
 #undef OUX_CASE

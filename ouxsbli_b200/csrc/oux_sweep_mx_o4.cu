@@ -10,7 +10,7 @@ int launch_sweeps_mx_o4(int dim, int vk, bool les, int dir, const StepArgs<float
     return dir < 0 ? launch_stage_sweeps<D, 4, V, L, float>(A, s)                            \
                    : launch_stage_sweep_dir<D, 4, V, L, float>(A, dir, s);
   OUX_CASE(3, VK_EULER, false) OUX_CASE(3, VK_C4, false) OUX_CASE(3, VK_GV2, false)
-  OUX_CASE(3, VK_C4W, false) OUX_CASE(3, VK_GV2W, false)
+  OUX_CASE(3, VK_C4W, false) OUX_CASE(3, VK_GV2W, false) OUX_CASE(3, VK_C4W, true) OUX_CASE(3, VK_GV2W, true)
   OUX_CASE(3, VK_C4, true) OUX_CASE(3, VK_GV2, true)
   OUX_CASE(2, VK_EULER, false) OUX_CASE(2, VK_2D4, false) OUX_CASE(2, VK_GV2, false)
 #undef OUX_CASE

@@ -95,7 +95,7 @@ def _axis(n_int, L, order, nonper):
     return n, x, d
 
 
-def wall_box(nx_int, ny, nz_int, order, rules, bc_x=0, bc_z=0, U=5.0, perturb=True, plate=False, **kw):
+def wall_box(nx_int, ny, nz_int, order, rules, bc_x=0, bc_z=0, U=5.0, perturb=True, plate=False, visc="NS", **kw):
     """A 3D viscous (Sutherland, air) shear flow over a y range of 1 mm with walls at
     y = 0 (and y = H), periodic or non-periodic in x and z: u = U sin(pi y / H)
     (channel) or U sin(pi y / 2H) (plate: u = U at the top), plus a 3D perturbation."""
@@ -130,6 +130,6 @@ def wall_box(nx_int, ny, nz_int, order, rules, bc_x=0, bc_z=0, U=5.0, perturb=Tr
             Q[:, :, :, k] = Q[:, :, :, g + (k - g) % N]
     qj = to_qj(Q, jacobian(dx, dy, dz))
     dt = 0.4 * min(dx.min(), dy.min(), dz.min()) / (U + math.sqrt(GAMMA * R * T0))
-    cfg = SolverConfig(dim=3, nx=nx, ny=ny, nz=nz, order=order, visc="NS", bc_x=bc_x, bc_y=1, bc_z=bc_z, dt=dt,
+    cfg = SolverConfig(dim=3, nx=nx, ny=ny, nz=nz, order=order, visc=visc, bc_x=bc_x, bc_y=1, bc_z=bc_z, dt=dt,
                        gamma=GAMMA, R=R, Pr=0.72, dx=dx, dy=dy, dz=dz, boundary=rules, **kw)
     return cfg, qj, y

@@ -45,12 +45,10 @@ def create(cfg):
     (dict(order=5), "order"),
     (dict(dim=4), "dim"),
     (dict(nx=6), "too small"),
-    (dict(bc_x=1, visc="LES"), "not LES"),
     (dict(order=4, visc="Euler", bc_z=3), "order 2"),
     (dict(bc_z=5), "bc_z"),
     (dict(bc_x=2), "boundaries"),
     (dict(dim=2, nz=1, order=2, ny=3, dy=np.full(2, 0.1), bc_y=1), "too small"),
-    (dict(order=2, bc_y=1, bc_z=1, visc="LES"), "not LES"),
     (dict(rk=2), "rk"),
     (dict(dim=2, nz=1, scheme="Roe"), "Roe"),
     (dict(visc="NS", visc_order=2), "calc_Ev2_in"),
@@ -69,10 +67,12 @@ def test_create_rejects_invalid(kw, msg):
     dict(bc_x=1, bc_y=1, bc_z=1, visc="NS", visc_order=4),
     dict(order=4, nx=14, ny=14, nz=14, bc_z=1, visc="NS", visc_order=2),
     dict(order=2, nx=12, ny=12, nz=12, bc_x=1, bc_y=1, bc_z=1, visc="NS"),
+    dict(bc_x=1, bc_y=1, visc="LES"),
+    dict(order=2, nx=12, ny=12, nz=12, bc_y=1, bc_z=1, visc="LES"),
 ])
 def test_create_accepts_3d_viscous_walls(kw):
-    """3D Navier-Stokes grids with non-periodic directions are accepted (the walled
-    sweep variants)."""
+    """3D Navier-Stokes and LES grids with non-periodic directions are accepted (the
+    walled sweep variants)."""
     rc, h = create(small_cfg(**kw))
     assert rc == 0, _lib.LIB.oux_last_error().decode()
     _lib.LIB.oux_destroy(h)
