@@ -85,11 +85,13 @@ typedef struct oux_config {
                                bc_y = 1 (2D): the same for y (calc_*_y), as the
                                BC_X = BC_Y = True cases build them (2D_solver/OS, BL).
                                Euler or NS.  3D non-periodic x / y / z (bc_z = 1):
-                               Euler and NS (not LES) at orders 2 / 4 / 6, one boundary
-                               cell a side; NS viscous faces outside the reference's
+                               Euler, NS and LES at orders 2 / 4 / 6, one boundary
+                               cell a side; viscous faces outside the reference's
                                high-order guard take its 2nd-order fallback
                                (3D_solver/src/calc_visc_high.f90.fypp), as the SBLI /
-                               TBL cases' BC_X = BC_Y = True builds do.  bc_z = 2, 3, 4 (3D, not LES): a z slab of a
+                               TBL cases' BC_X = BC_Y = True builds do; the SGS
+                               viscosity is 0 on no-slip walls.  bc_z = 2, 3, 4 (3D,
+                               not LES): a z slab of a
                                larger grid (COMMZ, 3D_solver/src/calc_para.f90:343-384):
                                its g ghost planes at the halo ends (enum oux_bc_z) are
                                written by the caller's halo exchange (oux_halo_pack /
