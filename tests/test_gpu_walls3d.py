@@ -87,12 +87,15 @@ def test_3d_les_walls_bitexact_vs_oracle(order, vo, stencil, scheme, rk, bc_x, b
 
 
 @pytest.mark.gpu
-def test_3d_viscous_walls_mixed_close_to_fp64(cuda_device):
-    """The mixed form on a walled 3D Navier-Stokes box (KEEP-6, Central-6, RK4): relative
-    L2 against FP64 within the mixed form's bound for switch-free schemes (1e-5)."""
+@pytest.mark.parametrize("visc", ["NS", "LES"])
+def test_3d_viscous_walls_mixed_close_to_fp64(visc, cuda_device):
+    """The mixed form on a walled 3D Navier-Stokes / LES box (KEEP-6, Central-6, RK4):
+    relative L2 against FP64 within the mixed form's bound for switch-free schemes
+    (1e-5)."""
     out = {}
     for prec in ("fp64", "mixed"):
-        cfg, qj, _ = wall_box(14, 16, 10, 6, CLOSED, bc_x=1, bc_z=1, scheme="KEEP", rk=4, precision=prec)
+        cfg, qj, _ = wall_box(14, 16, 10, 6, CLOSED, bc_x=1, bc_z=1, scheme="KEEP", rk=4, precision=prec,
+                              visc=visc)
         s = Solver(cfg, cuda_device)
         s.set_state(qj)
         s.step(10)
