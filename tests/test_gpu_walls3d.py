@@ -203,3 +203,64 @@ def test_3d_viscous_walls_smallest_and_ragged_grids(visc, sizes, bc_x, bc_z, rul
     per = lambda nonper: slice(cfg.g - 1, -(cfg.g - 1)) if not nonper and cfg.g > 1 else slice(None)
     upd = (per(bc_x), slice(None), slice(None), per(bc_z))
     assert_matches_oracle(cfg, r[upd], q, oracle.rhs(cfg, qj)[upd], oracle.step(cfg, qj, 3))
+
+
+@pytest.mark.gpu
+def test_3d_flat_plate_skin_friction(cuda_device):
+    """The 2D_solver/BL0 flow in 3D: Mach 2 over an adiabatic no-slip plate along the
+    whole floor (1025 x 129 nodes of BL0's grid, 4 periodic z cells; fixed free-stream
+    inflow, zero-gradient outflow, characteristic far-field top; NS SLAU-2 / Gaitonde-
+    Visbal, RK3, dt 3 ns, 0.4 ms).  The z-uniform flow stays identical in every z plane,
+    and the skin friction from the discrete wall shear follows the similarity law: Cf
+    sqrt(Re_x) constant downstream (spread < 3 %) and within 8 % of the Eckert
+    reference-temperature value, as for BL0 in 2D."""
+    from ouxsbli_b200.cases import CASES, _bl_derived, _bl_grid
+    from ouxsbli_b200.grid import jacobian, to_qj
+    from ouxsbli_b200.solver import SolverConfig
+    p = _bl_derived(CASES["BL0"].params)
+    x, dx, y, dy = _bl_grid(p)
+    nx, ny, nz = x.size, y.size, 6
+    dz = np.full(nz - 1, dx[0])
+    g, Rg, M0 = p["gamma"], p["R"], p["M0"]
+    rho0, u0, p0 = p["rho_bc"], p["u0"], p["p0"]
+    free = np.array([rho0, rho0 * u0, 0.0, 0.0, p0 / (g - 1.0) + 0.5 * rho0 * u0 ** 2])
+    Q = np.zeros((nx, 5, ny, nz), order="F")
+    Q[:] = free[None, :, None, None]
+    J = jacobian(dx, dy, dz)
+    inflow = (free[:, None, None] * (1.0 / J[0, :])[None, :, None] * np.ones(nz)[None, None, :])
+    rules = {"x_lo": ("fixed", inflow.reshape(5, ny * nz, order="F")), "x_hi": "zero_gradient",
+             "y_lo": "noslip_wall", "y_hi": ("farfield", rho0, u0, 0.0, p["c_bc"])}
+    cfg = SolverConfig(dim=3, nx=nx, ny=ny, nz=nz, order=2, scheme="SLAU", slau="HRSLAU2", tvd="none", visc="NS",
+                       rk=3, bc_x=1, bc_y=1, bc_z=0, dt=p["dt"], gamma=g, R=Rg, Pr=p["Pr"],
+                       threshold=p["threshold"], dx=dx, dy=dy, dz=dz, boundary=rules)
+    s = Solver(cfg, cuda_device)
+    s.set_state(to_qj(Q, J))
+    s.step(int(round(p["endT"] / p["dt"])))
+    q = s.get_state()
+    s.close()
+    for k in range(2, nz - 1):
+        np.testing.assert_array_equal(q[..., k], q[..., 1])
+    q = q[..., 1]
+    rho = q[:, 0] * J
+    u = q[:, 1] / q[:, 0]
+    v = q[:, 2] / q[:, 0]
+    pr = (g - 1.0) * (q[:, 4] * J - 0.5 * rho * (u * u + v * v))
+    T = pr / (rho * Rg)
+
+    def mu(t):
+        return 1.716e-5 * 384.2 * 273.2 ** -1.5 / (t + 111.0) * t ** 1.5
+
+    Te, rho_e, u_e = p["T0"], p["rho0"], p["u0"]
+    vals = []
+    for frac in np.linspace(0.45, 0.95, 6):
+        i = int(frac * (nx - 1))
+        tau = 0.5 * (mu(T[i, 0]) + mu(T[i, 1])) * (u[i, 1] - u[i, 0]) / (y[1] - y[0])
+        rex = rho_e * u_e * (x[i] - x[0]) / mu(Te)
+        vals.append(tau / (0.5 * rho_e * u_e ** 2) * math.sqrt(rex))
+    vals = np.array(vals)
+    Tw = Te * (1.0 + math.sqrt(p["Pr"]) * 0.5 * (g - 1.0) * M0 ** 2)
+    Ts = Te * (1.0 + 0.032 * M0 ** 2 + 0.58 * (Tw / Te - 1.0))
+    eckert = 0.664 * math.sqrt(mu(Ts) / mu(Te) * Te / Ts)
+    print("Cf sqrt(Re_x):", vals, "Eckert:", eckert)
+    assert vals.max() / vals.min() - 1.0 < 0.03, vals
+    assert abs(vals.mean() / eckert - 1.0) < 0.08, (vals, eckert)
