@@ -69,7 +69,13 @@ def test_single_process_without_group():
 
 
 # ---- z slabs (COMMZ) over two gloo ranks, each slab stepped by the oracle ----------
-def _slab_cfg(rk):
+def _slab_cfg(rk, kind="tgv"):
+    if kind == "walls":
+        # Navier-Stokes over a no-slip floor, zero-gradient x ends and top, periodic z
+        from helpers import wall_box
+        rules = {"x_lo": "zero_gradient", "x_hi": "zero_gradient", "y_lo": "noslip_wall", "y_hi": "zero_gradient"}
+        cfg, qj, _ = wall_box(10, 12, 12, 4, rules, bc_x=1, bc_z=0, scheme="Hybrid", rk=rk, tvd="hybrid")
+        return cfg, qj
     from ouxsbli_b200.cases import CASES, build_initial
     from ouxsbli_b200.grid import jacobian, to_qj
     from ouxsbli_b200.solver import SolverConfig
@@ -81,7 +87,7 @@ def _slab_cfg(rk):
     return cfg, to_qj(Q, jacobian(dx, dy, dz))
 
 
-def _slab_rank(rank, world, port, rk, nsteps, out):
+def _slab_rank(rank, world, port, rk, nsteps, out, kind="tgv"):
     import datetime
     import torch
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -90,7 +96,7 @@ def _slab_rank(rank, world, port, rk, nsteps, out):
     try:
         from oracle import oracle
         from ouxsbli_b200.slabs import halo_exchange, slab_config, slab_state
-        cfg, qj = _slab_cfg(rk)
+        cfg, qj = _slab_cfg(rk, kind)
         lcfg, k0 = slab_config(cfg, rank, world)
         st = oracle.Stepper(lcfg, slab_state(qj, cfg, rank, world))
         g, n = cfg.g, lcfg.nz
@@ -113,18 +119,19 @@ def _slab_rank(rank, world, port, rk, nsteps, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("rk", [3, 4])
-def test_two_gloo_ranks_z_slabs_match_the_global_oracle(rk):
+@pytest.mark.parametrize("rk,kind", [(3, "tgv"), (4, "tgv"), (3, "walls")])
+def test_two_gloo_ranks_z_slabs_match_the_global_oracle(rk, kind):
     """The halo exchange of the z-slab decomposition (which array after which stage,
     which planes go to which neighbour, the slab's z spacings): two ranks stepping
-    their slabs stage by stage reproduce the undivided solve bit for bit."""
+    their slabs stage by stage reproduce the undivided solve bit for bit, on a periodic
+    grid and on a walled Navier-Stokes one."""
     from oracle import oracle
-    cfg, qj = _slab_cfg(rk)
+    cfg, qj = _slab_cfg(rk, kind)
     nsteps = 2
     ctx = mp.get_context("spawn")
     with ctx.Manager() as mgr:
         out = mgr.dict()
-        mp.start_processes(_slab_rank, args=(2, _free_port(), rk, nsteps, out), nprocs=2, join=True,
+        mp.start_processes(_slab_rank, args=(2, _free_port(), rk, nsteps, out, kind), nprocs=2, join=True,
                            start_method="spawn")
         parts = [out[0], out[1]]
     g = cfg.g
