@@ -400,3 +400,25 @@ def test_3d_tbl_top_rules_of_the_oracle():
             np.testing.assert_allclose(pb / rb ** GAMMA, (RHO0 * c0 ** 2 / GAMMA) / RHO0 ** GAMMA, rtol=1e-12)
             np.testing.assert_allclose(ub, U, rtol=1e-13)
             assert np.all(wb == 0.0)
+
+
+@pytest.mark.parametrize("order,visc,vo,stencil", [(6, "NS", 6, "Central"), (6, "LES", 6, "ME4Base"),
+                                                   (4, "NS", 4, "Central"), (4, "NS", 2, "Central"),
+                                                   (2, "LES", 2, "Central"), (6, "Euler", 0, "Central")])
+def test_3d_walled_box_at_rest_stays_at_rest(order, visc, vo, stencil):
+    """The oracle's walled 3D paths (convective order fallback, viscous 2nd-order
+    fallback, SGS boundary values, slip and no-slip walls on every face) keep a uniform
+    fluid at rest: the residual is at rounding level, below 1e-12 of the residual of
+    the same box with its shear flow."""
+    from helpers import wall_box
+    from oracle import oracle
+    rules = {"x_lo": "slip_wall", "x_hi": "noslip_wall", "y_lo": "noslip_wall", "y_hi": "slip_wall",
+             "z_lo": "noslip_wall", "z_hi": "slip_wall"}
+    kw = dict(bc_x=1, bc_z=1, visc=visc, scheme="SLAU", rk=3, tvd="hybrid")
+    if visc != "Euler":
+        kw.update(visc_order=vo, visc_stencil=stencil)
+    cfg, moving, _ = wall_box(10, 12, 8, order, rules, **kw)
+    _, rest, _ = wall_box(10, 12, 8, order, rules, U=0.0, perturb=False, **kw)
+    r_rest = oracle.rhs(cfg, rest)
+    r_moving = oracle.rhs(cfg, moving)
+    assert np.abs(r_rest).max() <= 1e-12 * np.abs(r_moving).max(), np.abs(r_rest).max()
