@@ -233,6 +233,22 @@ def test_xy_mixed_close_to_fp64(cuda_device):
         assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-5, l
 
 
+def test_neumann_faces_2d_bitexact_vs_oracle(cuda_device):
+    """OUX_BC_NEUMANN on 2D faces (the top and the outflow of a supersonic duct with a
+    slip floor and fixed inflow; SLAU-4, RK3): the residual and the state after 6 steps
+    bit-identical to the oracle."""
+    rules = {"x_lo": "fixed", "x_hi": "neumann", "y_lo": "slip_wall", "y_hi": "neumann"}
+    cfg, qj = duct(41, 23, order=4, rules=rules, scheme="SLAU", tvd="hybrid", rk=3)
+    s = Solver(cfg, cuda_device)
+    s.set_state(qj)
+    r = s.rhs()
+    s.step(6)
+    q = s.get_state()
+    s.close()
+    np.testing.assert_array_equal(r, oracle.rhs(cfg, qj))
+    np.testing.assert_array_equal(q, oracle.step(cfg, qj, 6))
+
+
 def test_reflected_oblique_shock_vs_shock_relations(tmp_path, cuda_device):
     """ouxsbli/tests/test_os.py with its settings: M0 2, p_tot 100 kPa, T_tot 295 K,
     incident shock 37.2 deg, 257 x 129 nodes on 5 x 2 mm, dt 3 ns, 0.1 ms in one

@@ -422,3 +422,36 @@ def test_3d_walled_box_at_rest_stays_at_rest(order, visc, vo, stencil):
     r_rest = oracle.rhs(cfg, rest)
     r_moving = oracle.rhs(cfg, moving)
     assert np.abs(r_rest).max() <= 1e-12 * np.abs(r_moving).max(), np.abs(r_rest).max()
+
+
+def test_2d_neumann_rule_of_the_oracle():
+    """The oracle's Neumann rule in 2D carries the neighbour's primitive state (rho,
+    u, v, p) into the boundary cells of both non-periodic faces it is set on."""
+    from oracle import oracle
+    from ouxsbli_b200.grid import jacobian, to_qj
+    from ouxsbli_b200.solver import SolverConfig
+    nx, ny, g1 = 20, 14, 0.4
+    dx = np.full(nx - 1, 0.05)
+    dy = 0.03 * (1.0 + 0.05 * np.arange(ny - 1))  # stretched
+    x, y = np.concatenate([[0.0], np.cumsum(dx)]), np.concatenate([[0.0], np.cumsum(dy)])
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    rho, u, v, p = 1.0 + 0.1 * np.sin(3 * X) * Y, 1.5 + 0.2 * Y, 0.1 * np.cos(4 * X), 1.0 + 0.1 * X * Y
+    Q = np.zeros((nx, 4, ny), order="F")
+    Q[:, 0], Q[:, 1], Q[:, 2], Q[:, 3] = rho, rho * u, rho * v, p / g1 + 0.5 * rho * (u * u + v * v)
+    J = jacobian(dx, dy, None)
+    rules = {"x_lo": "slip_wall", "x_hi": "neumann", "y_lo": "noslip_wall", "y_hi": "neumann"}
+    cfg = SolverConfig(dim=2, nx=nx, ny=ny, nz=1, order=2, visc="Euler", bc_x=1, bc_y=1, dt=1e-3, gamma=1.4,
+                       R=1.0, dx=dx, dy=dy, dz=None, boundary=rules)
+    q = oracle.fill_ghosts(cfg, to_qj(Q, J))
+
+    def prim(qq, Jv):
+        r = qq[0] * Jv
+        uu, vv = qq[1] / qq[0], qq[2] / qq[0]
+        return np.array([r, uu, vv, g1 * (qq[3] * Jv - 0.5 * r * (uu * uu + vv * vv))])
+
+    for i in range(1, nx - 1):  # top row (corners take the x rules in this order)
+        np.testing.assert_allclose(prim(q[i, :, ny - 1], J[i, ny - 1]), prim(q[i, :, ny - 2], J[i, ny - 2]),
+                                   rtol=1e-13, atol=1e-15)
+    for j in range(1, ny - 1):  # x high column
+        np.testing.assert_allclose(prim(q[nx - 1, :, j], J[nx - 1, j]), prim(q[nx - 2, :, j], J[nx - 2, j]),
+                                   rtol=1e-13, atol=1e-15)
