@@ -50,8 +50,11 @@ def parse():
     ap.add_argument("--commz", action="store_true",
                     help="split the one grid into z slabs over the ranks (halo exchange after every stage; "
                          "strong scaling) instead of running independent replicas")
-    ap.add_argument("--workload", default="tgv256", choices=["tgv256", "large512"],
-                    help="large512: FP64 vs mixed on the 512^3 ME4 supersonic TGV (opt-in, minutes)")
+    ap.add_argument("--workload", default="tgv256", choices=["tgv256", "large512", "walls256"],
+                    help="large512: FP64 vs mixed on the 512^3 ME4 supersonic TGV (opt-in, minutes); "
+                         "walls256: a --n^3 Navier-Stokes shear layer, periodic and with no-slip walls")
+    ap.add_argument("--walls-config", default="all", choices=["all", "periodic", "y", "xy", "xyz"],
+                    help="walls256: which grid (all: the four in turn)")
     ap.add_argument("--large-steps", type=int, default=2000)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched 2D ensemble section")
     ap.add_argument("--ensemble-steps", type=int, default=500)
@@ -322,6 +325,94 @@ def run_reference(args):
     return 0
 
 
+WALL_GRIDS = {  # walls256: non-periodic x, z and the rules of the faces (y always has no-slip walls)
+    "periodic": None,
+    "y": (0, 0, {"y_lo": "noslip_wall", "y_hi": "noslip_wall"}),
+    "xy": (1, 0, {"x_lo": "zero_gradient", "x_hi": "zero_gradient", "y_lo": "noslip_wall", "y_hi": "zero_gradient"}),
+    "xyz": (1, 1, {"x_lo": "slip_wall", "x_hi": "slip_wall", "y_lo": "noslip_wall", "y_hi": "noslip_wall",
+                   "z_lo": "slip_wall", "z_hi": "noslip_wall"}),
+}
+
+
+def walled_workload(n: int, which: str):
+    """A viscous shear layer of air (Sutherland, 300 K) in a box of n^3 interior cells,
+    KEEP-6 / Central-6 NS, RK3: u = 5 sin(pi y / H) m/s with a 3D perturbation, H = 1 mm.
+    `which` picks the boundaries (WALL_GRIDS); "periodic" has all three axes periodic
+    (y then with its own ghost layers)."""
+    import math
+    from ouxsbli_b200.grid import cyclic_axis, jacobian, to_qj
+    from ouxsbli_b200.solver import SolverConfig
+    order, g = 6, 3
+    H, Rg, gam, T0, rho0, U = 1.0e-3, 287.03, 1.4, 300.0, 1.2, 5.0
+    spec = WALL_GRIDS[which]
+    bc_x, bc_z, rules = (0, 0, None) if spec is None else spec
+    bc_y = 0 if spec is None else 1
+
+    def axis(L, nonper):
+        if nonper:
+            m = n + 2
+            d = np.full(m - 1, L / (m - 1))
+            return m, np.concatenate([[0.0], np.cumsum(d)]), d
+        x, d = cyclic_axis(n + 2 * g, L, order)
+        return n + 2 * g, x, d
+
+    nx, x, dx = axis(0.5e-3, bc_x)
+    ny, y, dy = axis(H, bc_y)
+    nz, z, dz = axis(0.4e-3, bc_z)
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    sy = np.sin(math.pi * Y / H)
+    rho = rho0 * (1.0 + 0.02 * np.sin(2 * math.pi * X / 0.5e-3) * np.cos(2 * math.pi * Z / 0.4e-3) * sy)
+    u = U * sy
+    v = 0.3 * U * np.sin(2 * math.pi * X / 0.5e-3) * sy ** 2
+    w = 0.2 * U * np.sin(2 * math.pi * Z / 0.4e-3) * np.cos(2 * math.pi * X / 0.5e-3) * sy
+    Q = np.zeros((nx, 5, ny, nz), order="F")
+    Q[:, 0], Q[:, 1], Q[:, 2], Q[:, 3] = rho, rho * u, rho * v, rho * w
+    Q[:, 4] = rho0 * Rg * T0 / (gam - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    del X, Y, Z, sy, rho, u, v, w
+    dt = 0.4 * min(dx.min(), dy.min(), dz.min()) / (U + math.sqrt(gam * Rg * T0))
+    cfg = SolverConfig(dim=3, nx=nx, ny=ny, nz=nz, order=order, scheme="KEEP", visc="NS", rk=3, bc_x=bc_x,
+                       bc_y=bc_y, bc_z=bc_z, dt=dt, gamma=gam, R=Rg, Pr=0.72, dx=dx, dy=dy, dz=dz, boundary=rules)
+    return cfg, to_qj(Q, jacobian(dx, dy, dz))
+
+
+def run_walls(args):
+    """Step rate of --n^3 KEEP-6 / Central-6 NS grids with and without no-slip walls
+    (the walled sweep variants beside the periodic ones), per-kernel times included."""
+    import torch
+    from ouxsbli_b200 import _lib
+    from ouxsbli_b200.solver import Solver
+    dev = torch.device("cuda", 0)
+    kinds = ["prim", "sensor", "sgs", "sgs_edges", "sweep_x", "sweep_y", "sweep_z", "ghost"]
+    out = {"workload": "walls256", "n": args.n, "steps": args.steps, "warmup": args.warmup,
+           "config": "KEEP-6, Central-6 NS, RK3, FP64; u = 5 sin(pi y / H) m/s shear layer of air, H = 1 mm",
+           "grids": {}}
+    for which in (WALL_GRIDS if args.walls_config == "all" else [args.walls_config]):
+        cfg, qj = walled_workload(args.n, which)
+        s = Solver(cfg, dev)
+        s.set_state(qj)
+        del qj
+        s.step(args.warmup)
+        st = torch.cuda.current_stream(dev)
+        _lib.check(_lib.LIB.oux_profile(s._h, 1))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        a.record(st)
+        s.step(args.steps)
+        b.record(st)
+        b.synchronize()
+        kms, kcnt = (C.c_double * 8)(), (C.c_int64 * 8)()
+        _lib.check(_lib.LIB.oux_profile_read(s._h, kms, kcnt, 8))
+        _lib.check(_lib.LIB.oux_profile(s._h, 0))
+        ms = a.elapsed_time(b) / max(args.steps, 1)
+        out["grids"][which] = {
+            "ms_per_step": ms, "value": cfg.interior_cells() / (ms / 1e3) / 1e6, "unit": METRIC,
+            "status": s.check_state(),
+            "per_kernel_avg_ms": {k: kms[i] / kcnt[i] for i, k in enumerate(kinds) if kcnt[i]}}
+        s.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_large(args):
     """512^3 supersonic TGV (Ma 1.25, Re 1600, Hybrid-6, ME4 viscous, TVD-RK3): plain FP64
     against the mixed form over --large-steps steps -- throughput, HBM roofline at
@@ -428,6 +519,8 @@ def main():
         return run_reference(args)
     if args.workload == "large512":
         return run_large(args)
+    if args.workload == "walls256":
+        return run_walls(args)
     if args.commz:
         return run_commz(args)
     import torch
