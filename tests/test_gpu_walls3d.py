@@ -291,3 +291,24 @@ def test_3d_viscous_walls_in_z_slabs_match_one_solve(order, bc_z, rules, world, 
     slabs.close()
     gz = 1 if bc_z else cfg.g
     np.testing.assert_array_equal(got[..., gz:-gz], whole[..., gz:-gz])
+
+
+@pytest.mark.gpu
+def test_3d_tbl_configuration_les_vs_oracle(cuda_device):
+    """The numerics of 3D_solver/TBL (config.fypp: LES, Hybrid-6, RK3; set_bc: periodic
+    x by its ghost copies, a no-slip floor, the Riemann far-field top of
+    set_bc_tbl_sbli.f90, periodic z) on a plate-profile box: residual and state after 4
+    steps against the oracle within the LES tolerances."""
+    c0 = math.sqrt(GAMMA * R * T0)
+    rules = {"y_lo": "noslip_wall", "y_hi": ("farfield", RHO0, 5.0, 0.0, c0)}
+    cfg, qj, _ = wall_box(14, 16, 10, 6, rules, bc_x=0, bc_z=0, plate=True, visc="LES", scheme="Hybrid", rk=3,
+                          tvd="hybrid")
+    s = Solver(cfg, cuda_device)
+    s.set_state(qj)
+    r = s.rhs()
+    s.step(4)
+    q = s.get_state()
+    s.close()
+    g = cfg.g
+    upd = (slice(g - 1, -(g - 1)), slice(None), slice(None), slice(g - 1, -(g - 1)))
+    assert_matches_oracle(cfg, r[upd], q, oracle.rhs(cfg, qj)[upd], oracle.step(cfg, qj, 4))
