@@ -159,3 +159,16 @@ def test_3d_boundary_setters_without_a_device():
     assert L.oux_set_boundary(h, _lib.FACES["x_lo"], 6, None) == _lib.OUX_E_INVALID
     assert L.oux_set_boundary_cells(h, _lib.FACES["x_lo"], None) == _lib.OUX_E_INVALID
     L.oux_destroy(h)
+
+
+def test_bench_walls_grids_are_accepted():
+    """bench.py --workload walls256: each of its grids (periodic; y; x and y; x, y and z
+    walls) makes a valid configuration with the face rules its walls need."""
+    import bench
+    for which in bench.WALL_GRIDS:
+        cfg, qj = bench.walled_workload(12, which)
+        assert qj.shape == (cfg.nx, 5, cfg.ny, cfg.nz)
+        assert cfg.interior_cells() == 12 ** 3
+        rc, h = create(cfg)
+        assert rc == 0, _lib.LIB.oux_last_error().decode()
+        _lib.LIB.oux_destroy(h)
