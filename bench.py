@@ -1,16 +1,22 @@
 #!/usr/bin/env python
 """Benchmark of the explicit time step on one B200 (or N replicas).
 
-Workload (default): supersonic Taylor-Green vortex, 256^3 interior cells
-(262^3 with the 6th-order ghost layers), Ma = 1.25, Re = 1600, KEEP/SLAU
-hybrid with the Ducros sensor, 6th-order central differences, Central-6
-viscous fluxes, TVD-RK3, FP64.  A "step" is one full time step (three RK
-stages) of that grid.  Metric: Mcell-steps/s = interior cells x steps / s.
+Default workload (tgv512): the large single solve -- supersonic Taylor-Green vortex,
+512^3 interior cells (518^3 with the 6th-order ghost layers), Ma = 1.25, Re = 1600,
+KEEP/SLAU hybrid with the Ducros sensor (HRSLAU2, MUSCL with the hybrid TVD switch),
+6th-order central differences, ME4 viscous stencil, TVD-RK3, FP64.  A "step" is one
+full time step (three RK stages) of that grid.  Metric: Mcell-steps/s = interior
+cells x steps / s.  The mixed FP32/FP64 form runs beside it, with its error against
+the FP64 run after --mixed-check-steps steps from the same initial field.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload tgv512|tgv256|walls256]
 
 N > 1 runs N independent replicas (one per GPU, torch.distributed for the
 barrier and the max-over-ranks time); the solve itself has no cross-GPU step.
+--impl reference times the CPU restatement of the reference's kernels on the
+host cores instead (the reference is CUDA Fortran with no CPU build): each step is
+one RK3 step of a block of z planes of the same grid.
 """
 from __future__ import annotations
 
@@ -32,63 +38,109 @@ sys.path.insert(0, ROOT)
 METRIC = "Mcell-steps/s"
 ALG_BYTES_PER_CELL_STEP = 320.0  # FP64 RK3: 8 state accesses x 5 variables x 8 B
 
+# name -> (interior cells per axis, viscous stencil, description of the stencil)
+WORKLOADS = {
+    "tgv512": (512, "ME4Base", "ME4 viscous"),
+    "tgv256": (256, "Central", "Central-6 viscous"),
+}
+# z planes of the block the CPU legs time (per step: one RK3 step of that block)
+CPU_SAMPLE_PLANES = 32
+
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=256, help="interior cells per axis")
+    ap.add_argument("--workload", default="tgv512", choices=["tgv512", "tgv256", "walls256"],
+                    help="tgv512: the 512^3 ME4 supersonic TGV (default); tgv256: the 256^3 Central-6 one; "
+                         "walls256: a --n^3 Navier-Stokes shear layer, periodic and with no-slip walls")
+    ap.add_argument("--n", type=int, default=None, help="interior cells per axis (default: the workload's)")
     ap.add_argument("--scheme", default="Hybrid")
     ap.add_argument("--visc", default="NS")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--mixed-check-steps", type=int, default=1000,
-                    help="steps of the mixed-vs-FP64 accuracy check (the north star's 1000)")
+    ap.add_argument("--mixed-check-steps", type=int, default=2000,
+                    help="steps of the mixed-vs-FP64 accuracy check from the initial field")
+    ap.add_argument("--history-every", type=int, default=100,
+                    help="diagnostics (KE, entropy, enstrophy) every so many steps of the accuracy check")
     ap.add_argument("--commz", action="store_true",
                     help="split the one grid into z slabs over the ranks (halo exchange after every stage; "
                          "strong scaling) instead of running independent replicas")
-    ap.add_argument("--workload", default="tgv256", choices=["tgv256", "large512", "walls256"],
-                    help="large512: FP64 vs mixed on the 512^3 ME4 supersonic TGV (opt-in, minutes); "
-                         "walls256: a --n^3 Navier-Stokes shear layer, periodic and with no-slip walls")
     ap.add_argument("--walls-config", default="all", choices=["all", "periodic", "y", "xy", "xyz"],
                     help="walls256: which grid (all: the four in turn)")
-    ap.add_argument("--large-steps", type=int, default=2000)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched 2D ensemble section")
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream section")
     ap.add_argument("--serving-requests", type=int, default=16)
     ap.add_argument("--serving-rate", type=float, default=2.0)
     ap.add_argument("--serving-budget-gb", type=float, default=4.0)
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.n is None:
+        a.n = WORKLOADS.get(a.workload, (256,))[0]
+    return a
 
 
-def workload(n: int, scheme: str, visc: str, **kw):
-    """SolverConfig + initial QJ (reference layout) of the supersonic TGV."""
-    from ouxsbli_b200.cases import CASES, build_initial
-    from ouxsbli_b200.grid import jacobian, to_qj
-    from ouxsbli_b200.solver import SolverConfig
+def tgv_params(n: int):
+    """Derived parameters and cell-centre axes of the supersonic TGV on n^3 interior cells."""
+    from ouxsbli_b200.cases import CASES
+    from ouxsbli_b200.grid import cyclic_axis
     case = CASES["NSTGV"]
     p = dict(case.params)
     p.update(nx=n + 6, ny=n + 6, nz=n + 6, order=6, M0=1.25, Re=1600.0, rho_mode="uniform",
              cfl_mode="acoustic", CFL=0.5, dt=None)
-    p, xc, yc, zc, dx, dy, dz, Q = build_initial(case, p)
-    cfg = SolverConfig(dim=3, nx=p["nx"], ny=p["ny"], nz=p["nz"], order=6, scheme=scheme, visc=visc,
-                       tvd="hybrid", slau="HRSLAU2", rk=3, gamma=p["gamma"], R=p["R"], Pr=p["Pr"],
-                       Prt=p["Prt"], threshold=0.4, dt=p["dt"], dx=dx, dy=dy, dz=dz, **kw)
-    qj = to_qj(Q, jacobian(dx, dy, dz))
-    return cfg, qj
+    p = case.derived(p)
+    xc, dx = cyclic_axis(p["nx"], p["Lx"], 6)
+    yc, dy = cyclic_axis(p["ny"], p["Ly"], 6)
+    zc, dz = cyclic_axis(p["nz"], p["Lz"], 6)
+    return p, (xc, yc, zc), (dx, dy, dz)
 
 
-def config_json(args, cfg):
+def make_cfg(args, p, dx, dy, dz, nz=None, bc_z=0, **kw):
+    """SolverConfig of the workload (ouxsbli_b200.config: building it loads no GPU library)."""
+    from ouxsbli_b200.config import SolverConfig
+    stencil = WORKLOADS.get(args.workload, (0, "Central"))[1]
+    return SolverConfig(dim=3, nx=p["nx"], ny=p["ny"], nz=nz or p["nz"], order=6, scheme=args.scheme,
+                        visc=args.visc, visc_stencil=stencil, tvd="hybrid", slau="HRSLAU2", rk=3,
+                        gamma=p["gamma"], R=p["R"], Pr=p["Pr"], Prt=p["Prt"], threshold=0.4, dt=p["dt"],
+                        dx=dx, dy=dy, dz=dz, bc_z=bc_z, **kw)
+
+
+def workload(args, **kw):
+    """SolverConfig + initial QJ (reference layout) of the supersonic TGV."""
+    from ouxsbli_b200.cases import CASES
+    from ouxsbli_b200.grid import jacobian, to_qj
+    p, (xc, yc, zc), (dx, dy, dz) = tgv_params(args.n)
+    Q = CASES["NSTGV"].init(p, xc, yc, zc)
+    cfg = make_cfg(args, p, dx, dy, dz, **kw)
+    return cfg, to_qj(Q, jacobian(dx, dy, dz))
+
+
+def cpu_sample(args, planes: int = CPU_SAMPLE_PLANES):
+    """The block of the workload the CPU legs time: its z planes 0 .. planes-1 (all x
+    and y cells, the same spacings, scheme and physics) as a z slab whose ghost planes
+    hold the neighbouring planes' initial values (bc_z = 2, left alone by the fill)."""
+    from ouxsbli_b200.cases import tgv_planes
+    from ouxsbli_b200.grid import jacobian, to_qj
+    p, (xc, yc, zc), (dx, dy, dz) = tgv_params(args.n)
+    planes = min(planes, args.n)
+    Q = tgv_planes(p, xc, yc, zc, 0, planes + 6)
+    cfg = make_cfg(args, p, dx, dy, dz[:planes + 5], nz=planes + 6, bc_z=2)
+    return cfg, to_qj(Q, jacobian(dx, dy, dz))
+
+
+def config_json(args, cfg, world: int = 1):
+    stencil = WORKLOADS.get(args.workload, (0, "Central", "Central-6 viscous"))[2]
     return {"workload": f"supersonic Taylor-Green vortex {args.n}^3 (+6 ghost layers), Ma 1.25, Re 1600, "
-                        f"{args.scheme}-6 / {args.visc} Central-6 viscous, TVD-RK3",
+                        f"{args.scheme}-6 (HRSLAU2, MUSCL TVD hybrid) / {args.visc} {stencil}, TVD-RK3",
             "grid": [cfg.nx, cfg.ny, cfg.nz], "interior_cells": cfg.interior_cells(), "order": 6,
-            "scheme": args.scheme, "visc": args.visc, "rk": 3, "precision": "fp64",
+            "scheme": args.scheme, "visc": args.visc, "visc_stencil": cfg.visc_stencil, "rk": 3,
+            "precision": "fp64",
             "l2": "inputs larger than L2 (state %.2f GB + stage arrays %.2f GB)" % (
-                5 * cfg.nx * cfg.ny * cfg.nz * 8 / 1e9, 10 * cfg.nx * cfg.ny * cfg.nz * 8 / 1e9)}
+                5 * cfg.nx * cfg.ny * cfg.nz * 8 / 1e9, 10 * cfg.nx * cfg.ny * cfg.nz * 8 / 1e9),
+            "parallelism": f"{world} independent replicas"}
 
 
 class ClockSampler:
@@ -142,25 +194,44 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(cfg, qj, budget_s: float = 20.0):
-    """The oracle (C++/OpenMP restatement of the reference kernels) on the host cores."""
+def time_cpu_steps(cfg, qj, steps: int, warmup: int = 0, budget_s: float | None = None):
+    """Wall time of RK3 steps of the oracle (the C++/OpenMP restatement of the
+    reference's kernels) on all host cores; returns (steps timed, seconds, threads)."""
     from oracle import oracle
     threads = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
     oracle.build()
-    cells = cfg.interior_cells()
-    q = qj
+    st = oracle.Stepper(cfg, qj)
+
+    def one():
+        for k in range(st.stages):
+            st.stage(k)
+
+    for _ in range(warmup):
+        one()
     t0 = time.perf_counter()
-    steps = 0
-    while True:
-        q = oracle.step(cfg, q, 1)
-        steps += 1
-        el = time.perf_counter() - t0
-        if el >= budget_s * 0.5 or steps >= 3:
+    n = 0
+    while n < steps:
+        one()
+        n += 1
+        if budget_s is not None and time.perf_counter() - t0 >= budget_s:
             break
-    return {"value": cells * steps / el / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"{steps} full time step(s) of the {cfg.nx}x{cfg.ny}x{cfg.nz} grid "
-                      f"({el:.1f} s, OpenMP over z planes, FP64, no FMA)"}
+    return n, time.perf_counter() - t0, threads
+
+
+def sample_text(cfg, n: int, el: float, extra: str = "") -> str:
+    return (f"{n} RK3 step(s) of z planes 0..{cfg.nz - 7} of the grid: {cfg.nx - 6} x {cfg.ny - 6} x "
+            f"{cfg.nz - 6} interior cells with their ghost layers ({cfg.nx}x{cfg.ny}x{cfg.nz}), the same "
+            f"spacings, scheme and physics; the z ghost planes hold the neighbouring planes' initial values "
+            f"({el:.1f} s, OpenMP over z planes, FP64, no FMA{extra})")
+
+
+def cpu_baseline(args, budget_s: float = 15.0):
+    """The oracle on the host cores, on a bounded block of the same workload."""
+    cfg, qj = cpu_sample(args)
+    n, el, threads = time_cpu_steps(cfg, qj, steps=3, budget_s=budget_s)
+    return {"value": cfg.interior_cells() * n / el / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": sample_text(cfg, n, el)}
 
 
 def bench_ensemble(dev, steps: int, check_steps: int, single_steps: int, count: int = 64, seed: int = 0):
@@ -290,36 +361,28 @@ def bench_serving(dev, count: int, rate: float, budget_gb: float, seed: int = 0)
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU path is the oracle port (the CUDA-Fortran
-    reference has no CPU build and cannot be compiled here)."""
+    """--impl reference: the reference's own path is CUDA Fortran with no CPU build, and
+    it cannot be compiled here (no Fortran compiler, NVHPC, MPI or fypp), so its CPU
+    stand-in is the oracle, the C++/OpenMP restatement of its kernels, on all host cores.
+    Each step is one RK3 step of a block of z planes of the same workload (metric per
+    cell-step).  Nothing here maps liboux.so: the configuration and the initial field
+    come from ouxsbli_b200.config / cases / grid."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    from oracle import oracle
-    oracle.build()
-    threads = os.cpu_count() or 1
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    # bounded sample per step: a 64^3-interior grid of the same physics (a full
-    # 256^3 step takes tens of seconds on the host), metric is per cell-step
-    ns = 64
-    cfg, qj = workload(ns, args.scheme, args.visc)
-    q = qj
-    for _ in range(args.warmup):
-        q = oracle.step(cfg, q, 1)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        q = oracle.step(cfg, q, 1)
-    el = time.perf_counter() - t0
-    val = cfg.interior_cells() * args.steps / el / 1e6
+    cfg, qj = cpu_sample(args)
+    n, el, threads = time_cpu_steps(cfg, qj, steps=args.steps, warmup=args.warmup)
+    val = cfg.interior_cells() * n / el / 1e6
+    p, _, (dx, dy, dz) = tgv_params(args.n)
+    full = make_cfg(args, p, dx, dy, dz)
     line = {"metric": METRIC, "value": val, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "impl": "reference",
-            "config": config_json(args, workload(args.n, args.scheme, args.visc)[0]) | {
-                "sample_grid": [cfg.nx, cfg.ny, cfg.nz]},
+            "warmup": args.warmup, "ms_per_step": el * 1e3 / n,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic TGV initial field)", "impl": "reference",
+            "config": config_json(args, full, world),
             "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} timed steps (+{args.warmup} warm-up) of a "
-                                       f"{ns}^3-interior grid with the same scheme and physics"},
+                             "sample": sample_text(cfg, n, el, f"; after {args.warmup} warm-up step(s)")},
             "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -413,58 +476,6 @@ def run_walls(args):
     return 0
 
 
-def run_large(args):
-    """512^3 supersonic TGV (Ma 1.25, Re 1600, Hybrid-6, ME4 viscous, TVD-RK3): plain FP64
-    against the mixed form over --large-steps steps -- throughput, HBM roofline at
-    320 B / cell-step, per-field error and the enstrophy history and its peak."""
-    import dataclasses
-    import torch
-    from ouxsbli_b200.solver import Solver
-    dev = torch.device("cuda", 0)
-    cfg, qj = workload(512, "Hybrid", "NS", visc_order=6, visc_stencil="ME4Base")
-    cells = cfg.interior_cells()
-    every = 50
-    out = {"workload": "large512", "config": config_json(args, cfg) | {"visc_stencil": "ME4Base"},
-           "steps": args.large_steps, "history_every": every}
-    finals = {}
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    for prec in ("fp64", "mixed"):
-        s = Solver(dataclasses.replace(cfg, precision=prec), dev)
-        s.set_state(qj)
-        st = torch.cuda.current_stream(dev)
-        hist, ms = [s.diagnostics()], 0.0
-        for n in range(0, args.large_steps, every):
-            k = min(every, args.large_steps - n)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(st)
-            s.step(k)
-            b.record(st)
-            b.synchronize()
-            ms += a.elapsed_time(b)
-            hist.append(s.diagnostics())
-        finals[prec] = s.get_state()
-        s.close()
-        v = cells * args.large_steps / (ms / 1e3) / 1e6
-        ens = [h[2] for h in hist]
-        ipk = int(np.argmax(ens))
-        out[prec] = {"value": v, "unit": METRIC, "ms_per_step": ms / args.large_steps,
-                     "hbm_gbs_at_320B": 320.0 * v * 1e6 / 1e9,
-                     "roofline_frac_at_320B": 320.0 * v * 1e6 / 1e9 / float(peaks.get("hbm_gbs", 6650.0)),
-                     "enstrophy_history": ens, "ke_history": [h[0] for h in hist],
-                     "enstrophy_peak": ens[ipk], "enstrophy_peak_step": ipk * every}
-    g = cfg.g
-    sl = (slice(g, -g), slice(None), slice(g, -g), slice(g, -g))
-    a32, a64 = finals["mixed"][sl], finals["fp64"][sl]
-    out["mixed_vs_fp64"] = {
-        "rel_l2": [float(np.linalg.norm(a32[:, l] - a64[:, l]) / np.linalg.norm(a64[:, l])) for l in range(5)],
-        "enstrophy_peak_rel_dev": abs(out["mixed"]["enstrophy_peak"] - out["fp64"]["enstrophy_peak"])
-        / abs(out["fp64"]["enstrophy_peak"]),
-        "speedup": out["mixed"]["value"] / out["fp64"]["value"]}
-    print(json.dumps(out), flush=True)
-    return 0
-
-
 def run_commz(args):
     """The --n^3 workload split into z slabs over the torchrun ranks (one slab per GPU,
     halo exchange over NCCL after every stage, ouxsbli_b200.slabs): whole-grid
@@ -482,7 +493,7 @@ def run_commz(args):
     group = None
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    cfg, qj = workload(args.n, args.scheme, args.visc)
+    cfg, qj = workload(args)
     slab = SlabSolver(cfg, rank, world, dev, group)
     slab.set_global_state(qj)
     stream = torch.cuda.current_stream(dev)
@@ -506,23 +517,84 @@ def run_commz(args):
                           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                           "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
                           "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic TGV initial field)",
-                          "config": config_json(args, cfg) | {"parallelism": f"{world} z slabs (COMMZ)"},
+                          "config": config_json(args, cfg, world) | {"parallelism": f"{world} z slabs (COMMZ)"},
                           "gpu_launches": None}))
     slab.close()
     if world > 1:
         dist.destroy_process_group()
 
 
+# algorithmic HBM bytes per interior cell of each kernel launch (FP64, 3D, RK3 averaged
+# over the three stages): fields read / state and accumulators read and written once
+ALG_CELL = {"prim": 96.0, "sensor": 32.0, "sweep_x": 104.0, "sweep_y": 144.0,
+            "sweep_z": (184.0 + 224.0 + 224.0) / 3.0}
+KINDS = ["prim", "sensor", "sgs", "sgs_edges", "sweep_x", "sweep_y", "sweep_z", "ghost"]
+
+
+def read_profile(h):
+    """Per-kernel CUDA-event times recorded by oux_profile during the timed region."""
+    from ouxsbli_b200 import _lib
+    kms, kcnt = (C.c_double * 8)(), (C.c_int64 * 8)()
+    _lib.check(_lib.LIB.oux_profile_read(h, kms, kcnt, 8))
+    _lib.check(_lib.LIB.oux_profile(h, 0))
+    tot = sum(kms[i] for i in range(8)) or 1.0
+    return {nm: {"launches": int(kcnt[i]), "avg_ms": kms[i] / kcnt[i], "share": kms[i] / tot}
+            for i, nm in enumerate(KINDS) if kcnt[i]}
+
+
+def roofline_of(args, per_kernel, cells, ms_per_step, peaks):
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["share"]) if per_kernel else None
+    achieved = ALG_CELL.get(dom, 0.0) * cells / (per_kernel[dom]["avg_ms"] / 1e3) / 1e9 if dom else 0.0
+    # ncu figures of the same kernels on a small case of the same physics (profiles/):
+    # DRAM bytes per interior cell of one launch, scaled by the cells of one launch here,
+    # and the FP64-pipe utilisation
+    traffic, prof = None, {}
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "sweep_traffic.json"))).get(args.workload, {})
+        if dom in prof.get("dram_bytes_per_interior_cell", {}):
+            traffic = prof["dram_bytes_per_interior_cell"][dom] * cells
+    except Exception:
+        pass
+    step_achieved = ALG_BYTES_PER_CELL_STEP * cells / (ms_per_step / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": dom,
+            "alg_bytes_per_launch": f"{ALG_CELL.get(dom, 0.0):.1f} B x {cells} interior cells "
+                                    "(per-kernel table in DESIGN.md; mean over the 3 RK3 stages)",
+            "traffic_source": prof.get("source"), "fp64_pipe_pct_ncu": prof.get("fp64_pipe_pct"),
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "dominant_kernel": dom, "per_kernel": per_kernel,
+            "step": {"achieved": step_achieved, "frac": step_achieved / peak,
+                     "alg_bytes": "320 B per interior cell-step (8 state accesses x 5 vars x 8 B)"}}
+
+
+def accuracy_run(cfg, qj, dev, steps: int, every: int):
+    """Final state and (step, KE, entropy, enstrophy) history of `steps` steps from qj."""
+    from ouxsbli_b200.solver import Solver
+    s = Solver(cfg, dev)
+    s.set_state(qj)
+    hist = [(0,) + tuple(s.diagnostics())]
+    n = 0
+    while n < steps:
+        k = min(every, steps - n)
+        s.step(k)
+        n += k
+        hist.append((n,) + tuple(s.diagnostics()))
+    status = s.check_state()
+    q = s.get_state()
+    s.close()
+    return q, hist, status
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload == "large512":
-        return run_large(args)
     if args.workload == "walls256":
         return run_walls(args)
     if args.commz:
         return run_commz(args)
+    import dataclasses
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -534,9 +606,15 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     from ouxsbli_b200 import _lib
+    from ouxsbli_b200.replicas import job_rate, max_over_ranks
     from ouxsbli_b200.solver import Solver
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
 
-    cfg, qj = workload(args.n, args.scheme, args.visc)
+    cfg, qj = workload(args)
     s = Solver(cfg, dev)
     s.set_state(qj)
     stream = torch.cuda.current_stream(dev)
@@ -563,12 +641,7 @@ def main():
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     launches_per_step = s.launches() / max(args.steps, 1)
-    kinds = ["prim", "sensor", "sgs", "sgs_edges", "sweep_x", "sweep_y", "sweep_z", "ghost"]
-    kms = (C.c_double * 8)()
-    kcnt = (C.c_int64 * 8)()
-    _lib.check(_lib.LIB.oux_profile_read(s._h, kms, kcnt, 8))
-    _lib.check(_lib.LIB.oux_profile(s._h, 0))
-    from ouxsbli_b200.replicas import job_rate, max_over_ranks
+    per_kernel = read_profile(s._h)
     value, ms_max = job_rate(cells * args.steps, ms, dev)
     value /= 1e6
     ms_per_step = ms_max / args.steps
@@ -580,25 +653,24 @@ def main():
     # engines and the SMs work at the same time); the sequential figure is kept beside it.
     e2e = None
     if not args.no_e2e:
-        import torch as _t
         n_el = qj.size
         lib = _lib.LIB
-        h_in = _t.from_numpy(np.ascontiguousarray(qj.ravel(order="F"))).pin_memory()
+        h_in = torch.from_numpy(np.ascontiguousarray(qj.ravel(order="F"))).pin_memory()
         pin = C.cast(C.c_void_p(h_in.data_ptr()), C.POINTER(C.c_double))
-        NPIPE = 3
+        NPIPE = 2 if n_el * 8 > (2 << 30) else 3
         pipes = [s] + [Solver(cfg, dev) for _ in range(NPIPE - 1)]
         streams = [torch.cuda.Stream(dev) for _ in range(NPIPE)]
-        h_out = [_t.empty(n_el, dtype=_t.float64).pin_memory() for _ in range(NPIPE)]
+        h_out = [torch.empty(n_el, dtype=torch.float64).pin_memory() for _ in range(NPIPE)]
         pouts = [C.cast(C.c_void_p(h.data_ptr()), C.POINTER(C.c_double)) for h in h_out]
         k_e2e = max(NPIPE, args.steps)  # the same step count as the device-timed value
 
         def pipelined(k):
             for n in range(k):
-                p, st = n % NPIPE, streams[n % NPIPE]
+                q, st = n % NPIPE, streams[n % NPIPE]
                 sv_ = C.c_void_p(st.cuda_stream)
-                _lib.check(lib.oux_set_state(pipes[p]._h, pin, sv_))
-                _lib.check(lib.oux_step(pipes[p]._h, 1, sv_))
-                _lib.check(lib.oux_get_state_async(pipes[p]._h, pouts[p], sv_))
+                _lib.check(lib.oux_set_state(pipes[q]._h, pin, sv_))
+                _lib.check(lib.oux_step(pipes[q]._h, 1, sv_))
+                _lib.check(lib.oux_get_state_async(pipes[q]._h, pouts[q], sv_))
 
         def timed_multi(fn, k):
             barrier()
@@ -625,7 +697,7 @@ def main():
                 _lib.check(lib.oux_step(s._h, 1, sv_))
                 _lib.check(lib.oux_get_state(s._h, pouts[0], sv_))  # synchronizes
 
-        k_seq = max(1, min(args.steps, 5))
+        k_seq = max(1, min(args.steps, 3))
         ms_seq = timed_multi(sequential, k_seq)
         # every job advanced the same initial field by one step: all outputs agree
         for st in streams:
@@ -634,6 +706,7 @@ def main():
             raise RuntimeError("pipelined end-to-end jobs disagree")
         for q in pipes[1:]:
             q.close()
+        del pipes, h_out, pouts, h_in
         e2e = {"value": cells * k_e2e * world / (ms_pipe / 1e3) / 1e6, "unit": METRIC,
                "h2d_bytes_per_step": int(n_el * 8), "d2h_bytes_per_step": int(n_el * 8),
                "steps": k_e2e,
@@ -641,113 +714,74 @@ def main():
                        f"host QJ); steps round-robin over {NPIPE} handles / streams",
                "sequential": {"value": cells * k_seq * world / (ms_seq / 1e3) / 1e6, "steps": k_seq,
                               "path": "oux_set_state -> oux_step(1) -> oux_get_state (synchronous), one handle"}}
+    s.close()
+    del s
+    torch.cuda.empty_cache()
 
-    # mixed form on the same workload: throughput and its error against FP64 after
-    # the same number of steps from the same initial field
+    # mixed form on the same workload: throughput, and (one GPU) its error against the
+    # FP64 run after --mixed-check-steps steps from the same initial field
     mixed = None
     if not args.no_mixed:
-        import dataclasses
-        n_err = args.mixed_check_steps or (args.warmup + args.steps)
-        s.set_state(qj)
-        s.step(n_err)
-        q64 = s.get_state()
-        sm = Solver(dataclasses.replace(cfg, precision="mixed"), dev)
+        cfg_m = dataclasses.replace(cfg, precision="mixed")
+        sm = Solver(cfg_m, dev)
         sm.set_state(qj)
         sm.step(args.warmup)
         barrier()
-        barrier()
-        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         _lib.check(_lib.LIB.oux_profile(sm._h, 1))
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         m0.record(stream)
         sm.step(args.steps)
         m1.record(stream)
         barrier()
-        mkms = (C.c_double * 8)()
-        mkcnt = (C.c_int64 * 8)()
-        _lib.check(_lib.LIB.oux_profile_read(sm._h, mkms, mkcnt, 8))
-        _lib.check(_lib.LIB.oux_profile(sm._h, 0))
-        mixed_kernels = {kinds[i]: {"launches": int(mkcnt[i]), "avg_ms": mkms[i] / mkcnt[i]}
-                         for i in range(8) if mkcnt[i]}
-        tm = torch.tensor([max_over_ranks(m0.elapsed_time(m1), dev)], dtype=torch.float64)
-        sm.set_state(qj)
-        sm.step(n_err)
-        q32 = sm.get_state()
-        g = cfg.g
-        sl = (slice(g, -g), slice(None), slice(g, -g), slice(g, -g))
-        a32, a64 = q32[sl], q64[sl]
-        errs = [float(np.linalg.norm((a32[:, l] - a64[:, l]).ravel()) / np.linalg.norm(a64[:, l].ravel()))
-                for l in range(5)]
-        mnorm = np.linalg.norm(a64[:, 1:4].ravel())
-        errs_mom = [float(np.linalg.norm((a32[:, l] - a64[:, l]).ravel()) / mnorm) for l in (1, 2, 3)]
-        d64, d32 = s.diagnostics(), sm.diagnostics()
-        mval = cells * args.steps * world / (float(tm.item()) / 1e3) / 1e6
-        mixed = {"value": mval, "unit": METRIC, "ms_per_step": float(tm.item()) / args.steps,
-                 "speedup_vs_fp64": mval / value,
-                 "rel_l2_vs_fp64": errs, "rel_l2_momentum_vector_norm": errs_mom, "after_steps": n_err,
-                 "ke_rel_dev": abs(d32[0] - d64[0]) / abs(d64[0]),
-                 "enstrophy_rel_dev": abs(d32[2] - d64[2]) / abs(d64[2]),
-                 "per_kernel": mixed_kernels,
+        mixed_kernels = read_profile(sm._h)
+        sm.close()
+        del sm
+        tm = max_over_ranks(m0.elapsed_time(m1), dev)
+        mval = cells * args.steps * world / (tm / 1e3) / 1e6
+        mixed = {"value": mval, "unit": METRIC, "ms_per_step": tm / args.steps,
+                 "speedup_vs_fp64": mval / value, "per_kernel": mixed_kernels,
                  "form": "FP32 stage increments, primitive fields (p, T as deviations from per-solve references) "
                          "and face fluxes; FP64 Q^n, flux differences, RK combinations, diagnostics"}
-        sm.close()
+        if world == 1 and args.mixed_check_steps > 0:
+            n_err, every = args.mixed_check_steps, max(1, args.history_every)
+            q64, h64, st64 = accuracy_run(cfg, qj, dev, n_err, every)
+            q32, h32, st32 = accuracy_run(cfg_m, qj, dev, n_err, every)
+            g = cfg.g
+            sl = (slice(g, -g), slice(None), slice(g, -g), slice(g, -g))
+            a32, a64 = q32[sl], q64[sl]
+            errs = [float(np.linalg.norm((a32[:, l] - a64[:, l]).ravel()) / np.linalg.norm(a64[:, l].ravel()))
+                    for l in range(5)]
+            mnorm = np.linalg.norm(a64[:, 1:4].ravel())
+            errs_mom = [float(np.linalg.norm((a32[:, l] - a64[:, l]).ravel()) / mnorm) for l in (1, 2, 3)]
+            del a32, a64, q32, q64
+            ens64, ens32 = np.array([h[3] for h in h64]), np.array([h[3] for h in h32])
+            ke64, ke32 = np.array([h[1] for h in h64]), np.array([h[1] for h in h32])
+            ipk = int(np.argmax(ens64))
+            mixed |= {"after_steps": n_err, "rel_l2_vs_fp64": errs, "rel_l2_momentum_vector_norm": errs_mom,
+                      "fields": ["rho", "rho u", "rho v", "rho w", "E"],
+                      "ke_rel_dev_final": float(abs(ke32[-1] - ke64[-1]) / abs(ke64[-1])),
+                      "ke_rel_dev_max_over_history": float(np.max(np.abs(ke32 - ke64) / np.abs(ke64))),
+                      "enstrophy_rel_dev_final": float(abs(ens32[-1] - ens64[-1]) / abs(ens64[-1])),
+                      "enstrophy_rel_dev_max_over_history": float(np.max(np.abs(ens32 - ens64) / np.abs(ens64))),
+                      "enstrophy_peak_fp64": {"step": int(h64[ipk][0]), "value": float(ens64[ipk])},
+                      "enstrophy_peak_rel_dev": float(abs(np.max(ens32) - ens64[ipk]) / abs(ens64[ipk])),
+                      "history_every": every, "status_bits": [st64, st32],
+                      "history_fp64": [list(h) for h in h64], "history_mixed": [list(h) for h in h32]}
 
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    per_kernel = {}
-    tot = sum(kms[i] for i in range(8)) or 1.0
-    for i, nm in enumerate(kinds):
-        if kcnt[i]:
-            per_kernel[nm] = {"launches": int(kcnt[i]), "avg_ms": kms[i] / kcnt[i], "share": kms[i] / tot}
-    dom = max(per_kernel, key=lambda k: per_kernel[k]["share"]) if per_kernel else None
-    # algorithmic HBM bytes per interior cell of each kernel launch (FP64, 3D, RK3 averaged
-    # over the three stages): fields read / state and accumulators read and written once
-    alg_cell = {"prim": 96.0, "sensor": 32.0, "sweep_x": 104.0, "sweep_y": 144.0,
-                "sweep_z": (184.0 + 224.0 + 224.0) / 3.0}
-    achieved = alg_cell.get(dom, 0.0) * cells / (per_kernel[dom]["avg_ms"] / 1e3) / 1e9 if dom else 0.0
-    traffic = None
-    try:  # ncu-measured DRAM bytes per interior cell of one z-sweep launch (160^3 capture), scaled
-        tr = json.load(open(os.path.join(ROOT, "profiles", "sweep_z_traffic.json")))
-        if dom == "sweep_z":
-            traffic = tr["dram_bytes_per_interior_cell"] * cells
-    except Exception:
-        pass
-    step_achieved = ALG_BYTES_PER_CELL_STEP * cells / (ms_per_step / 1e3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic,
-                "kernel": "z-direction flux sweep + fused RK combination (k_sweep<3,2,6,C6,noLES,double>)",
-                "alg_bytes_per_launch": f"{alg_cell.get(dom, 0.0):.1f} B x {cells} interior cells "
-                                        "(8 FP64 fields + Racc + Q^n [+ Q^s] read, stage state written; "
-                                        "mean of the 3 RK3 stages)",
-                "traffic_source": "ncu dram__bytes_read+write of one stage-1 z-sweep launch at 160^3 "
-                                  "(bytes per interior cell), scaled by cells",
-                "limiter": "FP64 issue and latency: long-scoreboard stalls at 2 resident blocks/SM (ncu, profiles/)",
-                # the FP64 pipe of the sweeps (ncu --set full captures at 160^3, summarised in profiles/)
-                "fp64_pipe_pct_of_peak_ncu": {"sweep_z": 30.8, "sweep_x": 40.4,
-                                              "source": "profiles/sweep_z_tgv160_hybrid6_ns_fp64.md, "
-                                                        "profiles/sweep_x_tgv160_hybrid6_ns_fp64.md"},
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "dominant_kernel": dom, "per_kernel": per_kernel,
-                "step": {"achieved": step_achieved, "frac": step_achieved / peak,
-                         "alg_bytes": "320 B per interior cell-step (8 state accesses x 5 vars x 8 B)"}}
-
+    roofline = roofline_of(args, per_kernel, cells, ms_per_step, peaks)
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic TGV initial field)",
-            "config": config_json(args, cfg) | {"parallelism": f"{world} independent replicas"},
+            "config": config_json(args, cfg, world),
             "roofline": roofline, "clocks": clk, "e2e": e2e, "mixed": mixed,
             "gpu_launches": int(round(launches_per_step * args.steps))}
-    s.close()
-    # the batched-ensemble and serving sections run on rank 0 (their own GPU) only
-    if rank == 0 and not args.no_ensemble:
+    # the batched-ensemble and serving sections are single-GPU sub-lines (rank 0, N = 1)
+    if rank == 0 and world == 1 and not args.no_ensemble:
         line["ensemble2d"] = bench_ensemble(dev, args.ensemble_steps, 1000, 50)
-    if rank == 0 and not args.no_serving:
+    if rank == 0 and world == 1 and not args.no_serving:
         line["serving"] = bench_serving(dev, args.serving_requests, args.serving_rate, args.serving_budget_gb)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, qj)
+        line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -330,6 +330,12 @@ int oux_batch_destroy(oux_batch* b);
  * rejected with OUX_E_TOO_SMALL and a message giving both sizes; that is about
  * 200 000 cells (59^3 with ghosts) in 3D FP64.
  *
+ * The call has no handle, so it carries no boundary rules (oux_set_boundary):
+ * LES on a grid with a non-periodic direction is refused with OUX_E_INVALID, since
+ * the SGS viscosity of its wall cells depends on those rules.  Euler and
+ * Navier-Stokes grids with non-periodic directions give oux_rhs's result (their
+ * residual reads the boundary cells the caller filled, not the rules).
+ *
  * Inputs: cfg (precision must be OUX_FP64); state_dev, a 256-byte aligned
  * device array in the layout oux_layout_of() reports for cfg (the state buffer
  * of oux_bind, ghost cells already filled), only read.  Output: rhs_dev as for
@@ -337,8 +343,14 @@ int oux_batch_destroy(oux_batch* b);
  * they are page-locked they must stay valid until the stream reaches the call.
  *
  * The first call on a device looks up the array's device address on that
- * device (cudaGetSymbolAddress, once per device, with that device current);
- * make that first call before any stream capture.  Every call on a device
+ * device (cudaGetSymbolAddress, with that device current), and looks it up again
+ * only if the device's context has been made anew since (after cudaDeviceReset).
+ * With lazy module loading (CUDA_MODULE_LOADING=LAZY, the default since CUDA
+ * 12.2) that first call is also when the library's device code is loaded on the
+ * device and the array is created; if another allocator's pool already holds all
+ * free device memory then, it fails with OUX_E_CUDA (out of memory).  So make the
+ * first call on each device at start-up, before such pools fill the device and
+ * before any stream capture.  Every call on a device
  * shares the one array, which keeps the previous call's contents (the call
  * clears what must start at zero), so calls whose GPU work overlaps (other
  * streams, other host threads) race and give wrong results: order them on one

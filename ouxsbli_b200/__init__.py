@@ -21,7 +21,7 @@ _LAZY = {
     "RiemannIC": ("ouxsbli_b200.ic", "RiemannIC"),
     "PeriodicBC": ("ouxsbli_b200.ic", "PeriodicBC"),
     "Solver": ("ouxsbli_b200.solver", "Solver"),
-    "SolverConfig": ("ouxsbli_b200.solver", "SolverConfig"),
+    "SolverConfig": ("ouxsbli_b200.config", "SolverConfig"),
     "build": ("ouxsbli_b200.build", "build"),
 }
 

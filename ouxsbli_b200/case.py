@@ -116,7 +116,7 @@ class Case:
         self._case, self.config, self.globals = case, config, glob
 
     def _solver_config(self, p: dict, dx, dy, dz):
-        from .solver import SolverConfig
+        from .config import SolverConfig
         c = self.config
         return SolverConfig(
             dim=self._case.dim, nx=p["nx"], ny=p["ny"],

@@ -74,7 +74,11 @@ def _tgv_derived(p: dict) -> dict:
     return p
 
 
-def _tgv_init(p: dict, x, y, z) -> np.ndarray:
+def _tgv_init(p: dict, x, y, z, fill: bool = True) -> np.ndarray:
+    """The field on cell centres x, y, z (ghosts included).  fill=False keeps the
+    analytic values in the ghost cells instead of periodic images, for a block of z
+    planes cut out of a larger grid (its ghost planes then hold the neighbouring
+    planes' values, as a z slab's halo does)."""
     nx, ny, nz = x.size, y.size, z.size
     g = p["order"] // 2
     L0, V0, RHO0, p0, R, T0, gam = p["L0"], p["V0"], p["RHO0"], p["p0"], p["R"], p["T"], p["gamma"]
@@ -92,8 +96,15 @@ def _tgv_init(p: dict, x, y, z) -> np.ndarray:
     Q[:, 2] = rv
     Q[:, 3] = 0.0
     Q[:, 4] = pr / (gam - 1.0) + 0.5 * (ru ** 2 + rv ** 2) / rho
-    fill_periodic(Q, g)
+    if fill:
+        fill_periodic(Q, g)
     return Q
+
+
+def tgv_planes(p: dict, xc, yc, zc, k0: int, k1: int) -> np.ndarray:
+    """Q of the Taylor-Green grid `p` (derived parameters, cell centres of the whole
+    grid) on its z planes k0 .. k1-1 only, with analytic ghost values."""
+    return _tgv_init(p, xc, yc, zc[k0:k1], fill=False)
 
 
 # ---------------------------------------------------------------------------
@@ -707,7 +718,7 @@ class VortexMember:
 def vortex_member(m: VortexMember, order: int = 4, **cfg_kw):
     """SolverConfig and initial QJ of one 2D vortex (gamma 1.4, R 1, c_inf = 1)."""
     from .grid import jacobian, to_qj
-    from .solver import SolverConfig
+    from .config import SolverConfig
     nx = m.n + order
     Q = isentropic_vortex(nx, nx, order, m.L, m.beta, m.mach)
     _, dx = cyclic_axis(nx, m.L, order)

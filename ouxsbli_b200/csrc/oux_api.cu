@@ -634,20 +634,59 @@ void stage_array(oux_handle* h, int st, unsigned char** base, size_t* elem) {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[OUX_NOALLOC_SCRATCH_BYTES];
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
-std::atomic<unsigned char*> g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+// Per device: the context the address was looked up in (its driver-assigned id) and
+// the address.  A context made anew on the device (after cudaDeviceReset, or after
+// the primary context was released and retained again) reloads the library's device
+// code, and the array may then sit elsewhere, so a changed id means a new lookup.
+struct NoallocSlot {
+  std::atomic<unsigned long long> ctx{0};
+  std::atomic<unsigned char*> ptr{nullptr};
+};
+NoallocSlot g_noalloc[NOALLOC_MAX_DEVICES];
+
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points (no link
+// against libcuda): the id of the current context, 0 if it cannot be had.
+unsigned long long current_ctx_id() {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetCurrent>(f);
+  }();
+  static GetId get_id = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetId>(f);
+  }();
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 // Device address of g_noalloc_scratch on the current device, looked up once per
-// device (cudaGetSymbolAddress with that device current) and cached.
+// device context (cudaGetSymbolAddress with that device current) and cached.
 int noalloc_scratch(unsigned char** out) {
   int dev = -1;
   OUX_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(OUX_E_INVALID, "device ordinal out of range");
-  unsigned char* p = g_noalloc_ptr[dev].load(std::memory_order_acquire);
-  if (!p) {
+  // the runtime makes the device's primary context current on its first call above
+  const unsigned long long id = current_ctx_id();
+  NoallocSlot& slot = g_noalloc[dev];
+  unsigned char* p = slot.ptr.load(std::memory_order_acquire);
+  if (!p || id == 0 || slot.ctx.load(std::memory_order_acquire) != id) {
     void* a = nullptr;
     OUX_CUDA(cudaGetSymbolAddress(&a, g_noalloc_scratch));
     p = static_cast<unsigned char*>(a);
-    g_noalloc_ptr[dev].store(p, std::memory_order_release);
+    slot.ptr.store(p, std::memory_order_release);
+    slot.ctx.store(id, std::memory_order_release);
   }
   *out = p;
   return OUX_OK;
@@ -1158,6 +1197,11 @@ int oux_rhs_noalloc(const oux_config* cfg, const double* state_dev, double* rhs_
   if ((uintptr_t)state_dev & 255) return fail(OUX_E_INVALID, "state buffer must be 256-byte aligned");
   int vk = visc_kind(cfg, why);
   if (vk < 0) return fail(OUX_E_INVALID, why);
+  // The call has no handle and so no boundary rules: LES on a grid with a
+  // non-periodic face would give the wall cells' SGS viscosity from the default rule
+  // instead of the rule a handle carries (0 on a no-slip wall), so it is refused.
+  if (cfg->visc == OUX_LES && (cfg->bc_x || cfg->bc_y || (cfg->dim == 3 && cfg->bc_z)))
+    return fail(OUX_E_INVALID, "oux_rhs_noalloc: LES needs periodic x, y and z (no boundary rules without a handle)");
   // a handle on the stack: its host tables stay empty (nothing is allocated)
   oux_handle h;
   h.cfg = *cfg;
@@ -1198,6 +1242,7 @@ int oux_rhs_noalloc(const oux_config* cfg, const double* state_dev, double* rhs_
     h.M.dtdy = m;
     h.M.dtdxdy = h.M.dtdydz = h.M.dtdzdx = nullptr;
   }
+  h.G.bjac = h.M.jac;
   // raw spacings staged in the (unused here) stage-state region, then expanded on the device
   double* d = reinterpret_cast<double*>(scratch + P.q2);
   OUX_CUDA(cudaMemcpyAsync(d, cfg->dx, (size_t)(nx - 1) * sizeof(double), cudaMemcpyHostToDevice, s));

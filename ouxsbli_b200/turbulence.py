@@ -48,7 +48,7 @@ def decaying_turbulence(n: int, order: int = 6, seed: int = 0, mt: float = 0.3, 
                         k0: float = 4.0, T0: float = 300.0, R: float = 287.03, gamma: float = 1.4,
                         L0: float = 1.0e-3, cfl: float = 0.5, **cfg_kw):
     """SolverConfig and initial QJ of one decaying-turbulence request."""
-    from .solver import SolverConfig
+    from .config import SolverConfig
     g = order // 2
     nx = n + 2 * g
     L = 2.0 * math.pi * L0

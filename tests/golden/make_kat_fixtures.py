@@ -3,10 +3,10 @@ utilities (ouxsbli/tests/utils/sod_exact.py and oblique_shock.py of the referenc
 checkout), so that this project's independent restatements (tests/sod_exact.py,
 tests/oblique_shock.py) are pinned against them.
 
-Run in a container that holds the reference checkout (it is not needed by the tests,
-which read only the JSON):
+Run where a reference checkout is at hand, giving its root (the tests do not need
+it: they read only the JSON):
 
-    python tests/golden/make_kat_fixtures.py /root/reference
+    python tests/golden/make_kat_fixtures.py <path of the reference checkout>
 """
 from __future__ import annotations
 
@@ -56,4 +56,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_kat_fixtures.py <path of the reference checkout>")
+    main(sys.argv[1])

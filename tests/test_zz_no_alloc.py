@@ -62,6 +62,31 @@ def test_noalloc_matches_rhs_on_calls_in_a_row(cuda_device):
         s.close()
 
 
+@pytest.mark.gpu
+def test_noalloc_matches_rhs_on_stretched_and_walled_grids(cuda_device):
+    """Metric tables built on the device against the host's build_tables where the
+    spacings vary along every axis, and a 2D Navier-Stokes grid with no-slip walls in
+    y (boundary cells filled by the handle first; both calls read the same state)."""
+    import dataclasses
+    cfg, qj = tgv(16, mach=1.25, scheme="Hybrid", visc="NS", visc_stencil="ME4Base")
+    def stretch(d, a):
+        return d * (1.0 + a * np.sin(np.linspace(0.0, 2.0 * np.pi, d.size)))
+    cfg = dataclasses.replace(cfg, dx=stretch(cfg.dx, 0.10), dy=stretch(cfg.dy, 0.07), dz=stretch(cfg.dz, 0.05))
+    wcfg, wqj = vortex2d(24, order=4, scheme="SLAU", visc="NS", rk=3, mach=0.3)
+    wcfg = dataclasses.replace(wcfg, ny=wcfg.ny - 2, dy=wcfg.dy[:-2], bc_y=1,
+                               boundary={"y_lo": "noslip_wall", "y_hi": "slip_wall"})
+    wqj = np.asfortranarray(wqj[:, :, 1:-1])
+    for c, q in ((cfg, qj), (wcfg, wqj)):
+        s = Solver(c, cuda_device)
+        s.set_state(q)
+        s.fill_ghosts()
+        ref = rhs_handle(s)
+        assert np.isfinite(ref).all() and np.abs(ref).max() > 0
+        for _ in range(2):
+            np.testing.assert_array_equal(rhs_noalloc(c, s.state, cuda_device), ref)
+        s.close()
+
+
 def _cfg(n, **kw):
     d = np.full(n - 1, 0.1)
     base = dict(dim=3, nx=n, ny=n, nz=n, order=6, dx=d, dy=d, dz=d, dt=1e-4)
@@ -91,3 +116,9 @@ def test_noalloc_rejects_grids_beyond_the_fixed_scratch():
 def test_noalloc_rejects_mixed_precision():
     rc, msg = _call_without_device(_cfg(16, precision="mixed"))
     assert rc == _lib.OUX_E_INVALID and "FP64" in msg
+
+
+def test_noalloc_rejects_les_with_walls():
+    # no handle means no boundary rules: the SGS viscosity of wall cells would differ
+    rc, msg = _call_without_device(_cfg(16, visc="LES", bc_y=1))
+    assert rc == _lib.OUX_E_INVALID and "LES" in msg
