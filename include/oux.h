@@ -312,6 +312,18 @@ int oux_batch_step(oux_batch* b, int32_t nsteps, void* stream);
 int oux_batch_status(oux_batch* b, int32_t* fault_bits);
 /* Work-list size, phases per step and the persistent grid. */
 int oux_batch_info(const oux_batch* b, int64_t* items, int32_t* phases, int32_t* grid);
+/* Polls a dependency wait of the persistent kernel makes before it gives up,
+ * sets OUX_FAULT_TIMEOUT in the batch status word and ends its block (default
+ * OUX_BATCH_SPIN_LIMIT, 2^22 polls of >= 64 ns).  A captured step is released and
+ * captured anew at the next oux_batch_step.  No counterpart in the reference,
+ * whose kernels never wait on each other. */
+int oux_batch_set_spin_limit(oux_batch* b, int32_t polls);
+/* Byte offset, within the bound workspace, of the dependency record of
+ * (member, phase): two int32, the phase it waits for (-1: none) and the number of
+ * that phase's items it waits for.  For failure-injection tests, which make a wait
+ * run out by raising the count out of reach from the host.  No counterpart in the
+ * reference. */
+int oux_batch_dep_offset(const oux_batch* b, int32_t member, int32_t phase, size_t* offset);
 int oux_batch_destroy(oux_batch* b);
 
 /* --- allocation-free residual ---------------------------------------------

@@ -73,6 +73,8 @@ def _load() -> C.CDLL:
         "oux_batch_step": (C.c_int, [vp, i32, vp]),
         "oux_batch_status": (C.c_int, [vp, C.POINTER(i32)]),
         "oux_batch_info": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]),
+        "oux_batch_set_spin_limit": (C.c_int, [vp, i32]),
+        "oux_batch_dep_offset": (C.c_int, [vp, i32, i32, C.POINTER(C.c_size_t)]),
         "oux_batch_destroy": (C.c_int, [vp]),
     }
     for name, (res, args) in sig.items():

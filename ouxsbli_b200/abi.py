@@ -36,7 +36,8 @@ SYMBOLS = [
     "oux_diagnostics", "oux_check_state", "oux_status", "oux_profile", "oux_profile_read",
     "oux_host_ref_diagnostics", "oux_launch_count", "oux_rhs_noalloc",
     "oux_batch_create", "oux_batch_workspace_bytes", "oux_batch_bind", "oux_batch_step",
-    "oux_batch_status", "oux_batch_info", "oux_batch_destroy",
+    "oux_batch_status", "oux_batch_info", "oux_batch_set_spin_limit", "oux_batch_dep_offset",
+    "oux_batch_destroy",
 ]
 NOALLOC_SCRATCH_BYTES = 32 << 20  # OUX_NOALLOC_SCRATCH_BYTES
 FACES = {"x_lo": 0, "x_hi": 1, "y_lo": 2, "y_hi": 3, "z_lo": 4, "z_hi": 5}  # enum oux_face

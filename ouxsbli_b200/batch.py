@@ -85,6 +85,17 @@ class Batch:
             check(LIB.oux_batch_status(self._b, C.byref(v)))
         return v.value
 
+    def set_spin_limit(self, polls: int) -> None:
+        """Polls a dependency wait makes before it gives up with OUX_FAULT_TIMEOUT."""
+        check(LIB.oux_batch_set_spin_limit(self._b, int(polls)))
+
+    def dep_offset(self, member: int, phase: int) -> int:
+        """Byte offset in `workspace` of the (phase waited for, count) int32 pair of
+        (member, phase) -- for tests that make a wait run out."""
+        off = C.c_size_t()
+        check(LIB.oux_batch_dep_offset(self._b, int(member), int(phase), C.byref(off)))
+        return off.value
+
     def info(self) -> dict:
         items, phases, grid = C.c_int64(), C.c_int32(), C.c_int32()
         check(LIB.oux_batch_info(self._b, C.byref(items), C.byref(phases), C.byref(grid)))

@@ -229,6 +229,15 @@ Geo make_geo(const oux_config& c) {
   G.ylast = 0;
   G.bjac = nullptr;
   for (int f = 0; f < 6; ++f) G.bfix3[f] = nullptr;
+  G.uni = 0;
+  const double* d[3] = {c.dx, c.dy, c.dim == 3 ? c.dz : nullptr};
+  const int n[3] = {c.nx, c.ny, c.dim == 3 ? c.nz : 1};
+  for (int a = 0; a < 3; ++a) {
+    if (!d[a] || n[a] < 2) continue;
+    bool same = true;
+    for (int i = 1; i < n[a] - 1 && same; ++i) same = std::memcmp(&d[a][i], &d[a][0], sizeof(double)) == 0;
+    if (same) G.uni |= 1 << a;
+  }
   G.sx = round_up(c.nx, 4);
   G.plane = G.sx * c.ny;
   G.vs = round_up(G.plane * G.nz, 32);
@@ -515,8 +524,14 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   if (c.scheme != OUX_KEEP) {  // Ducros sensor
     Timed tm(h, KK_SENSOR, s);
     const dim3 gb = plane_grid(G);
-    if (G.dim == 3) k_sensor<3, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
-    else k_sensor<2, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
+    if constexpr (sizeof(T) < sizeof(double)) {
+      const float* dQ = std::is_same<TS, double>::value ? nullptr : reinterpret_cast<const float*>(src);
+      if (G.dim == 3) k_sensor_mx<3><<<gb, PLANE_THREADS, 0, s>>>(G, h->Q, dQ, h->Wf, h->M);
+      else k_sensor_mx<2><<<gb, PLANE_THREADS, 0, s>>>(G, h->Q, dQ, h->Wf, h->M);
+    } else {
+      if (G.dim == 3) k_sensor<3, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
+      else k_sensor<2, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
+    }
     h->launches++;
   }
   if (h->les) {

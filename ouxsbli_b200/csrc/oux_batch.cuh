@@ -16,8 +16,9 @@
 //
 // Progress.  An item only waits on items earlier in the list, which were
 // claimed earlier by blocks that are running, so every wait ends.  Each wait is
-// still bounded: after OUX_BATCH_SPIN_LIMIT polls the block sets
-// OUX_FAULT_TIMEOUT in the batch status word and returns.
+// still bounded: after spin_limit polls (OUX_BATCH_SPIN_LIMIT unless the batch
+// sets another) the block sets OUX_FAULT_TIMEOUT in the batch status word and
+// returns.
 //
 // Memory ordering.  A block publishes an item with __syncthreads, a gpu-scope
 // fence and a relaxed atomic add (release); a waiting block polls with
@@ -62,7 +63,7 @@ constexpr int batch_minb(int dim) { return dim == 2 ? 3 : OUX_BATCH_MINB; }
 
 struct PhaseDesc {
   int kind;
-  int src_qs;  // PH_PRIM: 1 = stage state
+  int src_qs;  // PH_PRIM, PH_SENSOR: 1 = the stage state (else Q^n)
   int last;    // sweeps: 1 = last sweep of the stage (applies the combination)
 };
 
@@ -85,6 +86,7 @@ template <class T> struct BatchArgs {
   int* status;               // OUX_FAULT_TIMEOUT on a wait that gave up
   int nitems, nphases;
   int chunk;                 // cells per point-wise unit
+  int spin_limit;            // polls of a dependency wait before it gives up (OUX_BATCH_SPIN_LIMIT)
 };
 
 __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
@@ -150,7 +152,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, batch_minb(DIM)) k_batch_step(B
           const int* ctr = B.done + bi.inst * B.nphases + d.dep_phase;
           int spins = 0;
           while (ld_acquire_gpu(ctr) < d.dep_count) {
-            if (++spins > OUX_BATCH_SPIN_LIMIT) {
+            if (++spins > B.spin_limit) {
               atomicOr(B.status, BATCH_FAULT_TIMEOUT);
               abort = 1;
               break;
@@ -192,7 +194,12 @@ __global__ void __launch_bounds__(BATCH_THREADS, batch_minb(DIM)) k_batch_step(B
       case PH_SENSOR: {
         if constexpr (!KONLY) {
           const int64_t c1 = batch_end(c0, bi.count, B.chunk, ncell);
-          for (int64_t t = c0 + tid; t < c1; t += BATCH_THREADS) sensor_cell<DIM, T>(G, A.W, A.M, t);
+          if constexpr (sizeof(T) < sizeof(double)) {
+            const float* dQ = ph.src_qs ? reinterpret_cast<const float*>(A.Qs) : nullptr;
+            for (int64_t t = c0 + tid; t < c1; t += BATCH_THREADS) sensor_mx_cell<DIM>(G, A.Qn, dQ, A.W, A.M, t);
+          } else {
+            for (int64_t t = c0 + tid; t < c1; t += BATCH_THREADS) sensor_cell<DIM, T>(G, A.W, A.M, t);
+          }
         }
         break;
       }

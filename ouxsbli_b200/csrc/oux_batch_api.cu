@@ -52,6 +52,7 @@ struct oux_batch {
   BatchArgs<double> B64{};
   BatchArgs<float> B32{};
   int nsm = 0, grid = 0;
+  int spin_limit = OUX_BATCH_SPIN_LIMIT;
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -97,7 +98,7 @@ int build_lists(oux_batch* b) {
   };
   for (int s = 0; s < stages; ++s) {
     add(PH_PRIM, s > 0, 0, s);
-    if (any_sensor) add(PH_SENSOR, 0, 0, s);
+    if (any_sensor) add(PH_SENSOR, s > 0, 0, s);
     if (b->les) { add(PH_MUT, 0, 0, s); add(PH_MUT_EDGES, 0, 0, s); }
     add(PH_SWEEP_X, 0, 0, s);
     if (b->dim == 3) { add(PH_SWEEP_Y, 0, 0, s); add(PH_SWEEP_Z, 0, 1, s); }
@@ -162,6 +163,7 @@ void fill_args(oux_batch* b, BatchArgs<T>& B) {
   B.nitems = (int)b->items.size();
   B.nphases = (int)b->phases.size();
   B.chunk = b->tune.chunk;
+  B.spin_limit = b->spin_limit;
 }
 
 int launch(oux_batch* b, cudaStream_t s, int dry) {
@@ -359,6 +361,25 @@ int oux_batch_info(const oux_batch* b, int64_t* items, int32_t* phases, int32_t*
   if (items) *items = (int64_t)b->items.size();
   if (phases) *phases = (int32_t)b->phases.size();
   if (grid) *grid = b->grid;
+  return OUX_OK;
+}
+
+int oux_batch_set_spin_limit(oux_batch* b, int32_t polls) {
+  if (!b) return fail(OUX_E_INVALID, "null batch");
+  if (polls < 1) return fail(OUX_E_INVALID, "the spin limit must be at least 1 poll");
+  b->spin_limit = polls;
+  b->B64.spin_limit = polls;
+  b->B32.spin_limit = polls;
+  release_graph(b);  // a captured step holds the kernel's arguments: capture anew
+  return OUX_OK;
+}
+
+int oux_batch_dep_offset(const oux_batch* b, int32_t member, int32_t phase, size_t* offset) {
+  if (!b || !offset) return fail(OUX_E_INVALID, "null argument");
+  const int np = (int)b->phases.size();
+  if (member < 0 || member >= (int)b->members.size() || phase < 0 || phase >= np)
+    return fail(OUX_E_INVALID, "member or phase out of range");
+  *offset = b->off_deps + ((size_t)member * np + phase) * sizeof(BatchDep);
   return OUX_OK;
 }
 

@@ -53,6 +53,9 @@ struct Geo {
   int ylast;                  // 1: y faces applied after x faces (corners take their y rule)
   const double* bjac;         // J(nx, ny), for the far-field and Neumann rules
   const double* bfix3[6];     // 3D: fixed values of the faces x lo .. z hi
+  int uni;                    // bit a: every spacing along axis a is the same double (so are
+                              // the inverse spacings), which lets the ME4 sweeps share the
+                              // values of a face position between the three faces using it
   __host__ __device__ int64_t at(int i, int j, int k) const { return (int64_t)k * plane + (int64_t)j * sx + i; }
 };
 
@@ -268,6 +271,82 @@ template <int DIM, class T>
 __global__ void __launch_bounds__(PLANE_THREADS) k_sensor(Geo G, Fields<T> W, Metrics M) {
   int i, j, k;
   if (plane_cell(G, i, j, k)) sensor_cell<DIM, T, false>(G, W, M, i, j, k);
+}
+
+// Mixed form: the sensor from FP64 velocities decoded from Q^n + the FP32 stage
+// increment (dQ, null for the first stage) the way prim_mx_cell decodes them, with the
+// FP64 sensor's arithmetic, rounded once when stored.  The FP32 velocity fields carry
+// relative rounding errors of 6e-8, and the velocity differences of the sensor cancel
+// them into much larger relative errors of the divergence; this way the sensor is the
+// FP64 solve's value for the same state to within one FP32 rounding, so the hybrid
+// threshold and the TVD switch flip only where a face value lies that close to 0.4.
+template <int DIM, bool RO = false>
+__device__ __forceinline__ void sensor_mx_cell(const Geo& G, const double* Qn, const float* dQ,
+                                               const Fields<float>& W, const Metrics& M, int i, int j, int k) {
+  if (i < 1 || i > G.nx - 2 || j < 1 || j > G.ny - 2) return;
+  if (DIM == 3 && (k < 1 || k > G.nz - 2)) return;
+  const int64_t o = G.at(i, j, k);
+  auto q = [&](int64_t c, int l) -> double {
+    const int64_t a = c + l * G.vs;
+    return ldro<RO>(Qn + a) + (dQ ? (double)ldro<RO>(dQ + a) : 0.0);
+  };
+  // velocities of cell c (prim_mx_cell: over = 1 / q0, u = q1 * over)
+  auto vel = [&](int64_t c, double (&v)[3]) {
+    const double over = 1.0 / q(c, 0);
+    v[0] = q(c, 1) * over;
+    v[1] = q(c, 2) * over;
+    v[2] = DIM == 3 ? q(c, 3) * over : 0.0;
+  };
+  const double eps = 1.0e-12;
+  const double dxt = 0.25 * (M.inv_dx[i - 1] + M.inv_dx[i]);
+  const double dyt = 0.25 * (M.inv_dy[j - 1] + M.inv_dy[j]);
+  double f;
+  double xm[3], xp[3], ym[3], yp[3];
+  vel(o - 1, xm);
+  vel(o + 1, xp);
+  vel(o - G.sx, ym);
+  vel(o + G.sx, yp);
+  if constexpr (DIM == 3) {
+    double zm[3], zp[3];
+    vel(o - G.plane, zm);
+    vel(o + G.plane, zp);
+    const double dzt = 0.25 * (M.inv_dz[k - 1] + M.inv_dz[k]);
+    const double dudx = (-xm[0] + xp[0]) * dxt, dvdx = (-xm[1] + xp[1]) * dxt, dwdx = (-xm[2] + xp[2]) * dxt;
+    const double dudy = (-ym[0] + yp[0]) * dyt, dvdy = (-ym[1] + yp[1]) * dyt, dwdy = (-ym[2] + yp[2]) * dyt;
+    const double dudz = (-zm[0] + zp[0]) * dzt, dvdz = (-zm[1] + zp[1]) * dzt, dwdz = (-zm[2] + zp[2]) * dzt;
+    const double div = dudx + dvdy + dwdz;
+    const double r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
+    f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
+  } else {
+    const double dudx = (-xm[0] + xp[0]) * dxt, dvdx = (-xm[1] + xp[1]) * dxt;
+    const double dudy = (-ym[0] + yp[0]) * dyt, dvdy = (-ym[1] + yp[1]) * dyt;
+    const double div = dudx + dvdy;
+    const double rot = dvdx - dudy;
+    f = (div * div) / (div * div + rot * rot + eps);
+  }
+  const float fs = (float)fmin_f(1.0, f);
+  W.sensor[o] = fs;
+  if (i == 1) W.sensor[G.at(0, j, k)] = fs; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = fs;
+  if (j == 1) W.sensor[G.at(i, 0, k)] = fs; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = fs;
+  if constexpr (DIM == 3) {
+    if (k == 1) W.sensor[G.at(i, j, 0)] = fs; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = fs;
+  }
+}
+
+template <int DIM, bool RO = false>
+__device__ __forceinline__ void sensor_mx_cell(const Geo& G, const double* Qn, const float* dQ,
+                                               const Fields<float>& W, const Metrics& M, int64_t t) {
+  int i, j, k;
+  cell_of(G, t, i, j, k);
+  sensor_mx_cell<DIM, RO>(G, Qn, dQ, W, M, i, j, k);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(PLANE_THREADS) k_sensor_mx(Geo G, const double* __restrict__ Qn,
+                                                             const float* __restrict__ dQ, Fields<float> W,
+                                                             Metrics M) {
+  int i, j, k;
+  if (plane_cell(G, i, j, k)) sensor_mx_cell<DIM, true>(G, Qn, dQ, W, M, i, j, k);
 }
 
 // ---- SMS sub-grid model: 3D_solver/src/calc_les.f90:30-125 -------------------

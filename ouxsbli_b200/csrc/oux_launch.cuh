@@ -4,10 +4,15 @@
 
 namespace oux {
 
-template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
+template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool SHARE = false>
 int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
-  constexpr size_t smem = sweep_smem<ORDER, DIR, T>() + sweep_pf_bytes<DIR, T>(sweep_pf_mode<DIM, DIR, T>());
-  auto kern = k_sweep<DIM, DIR, ORDER, VK, LES, T>;
+  // ME4 on an axis of uniform spacing: the shared-position variant of the sweep
+  if constexpr (VK == VK_ME4 && !SHARE) {
+    if ((A.G.uni >> DIR) & 1) return launch_one<DIM, DIR, ORDER, VK, LES, T, true>(A, last, s);
+  }
+  constexpr size_t smem = sweep_smem<ORDER, DIR, T>() + sweep_pf_bytes<DIR, T>(sweep_pf_mode<DIM, DIR, T>()) +
+                          (SHARE ? me4_share_bytes<DIR, T, LES>() : 0);
+  auto kern = k_sweep<DIM, DIR, ORDER, VK, LES, T, SHARE>;
   static const cudaError_t attr_rc =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (attr_rc != cudaSuccess) return 1;

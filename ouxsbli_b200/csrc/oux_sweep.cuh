@@ -48,6 +48,18 @@ __host__ __device__ constexpr size_t sweep_smem() {
          sizeof(double) * 5 * SweepShape<DIR, ROWS>::TX * SweepShape<DIR, ROWS>::TY;
 }
 
+// Terms of one shared ME4 face position (me4_position).
+template <bool LES> __host__ __device__ constexpr int me4_terms() { return LES ? 9 : 7; }
+// Shared ME4 face positions (me4_position): per pencil row 35 positions in the x sweep
+// (the 33 faces' neighbours), 32 x (ROWS + 3) in the y / z sweeps.
+template <int DIR, int ROWS = default_rows<DIR>()> __host__ __device__ constexpr int me4_positions() {
+  return DIR == 0 ? (SweepShape<DIR, ROWS>::TX + 2) * ROWS : 32 * (ROWS + 3);
+}
+template <int DIR, class T, bool LES, int ROWS = default_rows<DIR>()>
+__host__ __device__ constexpr size_t me4_share_bytes() {
+  return sizeof(T) * me4_terms<LES>() * me4_positions<DIR, ROWS>();
+}
+
 // Operand prefetch of a y/z sweep, PF = bit mask: 1 = the combination operands
 // (nv values of Q^n and of Qs or Rs, never needed together), 2 = the accumulator
 // Racc; copied into shared memory when the tile starts.
@@ -312,6 +324,96 @@ __device__ __forceinline__ void visc_high(const StepArgs<T>& A, const Acc& s, in
   out[0] = t[0]; out[1] = t[1]; out[2] = t[2];
   T e = wk[0] + wk[1] + wk[2] + kT;
   if constexpr (LES) e = e + Hs;
+  out[3] = e;
+}
+
+// ---- ME4 with shared face positions ----------------------------------------------
+// ME4 evaluates 4th-order stresses at three face positions (the faces with left cells
+// f-1, f, f+1) and combines them with flux4 (calc_visc_me4_base.f90:4-111); each
+// position serves three neighbouring faces.  On an axis whose spacings are all the
+// same double, a position's terms are the same bits whichever face asks for them, so
+// the sweep evaluates each position once into shared memory and every face combines
+// its three.  me4_position gives the terms of one position from its stencil cells
+// s(field, 0..3) (the position's left cell - 1 .. + 2), with the expression trees of
+// visc_high<VK_ME4> so that the results are bit for bit the same:
+//   0 heat flux k3, 1 normal stress, 2 its work term, 3 / 4 first cross stress and
+//   work term, 5 / 6 second cross stress and work term; LES: 7 mut3, 8 the position's
+//   total-enthalpy difference (used by the face at this position only).
+
+template <bool LES, class T, class Acc>
+__device__ __forceinline__ void me4_position(const StepArgs<T>& A, const Acc& s, int nd, T inv, T v[9]) {
+  const T two3 = T(2.0 / 3.0);
+  const int ca = nd == 0 ? 1 : 0, cb = nd == 2 ? 1 : 2;
+  const int fn = TF_U + nd, fa = TF_U + ca, fb = TF_U + cb;
+  const T mu3 = T(0.0625) * (T(9) * (s(TF_MU, 1) + s(TF_MU, 2)) - (s(TF_MU, 0) + s(TF_MU, 3)));
+  T mut3 = T(0);
+  if constexpr (LES) mut3 = T(0.0625) * (T(9) * (s(TF_MUT, 1) + s(TF_MUT, 2)) - (s(TF_MUT, 0) + s(TF_MUT, 3)));
+  v[0] = T(A.K.Cp_over_Pr) * mu3 *
+         (T(1.125) * (-s(TF_T, 1) + s(TF_T, 2)) - (-s(TF_T, 0) + s(TF_T, 3)) * T(1.0 / 24.0)) * inv;
+  {  // straight
+    const T a0 = s(fn, 0), a1 = s(fn, 1), a2 = s(fn, 2), a3 = s(fn, 3);
+    const T y0 = s(TF_D0, 0), y1 = s(TF_D0, 1), y2 = s(TF_D0, 2), y3 = s(TF_D0, 3);
+    const T z0 = s(TF_D1, 0), z1 = s(TF_D1, 1), z2 = s(TF_D1, 2), z3 = s(TF_D1, 3);
+    const T dd = (T(2.25) * (-a1 + a2) - (-a0 + a3) * T(1.0 / 12.0)) * inv;
+    const T un4 = T(0.0625) * (-a0 + T(9) * (a1 + a2) - a3);
+    if constexpr (!LES) {
+      const T t1 = two3 * mu3 * (dd - T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3) -
+                                 T(0.0625) * (-z0 + T(9) * (z1 + z2) - z3));
+      v[1] = t1;
+      v[2] = un4 * t1;
+    } else {
+      T t1 = dd;
+      t1 = t1 - T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3);
+      t1 = t1 - T(0.0625) * (-z0 + T(9) * (z1 + z2) - z3);
+      v[2] = un4 * (two3 * mu3 * t1);
+      v[1] = two3 * (mu3 + mut3) * t1;
+    }
+  }
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {  // cross terms: fa with D2, fb with D3
+    const int fv = side == 0 ? fa : fb, fd_ = side == 0 ? TF_D2 : TF_D3;
+    const T a0 = s(fv, 0), a1 = s(fv, 1), a2 = s(fv, 2), a3 = s(fv, 3);
+    const T y0 = s(fd_, 0), y1 = s(fd_, 1), y2 = s(fd_, 2), y3 = s(fd_, 3);
+    const T dd = (T(1.125) * (-a1 + a2) - (-a0 + a3) * T(1.0 / 24.0)) * inv;
+    const T v4 = T(0.0625) * (-a0 + T(9) * (a1 + a2) - a3);
+    if constexpr (!LES) {
+      const T t1 = mu3 * (dd + T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3));
+      v[3 + 2 * side] = t1;
+      v[4 + 2 * side] = v4 * t1;
+    } else {
+      T t1 = dd;
+      t1 = t1 + T(0.0625) * (-y0 + T(9) * (y1 + y2) - y3);
+      v[4 + 2 * side] = v4 * (mu3 * t1);
+      v[3 + 2 * side] = (mu3 + mut3) * t1;
+    }
+  }
+  if constexpr (LES) {
+    v[7] = mut3;
+    T H[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const T uu = s(TF_U, m), vv = s(TF_V, m), ww = s(TF_W, m);
+      H[m] = T(A.K.Cp) * s(TF_T, m) + T(0.5) * (uu * uu + vv * vv + ww * ww) + s(TF_QC2, m);
+    }
+    v[8] = T(1.125) * (-H[1] + H[2]) - (-H[0] + H[3]) * T(1.0 / 24.0);
+  }
+}
+
+// The four viscous terms of a face from the terms of its three positions:
+// P(k, q) = term k of position q (0: left cell f-1, 1: f, 2: f+1).
+template <bool LES, class T, class PosAcc>
+__device__ __forceinline__ void me4_face(const StepArgs<T>& A, const PosAcc& P, int nd, T inv, T out[4]) {
+  const int ca = nd == 0 ? 1 : 0, cb = nd == 2 ? 1 : 2;
+  const T kT = flux4(P(0, 0), P(0, 1), P(0, 2));
+  const T tn = flux4(P(1, 0), P(1, 1), P(1, 2)), wn = flux4(P(2, 0), P(2, 1), P(2, 2));
+  const T ta = flux4(P(3, 0), P(3, 1), P(3, 2)), wa = flux4(P(4, 0), P(4, 1), P(4, 2));
+  const T tb = flux4(P(5, 0), P(5, 1), P(5, 2)), wb = flux4(P(6, 0), P(6, 1), P(6, 2));
+  T t[3], wk[3];
+  t[nd] = tn; t[ca] = ta; t[cb] = tb;
+  wk[nd] = wn; wk[ca] = wa; wk[cb] = wb;
+  out[0] = t[0]; out[1] = t[1]; out[2] = t[2];
+  T e = wk[0] + wk[1] + wk[2] + kT;
+  if constexpr (LES) e = e + -flux4(P(7, 0), P(7, 1), P(7, 2)) * P(8, 1) * inv / T(A.K.Prt);
   out[3] = e;
 }
 
@@ -589,8 +691,11 @@ namespace oux {
 // PF: prefetch the cell operands of the combination (Q^n, Qs / Rs; PF = 2: and the
 // accumulator) into shared memory when the tile starts, so their latency overlaps
 // the face fluxes; needs sweep_pf_bytes(PF) more dynamic shared memory.
+// SHARE (ME4 on an axis of uniform spacing): the viscous terms of every face position
+// are evaluated once into shared memory (me4_position) and combined per face
+// (me4_face); needs me4_share_bytes() more dynamic shared memory after the prefetch.
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
-          bool RO = false, bool KONLY = false, int PF = 0>
+          bool RO = false, bool KONLY = false, int PF = 0, bool SHARE = false>
 __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
                                            unsigned char* smraw, int tid, int nthr_all) {
   constexpr int H = ORDER / 2;
@@ -635,6 +740,11 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   T* pfQs = reinterpret_cast<T*>(pfX);
   double* pfRs = pfX;
   double* pfR = pfQn + (PF_C ? 10 : 0) * PFC;
+  static_assert(!SHARE || VK == VK_ME4, "shared face positions are built for the periodic ME4 stencil");
+  constexpr int NPOS = me4_positions<DIR, ROWS>();
+  constexpr int PSTEP = DIR == 0 ? 1 : 32;                // next position along the sweep
+  constexpr int PROW = DIR == 0 ? TX + 2 : 32;            // x sweep: positions per pencil row
+  T* Vs = reinterpret_cast<T*>(smraw + sweep_smem<ORDER, DIR, T, ROWS>() + sweep_pf_bytes<DIR, T, ROWS>(PF));
   const int md = last ? A.mode : CM_ACCUM;
   const bool needQn = (!MXC && (md == CM_RK3_1 || md == CM_RK3_2 || md == CM_RK4_S)) || md == CM_RK3_3 ||
                       md == CM_RK4_4;
@@ -731,7 +841,24 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   }
   __syncthreads();
 
+  // ---- shared ME4 face positions (every thread, strided) ----
+  if constexpr (SHARE) {
+    const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
+    const T inv = (T)invd[DIR][0];  // the axis' spacings are all the same double
+    for (int c = tid; c < NPOS; c += nthr) {
+      // tile index of the position's first stencil cell (its left cell - 1)
+      const int t0 = DIR == 0 ? (c / PROW) * TL + c % PROW : c;
+      auto sp = [&](int field, int m) -> T { return tile[field * NC + t0 + m * PSTEP]; };
+      T v[9];
+      me4_position<LES>(A, sp, DIR, inv, v);
+#pragma unroll
+      for (int q = 0; q < me4_terms<LES>(); ++q) Vs[q * NPOS + c] = v[q];
+    }
+  }
+
   // ---- faces ----
+  bool face_valid = false;
+  int face_pos = 0;  // SHARE: position index of the face's left neighbour position
   {
     int fc[3] = {bx0, by0, bz0};  // left cell of this thread's face
     int base, step;
@@ -748,6 +875,8 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     }
     const int f = fc[DIR];
     const bool valid = act && rowok && f >= (DIR == 0 ? gx : DIR == 1 ? gy : gz) - 1 && f <= ext[DIR] - 1;
+    face_valid = valid;
+    face_pos = DIR == 0 ? ty * PROW + tx : ty * 32 + tx;
     if (valid) {
       T F[5];
       // tile position of cell f + off is base + (2 + off) * step
@@ -780,7 +909,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       } else {
         conv_flux<ORDER, KONLY>(A, sc, fd, DIR, F);
       }
-      if constexpr (VK != VK_EULER) {
+      if constexpr (VK != VK_EULER && !SHARE) {
         T vo[4];
         const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
         const T inv = (T)invd[DIR][f];
@@ -836,6 +965,23 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     }
   }
   __syncthreads();
+
+  // ---- shared ME4: each face combines its three positions ----
+  if constexpr (SHARE) {
+    if (face_valid) {
+      const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
+      const T inv = (T)invd[DIR][0];
+      auto P = [&](int k, int q) -> T { return Vs[k * NPOS + face_pos + q * PSTEP]; };
+      T vo[4];
+      me4_face<LES>(A, P, DIR, inv, vo);
+      // F[l] - vo in the compute type, as the unshared path does
+      Fs[1 * (TX * TY) + tid] = (double)((T)Fs[1 * (TX * TY) + tid] - vo[0]);
+      Fs[2 * (TX * TY) + tid] = (double)((T)Fs[2 * (TX * TY) + tid] - vo[1]);
+      if constexpr (DIM == 3) Fs[3 * (TX * TY) + tid] = (double)((T)Fs[3 * (TX * TY) + tid] - vo[2]);
+      Fs[4 * (TX * TY) + tid] = (double)((T)Fs[4 * (TX * TY) + tid] - vo[3]);
+    }
+    __syncthreads();
+  }
 
   // ---- cells: difference, accumulate, combine ----
   if (!act) return;
@@ -968,12 +1114,12 @@ template <int DIR> __host__ __device__ constexpr int sweep_threads() {
   return (SweepShape<DIR>::TX * SweepShape<DIR>::TY + 31) / 32 * 32;
 }
 
-template <int DIM, int DIR, int ORDER, int VK, bool LES, class T>
+template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool SHARE = false>
 __global__ void __launch_bounds__(sweep_threads<DIR>(), DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
 k_sweep(StepArgs<T> A, int last) {
   extern __shared__ __align__(16) unsigned char smraw[];
   // coherent loads: measured as fast as the read-only path for y/z and faster for x
-  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>()>(
+  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>(), SHARE>(
       A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.x, sweep_threads<DIR>());
 }
 

@@ -136,3 +136,36 @@ def test_batch_graph_mode_bitexact(precision, cuda_device):
     cases2 = vortex_ensemble()
     for x, y in zip(singles(cases2, 5, cuda_device), batched(cases2, 5, cuda_device, Tuning(mode="graph"))):
         np.testing.assert_array_equal(x, y)
+
+
+def test_batch_dependency_wait_runs_out(cuda_device):
+    """A dependency count that the work list can never reach, planted in the bound
+    workspace from the host, makes every wait on it run out after the batch's spin
+    limit: the kernel sets OUX_FAULT_TIMEOUT in the batch status word and its blocks
+    return (no trap, no hang), and the device stays usable for the next batch."""
+    import torch
+    from ouxsbli_b200 import _lib
+    cases = vortex_ensemble()[:2]
+    solvers = []
+    for cfg, qj in cases:
+        s = Solver(cfg, cuda_device)
+        s.set_state(qj)
+        solvers.append(s)
+    b = Batch(solvers, Tuning())
+    b.set_spin_limit(64)
+    # phase 1 of member 0 (its first x sweep) waits for all items of phase 0 (primitives)
+    off = b.dep_offset(0, 1)
+    dep = b.workspace[off:off + 8].view(torch.int32)
+    assert int(dep[0]) == 0 and int(dep[1]) > 0
+    dep[1] = 1 << 30
+    b.step(1)
+    torch.cuda.synchronize(cuda_device)
+    assert b.status() & _lib.FAULT_TIMEOUT
+    b.close()
+    for s in solvers:
+        s.close()
+    # a fresh batch on the same device steps cleanly and matches the single solves
+    want = singles(cases, 2, cuda_device)
+    got = batched(cases, 2, cuda_device)
+    for x, y in zip(want, got):
+        np.testing.assert_array_equal(x, y)
