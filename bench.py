@@ -351,13 +351,34 @@ def bench_serving(dev, count: int, rate: float, budget_gb: float, seed: int = 0)
     for s in rep:
         s.close()
     reqs = poisson_stream(count, rate, seed)
+    # the same requests one after another, each alone (device time per step of each grid
+    # size, measured after 3 warm-up steps): the rate without batching and host gaps
+    import torch
+    st = torch.cuda.current_stream(dev)
+    ms_per_step = {}
+    for n in sorted({r.n for r in reqs}):
+        cfg, qj = SolveRequest(rid=0, n=n, steps=1, seed=1).build(srv.physics)
+        s = Solver(cfg, dev)
+        s.set_state(qj)
+        s.step(3)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.step(20)
+        b.record(st)
+        b.synchronize()
+        ms_per_step[n] = a.elapsed_time(b) / 20
+        s.close()
+    solo_ms = sum(r.steps * ms_per_step[r.n] for r in reqs)
+    solo_rate = sum(r.n ** 3 * r.steps for r in reqs) / (solo_ms / 1e3) / 1e6
     res = srv.run(reqs)
     return summarize(res) | {"unit_latency": "s", "arrival_rate_per_s": rate, "hbm_budget_gb": budget_gb,
                              "grids": sorted({r.n for r in reqs}), "steps_range": [200, 2000],
                              "physics": "SLAU-6 HRSLAU2, SMS LES, TVD-RK3, mixed FP32/FP64",
                              "tuning": dataclasses.asdict(chosen),
                              "tuning_trials_ms_per_step": {t[1]["mode"] + (f"-p{t[1]['pencil']}" if t[1]["mode"] == "persistent" else ""): t[0] for t in trials},
-                             "server": srv.stats}
+                             "server": srv.stats,
+                             "solo_one_after_another": {"aggregate_mcell_steps_per_s": solo_rate,
+                                                        "device_ms_per_step_by_grid": ms_per_step}}
 
 
 def run_reference(args):
@@ -445,7 +466,7 @@ def run_walls(args):
     from ouxsbli_b200 import _lib
     from ouxsbli_b200.solver import Solver
     dev = torch.device("cuda", 0)
-    kinds = ["prim", "sensor", "sgs", "sgs_edges", "sweep_x", "sweep_y", "sweep_z", "ghost"]
+    kinds = KINDS
     out = {"workload": "walls256", "n": args.n, "steps": args.steps, "warmup": args.warmup,
            "config": "KEEP-6, Central-6 NS, RK3, FP64; u = 5 sin(pi y / H) m/s shear layer of air, H = 1 mm",
            "grids": {}}
@@ -463,8 +484,8 @@ def run_walls(args):
         s.step(args.steps)
         b.record(st)
         b.synchronize()
-        kms, kcnt = (C.c_double * 8)(), (C.c_int64 * 8)()
-        _lib.check(_lib.LIB.oux_profile_read(s._h, kms, kcnt, 8))
+        kms, kcnt = (C.c_double * len(kinds))(), (C.c_int64 * len(kinds))()
+        _lib.check(_lib.LIB.oux_profile_read(s._h, kms, kcnt, len(kinds)))
         _lib.check(_lib.LIB.oux_profile(s._h, 0))
         ms = a.elapsed_time(b) / max(args.steps, 1)
         out["grids"][which] = {
@@ -526,18 +547,22 @@ def run_commz(args):
 
 # algorithmic HBM bytes per interior cell of each kernel launch (FP64, 3D, RK3 averaged
 # over the three stages): fields read / state and accumulators read and written once
-ALG_CELL = {"prim": 96.0, "sensor": 32.0, "sweep_x": 104.0, "sweep_y": 144.0,
-            "sweep_z": (184.0 + 224.0 + 224.0) / 3.0}
-KINDS = ["prim", "sensor", "sgs", "sgs_edges", "sweep_x", "sweep_y", "sweep_z", "ghost"]
+ALG_CELL = {"prim": 96.0, "sensor": 32.0, "prim_sensor": 104.0, "grad": 96.0,
+            "sweep_x": 136.0, "sweep_y": 176.0, "sweep_z": (216.0 + 256.0 + 256.0) / 3.0}
+# kernel kinds of oux_profile_read (enum KernelKind of oux_api.cu); prim_sensor: the fused
+# primitives + Ducros sensor pass of 3D stages with a sensor scheme; grad: the node
+# velocity gradients of the high-order viscous stencils
+KINDS = ["prim", "sensor", "sgs", "sgs_edges", "sweep_x", "sweep_y", "sweep_z", "ghost", "prim_sensor", "grad"]
 
 
 def read_profile(h):
     """Per-kernel CUDA-event times recorded by oux_profile during the timed region."""
     from ouxsbli_b200 import _lib
-    kms, kcnt = (C.c_double * 8)(), (C.c_int64 * 8)()
-    _lib.check(_lib.LIB.oux_profile_read(h, kms, kcnt, 8))
+    n = len(KINDS)
+    kms, kcnt = (C.c_double * n)(), (C.c_int64 * n)()
+    _lib.check(_lib.LIB.oux_profile_read(h, kms, kcnt, n))
     _lib.check(_lib.LIB.oux_profile(h, 0))
-    tot = sum(kms[i] for i in range(8)) or 1.0
+    tot = sum(kms[i] for i in range(n)) or 1.0
     return {nm: {"launches": int(kcnt[i]), "avg_ms": kms[i] / kcnt[i], "share": kms[i] / tot}
             for i, nm in enumerate(KINDS) if kcnt[i]}
 

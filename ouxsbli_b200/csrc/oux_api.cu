@@ -251,13 +251,22 @@ struct ScratchPlan {
 
 constexpr int DIAG_BLOCKS = 1184;  // 8 blocks per SM on 148 SMs; fixed for a deterministic sum
 
+// Whether a configuration's sweeps read the node velocity gradients from fields
+// (k_grad; sweep_uses_grads): periodic 3D grids with Central-4/6 or ME4 viscous stencils.
+bool uses_grads(const oux_config& c) {
+  std::string why;
+  const int vk = visc_kind(&c, why);
+  return c.dim == 3 && (vk == VK_C6 || vk == VK_C4 || vk == VK_ME4);
+}
+
 ScratchPlan plan_scratch(const oux_config& c) {
   Geo G = make_geo(c);
   int nv = c.dim + 2;
   ScratchPlan P;
   size_t vsb = (size_t)G.vs * sizeof(double);
   size_t vse = (size_t)G.vs * (c.precision == OUX_MIXED ? sizeof(float) : sizeof(double));
-  P.nfield_arrays = 10;  // rho,u,v,w,p,T,mu,sensor,mut,qc2
+  // rho,u,v,w,p,T,mu,sensor,mut,qc2 [+ the 9 velocity gradients]
+  P.nfield_arrays = uses_grads(c) ? 19 : 10;
   size_t off = 0;
   P.fields = off; off += round_up((size_t)P.nfield_arrays * vse, 256);
   P.racc = off; off += (size_t)nv * vsb;
@@ -421,12 +430,12 @@ void carve(oux_handle* h) {
     double* f = reinterpret_cast<double*>(h->scratch + P.fields);
     double** fp[10] = {&h->W.rho, &h->W.u, &h->W.v, &h->W.w, &h->W.p, &h->W.T_, &h->W.mu, &h->W.sensor, &h->W.mut, &h->W.qc2};
     for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
-    for (int q = 0; q < 9; ++q) h->W.grad[q] = nullptr;
+    for (int q = 0; q < 9; ++q) h->W.grad[q] = P.nfield_arrays == 19 ? f + (10 + q) * vsb : nullptr;
   } else {
     float* f = reinterpret_cast<float*>(h->scratch + P.fields);
     float** fp[10] = {&h->Wf.rho, &h->Wf.u, &h->Wf.v, &h->Wf.w, &h->Wf.p, &h->Wf.T_, &h->Wf.mu, &h->Wf.sensor, &h->Wf.mut, &h->Wf.qc2};
     for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
-    for (int q = 0; q < 9; ++q) h->Wf.grad[q] = nullptr;
+    for (int q = 0; q < 9; ++q) h->Wf.grad[q] = P.nfield_arrays == 19 ? f + (10 + q) * vsb : nullptr;
   }
   h->Racc = reinterpret_cast<double*>(h->scratch + P.racc);
   h->Qs = h->scratch + P.q2;
@@ -457,7 +466,8 @@ void carve(oux_handle* h) {
 }
 
 // kinds reported by oux_profile_read
-enum KernelKind { KK_PRIM = 0, KK_SENSOR, KK_MUT, KK_MUT_EDGES, KK_SWEEP_X, KK_SWEEP_Y, KK_SWEEP_Z, KK_GHOST, KK_COUNT };
+enum KernelKind { KK_PRIM = 0, KK_SENSOR, KK_MUT, KK_MUT_EDGES, KK_SWEEP_X, KK_SWEEP_Y, KK_SWEEP_Z, KK_GHOST,
+                  KK_PRIM_SENSOR, KK_GRAD, KK_COUNT };
 
 struct Timed {
   oux_handle* h;
@@ -497,7 +507,20 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   Fields<T>& W = fields_of<T>(h);
   int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
   bool visc = c.visc != OUX_EULER;
-  {
+  if (G.dim == 3 && c.scheme != OUX_KEEP) {
+    // primitives and sensor in one z-marching pass
+    Timed tm(h, KK_PRIM_SENSOR, s);
+    const dim3 gb = prim_sensor_grid(G);
+    if constexpr (sizeof(T) < sizeof(double)) {
+      const float* dQ = std::is_same<TS, double>::value ? nullptr : reinterpret_cast<const float*>(src);
+      if (visc) k_prim_sensor<true, true, double, float><<<gb, PS_TX * PS_TY, 0, s>>>(h->Q, dQ, G, h->Wf, h->M, h->K);
+      else k_prim_sensor<false, true, double, float><<<gb, PS_TX * PS_TY, 0, s>>>(h->Q, dQ, G, h->Wf, h->M, h->K);
+    } else {
+      if (visc) k_prim_sensor<true, false, TS, T><<<gb, PS_TX * PS_TY, 0, s>>>(src, nullptr, G, W, h->M, h->K);
+      else k_prim_sensor<false, false, TS, T><<<gb, PS_TX * PS_TY, 0, s>>>(src, nullptr, G, W, h->M, h->K);
+    }
+    h->launches++;
+  } else {
     Timed tm(h, KK_PRIM, s);
     const dim3 gb = plane_grid(G);
     if constexpr (sizeof(T) < sizeof(double)) {
@@ -519,9 +542,9 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
         else k_prim<2, false, TS, T><<<gb, PLANE_THREADS, 0, s>>>(src, G, W, h->M.jac, h->K);
       }
     }
+    h->launches++;
   }
-  h->launches++;
-  if (c.scheme != OUX_KEEP) {  // Ducros sensor
+  if (G.dim == 2 && c.scheme != OUX_KEEP) {  // Ducros sensor (3D: fused above)
     Timed tm(h, KK_SENSOR, s);
     const dim3 gb = plane_grid(G);
     if constexpr (sizeof(T) < sizeof(double)) {
@@ -532,6 +555,13 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
       if (G.dim == 3) k_sensor<3, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
       else k_sensor<2, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
     }
+    h->launches++;
+  }
+  if (W.grad[0]) {  // node velocity gradients for the high-order viscous stencils
+    Timed tm(h, KK_GRAD, s);
+    const dim3 gb = plane_grid(G);
+    if (h->vk == VK_C6) k_grad<true, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
+    else k_grad<false, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
     h->launches++;
   }
   if (h->les) {

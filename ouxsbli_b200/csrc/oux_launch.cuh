@@ -6,8 +6,11 @@ namespace oux {
 
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool SHARE = false>
 int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
-  // ME4 on an axis of uniform spacing: the shared-position variant of the sweep
-  if constexpr (VK == VK_ME4 && !SHARE) {
+  // ME4 on an axis of uniform spacing: the shared-position variant of the x and y
+  // sweeps (measured on B200 at 512^3: y 9.98 -> 9.66 ms, x unchanged; the z sweep,
+  // whose operand prefetch already holds 82 KB of shared memory per block, lost L1
+  // capacity to the extra 20 KB and ran slower, 11.1 -> 14.3 ms)
+  if constexpr (VK == VK_ME4 && !SHARE && DIR < 2) {
     if ((A.G.uni >> DIR) & 1) return launch_one<DIM, DIR, ORDER, VK, LES, T, true>(A, last, s);
   }
   constexpr size_t smem = sweep_smem<ORDER, DIR, T>() + sweep_pf_bytes<DIR, T>(sweep_pf_mode<DIM, DIR, T>()) +

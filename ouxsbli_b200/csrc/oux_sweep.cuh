@@ -694,8 +694,10 @@ namespace oux {
 // SHARE (ME4 on an axis of uniform spacing): the viscous terms of every face position
 // are evaluated once into shared memory (me4_position) and combined per face
 // (me4_face); needs me4_share_bytes() more dynamic shared memory after the prefetch.
+// GR: the transverse node derivatives are staged from the gradient fields W.grad
+// (k_grad) instead of being differenced from the velocities in the tile load.
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
-          bool RO = false, bool KONLY = false, int PF = 0, bool SHARE = false>
+          bool RO = false, bool KONLY = false, int PF = 0, bool SHARE = false, bool GR = false>
 __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
                                            unsigned char* smraw, int tid, int nthr_all) {
   constexpr int H = ORDER / 2;
@@ -804,7 +806,15 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       tile[TF_MUT * NC + c] = ldro<RO>(A.W.mut + o);
       tile[TF_QC2 * NC + c] = ldro<RO>(A.W.qc2 + o);
     }
-    if constexpr (HIGH) {  // transverse node derivatives (the viscous loaders' stencils)
+    if constexpr (HIGH && GR) {  // transverse node derivatives from the gradient fields
+      static_assert(DIM == 3 && !WALL, "gradient fields are built for periodic 3D grids");
+      constexpr int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
+      constexpr int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
+      tile[TF_D0 * NC + c] = ldro<RO>(A.W.grad[3 * a1 + a1] + o);
+      tile[TF_D1 * NC + c] = ldro<RO>(A.W.grad[3 * a2 + a2] + o);
+      tile[TF_D2 * NC + c] = ldro<RO>(A.W.grad[3 * n + ca] + o);
+      tile[TF_D3 * NC + c] = ldro<RO>(A.W.grad[3 * n + cb] + o);
+    } else if constexpr (HIGH) {  // transverse node derivatives (the viscous loaders' stencils)
       const T* vel[3] = {A.W.u, A.W.v, A.W.w};
       const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
       if constexpr (DIM == 3) {
@@ -1114,13 +1124,20 @@ template <int DIR> __host__ __device__ constexpr int sweep_threads() {
   return (SweepShape<DIR>::TX * SweepShape<DIR>::TY + 31) / 32 * 32;
 }
 
+// Single-solve sweeps of periodic 3D grids with a high-order viscous stencil read the
+// transverse node derivatives from the gradient fields (k_grad runs before them).
+template <int DIM, int VK> __host__ __device__ constexpr bool sweep_uses_grads() {
+  return DIM == 3 && (VK == VK_C6 || VK == VK_C4 || VK == VK_ME4);
+}
+
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool SHARE = false>
 __global__ void __launch_bounds__(sweep_threads<DIR>(), DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
 k_sweep(StepArgs<T> A, int last) {
   extern __shared__ __align__(16) unsigned char smraw[];
   // coherent loads: measured as fast as the read-only path for y/z and faster for x
-  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>(), SHARE>(
-      A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.x, sweep_threads<DIR>());
+  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>(), SHARE,
+             sweep_uses_grads<DIM, VK>()>(A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.x,
+                                           sweep_threads<DIR>());
 }
 
 }  // namespace oux

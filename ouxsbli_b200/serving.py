@@ -142,7 +142,24 @@ class Server:
         dirty = True
         steps_run = quanta = 0
         peak_bytes = peak_active = 0
+        # where the wall time goes (host seconds per part of the loop, device time of the quanta)
+        split = {"arrivals_s": 0.0, "admit_s": 0.0, "batch_build_s": 0.0, "step_enqueue_s": 0.0,
+                 "wait_device_s": 0.0, "retire_s": 0.0, "idle_s": 0.0}
+        gpu_ms = 0.0
+        stream = torch.cuda.current_stream(dev)
+
+        class _Part:
+            def __init__(self, key):
+                self.key = key
+
+            def __enter__(self):
+                self.t = time.perf_counter()
+
+            def __exit__(self, *exc):
+                split[self.key] += time.perf_counter() - self.t
+
         t0 = clock()
+        wall0 = time.perf_counter()
 
         def arrivals(now: float) -> None:
             # build the initial fields of every request that has arrived (host work)
@@ -155,52 +172,67 @@ class Server:
                 queue.append((r, cfg, qj, need))
 
         while pending or queue or active:
-            arrivals(clock() - t0)
+            with _Part("arrivals_s"):
+                arrivals(clock() - t0)
             # admission: FIFO while memory and slots allow
-            while queue and len(active) < self.max_active and used + queue[0][3] <= self.hbm_budget:
-                r, cfg, qj, need = queue.pop(0)
-                s = Solver(cfg, dev)
-                s.set_state(qj)
-                active.append(_Active(r, s, need, r.steps, clock() - t0))
-                used += need
-                dirty = True
+            with _Part("admit_s"):
+                while queue and len(active) < self.max_active and used + queue[0][3] <= self.hbm_budget:
+                    r, cfg, qj, need = queue.pop(0)
+                    s = Solver(cfg, dev)
+                    s.set_state(qj)
+                    active.append(_Active(r, s, need, r.steps, clock() - t0))
+                    used += need
+                    dirty = True
             peak_bytes = max(peak_bytes, used)
             peak_active = max(peak_active, len(active))
             if not active:
                 if pending:
-                    sleep(max(0.0, min(pending[0].arrival - (clock() - t0), 0.05)))
+                    with _Part("idle_s"):
+                        sleep(max(0.0, min(pending[0].arrival - (clock() - t0), 0.05)))
                 continue
             if dirty:
-                if batch is not None:
-                    batch.close()
-                solvers = [a.solver for a in active]
-                batch = Batch(solvers, self._tuning(solvers))
-                dirty = False
+                with _Part("batch_build_s"):
+                    if batch is not None:
+                        batch.close()
+                    solvers = [a.solver for a in active]
+                    batch = Batch(solvers, self._tuning(solvers))
+                    dirty = False
             k = min(self.quantum, min(a.remaining for a in active))
-            batch.step(k)                      # asynchronous on the device
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with _Part("step_enqueue_s"):
+                e0.record(stream)
+                batch.step(k)                      # asynchronous on the device
+                e1.record(stream)
             steps_run += k
             quanta += 1
-            arrivals(clock() - t0)             # overlaps the quantum
-            torch.cuda.current_stream(dev).synchronize()
+            with _Part("arrivals_s"):
+                arrivals(clock() - t0)             # overlaps the quantum
+            with _Part("wait_device_s"):
+                stream.synchronize()
+            gpu_ms += e0.elapsed_time(e1)
             done_t = clock() - t0
             keep = []
-            for a in active:
-                a.remaining -= k
-                if a.remaining > 0:
-                    keep.append(a)
-                    continue
-                st = a.solver.get_state() if self.keep_states else None
-                results.append(SolveResult(a.req.rid, a.req.n, a.req.steps, a.req.arrival, a.admitted, done_t,
-                                           a.solver.diagnostics(), st))
-                a.solver.close()
-                used -= a.bytes
-                dirty = True
-            if dirty and batch is not None:
-                batch.close()
-                batch = None
+            with _Part("retire_s"):
+                for a in active:
+                    a.remaining -= k
+                    if a.remaining > 0:
+                        keep.append(a)
+                        continue
+                    st = a.solver.get_state() if self.keep_states else None
+                    results.append(SolveResult(a.req.rid, a.req.n, a.req.steps, a.req.arrival, a.admitted, done_t,
+                                               a.solver.diagnostics(), st))
+                    a.solver.close()
+                    used -= a.bytes
+                    dirty = True
+                if dirty and batch is not None:
+                    batch.close()
+                    batch = None
             active = keep
         if batch is not None:
             batch.close()
+        wall = time.perf_counter() - wall0
         self.stats = {"batched_steps": steps_run, "quanta": quanta, "wall_s": clock() - t0,
-                      "peak_bytes": peak_bytes, "peak_active": peak_active}
+                      "peak_bytes": peak_bytes, "peak_active": peak_active,
+                      "split": {"host_wall_s": wall, "device_busy_s": gpu_ms / 1e3,
+                                "device_busy_frac": gpu_ms / 1e3 / max(wall, 1e-9)} | split}
         return sorted(results, key=lambda r: r.rid)
