@@ -252,7 +252,8 @@ struct ScratchPlan {
 constexpr int DIAG_BLOCKS = 1184;  // 8 blocks per SM on 148 SMs; fixed for a deterministic sum
 
 // Whether a configuration's sweeps read the node velocity gradients from fields
-// (k_grad; sweep_uses_grads): periodic 3D grids with Central-4/6 or ME4 viscous stencils.
+// (k_prim_fused writes them; sweep_uses_grads): periodic 3D grids with Central-4/6 or ME4
+// viscous stencils.
 bool uses_grads(const oux_config& c) {
   std::string why;
   const int vk = visc_kind(&c, why);
@@ -467,7 +468,7 @@ void carve(oux_handle* h) {
 
 // kinds reported by oux_profile_read
 enum KernelKind { KK_PRIM = 0, KK_SENSOR, KK_MUT, KK_MUT_EDGES, KK_SWEEP_X, KK_SWEEP_Y, KK_SWEEP_Z, KK_GHOST,
-                  KK_PRIM_SENSOR, KK_GRAD, KK_COUNT };
+                  KK_PRIM_FUSED, KK_COUNT };
 
 struct Timed {
   oux_handle* h;
@@ -498,6 +499,39 @@ int launch_sweeps_t<float>(int dim, int order, int vk, bool les, int dir, const 
   return dir < 0 ? launch_sweeps_mx(dim, order, vk, les, A, s) : launch_sweep_dir_mx(dim, order, vk, les, dir, A, s);
 }
 
+// k_prim_fused with the ring width hd (1: sensor only; 2 / 3: gradients of 4th / 6th
+// order), on `q` (FP64 form: the stage source; mixed form: Q^n, with the FP32 increment
+// `inc` unless the source is Q^n itself).
+template <int HD, bool SENS, bool VISC, bool MX, class TQ, class T>
+int launch_prim_fused_t(const TQ* q, const float* inc, const Geo& G, Fields<T>& W, oux_handle* h, cudaStream_t s) {
+  constexpr size_t smem = prim_fused_smem<HD>();
+  auto kern = k_prim_fused<HD, SENS, VISC, MX, TQ, T>;
+  static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (attr != cudaSuccess) return 1;
+  kern<<<prim_fused_grid(G), PS_TX * PS_TY, smem, s>>>(q, inc, G, W, h->M, h->K);
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
+}
+
+template <class TQ, class T, class TS>
+int launch_prim_fused(int hd, bool sens, bool visc, const TQ* q, const TS* src, const Geo& G, Fields<T>& W,
+                      oux_handle* h, cudaStream_t s) {
+  const float* inc = nullptr;
+  if constexpr (sizeof(T) < sizeof(double)) {
+    if (!std::is_same<TS, double>::value) inc = reinterpret_cast<const float*>(src);
+  }
+  constexpr bool MX = sizeof(T) < sizeof(double);
+  if (hd == 1) {
+    if (visc) return launch_prim_fused_t<1, true, true, MX>(q, inc, G, W, h, s);
+    return launch_prim_fused_t<1, true, false, MX>(q, inc, G, W, h, s);
+  }
+  if (hd == 2) {
+    if (sens) return launch_prim_fused_t<2, true, true, MX>(q, inc, G, W, h, s);
+    return launch_prim_fused_t<2, false, true, MX>(q, inc, G, W, h, s);
+  }
+  if (sens) return launch_prim_fused_t<3, true, true, MX>(q, inc, G, W, h, s);
+  return launch_prim_fused_t<3, false, true, MX>(q, inc, G, W, h, s);
+}
+
 // One stage: primitives of `src` (FP64 Q^n or the stage state), sensor, SGS
 // viscosity, then the sweeps.
 template <class T, class TS>
@@ -507,18 +541,16 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   Fields<T>& W = fields_of<T>(h);
   int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
   bool visc = c.visc != OUX_EULER;
-  if (G.dim == 3 && c.scheme != OUX_KEEP) {
-    // primitives and sensor in one z-marching pass
-    Timed tm(h, KK_PRIM_SENSOR, s);
-    const dim3 gb = prim_sensor_grid(G);
-    if constexpr (sizeof(T) < sizeof(double)) {
-      const float* dQ = std::is_same<TS, double>::value ? nullptr : reinterpret_cast<const float*>(src);
-      if (visc) k_prim_sensor<true, true, double, float><<<gb, PS_TX * PS_TY, 0, s>>>(h->Q, dQ, G, h->Wf, h->M, h->K);
-      else k_prim_sensor<false, true, double, float><<<gb, PS_TX * PS_TY, 0, s>>>(h->Q, dQ, G, h->Wf, h->M, h->K);
-    } else {
-      if (visc) k_prim_sensor<true, false, TS, T><<<gb, PS_TX * PS_TY, 0, s>>>(src, nullptr, G, W, h->M, h->K);
-      else k_prim_sensor<false, false, TS, T><<<gb, PS_TX * PS_TY, 0, s>>>(src, nullptr, G, W, h->M, h->K);
-    }
+  const bool sens = c.scheme != OUX_KEEP;
+  const bool grads = W.grad[0] != nullptr;  // the high-order viscous stencils' node gradients
+  if (G.dim == 3 && (sens || grads)) {
+    // primitives, sensor and gradients in one z-marching pass
+    Timed tm(h, KK_PRIM_FUSED, s);
+    const int hd = !grads ? 1 : (h->vk == VK_C6 ? 3 : 2);
+    int rc;
+    if constexpr (sizeof(T) < sizeof(double)) rc = launch_prim_fused<double, T>(hd, sens, visc, h->Q, src, G, W, h, s);
+    else rc = launch_prim_fused<TS, T>(hd, sens, visc, src, src, G, W, h, s);
+    if (rc) return fail(OUX_E_CUDA, std::string("fused primitive pass: ") + cudaGetErrorString(cudaGetLastError()));
     h->launches++;
   } else {
     Timed tm(h, KK_PRIM, s);
@@ -555,13 +587,6 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
       if (G.dim == 3) k_sensor<3, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
       else k_sensor<2, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
     }
-    h->launches++;
-  }
-  if (W.grad[0]) {  // node velocity gradients for the high-order viscous stencils
-    Timed tm(h, KK_GRAD, s);
-    const dim3 gb = plane_grid(G);
-    if (h->vk == VK_C6) k_grad<true, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
-    else k_grad<false, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
     h->launches++;
   }
   if (h->les) {

@@ -349,41 +349,60 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_sensor_mx(Geo G, const double
   if (plane_cell(G, i, j, k)) sensor_mx_cell<DIM, true>(G, Qn, dQ, W, M, i, j, k);
 }
 
-// ---- primitives and Ducros sensor in one pass (3D) --------------------------------
+// ---- primitives, Ducros sensor and node velocity gradients in one pass (3D) --------
 // A block owns a PS_TX x PS_TY column of cells (x, y) over PS_PLANES z planes and
 // marches along z.  For every plane it decodes the velocities of its cells and of a
-// one-cell ring around them into shared memory (three consecutive planes are kept),
-// writes its own cells' primitive fields (prim_cell / prim_mx_cell), and evaluates the
-// previous plane's sensor from shared memory with the FP64 sensor's arithmetic.  Q is
-// read once per cell (plus the ring, mostly from L2), and the sensor's neighbour
-// velocities never leave the SM.  FP64 form: the same bits as k_prim then k_sensor.
-// Mixed form (MX): velocities decoded in FP64 from Q^n + the FP32 increment dQ, so
-// the sensor is sensor_mx_cell's value.
+// ring of HD cells around them into shared memory (the last 2 HD + 1 planes are
+// kept), writes its own cells' primitive fields (prim_cell / prim_mx_cell), and from
+// shared memory evaluates the Ducros sensor of the plane behind (SENSOR) and the nine
+// node velocity gradients of the plane HD behind (HD = 2: the 4th-order node
+// derivative of Central-4 / ME4; HD = 3: the 6th-order one of Central-6; HD = 1:
+// sensor only).  Q is read once per cell plus the ring (mostly from L2), and neither
+// the sensor's nor the gradients' neighbour velocities leave the SM.
+//   FP64 form: the same bits as k_prim and k_sensor, and as the sweeps' in-tile node
+//   derivatives (the same expressions on the same values).
+//   Mixed form (MX): velocities decoded in FP64 from Q^n + the FP32 increment dQ, so
+//   the sensor is sensor_mx_cell's value and the gradients are FP64 derivatives of
+//   FP64 velocities, each rounded once when stored.
+// The sensor: calc_Ducros (3D_solver/src/calc_hybrid.f90:11-72), with the
+// reference's copies to the outer faces; the gradients: the node derivatives of
+// load_smem_visc_cent.f90.fypp:51-70 and load_smem_visc_me4_base.f90:120-127 at every
+// cell whose stencil fits in the grid (else 0: no sweep reads those).
 constexpr int PS_TX = 32, PS_TY = 8, PS_PLANES = 32;
-constexpr int PS_RX = PS_TX + 2, PS_RY = PS_TY + 2;  // the block's cells and the ring around them
 
-inline dim3 prim_sensor_grid(const Geo& G) {
+template <int HD> __host__ __device__ constexpr size_t prim_fused_smem() {
+  return sizeof(double) * (2 * HD + 1) * 3 * (PS_TY + 2 * HD) * (PS_TX + 2 * HD);
+}
+
+inline dim3 prim_fused_grid(const Geo& G) {
   return dim3((unsigned)((G.nx + PS_TX - 1) / PS_TX), (unsigned)((G.ny + PS_TY - 1) / PS_TY),
               (unsigned)((G.nz + PS_PLANES - 1) / PS_PLANES));
 }
 
-template <bool VISC, bool MX, class TS, class T>
-__global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_sensor(const TS* __restrict__ Q, const float* __restrict__ dQ,
-                                                               Geo G, Fields<T> W, Metrics M, PhysConst K) {
-  __shared__ double vel[3][3][PS_RY][PS_RX];  // [plane slot][component][y][x]
+template <int HD, bool SENSOR, bool VISC, bool MX, class TS, class T>
+__global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_fused(const TS* __restrict__ Q, const float* __restrict__ dQ,
+                                                              Geo G, Fields<T> W, Metrics M, PhysConst K) {
+  static_assert(HD >= 1 && HD <= 3, "ring of 1 to 3 cells");
+  constexpr int NW = 2 * HD + 1;                      // planes kept
+  constexpr int RX = PS_TX + 2 * HD, RY = PS_TY + 2 * HD;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* vel = reinterpret_cast<double*>(smraw);     // [plane slot][component][ry][rx]
+  auto V = [&](int slot, int c, int y, int x) -> double& { return vel[((slot * 3 + c) * RY + y) * RX + x]; };
   const int tid = threadIdx.x;
   const int bx = blockIdx.x * PS_TX, by = blockIdx.y * PS_TY;
   const int k0 = blockIdx.z * PS_PLANES, k1 = min(G.nz, k0 + PS_PLANES);
   const int tx = tid % PS_TX, ty = tid / PS_TX;
   const int oi = bx + tx, oj = by + ty;  // this thread's own cell
   const bool own = oi < G.nx && oj < G.ny;
-  for (int kk = k0 - 1; kk <= k1; ++kk) {
-    // 1. velocities of plane kk (block cells and ring) into slot kk mod 3
+  const int rx = tx + HD, ry = ty + HD;  // and its place in the ring
+  auto slot_of = [](int k) { return (k % NW + NW) % NW; };
+  for (int kk = k0 - HD; kk < k1 + HD; ++kk) {
+    // 1. velocities of plane kk (block cells and ring)
     if (kk >= 0 && kk < G.nz) {
-      const int slot = (kk + 3) % 3;
-      for (int c = tid; c < PS_RX * PS_RY; c += PS_TX * PS_TY) {
-        const int rx = c % PS_RX, ry = c / PS_RX;
-        const int i = bx - 1 + rx, j = by - 1 + ry;
+      const int slot = slot_of(kk);
+      for (int c = tid; c < RX * RY; c += PS_TX * PS_TY) {
+        const int cx = c % RX, cy = c / RX;
+        const int i = bx - HD + cx, j = by - HD + cy;
         if (i < 0 || i >= G.nx || j < 0 || j >= G.ny) continue;
         const int64_t o = G.at(i, j, kk);
         double q0, q1, q2, q3;
@@ -393,20 +412,16 @@ __global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_sensor(const TS* __restr
           q1 = __ldg(Qd + o + G.vs) + (dQ ? (double)__ldg(dQ + o + G.vs) : 0.0);
           q2 = __ldg(Qd + o + 2 * G.vs) + (dQ ? (double)__ldg(dQ + o + 2 * G.vs) : 0.0);
           q3 = __ldg(Qd + o + 3 * G.vs) + (dQ ? (double)__ldg(dQ + o + 3 * G.vs) : 0.0);
-          const double over = 1.0 / q0;
-          vel[slot][0][ry][rx] = q1 * over;
-          vel[slot][1][ry][rx] = q2 * over;
-          vel[slot][2][ry][rx] = q3 * over;
         } else {
           q0 = (double)__ldg(Q + o);
           q1 = (double)__ldg(Q + o + G.vs);
           q2 = (double)__ldg(Q + o + 2 * G.vs);
           q3 = (double)__ldg(Q + o + 3 * G.vs);
-          const double over_Q1 = 1.0 / q0;  // prim_cell: T(1) / q1 with T = double
-          vel[slot][0][ry][rx] = q1 * over_Q1;
-          vel[slot][1][ry][rx] = q2 * over_Q1;
-          vel[slot][2][ry][rx] = q3 * over_Q1;
         }
+        const double over = 1.0 / q0;  // prim_cell / prim_mx_cell: u = q1 * (1 / q0)
+        V(slot, 0, cy, cx) = q1 * over;
+        V(slot, 1, cy, cx) = q2 * over;
+        V(slot, 2, cy, cx) = q3 * over;
       }
       // 2. the block's own cells: every primitive field
       if (own && kk >= k0 && kk < k1) {
@@ -415,73 +430,68 @@ __global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_sensor(const TS* __restr
       }
     }
     __syncthreads();
-    // 3. the sensor of plane k = kk - 1 from the three planes k - 1, k, k + 1
-    const int k = kk - 1;
-    if (own && k >= k0 && k < k1 && oi >= 1 && oi <= G.nx - 2 && oj >= 1 && oj <= G.ny - 2 && k >= 1 &&
-        k <= G.nz - 2) {
-      const int sm = (k - 1 + 3) % 3, s0 = (k + 3) % 3, sp = (k + 1 + 3) % 3;
-      const int rx = tx + 1, ry = ty + 1;
-      const double dxt = 0.25 * (M.inv_dx[oi - 1] + M.inv_dx[oi]);
-      const double dyt = 0.25 * (M.inv_dy[oj - 1] + M.inv_dy[oj]);
-      const double dzt = 0.25 * (M.inv_dz[k - 1] + M.inv_dz[k]);
-      auto V = [&](int sl, int c, int y, int x) -> double { return vel[sl][c][y][x]; };
-      const double dudx = (-V(s0, 0, ry, rx - 1) + V(s0, 0, ry, rx + 1)) * dxt;
-      const double dvdx = (-V(s0, 1, ry, rx - 1) + V(s0, 1, ry, rx + 1)) * dxt;
-      const double dwdx = (-V(s0, 2, ry, rx - 1) + V(s0, 2, ry, rx + 1)) * dxt;
-      const double dudy = (-V(s0, 0, ry - 1, rx) + V(s0, 0, ry + 1, rx)) * dyt;
-      const double dvdy = (-V(s0, 1, ry - 1, rx) + V(s0, 1, ry + 1, rx)) * dyt;
-      const double dwdy = (-V(s0, 2, ry - 1, rx) + V(s0, 2, ry + 1, rx)) * dyt;
-      const double dudz = (-V(sm, 0, ry, rx) + V(sp, 0, ry, rx)) * dzt;
-      const double dvdz = (-V(sm, 1, ry, rx) + V(sp, 1, ry, rx)) * dzt;
-      const double dwdz = (-V(sm, 2, ry, rx) + V(sp, 2, ry, rx)) * dzt;
-      const double div = dudx + dvdy + dwdz;
-      const double r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
-      double f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + 1.0e-12);
-      f = fmin_f(1.0, f);
-      const T fs = (T)f;
-      const int i = oi, j = oj;
-      W.sensor[G.at(i, j, k)] = fs;
-      if (i == 1) W.sensor[G.at(0, j, k)] = fs; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = fs;
-      if (j == 1) W.sensor[G.at(i, 0, k)] = fs; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = fs;
-      if (k == 1) W.sensor[G.at(i, j, 0)] = fs; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = fs;
+    // 3. the sensor of plane k = kk - 1 from the planes k - 1, k, k + 1
+    if constexpr (SENSOR) {
+      const int k = kk - 1;
+      if (own && k >= k0 && k < k1 && oi >= 1 && oi <= G.nx - 2 && oj >= 1 && oj <= G.ny - 2 && k >= 1 &&
+          k <= G.nz - 2) {
+        const int sm = slot_of(k - 1), s0 = slot_of(k), sp = slot_of(k + 1);
+        const double dxt = 0.25 * (M.inv_dx[oi - 1] + M.inv_dx[oi]);
+        const double dyt = 0.25 * (M.inv_dy[oj - 1] + M.inv_dy[oj]);
+        const double dzt = 0.25 * (M.inv_dz[k - 1] + M.inv_dz[k]);
+        const double dudx = (-V(s0, 0, ry, rx - 1) + V(s0, 0, ry, rx + 1)) * dxt;
+        const double dvdx = (-V(s0, 1, ry, rx - 1) + V(s0, 1, ry, rx + 1)) * dxt;
+        const double dwdx = (-V(s0, 2, ry, rx - 1) + V(s0, 2, ry, rx + 1)) * dxt;
+        const double dudy = (-V(s0, 0, ry - 1, rx) + V(s0, 0, ry + 1, rx)) * dyt;
+        const double dvdy = (-V(s0, 1, ry - 1, rx) + V(s0, 1, ry + 1, rx)) * dyt;
+        const double dwdy = (-V(s0, 2, ry - 1, rx) + V(s0, 2, ry + 1, rx)) * dyt;
+        const double dudz = (-V(sm, 0, ry, rx) + V(sp, 0, ry, rx)) * dzt;
+        const double dvdz = (-V(sm, 1, ry, rx) + V(sp, 1, ry, rx)) * dzt;
+        const double dwdz = (-V(sm, 2, ry, rx) + V(sp, 2, ry, rx)) * dzt;
+        const double div = dudx + dvdy + dwdz;
+        const double r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
+        double f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + 1.0e-12);
+        f = fmin_f(1.0, f);
+        const T fs = (T)f;
+        const int i = oi, j = oj;
+        W.sensor[G.at(i, j, k)] = fs;
+        if (i == 1) W.sensor[G.at(0, j, k)] = fs; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = fs;
+        if (j == 1) W.sensor[G.at(i, 0, k)] = fs; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = fs;
+        if (k == 1) W.sensor[G.at(i, j, 0)] = fs; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = fs;
+      }
+    }
+    // 4. the node velocity gradients of plane k = kk - HD
+    if constexpr (HD >= 2) {
+      constexpr bool SIXTH = HD == 3;
+      const int k = kk - HD;
+      if (own && k >= k0 && k < k1) {
+        const int c[3] = {oi, oj, k};
+        const int n[3] = {G.nx, G.ny, G.nz};
+        const double* invd[3] = {M.inv_dx, M.inv_dy, M.inv_dz};
+        const int64_t o = G.at(oi, oj, k);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const bool fits = c[a] >= HD && c[a] + HD < n[a];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            double d = 0.0;
+            if (fits) {
+              auto A = [&](int m) -> double {
+                return a == 0 ? V(slot_of(k), q, ry, rx + m) : (a == 1 ? V(slot_of(k), q, ry + m, rx)
+                                                                       : V(slot_of(k + m), q, ry, rx));
+              };
+              const double inv = invd[a][c[a]];
+              if constexpr (SIXTH)
+                d = ((1.0 / 60.0) * (-A(-3) + A(3)) + 0.15 * (A(-2) - A(2)) + 0.75 * (-A(-1) + A(1))) * inv;
+              else
+                d = ((2.0 / 3.0) * (-A(-1) + A(1)) - (1.0 / 12.0) * (-A(-2) + A(2))) * inv;
+            }
+            W.grad[3 * q + a][o] = (T)d;
+          }
+        }
+      }
     }
     __syncthreads();
-  }
-}
-
-// ---- node velocity gradients (3D, the high-order viscous stencils) -------------------
-// grad[3c + a] = d(velocity c)/d(axis a) at every cell where the stencil fits in the
-// grid (else 0: no sweep reads those), by the 6th-order (Central-6) or 4th-order
-// (Central-4, ME4) central node derivative the viscous loaders use
-// (load_smem_visc_cent.f90.fypp:51-70, load_smem_visc_me4_base.f90:120-127).  The
-// sweeps then stage these values as plain copies instead of gathering six
-// neighbours per value along the two transverse axes in every tile.
-template <bool SIXTH, class T, bool RO = true>
-__device__ __forceinline__ T node_deriv(const T* a, int64_t o, int64_t st, T inv) {
-  auto A = [&](int64_t q) { return ldro<RO>(a + q); };
-  if constexpr (SIXTH)
-    return (T(1.0 / 60.0) * (-A(o - 3 * st) + A(o + 3 * st)) + T(0.15) * (A(o - 2 * st) - A(o + 2 * st)) +
-            T(0.75) * (-A(o - st) + A(o + st))) * inv;
-  else
-    return (T(2.0 / 3.0) * (-A(o - st) + A(o + st)) - T(1.0 / 12.0) * (-A(o - 2 * st) + A(o + 2 * st))) * inv;
-}
-
-template <bool SIXTH, class T>
-__global__ void __launch_bounds__(PLANE_THREADS) k_grad(Geo G, Fields<T> W, Metrics M) {
-  int c[3];
-  if (!plane_cell(G, c[0], c[1], c[2])) return;
-  constexpr int HD = SIXTH ? 3 : 2;
-  const int n[3] = {G.nx, G.ny, G.nz};
-  const int64_t st[3] = {1, G.sx, G.plane};
-  const double* invd[3] = {M.inv_dx, M.inv_dy, M.inv_dz};
-  const T* vel[3] = {W.u, W.v, W.w};
-  const int64_t o = G.at(c[0], c[1], c[2]);
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const bool fits = c[a] >= HD && c[a] + HD < n[a];
-    const T inv = fits ? (T)invd[a][c[a]] : T(0);
-#pragma unroll
-    for (int q = 0; q < 3; ++q) W.grad[3 * q + a][o] = fits ? node_deriv<SIXTH, T>(vel[q], o, st[a], inv) : T(0);
   }
 }
 

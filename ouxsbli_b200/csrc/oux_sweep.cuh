@@ -89,6 +89,9 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // transverse node derivative of `a` along axis `ax` at offset o (4th/6th order)
 template <bool SIXTH, bool RO, class T>
@@ -695,9 +698,13 @@ namespace oux {
 // are evaluated once into shared memory (me4_position) and combined per face
 // (me4_face); needs me4_share_bytes() more dynamic shared memory after the prefetch.
 // GR: the transverse node derivatives are staged from the gradient fields W.grad
-// (k_grad) instead of being differenced from the velocities in the tile load.
+// (written by k_prim_fused) instead of being differenced from the velocities in the
+// tile load.
+// AT: the tile fields are plain copies (no derivative is differenced in the load), so
+// they are staged with asynchronous global -> shared copies (cp.async): no register
+// staging, and every copy of the tile is in flight at once.
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
-          bool RO = false, bool KONLY = false, int PF = 0, bool SHARE = false, bool GR = false>
+          bool RO = false, bool KONLY = false, int PF = 0, bool SHARE = false, bool GR = false, bool AT = false>
 __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
                                            unsigned char* smraw, int tid, int nthr_all) {
   constexpr int H = ORDER / 2;
@@ -753,7 +760,9 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   const bool needQs = md == CM_RK3_2 || md == CM_RK3_3;
   const bool needRs = md == CM_RK4_S || md == CM_RK4_4;
   const int slot = ty * 32 + tx;
-  if constexpr (PF_ON) {
+  // the prefetch is one cp.async group; with AT it is issued after the tile's group, so
+  // that waiting for the tile (wait_group 1) leaves the prefetch in flight
+  auto issue_prefetch = [&]() {
     if (act && ty < TY - 1) {
       int pc[3];
       pc[0] = bx0 + tx;
@@ -772,7 +781,8 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       }
     }
     cp_async_commit();
-  }
+  };
+  if constexpr (PF_ON && !AT) issue_prefetch();
 
   // ---- tile load (cooperative) ----
   for (int c = tid; c < NC; c += nthr) {
@@ -794,6 +804,31 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       if (a != DIR && (a < DIM) && ci[a] >= ext[a]) ok = false;
     if (!ok) continue;
     const int64_t o = G.at(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
+    if constexpr (AT) {
+      static_assert(!HIGH || GR, "asynchronous tile loads need the derivatives as fields");
+      cp_async<sizeof(T)>(&tile[TF_RHO * NC + c], A.W.rho + o);
+      cp_async<sizeof(T)>(&tile[TF_U * NC + c], A.W.u + o);
+      cp_async<sizeof(T)>(&tile[TF_V * NC + c], A.W.v + o);
+      if constexpr (DIM == 3) cp_async<sizeof(T)>(&tile[TF_W * NC + c], A.W.w + o);
+      else tile[TF_W * NC + c] = T(0);
+      cp_async<sizeof(T)>(&tile[TF_P * NC + c], A.W.p + o);
+      cp_async<sizeof(T)>(&tile[TF_T * NC + c], A.W.T_ + o);
+      if (!KONLY && A.scheme != 0) cp_async<sizeof(T)>(&tile[TF_SEN * NC + c], A.W.sensor + o);
+      if constexpr (VK != VK_EULER) cp_async<sizeof(T)>(&tile[TF_MU * NC + c], A.W.mu + o);
+      if constexpr (LES) {
+        cp_async<sizeof(T)>(&tile[TF_MUT * NC + c], A.W.mut + o);
+        cp_async<sizeof(T)>(&tile[TF_QC2 * NC + c], A.W.qc2 + o);
+      }
+      if constexpr (HIGH) {
+        constexpr int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
+        constexpr int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
+        cp_async<sizeof(T)>(&tile[TF_D0 * NC + c], A.W.grad[3 * a1 + a1] + o);
+        cp_async<sizeof(T)>(&tile[TF_D1 * NC + c], A.W.grad[3 * a2 + a2] + o);
+        cp_async<sizeof(T)>(&tile[TF_D2 * NC + c], A.W.grad[3 * n + ca] + o);
+        cp_async<sizeof(T)>(&tile[TF_D3 * NC + c], A.W.grad[3 * n + cb] + o);
+      }
+      continue;
+    }
     tile[TF_RHO * NC + c] = ldro<RO>(A.W.rho + o);
     tile[TF_U * NC + c] = ldro<RO>(A.W.u + o);
     tile[TF_V * NC + c] = ldro<RO>(A.W.v + o);
@@ -847,6 +882,15 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
           tile[TF_D2 * NC + c] = T(0);
         }
       }
+    }
+  }
+  if constexpr (AT) {
+    cp_async_commit();
+    if constexpr (PF_ON) {
+      issue_prefetch();
+      cp_async_wait_group<1>();  // this thread's tile copies have landed; the prefetch may not have
+    } else {
+      cp_async_wait_all();
     }
   }
   __syncthreads();
@@ -1125,7 +1169,7 @@ template <int DIR> __host__ __device__ constexpr int sweep_threads() {
 }
 
 // Single-solve sweeps of periodic 3D grids with a high-order viscous stencil read the
-// transverse node derivatives from the gradient fields (k_grad runs before them).
+// transverse node derivatives from the gradient fields (k_prim_fused writes them).
 template <int DIM, int VK> __host__ __device__ constexpr bool sweep_uses_grads() {
   return DIM == 3 && (VK == VK_C6 || VK == VK_C4 || VK == VK_ME4);
 }
@@ -1135,9 +1179,11 @@ __global__ void __launch_bounds__(sweep_threads<DIR>(), DIR == 0 ? OUX_SWEEP_MIN
 k_sweep(StepArgs<T> A, int last) {
   extern __shared__ __align__(16) unsigned char smraw[];
   // coherent loads: measured as fast as the read-only path for y/z and faster for x
+  constexpr int VB = vk_base(VK);
+  constexpr bool HIGH = (VB == VK_C6 || VB == VK_C4 || VB == VK_ME4 || VB == VK_2D4);
+  constexpr bool GR = sweep_uses_grads<DIM, VK>();
   sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>(), SHARE,
-             sweep_uses_grads<DIM, VK>()>(A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.x,
-                                           sweep_threads<DIR>());
+             GR, !HIGH || GR>(A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.x, sweep_threads<DIR>());
 }
 
 }  // namespace oux

@@ -8,8 +8,8 @@ solves together with one batched persistent-kernel launch per time step
 after each quantum finished solves are retired (their memory freed) and newly
 arrived requests join, so a request that arrives while others are on the GPU runs
 in the same launches as theirs from the next quantum on.  While the GPU runs a
-quantum the host builds the initial fields of requests that have arrived, so that
-work overlaps the device's.
+quantum host threads build the initial fields of requests that have arrived, so
+that work overlaps the device's and never holds up the loop that feeds it.
 
 Each solve's arithmetic does not depend on which other solves share its batch: a
 result is bit-for-bit the same alone and in a mix.
@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import ctypes as C
 import time
+from concurrent.futures import Future, ThreadPoolExecutor
 from dataclasses import dataclass, field
 from typing import Callable, Sequence
 
@@ -89,6 +90,18 @@ def request_bytes(cfg: SolverConfig) -> int:
     return int(sb.value + kb.value)
 
 
+def request_bytes_for(n: int, physics: dict) -> int:
+    """Device bytes of a request of n^3 interior cells with the given physics, from its
+    configuration alone (the initial field is not needed to size it)."""
+    from .grid import cyclic_axis
+    order = physics.get("order", 6)
+    nx = n + order
+    _, d = cyclic_axis(nx, 1.0, order)
+    cfg = SolverConfig(dim=3, nx=nx, ny=nx, nz=nx, order=order, dx=d, dy=d.copy(), dz=d.copy(),
+                       **{k: v for k, v in physics.items() if k != "order"})
+    return request_bytes(cfg)
+
+
 def summarize(results: Sequence[SolveResult]) -> dict:
     """p50 / p99 completion latency and aggregate Mcell-steps/s of a served stream."""
     lat = np.array([r.latency for r in results])
@@ -120,6 +133,7 @@ class Server:
                                                        precision="mixed"))
     tuner: Autotuner | None = None      # cached tunings are used when present
     keep_states: bool = False           # return each final state (host copy)
+    build_workers: int = 2              # host threads that build arriving requests' initial fields
     default_tuning: Tuning = field(default_factory=Tuning)  # when the tuner has nothing cached
     stats: dict = field(default_factory=dict)
 
@@ -134,7 +148,10 @@ class Server:
             sleep: Callable[[float], None] = time.sleep) -> list[SolveResult]:
         dev = torch.device(self.device)
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
-        queue: list[tuple[SolveRequest, SolverConfig, np.ndarray, int]] = []
+        # waiting requests in arrival order: (request, device bytes, future of (cfg, initial QJ))
+        queue: list[tuple[SolveRequest, int, Future]] = []
+        pool = ThreadPoolExecutor(max_workers=max(1, self.build_workers))
+        sizes: dict[int, int] = {}
         active: list[_Active] = []
         results: list[SolveResult] = []
         used = 0
@@ -146,7 +163,7 @@ class Server:
         split = {"arrivals_s": 0.0, "admit_s": 0.0, "batch_build_s": 0.0, "step_enqueue_s": 0.0,
                  "wait_device_s": 0.0, "retire_s": 0.0, "idle_s": 0.0}
         gpu_ms = 0.0
-        stream = torch.cuda.current_stream(dev)
+        stream = None  # the device's current stream, looked up when the first quantum runs
 
         class _Part:
             def __init__(self, key):
@@ -162,72 +179,84 @@ class Server:
         wall0 = time.perf_counter()
 
         def arrivals(now: float) -> None:
-            # build the initial fields of every request that has arrived (host work)
+            # every request that has arrived joins the queue; its initial field is built
+            # on a host thread, off the loop that feeds the device
             while pending and pending[0].arrival <= now:
                 r = pending.pop(0)
-                cfg, qj = r.build(self.physics)
-                need = request_bytes(cfg)
+                if r.n not in sizes:
+                    sizes[r.n] = request_bytes_for(r.n, self.physics)
+                need = sizes[r.n]
                 if need > self.hbm_budget:
                     raise ValueError(f"request {r.rid} needs {need} bytes, more than the budget {self.hbm_budget}")
-                queue.append((r, cfg, qj, need))
+                queue.append((r, need, pool.submit(r.build, self.physics)))
 
-        while pending or queue or active:
-            with _Part("arrivals_s"):
-                arrivals(clock() - t0)
-            # admission: FIFO while memory and slots allow
-            with _Part("admit_s"):
-                while queue and len(active) < self.max_active and used + queue[0][3] <= self.hbm_budget:
-                    r, cfg, qj, need = queue.pop(0)
-                    s = Solver(cfg, dev)
-                    s.set_state(qj)
-                    active.append(_Active(r, s, need, r.steps, clock() - t0))
-                    used += need
-                    dirty = True
-            peak_bytes = max(peak_bytes, used)
-            peak_active = max(peak_active, len(active))
-            if not active:
-                if pending:
-                    with _Part("idle_s"):
-                        sleep(max(0.0, min(pending[0].arrival - (clock() - t0), 0.05)))
-                continue
-            if dirty:
-                with _Part("batch_build_s"):
-                    if batch is not None:
+        try:
+            while pending or queue or active:
+                with _Part("arrivals_s"):
+                    arrivals(clock() - t0)
+                # admission: FIFO while memory and slots allow
+                with _Part("admit_s"):
+                    # FIFO while memory and slots allow; a request whose initial field is still
+                    # being built waits for it only when nothing else is on the device
+                    while queue and len(active) < self.max_active and used + queue[0][1] <= self.hbm_budget:
+                        if active and not queue[0][2].done():
+                            break
+                        r, need, fut = queue.pop(0)
+                        cfg, qj = fut.result()
+                        s = Solver(cfg, dev)
+                        s.set_state(qj)
+                        active.append(_Active(r, s, need, r.steps, clock() - t0))
+                        used += need
+                        dirty = True
+                peak_bytes = max(peak_bytes, used)
+                peak_active = max(peak_active, len(active))
+                if not active:
+                    if pending:
+                        with _Part("idle_s"):
+                            sleep(max(0.0, min(pending[0].arrival - (clock() - t0), 0.05)))
+                    continue
+                if dirty:
+                    with _Part("batch_build_s"):
+                        if batch is not None:
+                            batch.close()
+                        solvers = [a.solver for a in active]
+                        batch = Batch(solvers, self._tuning(solvers))
+                        dirty = False
+                k = min(self.quantum, min(a.remaining for a in active))
+                if stream is None:
+                    stream = torch.cuda.current_stream(dev)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with _Part("step_enqueue_s"):
+                    e0.record(stream)
+                    batch.step(k)                      # asynchronous on the device
+                    e1.record(stream)
+                steps_run += k
+                quanta += 1
+                with _Part("arrivals_s"):
+                    arrivals(clock() - t0)             # overlaps the quantum
+                with _Part("wait_device_s"):
+                    stream.synchronize()
+                gpu_ms += e0.elapsed_time(e1)
+                done_t = clock() - t0
+                keep = []
+                with _Part("retire_s"):
+                    for a in active:
+                        a.remaining -= k
+                        if a.remaining > 0:
+                            keep.append(a)
+                            continue
+                        st = a.solver.get_state() if self.keep_states else None
+                        results.append(SolveResult(a.req.rid, a.req.n, a.req.steps, a.req.arrival, a.admitted, done_t,
+                                                   a.solver.diagnostics(), st))
+                        a.solver.close()
+                        used -= a.bytes
+                        dirty = True
+                    if dirty and batch is not None:
                         batch.close()
-                    solvers = [a.solver for a in active]
-                    batch = Batch(solvers, self._tuning(solvers))
-                    dirty = False
-            k = min(self.quantum, min(a.remaining for a in active))
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            with _Part("step_enqueue_s"):
-                e0.record(stream)
-                batch.step(k)                      # asynchronous on the device
-                e1.record(stream)
-            steps_run += k
-            quanta += 1
-            with _Part("arrivals_s"):
-                arrivals(clock() - t0)             # overlaps the quantum
-            with _Part("wait_device_s"):
-                stream.synchronize()
-            gpu_ms += e0.elapsed_time(e1)
-            done_t = clock() - t0
-            keep = []
-            with _Part("retire_s"):
-                for a in active:
-                    a.remaining -= k
-                    if a.remaining > 0:
-                        keep.append(a)
-                        continue
-                    st = a.solver.get_state() if self.keep_states else None
-                    results.append(SolveResult(a.req.rid, a.req.n, a.req.steps, a.req.arrival, a.admitted, done_t,
-                                               a.solver.diagnostics(), st))
-                    a.solver.close()
-                    used -= a.bytes
-                    dirty = True
-                if dirty and batch is not None:
-                    batch.close()
-                    batch = None
-            active = keep
+                        batch = None
+                active = keep
+        finally:
+            pool.shutdown(wait=True, cancel_futures=True)
         if batch is not None:
             batch.close()
         wall = time.perf_counter() - wall0
