@@ -245,14 +245,15 @@ Geo make_geo(const oux_config& c) {
 }
 
 struct ScratchPlan {
-  size_t fields = 0, racc = 0, q2 = 0, rs = 0, metrics = 0, partials = 0, status = 0, total = 0;
+  size_t fields = 0, racc = 0, q2 = 0, rs = 0, prim64 = 0, metrics = 0, partials = 0, status = 0, total = 0;
+  bool has_prim64 = false;  // the mixed form's FP64 primitives (hybrid scheme)
   int nfield_arrays = 0;
 };
 
 constexpr int DIAG_BLOCKS = 1184;  // 8 blocks per SM on 148 SMs; fixed for a deterministic sum
 
 // Whether a configuration's sweeps read the node velocity gradients from fields
-// (k_prim_fused writes them; sweep_uses_grads): periodic 3D grids with Central-4/6 or ME4
+// (k_grad writes them; sweep_uses_grads): periodic 3D grids with Central-4/6 or ME4
 // viscous stencils.
 bool uses_grads(const oux_config& c) {
   std::string why;
@@ -273,6 +274,8 @@ ScratchPlan plan_scratch(const oux_config& c) {
   P.racc = off; off += (size_t)nv * vsb;
   P.q2 = off; off += round_up((size_t)nv * vse, 256);
   P.rs = off; off += (c.rk == 4 ? (size_t)nv * vsb : 0);
+  P.has_prim64 = c.precision == OUX_MIXED && c.scheme == OUX_HYBRID;
+  P.prim64 = off; off += P.has_prim64 ? 5 * vsb : 0;
   P.metrics = off;
   int nx = c.nx, ny = c.ny, nz = c.dim == 3 ? c.nz : 1;
   size_t mcount = (size_t)(nx - 1) + (ny - 1) + (c.dim == 3 ? nz - 1 : 1) + (size_t)nx * ny;
@@ -432,11 +435,14 @@ void carve(oux_handle* h) {
     double** fp[10] = {&h->W.rho, &h->W.u, &h->W.v, &h->W.w, &h->W.p, &h->W.T_, &h->W.mu, &h->W.sensor, &h->W.mut, &h->W.qc2};
     for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
     for (int q = 0; q < 9; ++q) h->W.grad[q] = P.nfield_arrays == 19 ? f + (10 + q) * vsb : nullptr;
+    for (int q = 0; q < 5; ++q) h->W.prim64[q] = nullptr;
   } else {
     float* f = reinterpret_cast<float*>(h->scratch + P.fields);
     float** fp[10] = {&h->Wf.rho, &h->Wf.u, &h->Wf.v, &h->Wf.w, &h->Wf.p, &h->Wf.T_, &h->Wf.mu, &h->Wf.sensor, &h->Wf.mut, &h->Wf.qc2};
     for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
     for (int q = 0; q < 9; ++q) h->Wf.grad[q] = P.nfield_arrays == 19 ? f + (10 + q) * vsb : nullptr;
+    double* p64 = reinterpret_cast<double*>(h->scratch + P.prim64);
+    for (int q = 0; q < 5; ++q) h->Wf.prim64[q] = P.has_prim64 ? p64 + q * vsb : nullptr;
   }
   h->Racc = reinterpret_cast<double*>(h->scratch + P.racc);
   h->Qs = h->scratch + P.q2;
@@ -468,7 +474,7 @@ void carve(oux_handle* h) {
 
 // kinds reported by oux_profile_read
 enum KernelKind { KK_PRIM = 0, KK_SENSOR, KK_MUT, KK_MUT_EDGES, KK_SWEEP_X, KK_SWEEP_Y, KK_SWEEP_Z, KK_GHOST,
-                  KK_PRIM_FUSED, KK_COUNT };
+                  KK_PRIM_FUSED, KK_GRAD, KK_COUNT };
 
 struct Timed {
   oux_handle* h;
@@ -499,37 +505,32 @@ int launch_sweeps_t<float>(int dim, int order, int vk, bool les, int dir, const 
   return dir < 0 ? launch_sweeps_mx(dim, order, vk, les, A, s) : launch_sweep_dir_mx(dim, order, vk, les, dir, A, s);
 }
 
-// k_prim_fused with the ring width hd (1: sensor only; 2 / 3: gradients of 4th / 6th
-// order), on `q` (FP64 form: the stage source; mixed form: Q^n, with the FP32 increment
-// `inc` unless the source is Q^n itself).
-template <int HD, bool SENS, bool VISC, bool MX, class TQ, class T>
-int launch_prim_fused_t(const TQ* q, const float* inc, const Geo& G, Fields<T>& W, oux_handle* h, cudaStream_t s) {
-  constexpr size_t smem = prim_fused_smem<HD>();
-  auto kern = k_prim_fused<HD, SENS, VISC, MX, TQ, T>;
+// k_prim_fused (primitives + sensor) on `q` (FP64 form: the stage source; mixed form:
+// Q^n, with the FP32 increment of the stage source unless that is Q^n itself).
+template <bool VISC, class TQ, class T, class TS>
+int launch_prim_fused(const TQ* q, const TS* src, const Geo& G, Fields<T>& W, oux_handle* h, cudaStream_t s) {
+  constexpr bool MX = sizeof(T) < sizeof(double);
+  const float* inc = nullptr;
+  if constexpr (MX) {
+    if (!std::is_same<TS, double>::value) inc = reinterpret_cast<const float*>(src);
+  }
+  constexpr size_t smem = prim_fused_smem<1>();
+  auto kern = k_prim_fused<1, true, VISC, MX, TQ, T>;
   static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (attr != cudaSuccess) return 1;
   kern<<<prim_fused_grid(G), PS_TX * PS_TY, smem, s>>>(q, inc, G, W, h->M, h->K);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }
 
-template <class TQ, class T, class TS>
-int launch_prim_fused(int hd, bool sens, bool visc, const TQ* q, const TS* src, const Geo& G, Fields<T>& W,
-                      oux_handle* h, cudaStream_t s) {
-  const float* inc = nullptr;
-  if constexpr (sizeof(T) < sizeof(double)) {
-    if (!std::is_same<TS, double>::value) inc = reinterpret_cast<const float*>(src);
-  }
-  constexpr bool MX = sizeof(T) < sizeof(double);
-  if (hd == 1) {
-    if (visc) return launch_prim_fused_t<1, true, true, MX>(q, inc, G, W, h, s);
-    return launch_prim_fused_t<1, true, false, MX>(q, inc, G, W, h, s);
-  }
-  if (hd == 2) {
-    if (sens) return launch_prim_fused_t<2, true, true, MX>(q, inc, G, W, h, s);
-    return launch_prim_fused_t<2, false, true, MX>(q, inc, G, W, h, s);
-  }
-  if (sens) return launch_prim_fused_t<3, true, true, MX>(q, inc, G, W, h, s);
-  return launch_prim_fused_t<3, false, true, MX>(q, inc, G, W, h, s);
+// k_grad with a ring of HD cells, for the compute type T
+template <int HD, class T>
+int launch_grad(const Geo& G, Fields<T>& W, const Metrics& M, cudaStream_t s) {
+  const size_t smem = grad_smem<HD>(sizeof(T));
+  auto kern = k_grad<HD, T>;
+  static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (attr != cudaSuccess) return 1;
+  kern<<<grad_grid(G), GR_TX * GR_TY, smem, s>>>(G, W, M);
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }
 
 // One stage: primitives of `src` (FP64 Q^n or the stage state), sensor, SGS
@@ -542,15 +543,16 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
   bool visc = c.visc != OUX_EULER;
   const bool sens = c.scheme != OUX_KEEP;
-  const bool grads = W.grad[0] != nullptr;  // the high-order viscous stencils' node gradients
-  if (G.dim == 3 && (sens || grads)) {
-    // primitives, sensor and gradients in one z-marching pass
+  if (G.dim == 3 && sens) {
+    // primitives and sensor in one z-marching pass
     Timed tm(h, KK_PRIM_FUSED, s);
-    const int hd = !grads ? 1 : (h->vk == VK_C6 ? 3 : 2);
     int rc;
-    if constexpr (sizeof(T) < sizeof(double)) rc = launch_prim_fused<double, T>(hd, sens, visc, h->Q, src, G, W, h, s);
-    else rc = launch_prim_fused<TS, T>(hd, sens, visc, src, src, G, W, h, s);
-    if (rc) return fail(OUX_E_CUDA, std::string("fused primitive pass: ") + cudaGetErrorString(cudaGetLastError()));
+    if constexpr (sizeof(T) < sizeof(double)) {
+      rc = visc ? launch_prim_fused<true>(h->Q, src, G, W, h, s) : launch_prim_fused<false>(h->Q, src, G, W, h, s);
+    } else {
+      rc = visc ? launch_prim_fused<true>(src, src, G, W, h, s) : launch_prim_fused<false>(src, src, G, W, h, s);
+    }
+    if (rc) return fail(OUX_E_CUDA, std::string("primitive + sensor pass: ") + cudaGetErrorString(cudaGetLastError()));
     h->launches++;
   } else {
     Timed tm(h, KK_PRIM, s);
@@ -587,6 +589,12 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
       if (G.dim == 3) k_sensor<3, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
       else k_sensor<2, T><<<gb, PLANE_THREADS, 0, s>>>(G, W, h->M);
     }
+    h->launches++;
+  }
+  if (W.grad[0]) {  // node velocity gradients of the high-order viscous stencils
+    Timed tm(h, KK_GRAD, s);
+    const int rc = h->vk == VK_C6 ? launch_grad<3>(G, W, h->M, s) : launch_grad<2>(G, W, h->M, s);
+    if (rc) return fail(OUX_E_CUDA, std::string("gradient pass: ") + cudaGetErrorString(cudaGetLastError()));
     h->launches++;
   }
   if (h->les) {

@@ -64,6 +64,9 @@ template <class T> struct Fields {
   T *rho, *u, *v, *w, *p, *T_, *mu, *sensor, *mut, *qc2;
   // node velocity gradient d(vel_c)/d(x_a) at index 3*c + a (3D: 9, 2D: c,a < 2)
   T* grad[9];
+  // mixed form with the hybrid scheme: FP64 rho, u, v, w, p (the decode before it is
+  // rounded), for the shock-capturing faces, which reconstruct and evaluate in FP64
+  double* prim64[5];
 };
 
 struct Metrics {
@@ -187,6 +190,9 @@ __device__ __forceinline__ void prim_mx_cell(const double* Qn, const float* dQ, 
     p = K.gamma_1 * (Jv * q[3] - 0.5 * rho * (u * u + v * v));
   }
   double temp = p / (K.R * rho);
+  if (W.prim64[0]) {
+    W.prim64[0][o] = rho; W.prim64[1][o] = u; W.prim64[2][o] = v; W.prim64[3][o] = w; W.prim64[4][o] = p;
+  }
   W.rho[o] = (float)rho; W.u[o] = (float)u; W.v[o] = (float)v;
   if constexpr (DIM == 3) W.w[o] = (float)w;
   W.p[o] = (float)(p - K.p_ref);
@@ -349,25 +355,19 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_sensor_mx(Geo G, const double
   if (plane_cell(G, i, j, k)) sensor_mx_cell<DIM, true>(G, Qn, dQ, W, M, i, j, k);
 }
 
-// ---- primitives, Ducros sensor and node velocity gradients in one pass (3D) --------
+// ---- primitives and Ducros sensor in one pass (3D) --------------------------------
 // A block owns a PS_TX x PS_TY column of cells (x, y) over PS_PLANES z planes and
 // marches along z.  For every plane it decodes the velocities of its cells and of a
-// ring of HD cells around them into shared memory (the last 2 HD + 1 planes are
-// kept), writes its own cells' primitive fields (prim_cell / prim_mx_cell), and from
-// shared memory evaluates the Ducros sensor of the plane behind (SENSOR) and the nine
-// node velocity gradients of the plane HD behind (HD = 2: the 4th-order node
-// derivative of Central-4 / ME4; HD = 3: the 6th-order one of Central-6; HD = 1:
-// sensor only).  Q is read once per cell plus the ring (mostly from L2), and neither
-// the sensor's nor the gradients' neighbour velocities leave the SM.
-//   FP64 form: the same bits as k_prim and k_sensor, and as the sweeps' in-tile node
-//   derivatives (the same expressions on the same values).
+// one-cell ring around them into shared memory (the last three planes are kept),
+// writes its own cells' primitive fields (prim_cell / prim_mx_cell), and evaluates the
+// previous plane's sensor from shared memory with the FP64 sensor's arithmetic
+// (calc_Ducros, 3D_solver/src/calc_hybrid.f90:11-72, with the reference's copies to
+// the outer faces).  Q is read once per cell plus the ring (mostly from L2), and the
+// sensor's neighbour velocities never leave the SM.
+//   FP64 form: the same bits as k_prim then k_sensor (the same expressions on the
+//   same values).
 //   Mixed form (MX): velocities decoded in FP64 from Q^n + the FP32 increment dQ, so
-//   the sensor is sensor_mx_cell's value and the gradients are FP64 derivatives of
-//   FP64 velocities, each rounded once when stored.
-// The sensor: calc_Ducros (3D_solver/src/calc_hybrid.f90:11-72), with the
-// reference's copies to the outer faces; the gradients: the node derivatives of
-// load_smem_visc_cent.f90.fypp:51-70 and load_smem_visc_me4_base.f90:120-127 at every
-// cell whose stencil fits in the grid (else 0: no sweep reads those).
+//   the sensor is sensor_mx_cell's value, rounded once when stored.
 constexpr int PS_TX = 32, PS_TY = 8, PS_PLANES = 32;
 
 template <int HD> __host__ __device__ constexpr size_t prim_fused_smem() {
@@ -382,7 +382,7 @@ inline dim3 prim_fused_grid(const Geo& G) {
 template <int HD, bool SENSOR, bool VISC, bool MX, class TS, class T>
 __global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_fused(const TS* __restrict__ Q, const float* __restrict__ dQ,
                                                               Geo G, Fields<T> W, Metrics M, PhysConst K) {
-  static_assert(HD >= 1 && HD <= 3, "ring of 1 to 3 cells");
+  static_assert(HD == 1, "the sensor's ring is one cell wide");
   constexpr int NW = 2 * HD + 1;                      // planes kept
   constexpr int RX = PS_TX + 2 * HD, RY = PS_TY + 2 * HD;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -460,39 +460,101 @@ __global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_fused(const TS* __restri
         if (k == 1) W.sensor[G.at(i, j, 0)] = fs; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = fs;
       }
     }
-    // 4. the node velocity gradients of plane k = kk - HD
-    if constexpr (HD >= 2) {
-      constexpr bool SIXTH = HD == 3;
-      const int k = kk - HD;
-      if (own && k >= k0 && k < k1) {
-        const int c[3] = {oi, oj, k};
-        const int n[3] = {G.nx, G.ny, G.nz};
-        const double* invd[3] = {M.inv_dx, M.inv_dy, M.inv_dz};
-        const int64_t o = G.at(oi, oj, k);
+    __syncthreads();
+  }
+}
+
+// ---- node velocity gradients (3D, the high-order viscous stencils) ----------------
+// grad[3c + a] = d(velocity c)/d(axis a) by the 6th-order (HD = 3: Central-6) or
+// 4th-order (HD = 2: Central-4, ME4) central node derivative of the viscous loaders
+// (load_smem_visc_cent.f90.fypp:51-70, load_smem_visc_me4_base.f90:120-127), at every
+// cell whose stencil fits in the grid (else 0: no sweep reads those).  A block owns a
+// GR_TX x GR_TY column of cells and marches along z; the velocities of each plane
+// (its cells and a ring of HD cells) come into a shared-memory ring with asynchronous
+// copies issued one plane ahead, so the copies of plane k + 1 are in flight while the
+// derivatives of plane k - HD are evaluated.
+constexpr int GR_TX = 32, GR_TY = 8, GR_PLANES = 32;
+
+template <int HD> __host__ __device__ constexpr size_t grad_smem(int tsize) {
+  return (size_t)tsize * (2 * HD + 2) * 3 * (GR_TY + 2 * HD) * (GR_TX + 2 * HD);
+}
+
+inline dim3 grad_grid(const Geo& G) {
+  return dim3((unsigned)((G.nx + GR_TX - 1) / GR_TX), (unsigned)((G.ny + GR_TY - 1) / GR_TY),
+              (unsigned)((G.nz + GR_PLANES - 1) / GR_PLANES));
+}
+
+template <int HD, class T>
+__global__ void __launch_bounds__(GR_TX * GR_TY) k_grad(Geo G, Fields<T> W, Metrics M) {
+  constexpr int NS = 2 * HD + 2;  // ring slots: the 2 HD + 1 planes of a stencil and the one in flight
+  constexpr int RX = GR_TX + 2 * HD, RY = GR_TY + 2 * HD;
+  constexpr bool SIXTH = HD == 3;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* ring = reinterpret_cast<T*>(smraw);  // [slot][component][ry][rx]
+  auto R = [&](int slot, int c, int y, int x) -> T& { return ring[((slot * 3 + c) * RY + y) * RX + x]; };
+  const int tid = threadIdx.x;
+  const int bx = blockIdx.x * GR_TX, by = blockIdx.y * GR_TY;
+  const int k0 = blockIdx.z * GR_PLANES, k1 = min(G.nz, k0 + GR_PLANES);
+  const int tx = tid % GR_TX, ty = tid / GR_TX;
+  const int oi = bx + tx, oj = by + ty;
+  const bool own = oi < G.nx && oj < G.ny;
+  const int rx = tx + HD, ry = ty + HD;
+  const T* vel[3] = {W.u, W.v, W.w};
+  auto slot_of = [](int k) { return (k % NS + NS) % NS; };
+  // asynchronous copies of plane k's velocities (one cp.async group per plane)
+  auto fetch = [&](int k) {
+    if (k >= 0 && k < G.nz) {
+      const int slot = slot_of(k);
+      for (int c = tid; c < RX * RY; c += GR_TX * GR_TY) {
+        const int cx = c % RX, cy = c / RX;
+        const int i = bx - HD + cx, j = by - HD + cy;
+        if (i < 0 || i >= G.nx || j < 0 || j >= G.ny) continue;
+        const int64_t o = G.at(i, j, k);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const bool fits = c[a] >= HD && c[a] + HD < n[a];
-#pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            double d = 0.0;
-            if (fits) {
-              auto A = [&](int m) -> double {
-                return a == 0 ? V(slot_of(k), q, ry, rx + m) : (a == 1 ? V(slot_of(k), q, ry + m, rx)
-                                                                       : V(slot_of(k + m), q, ry, rx));
-              };
-              const double inv = invd[a][c[a]];
-              if constexpr (SIXTH)
-                d = ((1.0 / 60.0) * (-A(-3) + A(3)) + 0.15 * (A(-2) - A(2)) + 0.75 * (-A(-1) + A(1))) * inv;
-              else
-                d = ((2.0 / 3.0) * (-A(-1) + A(1)) - (1.0 / 12.0) * (-A(-2) + A(2))) * inv;
-            }
-            W.grad[3 * q + a][o] = (T)d;
-          }
+        for (int q = 0; q < 3; ++q) {
+          const unsigned sa = (unsigned)__cvta_generic_to_shared(&R(slot, q, cy, cx));
+          asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(vel[q] + o), "n"(sizeof(T))
+                       : "memory");
         }
       }
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  fetch(k0 - HD);
+  for (int kk = k0 - HD; kk < k1 + HD; ++kk) {
+    fetch(kk + 1);                                             // the next plane, in flight
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");     // plane kk has landed
     __syncthreads();
+    const int k = kk - HD;  // its derivatives use planes k - HD .. k + HD = kk
+    if (own && k >= k0 && k < k1) {
+      const int c3[3] = {oi, oj, k};
+      const int n[3] = {G.nx, G.ny, G.nz};
+      const double* invd[3] = {M.inv_dx, M.inv_dy, M.inv_dz};
+      const int64_t o = G.at(oi, oj, k);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const bool fits = c3[a] >= HD && c3[a] + HD < n[a];
+        const T inv = fits ? (T)invd[a][c3[a]] : T(0);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          T d = T(0);
+          if (fits) {
+            auto A = [&](int m) -> T {
+              return a == 0 ? R(slot_of(k), q, ry, rx + m)
+                            : (a == 1 ? R(slot_of(k), q, ry + m, rx) : R(slot_of(k + m), q, ry, rx));
+            };
+            if constexpr (SIXTH)
+              d = (T(1.0 / 60.0) * (-A(-3) + A(3)) + T(0.15) * (A(-2) - A(2)) + T(0.75) * (-A(-1) + A(1))) * inv;
+            else
+              d = (T(2.0 / 3.0) * (-A(-1) + A(1)) - T(1.0 / 12.0) * (-A(-2) + A(2))) * inv;
+          }
+          W.grad[3 * q + a][o] = d;
+        }
+      }
+    }
+    __syncthreads();  // the slot of plane kk - 2 HD is refilled by the next iteration's fetch
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // ---- SMS sub-grid model: 3D_solver/src/calc_les.f90:30-125 -------------------
