@@ -157,6 +157,15 @@ int oux_unpack_state(const oux_handle* h, const void* dev_layout_host, double* r
  * hi) into the lower ghost planes and the one from the rank above (its lo) into
  * the upper ones. */
 int oux_stage(oux_handle* h, int32_t stage, void* stream);
+/* One stage in two parts, so that a z slab's halo exchange overlaps the stage, as
+ * the reference posts its COMMZ exchange, computes the faces of the interior planes
+ * and then finishes the halo (3D_solver/src/calc_time_dev.f90.fypp:465-470,
+ * calc_para.f90:343-384).  part 1 updates the cells of planes [2g, nz-2g), which do
+ * not read the ghost planes, so the halo of the stage's source may still be in
+ * flight; part 2, after oux_halo_unpack, updates the planes next to both ends and
+ * fills the ghost cells.  Parts 1 then 2 give the bits of oux_stage; part 0 is
+ * oux_stage.  3D Euler / Navier-Stokes grids (not LES). */
+int oux_stage_part(oux_handle* h, int32_t stage, int32_t part, void* stream);
 int oux_halo_bytes(const oux_handle* h, int32_t stage, size_t* bytes);
 int oux_halo_pack(oux_handle* h, int32_t stage, void* lo_dev, void* hi_dev, void* stream);
 int oux_halo_unpack(oux_handle* h, int32_t stage, const void* lo_dev, const void* hi_dev, void* stream);

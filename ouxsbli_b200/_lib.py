@@ -52,6 +52,7 @@ def _load() -> C.CDLL:
         "oux_set_boundary_cells": (C.c_int, [vp, C.c_int32, vp]),
         "oux_set_boundary_order": (C.c_int, [vp, C.c_int32]),
         "oux_stage": (C.c_int, [vp, C.c_int32, vp]),
+        "oux_stage_part": (C.c_int, [vp, C.c_int32, C.c_int32, vp]),
         "oux_halo_bytes": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_size_t)]),
         "oux_halo_pack": (C.c_int, [vp, C.c_int32, vp, vp, vp]),
         "oux_halo_unpack": (C.c_int, [vp, C.c_int32, vp, vp, vp]),

@@ -31,7 +31,7 @@ SYMBOLS = [
     "oux_create", "oux_destroy", "oux_last_error", "oux_abi_version", "oux_state_bytes",
     "oux_scratch_bytes", "oux_layout_of", "oux_bind", "oux_set_state", "oux_get_state",
     "oux_pack_state", "oux_unpack_state", "oux_set_boundary", "oux_fill_ghosts", "oux_rhs",
-    "oux_stage", "oux_halo_bytes", "oux_halo_pack", "oux_halo_unpack",
+    "oux_stage", "oux_stage_part", "oux_halo_bytes", "oux_halo_pack", "oux_halo_unpack",
     "oux_set_boundary_farfield", "oux_set_boundary_cells", "oux_set_boundary_order", "oux_step", "oux_get_state_async",
     "oux_diagnostics", "oux_check_state", "oux_status", "oux_profile", "oux_profile_read",
     "oux_host_ref_diagnostics", "oux_launch_count", "oux_rhs_noalloc",

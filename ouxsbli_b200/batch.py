@@ -229,7 +229,7 @@ def _main(argv=None) -> int:
     """Run the seeded 2D vortex ensemble as one batch (a driver for profiling):
 
         python -m ouxsbli_b200.batch [--count 64] [--seed 0] [--steps 5] [--precision fp64]
-                                     [--pencil 8] [--chunk 2304]
+                                     [--pencil 8] [--chunk 2304] [--mode persistent|graph]
     """
     import argparse
     from .cases import vortex_ensemble, vortex_member
@@ -240,6 +240,7 @@ def _main(argv=None) -> int:
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--pencil", type=int, default=8)
     ap.add_argument("--chunk", type=int, default=8 * BATCH_THREADS)
+    ap.add_argument("--mode", default="persistent", choices=["persistent", "graph"])
     a = ap.parse_args(argv)
     dev = torch.device("cuda:0")
     solvers = []
@@ -248,7 +249,7 @@ def _main(argv=None) -> int:
         s = Solver(cfg, dev)
         s.set_state(qj)
         solvers.append(s)
-    b = Batch(solvers, Tuning(pencil=a.pencil, chunk=a.chunk))
+    b = Batch(solvers, Tuning(pencil=a.pencil, chunk=a.chunk, mode=a.mode))
     ms = _event_timer(b, a.steps)
     st = b.status()
     print(json.dumps({"solves": a.count, "interior_cells": b.interior_cells(), "ms_per_step": ms,

@@ -2,6 +2,7 @@
 // the stage driver that sequences the kernels of oux_kernels.cuh /
 // oux_sweep.cuh, and the C ABI declared in include/oux.h.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -229,6 +230,12 @@ Geo make_geo(const oux_config& c) {
   G.ylast = 0;
   G.bjac = nullptr;
   for (int f = 0; f < 6; ++f) G.bfix3[f] = nullptr;
+  G.pk0 = 0;
+  G.pk1 = G.nz;
+  G.gk0 = 0;
+  G.gk1 = G.nz;
+  G.sk0 = c.dim == 3 ? G.gz : 0;
+  G.sk1 = c.dim == 3 ? G.nz - G.gz : 1;
   G.uni = 0;
   const double* d[3] = {c.dx, c.dy, c.dim == 3 ? c.dz : nullptr};
   const int n[3] = {c.nx, c.ny, c.dim == 3 ? c.nz : 1};
@@ -245,8 +252,7 @@ Geo make_geo(const oux_config& c) {
 }
 
 struct ScratchPlan {
-  size_t fields = 0, racc = 0, q2 = 0, rs = 0, prim64 = 0, metrics = 0, partials = 0, status = 0, total = 0;
-  bool has_prim64 = false;  // the mixed form's FP64 primitives (hybrid scheme)
+  size_t fields = 0, racc = 0, q2 = 0, rs = 0, metrics = 0, partials = 0, status = 0, total = 0;
   int nfield_arrays = 0;
 };
 
@@ -274,8 +280,6 @@ ScratchPlan plan_scratch(const oux_config& c) {
   P.racc = off; off += (size_t)nv * vsb;
   P.q2 = off; off += round_up((size_t)nv * vse, 256);
   P.rs = off; off += (c.rk == 4 ? (size_t)nv * vsb : 0);
-  P.has_prim64 = c.precision == OUX_MIXED && c.scheme == OUX_HYBRID;
-  P.prim64 = off; off += P.has_prim64 ? 5 * vsb : 0;
   P.metrics = off;
   int nx = c.nx, ny = c.ny, nz = c.dim == 3 ? c.nz : 1;
   size_t mcount = (size_t)(nx - 1) + (ny - 1) + (c.dim == 3 ? nz - 1 : 1) + (size_t)nx * ny;
@@ -435,14 +439,11 @@ void carve(oux_handle* h) {
     double** fp[10] = {&h->W.rho, &h->W.u, &h->W.v, &h->W.w, &h->W.p, &h->W.T_, &h->W.mu, &h->W.sensor, &h->W.mut, &h->W.qc2};
     for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
     for (int q = 0; q < 9; ++q) h->W.grad[q] = P.nfield_arrays == 19 ? f + (10 + q) * vsb : nullptr;
-    for (int q = 0; q < 5; ++q) h->W.prim64[q] = nullptr;
   } else {
     float* f = reinterpret_cast<float*>(h->scratch + P.fields);
     float** fp[10] = {&h->Wf.rho, &h->Wf.u, &h->Wf.v, &h->Wf.w, &h->Wf.p, &h->Wf.T_, &h->Wf.mu, &h->Wf.sensor, &h->Wf.mut, &h->Wf.qc2};
     for (int q = 0; q < 10; ++q) *fp[q] = f + q * vsb;
     for (int q = 0; q < 9; ++q) h->Wf.grad[q] = P.nfield_arrays == 19 ? f + (10 + q) * vsb : nullptr;
-    double* p64 = reinterpret_cast<double*>(h->scratch + P.prim64);
-    for (int q = 0; q < 5; ++q) h->Wf.prim64[q] = P.has_prim64 ? p64 + q * vsb : nullptr;
   }
   h->Racc = reinterpret_cast<double*>(h->scratch + P.racc);
   h->Qs = h->scratch + P.q2;
@@ -522,17 +523,6 @@ int launch_prim_fused(const TQ* q, const TS* src, const Geo& G, Fields<T>& W, ou
   return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }
 
-// k_grad with a ring of HD cells, for the compute type T
-template <int HD, class T>
-int launch_grad(const Geo& G, Fields<T>& W, const Metrics& M, cudaStream_t s) {
-  const size_t smem = grad_smem<HD>(sizeof(T));
-  auto kern = k_grad<HD, T>;
-  static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (attr != cudaSuccess) return 1;
-  kern<<<grad_grid(G), GR_TX * GR_TY, smem, s>>>(G, W, M);
-  return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
-}
-
 // One stage: primitives of `src` (FP64 Q^n or the stage state), sensor, SGS
 // viscosity, then the sweeps.
 template <class T, class TS>
@@ -593,9 +583,11 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   }
   if (W.grad[0]) {  // node velocity gradients of the high-order viscous stencils
     Timed tm(h, KK_GRAD, s);
-    const int rc = h->vk == VK_C6 ? launch_grad<3>(G, W, h->M, s) : launch_grad<2>(G, W, h->M, s);
-    if (rc) return fail(OUX_E_CUDA, std::string("gradient pass: ") + cudaGetErrorString(cudaGetLastError()));
-    h->launches++;
+    if (G.gk1 > G.gk0) {
+      if (h->vk == VK_C6) k_grad<true, T><<<grad_grid(G), PLANE_THREADS, 0, s>>>(G, W, h->M);
+      else k_grad<false, T><<<grad_grid(G), PLANE_THREADS, 0, s>>>(G, W, h->M);
+      h->launches++;
+    }
   }
   if (h->les) {
     dim3 b(32, 4, 1), gr((G.nx - 2 + 31) / 32, (G.ny - 2 + 3) / 4, G.nz - 2);
@@ -642,41 +634,85 @@ int ghost(oux_handle* h, T* Q, cudaStream_t s) {
 // Stage st (0-based) of one time step with compute type T (double: plain FP64 form;
 // float: mixed form), followed by the ghost / boundary fill of the array it wrote.
 template <class T>
-int run_stage_n(oux_handle* h, int st, cudaStream_t s) {
+int run_stage_n(oux_handle* h, int st, cudaStream_t s, int part = 0) {
   double* Qn = h->Q;
   T* Qs = reinterpret_cast<T*>(h->Qs);
-  StepArgs<T> A = base_args<T>(h);
-  int rc;
-  if (h->cfg.rk == 3) {
-    // calc_time_dev.f90.fypp:81-101
-    if (st == 0) {
-      A.mode = CM_RK3_1; A.coef = 1.0;
-      if ((rc = run_stage<T, double>(h, Qn, A, s))) return rc;
-      ghost<T>(h, Qs, s);
-    } else if (st == 1) {
-      A.mode = CM_RK3_2; A.coef = 0.25; A.c1 = 0.75; A.c2 = 0.25; A.c4 = 1.0;
-      if ((rc = run_stage<T, T>(h, Qs, A, s))) return rc;
-      ghost<T>(h, Qs, s);
+  const int nst = h->cfg.rk == 3 ? 3 : 4;
+  // the stage's combination: calc_time_dev.f90.fypp:81-101 (RK3), 264-287 (RK4)
+  auto args = [&]() {
+    StepArgs<T> A = base_args<T>(h);
+    if (h->cfg.rk == 3) {
+      if (st == 0) {
+        A.mode = CM_RK3_1; A.coef = 1.0;
+      } else if (st == 1) {
+        A.mode = CM_RK3_2; A.coef = 0.25; A.c1 = 0.75; A.c2 = 0.25; A.c4 = 1.0;
+      } else {
+        A.mode = CM_RK3_3; A.coef = 2.0; A.c1 = 2.0; A.c2 = 1.0; A.c4 = 1.0 / 3.0;
+      }
     } else {
-      A.mode = CM_RK3_3; A.coef = 2.0; A.c1 = 2.0; A.c2 = 1.0; A.c4 = 1.0 / 3.0;
-      if ((rc = run_stage<T, T>(h, Qs, A, s))) return rc;
-      ghost<double>(h, Qn, s);
+      const double c1[3] = {0.5, 0.5, 1.0}, c2[3] = {1.0, 2.0, 2.0};
+      if (st < 3) {
+        A.mode = CM_RK4_S; A.coef = 1.0; A.c1 = c1[st]; A.c2 = c2[st];
+      } else {
+        A.mode = CM_RK4_4; A.coef = 1.0;
+      }
     }
+    return A;
+  };
+  // per-cell passes and sweeps over the plane ranges h->G holds
+  auto body = [&]() -> int {
+    StepArgs<T> A = args();
+    return st == 0 ? run_stage<T, double>(h, Qn, A, s) : run_stage<T, T>(h, Qs, A, s);
+  };
+  int rc = 0;
+  if (part == 0) {
+    if ((rc = body())) return rc;
   } else {
-    // calc_time_dev.f90.fypp:264-287
-    const double c1[3] = {0.5, 0.5, 1.0}, c2[3] = {1.0, 2.0, 2.0};
-    if (st < 3) {
-      A.mode = CM_RK4_S; A.coef = 1.0; A.c1 = c1[st]; A.c2 = c2[st];
-      if (st == 0) rc = run_stage<T, double>(h, Qn, A, s);
-      else rc = run_stage<T, T>(h, Qs, A, s);
-      if (rc) return rc;
-      ghost<T>(h, Qs, s);
+    // A z slab's stage in two parts (the reference's overlap of the COMMZ exchange,
+    // calc_time_dev.f90.fypp:465-470): part 1 updates the cells of planes [2g, nz-2g),
+    // whose stencils (g planes deep) do not reach the ghost planes, so it can run while
+    // the halo of its source is in flight; part 2, once the halo is unpacked, redoes
+    // the per-cell passes next to both ends (their ghost-plane inputs are now valid)
+    // and updates the cells of planes [g, 2g) and [nz-2g, nz-g), then fills the ghosts.
+    // Only a slab with halo planes at both ends (bc_z = 2), a halo of at least 2 planes
+    // and an interior part is split; otherwise part 1 does nothing and part 2 is the
+    // whole stage.
+    const Geo keep = h->G;
+    const int g = keep.g, nz = keep.nz;
+    const int hd = h->vk == VK_C6 ? 3 : 2;  // reach of the gradient pass along z
+    const bool split = keep.bcz == 2 && g >= 2 && nz - 2 * g > 2 * g;
+    auto narrow = [&](int p0, int p1, int q0, int q1, int c0, int c1) {
+      h->G.pk0 = p0; h->G.pk1 = p1; h->G.gk0 = q0; h->G.gk1 = q1; h->G.sk0 = c0; h->G.sk1 = c1;
+    };
+    if (!split) {
+      if (part == 2) rc = body();
+    } else if (part == 1) {
+      // per-cell passes over every plane (the values that read stale ghost planes are
+      // redone in part 2), the sweeps for the cells of [2g, nz-2g)
+      narrow(0, nz, 0, nz, 2 * g, nz - 2 * g);
+      rc = body();
     } else {
-      A.mode = CM_RK4_4; A.coef = 1.0;
-      if ((rc = run_stage<T, T>(h, Qs, A, s))) return rc;
-      ghost<double>(h, Qn, s);
+      // Part 1 has overwritten the cells of [2g, nz-2g) of the stage's output, which for
+      // an in-place stage is its source, so part 2 redoes only the per-cell values whose
+      // inputs reached the ghost planes, all of them computed from planes below 2g (above
+      // nz-2g): the primitives and sensor of planes [0, g+1) (their velocities reach g+2
+      // <= 2g-1... the sensor's ring one plane further) and the gradients of [0, g+hd)
+      // (they read the velocity fields, which the sweeps do not write).  Then it updates
+      // the cells of [g, 2g) and [nz-2g, nz-g).
+      narrow(0, g + 1, 0, g + hd, g, 2 * g);
+      rc = body();
+      if (!rc) {
+        narrow(nz - g - 1, nz, nz - g - hd, nz, nz - 2 * g, nz - g);
+        rc = body();
+      }
     }
+    h->G = keep;
+    if (rc) return rc;
+    if (part == 1) return OUX_OK;
   }
+  // ghost / boundary fill of the array the stage wrote
+  if (st == nst - 1) ghost<double>(h, Qn, s);
+  else ghost<T>(h, Qs, s);
   return OUX_OK;
 }
 
@@ -1029,6 +1065,21 @@ int oux_stage(oux_handle* h, int32_t stage, void* stream) {
   if (stage < 0 || stage >= nst) return fail(OUX_E_INVALID, "stage out of range (0..2 for RK3, 0..3 for RK4)");
   cudaStream_t s = (cudaStream_t)stream;
   int rc = h->mixed ? run_stage_n<float>(h, stage, s) : run_stage_n<double>(h, stage, s);
+  if (rc) return rc;
+  OUX_CUDA(cudaGetLastError());
+  return OUX_OK;
+}
+
+int oux_stage_part(oux_handle* h, int32_t stage, int32_t part, void* stream) {
+  if (!h) return fail(OUX_E_INVALID, "null handle");
+  const int nst = h->cfg.rk == 3 ? 3 : 4;
+  if (stage < 0 || stage >= nst) return fail(OUX_E_INVALID, "stage out of range (0..2 for RK3, 0..3 for RK4)");
+  if (part < 0 || part > 2) return fail(OUX_E_INVALID, "part must be 0 (whole stage), 1 (interior) or 2 (ends)");
+  if (part != 0 && (h->cfg.dim != 3 || h->les))
+    return fail(OUX_E_INVALID, "stage parts are built for 3D Euler / Navier-Stokes grids");
+  if (!h->Q) return fail(OUX_E_UNBOUND, "no device buffers bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = h->mixed ? run_stage_n<float>(h, stage, s, part) : run_stage_n<double>(h, stage, s, part);
   if (rc) return rc;
   OUX_CUDA(cudaGetLastError());
   return OUX_OK;

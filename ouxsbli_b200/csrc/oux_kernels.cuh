@@ -53,6 +53,12 @@ struct Geo {
   int ylast;                  // 1: y faces applied after x faces (corners take their y rule)
   const double* bjac;         // J(nx, ny), for the far-field and Neumann rules
   const double* bfix3[6];     // 3D: fixed values of the faces x lo .. z hi
+  int pk0, pk1;               // z planes [pk0, pk1) the primitive (+ sensor) pass of a stage covers
+  int gk0, gk1;               // z planes [gk0, gk1) the gradient pass covers
+  int sk0, sk1;               // z planes [sk0, sk1) of the cells the sweeps update
+                              // (defaults: every plane / every plane / every interior plane; a z
+                              // slab's stage split into an interior part and the parts next to
+                              // its ends narrows them, oux_stage_part)
   int uni;                    // bit a: every spacing along axis a is the same double (so are
                               // the inverse spacings), which lets the ME4 sweeps share the
                               // values of a face position between the three faces using it
@@ -64,9 +70,6 @@ template <class T> struct Fields {
   T *rho, *u, *v, *w, *p, *T_, *mu, *sensor, *mut, *qc2;
   // node velocity gradient d(vel_c)/d(x_a) at index 3*c + a (3D: 9, 2D: c,a < 2)
   T* grad[9];
-  // mixed form with the hybrid scheme: FP64 rho, u, v, w, p (the decode before it is
-  // rounded), for the shock-capturing faces, which reconstruct and evaluate in FP64
-  double* prim64[5];
 };
 
 struct Metrics {
@@ -120,11 +123,11 @@ __device__ __forceinline__ bool plane_cell(const Geo& G, int& i, int& j, int& k)
   if (t >= G.nx * G.ny) return false;
   j = t / G.nx;
   i = t - j * G.nx;
-  k = blockIdx.y;
+  k = G.pk0 + blockIdx.y;
   return true;
 }
 inline dim3 plane_grid(const Geo& G) {
-  return dim3((unsigned)((G.nx * G.ny + PLANE_THREADS - 1) / PLANE_THREADS), (unsigned)G.nz, 1);
+  return dim3((unsigned)((G.nx * G.ny + PLANE_THREADS - 1) / PLANE_THREADS), (unsigned)(G.pk1 - G.pk0), 1);
 }
 
 // ---- prim: src/calc_physical_quantities.f90:60-116 (3D), :7-57 (2D) -------
@@ -190,9 +193,6 @@ __device__ __forceinline__ void prim_mx_cell(const double* Qn, const float* dQ, 
     p = K.gamma_1 * (Jv * q[3] - 0.5 * rho * (u * u + v * v));
   }
   double temp = p / (K.R * rho);
-  if (W.prim64[0]) {
-    W.prim64[0][o] = rho; W.prim64[1][o] = u; W.prim64[2][o] = v; W.prim64[3][o] = w; W.prim64[4][o] = p;
-  }
   W.rho[o] = (float)rho; W.u[o] = (float)u; W.v[o] = (float)v;
   if constexpr (DIM == 3) W.w[o] = (float)w;
   W.p[o] = (float)(p - K.p_ref);
@@ -376,7 +376,7 @@ template <int HD> __host__ __device__ constexpr size_t prim_fused_smem() {
 
 inline dim3 prim_fused_grid(const Geo& G) {
   return dim3((unsigned)((G.nx + PS_TX - 1) / PS_TX), (unsigned)((G.ny + PS_TY - 1) / PS_TY),
-              (unsigned)((G.nz + PS_PLANES - 1) / PS_PLANES));
+              (unsigned)((G.pk1 - G.pk0 + PS_PLANES - 1) / PS_PLANES));
 }
 
 template <int HD, bool SENSOR, bool VISC, bool MX, class TS, class T>
@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_fused(const TS* __restri
   auto V = [&](int slot, int c, int y, int x) -> double& { return vel[((slot * 3 + c) * RY + y) * RX + x]; };
   const int tid = threadIdx.x;
   const int bx = blockIdx.x * PS_TX, by = blockIdx.y * PS_TY;
-  const int k0 = blockIdx.z * PS_PLANES, k1 = min(G.nz, k0 + PS_PLANES);
+  const int k0 = G.pk0 + blockIdx.z * PS_PLANES, k1 = min(G.pk1, k0 + PS_PLANES);
   const int tx = tid % PS_TX, ty = tid / PS_TX;
   const int oi = bx + tx, oj = by + ty;  // this thread's own cell
   const bool own = oi < G.nx && oj < G.ny;
@@ -465,96 +465,48 @@ __global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_fused(const TS* __restri
 }
 
 // ---- node velocity gradients (3D, the high-order viscous stencils) ----------------
-// grad[3c + a] = d(velocity c)/d(axis a) by the 6th-order (HD = 3: Central-6) or
-// 4th-order (HD = 2: Central-4, ME4) central node derivative of the viscous loaders
+// grad[3c + a] = d(velocity c)/d(axis a) by the 6th-order (SIXTH: Central-6) or 4th-order
+// (Central-4, ME4) central node derivative of the viscous loaders
 // (load_smem_visc_cent.f90.fypp:51-70, load_smem_visc_me4_base.f90:120-127), at every
-// cell whose stencil fits in the grid (else 0: no sweep reads those).  A block owns a
-// GR_TX x GR_TY column of cells and marches along z; the velocities of each plane
-// (its cells and a ring of HD cells) come into a shared-memory ring with asynchronous
-// copies issued one plane ahead, so the copies of plane k + 1 are in flight while the
-// derivatives of plane k - HD are evaluated.
-constexpr int GR_TX = 32, GR_TY = 8, GR_PLANES = 32;
-
-template <int HD> __host__ __device__ constexpr size_t grad_smem(int tsize) {
-  return (size_t)tsize * (2 * HD + 2) * 3 * (GR_TY + 2 * HD) * (GR_TX + 2 * HD);
+// cell whose stencil fits in the grid (else 0: no sweep reads those), on the z planes
+// [gk0, gk1).  Plane-flattened like k_prim: the neighbours come through L1 / L2.  (A
+// z-marching variant with a shared-memory ring of the velocities filled by cp.async one
+// plane ahead measured slower on B200 at 518^3: 3.78 against 2.96 ms.)
+template <bool SIXTH, class T>
+__device__ __forceinline__ T node_deriv(const T* a, int64_t o, int64_t st, T inv) {
+  auto A = [&](int64_t q) { return __ldg(a + q); };
+  if constexpr (SIXTH)
+    return (T(1.0 / 60.0) * (-A(o - 3 * st) + A(o + 3 * st)) + T(0.15) * (A(o - 2 * st) - A(o + 2 * st)) +
+            T(0.75) * (-A(o - st) + A(o + st))) * inv;
+  else
+    return (T(2.0 / 3.0) * (-A(o - st) + A(o + st)) - T(1.0 / 12.0) * (-A(o - 2 * st) + A(o + 2 * st))) * inv;
 }
 
 inline dim3 grad_grid(const Geo& G) {
-  return dim3((unsigned)((G.nx + GR_TX - 1) / GR_TX), (unsigned)((G.ny + GR_TY - 1) / GR_TY),
-              (unsigned)((G.nz + GR_PLANES - 1) / GR_PLANES));
+  return dim3((unsigned)((G.nx * G.ny + PLANE_THREADS - 1) / PLANE_THREADS), (unsigned)(G.gk1 - G.gk0), 1);
 }
 
-template <int HD, class T>
-__global__ void __launch_bounds__(GR_TX * GR_TY) k_grad(Geo G, Fields<T> W, Metrics M) {
-  constexpr int NS = 2 * HD + 2;  // ring slots: the 2 HD + 1 planes of a stencil and the one in flight
-  constexpr int RX = GR_TX + 2 * HD, RY = GR_TY + 2 * HD;
-  constexpr bool SIXTH = HD == 3;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* ring = reinterpret_cast<T*>(smraw);  // [slot][component][ry][rx]
-  auto R = [&](int slot, int c, int y, int x) -> T& { return ring[((slot * 3 + c) * RY + y) * RX + x]; };
-  const int tid = threadIdx.x;
-  const int bx = blockIdx.x * GR_TX, by = blockIdx.y * GR_TY;
-  const int k0 = blockIdx.z * GR_PLANES, k1 = min(G.nz, k0 + GR_PLANES);
-  const int tx = tid % GR_TX, ty = tid / GR_TX;
-  const int oi = bx + tx, oj = by + ty;
-  const bool own = oi < G.nx && oj < G.ny;
-  const int rx = tx + HD, ry = ty + HD;
+template <bool SIXTH, class T>
+__global__ void __launch_bounds__(PLANE_THREADS) k_grad(Geo G, Fields<T> W, Metrics M) {
+  const int t = blockIdx.x * PLANE_THREADS + threadIdx.x;
+  if (t >= G.nx * G.ny) return;
+  int c[3];
+  c[1] = t / G.nx;
+  c[0] = t - c[1] * G.nx;
+  c[2] = G.gk0 + blockIdx.y;
+  constexpr int HD = SIXTH ? 3 : 2;
+  const int n[3] = {G.nx, G.ny, G.nz};
+  const int64_t st[3] = {1, G.sx, G.plane};
+  const double* invd[3] = {M.inv_dx, M.inv_dy, M.inv_dz};
   const T* vel[3] = {W.u, W.v, W.w};
-  auto slot_of = [](int k) { return (k % NS + NS) % NS; };
-  // asynchronous copies of plane k's velocities (one cp.async group per plane)
-  auto fetch = [&](int k) {
-    if (k >= 0 && k < G.nz) {
-      const int slot = slot_of(k);
-      for (int c = tid; c < RX * RY; c += GR_TX * GR_TY) {
-        const int cx = c % RX, cy = c / RX;
-        const int i = bx - HD + cx, j = by - HD + cy;
-        if (i < 0 || i >= G.nx || j < 0 || j >= G.ny) continue;
-        const int64_t o = G.at(i, j, k);
+  const int64_t o = G.at(c[0], c[1], c[2]);
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          const unsigned sa = (unsigned)__cvta_generic_to_shared(&R(slot, q, cy, cx));
-          asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(vel[q] + o), "n"(sizeof(T))
-                       : "memory");
-        }
-      }
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-  };
-  fetch(k0 - HD);
-  for (int kk = k0 - HD; kk < k1 + HD; ++kk) {
-    fetch(kk + 1);                                             // the next plane, in flight
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");     // plane kk has landed
-    __syncthreads();
-    const int k = kk - HD;  // its derivatives use planes k - HD .. k + HD = kk
-    if (own && k >= k0 && k < k1) {
-      const int c3[3] = {oi, oj, k};
-      const int n[3] = {G.nx, G.ny, G.nz};
-      const double* invd[3] = {M.inv_dx, M.inv_dy, M.inv_dz};
-      const int64_t o = G.at(oi, oj, k);
+  for (int a = 0; a < 3; ++a) {
+    const bool fits = c[a] >= HD && c[a] + HD < n[a];
+    const T inv = fits ? (T)invd[a][c[a]] : T(0);
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const bool fits = c3[a] >= HD && c3[a] + HD < n[a];
-        const T inv = fits ? (T)invd[a][c3[a]] : T(0);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          T d = T(0);
-          if (fits) {
-            auto A = [&](int m) -> T {
-              return a == 0 ? R(slot_of(k), q, ry, rx + m)
-                            : (a == 1 ? R(slot_of(k), q, ry + m, rx) : R(slot_of(k + m), q, ry, rx));
-            };
-            if constexpr (SIXTH)
-              d = (T(1.0 / 60.0) * (-A(-3) + A(3)) + T(0.15) * (A(-2) - A(2)) + T(0.75) * (-A(-1) + A(1))) * inv;
-            else
-              d = (T(2.0 / 3.0) * (-A(-1) + A(1)) - T(1.0 / 12.0) * (-A(-2) + A(2))) * inv;
-          }
-          W.grad[3 * q + a][o] = d;
-        }
-      }
-    }
-    __syncthreads();  // the slot of plane kk - 2 HD is refilled by the next iteration's fetch
+    for (int q = 0; q < 3; ++q) W.grad[3 * q + a][o] = fits ? node_deriv<SIXTH, T>(vel[q], o, st[a], inv) : T(0);
   }
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // ---- SMS sub-grid model: 3D_solver/src/calc_les.f90:30-125 -------------------

@@ -21,7 +21,8 @@ int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
   if (attr_rc != cudaSuccess) return 1;
   const Geo& G = A.G;
   const int g = G.g;
-  const int Nx = G.nx - 2 * G.gx, Ny = G.ny - 2 * G.gy, Nz = DIM == 3 ? G.nz - 2 * G.gz : 1;
+  const int Nx = G.nx - 2 * G.gx, Ny = G.ny - 2 * G.gy, Nz = DIM == 3 ? G.sk1 - G.sk0 : 1;
+  if (Nz <= 0) return 0;  // an empty part of a split stage
   dim3 block(sweep_threads<DIR>(), 1, 1);
   dim3 grid;
   if (DIR == 0) grid = dim3((Nx + 31) / 32, (Ny + SWEEP_BR - 1) / SWEEP_BR, Nz);

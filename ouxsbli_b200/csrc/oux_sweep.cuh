@@ -9,7 +9,6 @@
 // sweep; it holds rho,u,v,w,p,T,mu,mut,qc2,sensor and the four transverse
 // velocity derivatives the viscous stencils need.
 #pragma once
-#include <type_traits>
 #include "oux_kernels.cuh"
 
 namespace oux {
@@ -109,34 +108,8 @@ __device__ __forceinline__ T node_d(const T* a, int64_t o, int64_t st, T inv) {
 // s(f,m) reads tile field f at stencil point m (0 .. 2io+1).
 // KONLY: every solve of the launch uses KEEP (compile-time; the other schemes'
 // code and registers drop out).
-// The mixed form's shock-capturing faces (the hybrid scheme's HRSLAU2 faces): MUSCL
-// reconstruction, with its TVD limiter decisions, and HRSLAU2 in FP64 from the FP64
-// primitives at the stencil's global offsets q, so that those decisions are the ones
-// the FP64 solve makes for the same state.  The sweep evaluates these faces in a phase
-// of their own, after the FP32 faces, so that their FP64 registers do not add to the
-// FP32 flux path's.
-template <int ORDER>
-__device__ __forceinline__ void shock_face_fp64(double* const prim64[5], const int64_t (&q)[ORDER], int tvd, int slau,
-                                             double thr, double fd, int nd, double gam, double g_g1, double Fd[5]) {
-  double r6[ORDER], u6[ORDER], v6[ORDER], w6[ORDER], p6[ORDER];
-#pragma unroll
-  for (int m = 0; m < ORDER; ++m) {
-    r6[m] = prim64[0][q[m]]; u6[m] = prim64[1][q[m]]; v6[m] = prim64[2][q[m]];
-    w6[m] = prim64[3][q[m]]; p6[m] = prim64[4][q[m]];
-  }
-  double Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, Lp, Rp;
-  reconstruct<ORDER>(tvd, thr, fd, r6, Lr, Rr);
-  reconstruct<ORDER>(tvd, thr, fd, u6, Lu, Ru);
-  reconstruct<ORDER>(tvd, thr, fd, v6, Lv, Rv);
-  reconstruct<ORDER>(tvd, thr, fd, w6, Lw, Rw);
-  reconstruct<ORDER>(tvd, thr, fd, p6, Lp, Rp);
-  const double un1 = nd == 0 ? Lu : (nd == 1 ? Lv : Lw), un2 = nd == 0 ? Ru : (nd == 1 ? Rv : Rw);
-  slau_flux<double, false>(slau == 1, Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, un1, un2, Lp, Rp, nd, 1.0, gam, g_g1, Fd);
-}
-
-// off(m): the global offset of stencil point m (used by the mixed form's FP64 faces).
-template <int ORDER, bool KONLY, class T, class Acc, class Off>
-__device__ __forceinline__ void conv_flux(const StepArgs<T>& A, const Acc& s, T fd, int nd, T F[5], const Off& off) {
+template <int ORDER, bool KONLY, class T, class Acc>
+__device__ __forceinline__ void conv_flux(const StepArgs<T>& A, const Acc& s, T fd, int nd, T F[5]) {
   constexpr int NS = ORDER;  // 2io+2 stencil points
   T rho[NS], u[NS], v[NS], w[NS], p[NS], Tt[NS];
 #pragma unroll
@@ -152,14 +125,6 @@ __device__ __forceinline__ void conv_flux(const StepArgs<T>& A, const Acc& s, T 
   if (KONLY || scheme == 0 || (scheme == 3 && fd <= T(A.K.threshold))) {
     keep_flux<ORDER, T, MX>(rho, u, v, w, un, p, Tt, nd, T(A.K.R_over_gamma_1), F, pr, tr);
     return;
-  }
-  if constexpr (MX) {
-    // the hybrid scheme's shock-capturing faces: their convective flux is evaluated in
-    // FP64 in a later phase of the sweep (shock_face_fp64); here it is left at 0
-    if (scheme == 3 && A.W.prim64[0]) {
-      F[0] = F[1] = F[2] = F[3] = F[4] = T(0);
-      return;
-    }
   }
   T Lr, Rr, Lu, Ru, Lv, Rv, Lw, Rw, Lp, Rp;
   const T thr = T(A.K.threshold);
@@ -762,16 +727,17 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   const int nthr = nthr_all;
   // block origin (first owned cell) in padded coordinates
   int bx0, by0, bz0;
+  // z: the cells of planes [sk0, sk1) (every interior plane unless a stage part narrows it)
   if constexpr (DIR == 0) {
-    bx0 = gx + 32 * b0; by0 = gy + ROWS * b1; bz0 = (DIM == 3) ? gz + b2 : 0;
+    bx0 = gx + 32 * b0; by0 = gy + ROWS * b1; bz0 = (DIM == 3) ? G.sk0 + b2 : 0;
   } else if constexpr (DIR == 1) {
-    bx0 = gx + 32 * b0; by0 = gy + ROWS * b1; bz0 = (DIM == 3) ? gz + b2 : 0;
+    bx0 = gx + 32 * b0; by0 = gy + ROWS * b1; bz0 = (DIM == 3) ? G.sk0 + b2 : 0;
   } else {
-    bx0 = gx + 32 * b0; bz0 = gz + ROWS * b1; by0 = gy + b2;
+    bx0 = gx + 32 * b0; bz0 = G.sk0 + ROWS * b1; by0 = gy + b2;
   }
   const int64_t stv[3] = {1, G.sx, G.plane};
   const int nsweep = DIR == 0 ? G.nx : (DIR == 1 ? G.ny : G.nz);
-  const int ext[3] = {gx + Nx, gy + Ny, gz + Nz};
+  const int ext[3] = {gx + Nx, gy + Ny, DIM == 3 ? G.sk1 : gz + Nz};
 
   // ---- operand prefetch (y/z sweeps): the thread that owns a cell copies it ----
   constexpr bool PF_ON = PF > 0 && DIR != 0;
@@ -974,12 +940,6 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       auto sc = [&](int field, int m) -> T { return tile[field * NC + cb + m * step]; };
       T fd = T(0);
       if (!KONLY && A.scheme != 0) fd = T(0.5) * (st0(TF_SEN, 2) + st0(TF_SEN, 3));
-      // global offsets of the stencil of a face evaluated at order `ord`: point m is the
-      // cell f - (ord / 2 - 1) + m along the sweep
-      const int64_t of = G.at(fc[0], fc[1], DIM == 3 ? fc[2] : 0);
-      auto off_of = [&](int ord) {
-        return [=](int m) -> int64_t { return of + (int64_t)(m - (ord / 2 - 1)) * stv[DIR]; };
-      };
       if constexpr (DIM == 2 || VK == VK_EULER || WALL) {
         // non-periodic x / y (/ z): every face, the stencil order lowered next to the
         // boundary as the reference's boundary kernels do (2D_solver/src/calc_{slau,
@@ -993,16 +953,16 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         if (nonper)
           lo = (ORDER == 6 && f >= 2 && f <= nn - 4) ? 6 : (ORDER >= 4 && f >= 1 && f <= nn - 3) ? 4 : 2;
         if (lo == ORDER) {
-          conv_flux<ORDER, KONLY>(A, sc, fd, DIR, F, off_of(ORDER));
+          conv_flux<ORDER, KONLY>(A, sc, fd, DIR, F);
         } else if (lo == 4) {
           auto s4 = [&](int field, int m) -> T { return tile[field * NC + base + (TILE_HALO - 2 + m) * step]; };
-          conv_flux<4, KONLY>(A, s4, fd, DIR, F, off_of(4));
+          conv_flux<4, KONLY>(A, s4, fd, DIR, F);
         } else {
           auto s2 = [&](int field, int m) -> T { return tile[field * NC + base + (TILE_HALO - 1 + m) * step]; };
-          conv_flux<2, KONLY>(A, s2, fd, DIR, F, off_of(2));
+          conv_flux<2, KONLY>(A, s2, fd, DIR, F);
         }
       } else {
-        conv_flux<ORDER, KONLY>(A, sc, fd, DIR, F, off_of(ORDER));
+        conv_flux<ORDER, KONLY>(A, sc, fd, DIR, F);
       }
       if constexpr (VK != VK_EULER && !SHARE) {
         T vo[4];
@@ -1076,51 +1036,6 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       Fs[4 * (TX * TY) + tid] = (double)((T)Fs[4 * (TX * TY) + tid] - vo[3]);
     }
     __syncthreads();
-  }
-
-  // ---- mixed form, hybrid scheme: the shock-capturing faces' convective flux in FP64 ----
-  // (the face phase left it at 0 and subtracted the viscous terms; adding them in the
-  // compute type gives the rounding of the one-pass flux F - vo)
-  if constexpr (MXC && !KONLY) {
-    if (A.scheme == 3 && A.W.prim64[0]) {
-      if (face_valid) {
-        int fc[3] = {bx0, by0, bz0};
-        int base, step;
-        if constexpr (DIR == 0) {
-          fc[0] = bx0 - 1 + tx; fc[1] = by0 + ty; base = ty * TL + tx; step = 1;
-        } else {
-          fc[0] = bx0 + tx; fc[DIR] = (DIR == 1 ? by0 : bz0) - 1 + ty; base = ty * 32 + tx; step = 32;
-        }
-        const T fd = T(0.5) * (tile[TF_SEN * NC + base + 2 * step] + tile[TF_SEN * NC + base + 3 * step]);
-        if (!(fd <= T(A.K.threshold))) {
-          // the face's stencil order (lowered next to a non-periodic boundary as in the face phase)
-          const int f = fc[DIR];
-          int lo = ORDER;
-          if constexpr (DIM == 2 || VK == VK_EULER || WALL) {
-            const int nn = DIR == 0 ? G.nx : (DIR == 1 ? G.ny : G.nz);
-            const bool nonper = DIR == 0 ? (bool)G.bcx : (DIR == 1 ? (bool)G.bcy : G.bcz == 1);
-            if (nonper)
-              lo = (ORDER == 6 && f >= 2 && f <= nn - 4) ? 6 : (ORDER >= 4 && f >= 1 && f <= nn - 3) ? 4 : 2;
-          }
-          const int64_t of = G.at(fc[0], fc[1], DIM == 3 ? fc[2] : 0);
-          double Fd[5];
-          auto run = [&](auto ord_c) {
-            constexpr int OR = decltype(ord_c)::value;
-            int64_t q[OR];
-#pragma unroll
-            for (int m = 0; m < OR; ++m) q[m] = of + (int64_t)(m - (OR / 2 - 1)) * stv[DIR];
-            shock_face_fp64<OR>(A.W.prim64, q, A.tvd, A.slau, A.K.threshold, (double)fd, DIR, A.K.gamma,
-                                A.K.gamma_over_gamma_1, Fd);
-          };
-          if (lo == 6) run(std::integral_constant<int, 6>{});
-          else if (lo == 4) run(std::integral_constant<int, 4>{});
-          else run(std::integral_constant<int, 2>{});
-#pragma unroll
-          for (int l = 0; l < 5; ++l) Fs[l * (TX * TY) + tid] = (double)((T)Fd[l] + (T)Fs[l * (TX * TY) + tid]);
-        }
-      }
-      __syncthreads();
-    }
   }
 
   // ---- cells: difference, accumulate, combine ----

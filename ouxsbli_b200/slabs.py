@@ -97,11 +97,19 @@ def halo_exchange(send_lo: torch.Tensor, send_hi: torch.Tensor, recv_lo: torch.T
     Sends and receives are posted in the same order on every rank (up first, then
     down) and tagged, so two ranks that are each other's upper and lower neighbour
     match them correctly."""
+    for req in post_halo_exchange(send_lo, send_hi, recv_lo, recv_hi, rank, world, group, periodic):
+        req.wait()
+
+
+def post_halo_exchange(send_lo: torch.Tensor, send_hi: torch.Tensor, recv_lo: torch.Tensor, recv_hi: torch.Tensor,
+                       rank: int, world: int, group=None, periodic: bool = True) -> list:
+    """halo_exchange without the wait: the posted requests (NCCL: waiting on one makes
+    the current CUDA stream wait for it, so the caller can queue work in between)."""
     if world == 1:
         if periodic:
             recv_lo.copy_(send_hi)
             recv_hi.copy_(send_lo)
-        return
+        return []
     up, down = (rank + 1) % world, (rank - 1) % world
     has_up = periodic or rank < world - 1
     has_down = periodic or rank > 0
@@ -113,9 +121,7 @@ def halo_exchange(send_lo: torch.Tensor, send_hi: torch.Tensor, recv_lo: torch.T
         ops.append(dist.P2POp(dist.isend, send_lo, down, group, TAG_DOWN))
     if has_up:
         ops.append(dist.P2POp(dist.irecv, recv_hi, up, group, TAG_DOWN))
-    if ops:
-        for req in dist.batch_isend_irecv(ops):
-            req.wait()
+    return dist.batch_isend_irecv(ops) if ops else []
 
 
 class SlabSolver:
@@ -142,11 +148,13 @@ class SlabSolver:
     def get_state(self) -> np.ndarray:
         return self.solver.get_state()
 
-    # the three steps of one stage, split so that a group of slabs in one process can
+    # the steps of one stage, split so that a group of slabs in one process can
     # interleave them
-    def run_stage(self, st: int) -> None:
+    def run_stage(self, st: int, part: int = 0) -> None:
+        """Stage st whole (part 0), or its interior planes (1) / its end planes and the
+        ghost fill (2): oux_stage_part."""
         with torch.cuda.device(self.device):
-            check(LIB.oux_stage(self.solver._h, st, self.solver._s()))
+            check(LIB.oux_stage_part(self.solver._h, st, part, self.solver._s()))
 
     def pack(self, st: int) -> tuple[torch.Tensor, torch.Tensor]:
         n = self._halo_bytes(st)
@@ -167,15 +175,44 @@ class SlabSolver:
                                       self.solver._s()))
 
     def step(self, nsteps: int = 1) -> None:
-        """nsteps time steps, exchanging halos with the neighbouring ranks after each stage."""
+        """nsteps time steps, exchanging halos with the neighbouring ranks after each stage.
+
+        Each exchange overlaps the next stage's interior part: the stage's end planes are
+        packed and posted, the next stage updates its interior planes (which do not read
+        the ghost planes), then waits for the halo, unpacks it and updates its end
+        planes (calc_time_dev.f90.fypp:465-470).  The last exchange completes before
+        returning."""
+        if self.world == 1:  # a slab exchanging with itself has nothing to overlap
+            for _ in range(nsteps):
+                for st in range(self.stages):
+                    self.run_stage(st)
+                    self._finish(self._post(st))
+            return
+        pending = None
         for _ in range(nsteps):
             for st in range(self.stages):
-                self.run_stage(st)
-                send_lo, send_hi = self.pack(st)
-                recv_lo, recv_hi = self.recv_buffers(st)
-                halo_exchange(send_lo, send_hi, recv_lo, recv_hi, self.rank, self.world, self.group,
-                              periodic=self.global_cfg.bc_z == 0)
-                self.unpack(st)
+                self.run_stage(st, 1)
+                pending = self._finish(pending)
+                self.run_stage(st, 2)
+                pending = self._post(st)
+        self._finish(pending)
+
+    def _post(self, st: int):
+        send_lo, send_hi = self.pack(st)
+        recv_lo, recv_hi = self.recv_buffers(st)
+        with torch.cuda.device(self.device):
+            reqs = post_halo_exchange(send_lo, send_hi, recv_lo, recv_hi, self.rank, self.world, self.group,
+                                      periodic=self.global_cfg.bc_z == 0)
+        return reqs, st
+
+    def _finish(self, pending):
+        if pending is not None:
+            reqs, st = pending
+            with torch.cuda.device(self.device):
+                for req in reqs:
+                    req.wait()
+            self.unpack(st)
+        return None
 
     def close(self) -> None:
         self.solver.close()
@@ -195,21 +232,33 @@ class LocalSlabs:
             s.set_global_state(qj)
 
     def step(self, nsteps: int = 1) -> None:
+        """As SlabSolver.step, every slab's part at a time: interior parts, then the
+        previous stage's halo copies and unpacks, then the end parts and packs."""
         W = self.world
+        periodic = self.cfg.bc_z == 0
+        sent = prev = None
         for _ in range(nsteps):
             for st in range(self.slabs[0].stages):
                 for s in self.slabs:
-                    s.run_stage(st)
-                sent = [s.pack(st) for s in self.slabs]
-                periodic = self.cfg.bc_z == 0
-                for r, s in enumerate(self.slabs):
-                    recv_lo, recv_hi = s.recv_buffers(st)
-                    if periodic or r > 0:
-                        recv_lo.copy_(sent[(r - 1) % W][1])  # the highest planes of the slab below
-                    if periodic or r < W - 1:
-                        recv_hi.copy_(sent[(r + 1) % W][0])  # the lowest planes of the slab above
+                    s.run_stage(st, 1)
+                if sent is not None:
+                    self._deliver(sent, prev, periodic)
                 for s in self.slabs:
-                    s.unpack(st)
+                    s.run_stage(st, 2)
+                sent, prev = [s.pack(st) for s in self.slabs], st
+        if sent is not None:
+            self._deliver(sent, prev, periodic)
+
+    def _deliver(self, sent, st: int, periodic: bool) -> None:
+        W = self.world
+        for r, s in enumerate(self.slabs):
+            recv_lo, recv_hi = s.recv_buffers(st)
+            if periodic or r > 0:
+                recv_lo.copy_(sent[(r - 1) % W][1])  # the highest planes of the slab below
+            if periodic or r < W - 1:
+                recv_hi.copy_(sent[(r + 1) % W][0])  # the lowest planes of the slab above
+        for s in self.slabs:
+            s.unpack(st)
 
     def get_state(self) -> np.ndarray:
         """The global state reassembled (ghost planes from the first and last slab)."""

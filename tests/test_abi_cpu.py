@@ -172,3 +172,19 @@ def test_bench_walls_grids_are_accepted():
         rc, h = create(cfg)
         assert rc == 0, _lib.LIB.oux_last_error().decode()
         _lib.LIB.oux_destroy(h)
+
+
+def test_stage_part_argument_checks_without_a_device():
+    """oux_stage_part: part 0..2 only; the split parts are built for 3D Euler /
+    Navier-Stokes (not LES, not 2D); the checks come before any device work."""
+    rc, h = create(small_cfg(bc_z=2))
+    assert rc == 0
+    assert _lib.LIB.oux_stage_part(h, 0, 3, None) == _lib.OUX_E_INVALID
+    assert _lib.LIB.oux_stage_part(h, 3, 1, None) == _lib.OUX_E_INVALID  # RK3 has stages 0..2
+    assert _lib.LIB.oux_stage_part(h, 0, 1, None) == _lib.OUX_E_UNBOUND  # valid arguments, nothing bound
+    _lib.LIB.oux_destroy(h)
+    rc, h = create(small_cfg(visc="LES"))
+    assert rc == 0
+    assert _lib.LIB.oux_stage_part(h, 0, 1, None) == _lib.OUX_E_INVALID
+    assert "Navier-Stokes" in _lib.LIB.oux_last_error().decode()
+    _lib.LIB.oux_destroy(h)
