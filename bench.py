@@ -547,11 +547,12 @@ def run_commz(args):
 
 # algorithmic HBM bytes per interior cell of each kernel launch (FP64, 3D, RK3 averaged
 # over the three stages): fields read / state and accumulators read and written once
-ALG_CELL = {"prim": 96.0, "sensor": 32.0, "prim_sensor": 104.0, "grad": 96.0,
+ALG_CELL = {"prim": 96.0, "sensor": 32.0, "prim_sensor": 104.0, "grad": 104.0,
             "sweep_x": 136.0, "sweep_y": 176.0, "sweep_z": (216.0 + 256.0 + 256.0) / 3.0}
 # kernel kinds of oux_profile_read (enum KernelKind of oux_api.cu); prim_sensor: the 3D
-# pass that writes the primitive fields and the Ducros sensor (sensor schemes); grad:
-# the node velocity gradients (Central-4/6 and ME4 viscous stencils)
+# pass that writes the primitive fields and the Ducros sensor (the mixed form's sensor
+# schemes); grad: the node velocity gradients (Central-4/6 and ME4 viscous stencils), and
+# in FP64 the Ducros sensor too
 KINDS = ["prim", "sensor", "sgs", "sgs_edges", "sweep_x", "sweep_y", "sweep_z", "ghost", "prim_sensor", "grad"]
 
 

@@ -259,12 +259,14 @@ struct ScratchPlan {
 constexpr int DIAG_BLOCKS = 1184;  // 8 blocks per SM on 148 SMs; fixed for a deterministic sum
 
 // Whether a configuration's sweeps read the node velocity gradients from fields
-// (k_grad writes them; sweep_uses_grads): periodic 3D grids with Central-4/6 or ME4
-// viscous stencils.
+// (k_grad writes them; sweep_uses_grads): 3D grids with Central-4/6 or ME4 viscous
+// stencils, periodic or walled.
 bool uses_grads(const oux_config& c) {
   std::string why;
   const int vk = visc_kind(&c, why);
-  return c.dim == 3 && (vk == VK_C6 || vk == VK_C4 || vk == VK_ME4);
+  if (vk < 0) return false;
+  const int vb = vk_base(vk);
+  return c.dim == 3 && (vb == VK_C6 || vb == VK_C4 || vb == VK_ME4);
 }
 
 ScratchPlan plan_scratch(const oux_config& c) {
@@ -533,7 +535,11 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
   bool visc = c.visc != OUX_EULER;
   const bool sens = c.scheme != OUX_KEEP;
-  if (G.dim == 3 && sens) {
+  // FP64 with gradient fields: the plain primitive pass, and the sensor in the gradient
+  // pass (which reads the neighbour velocities anyway); otherwise a 3D sensor scheme
+  // takes the fused primitive + sensor pass (the mixed form's sensor from FP64 velocities)
+  const bool sens_in_grad = sens && W.grad[0] != nullptr && sizeof(T) == sizeof(double);
+  if (G.dim == 3 && sens && !sens_in_grad) {
     // primitives and sensor in one z-marching pass
     Timed tm(h, KK_PRIM_FUSED, s);
     int rc;
@@ -568,7 +574,7 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
     }
     h->launches++;
   }
-  if (G.dim == 2 && c.scheme != OUX_KEEP) {  // Ducros sensor (3D: fused above)
+  if (G.dim == 2 && c.scheme != OUX_KEEP) {  // Ducros sensor (3D: fused into another pass)
     Timed tm(h, KK_SENSOR, s);
     const dim3 gb = plane_grid(G);
     if constexpr (sizeof(T) < sizeof(double)) {
@@ -584,8 +590,13 @@ int run_stage(oux_handle* h, const TS* src, StepArgs<T> A, cudaStream_t s) {
   if (W.grad[0]) {  // node velocity gradients of the high-order viscous stencils
     Timed tm(h, KK_GRAD, s);
     if (G.gk1 > G.gk0) {
-      if (h->vk == VK_C6) k_grad<true, T><<<grad_grid(G), PLANE_THREADS, 0, s>>>(G, W, h->M);
-      else k_grad<false, T><<<grad_grid(G), PLANE_THREADS, 0, s>>>(G, W, h->M);
+      if (sens_in_grad) {
+        if (vk_base(h->vk) == VK_C6) k_grad<true, T, true><<<grad_grid(G), PLANE_THREADS, 0, s>>>(G, W, h->M);
+        else k_grad<false, T, true><<<grad_grid(G), PLANE_THREADS, 0, s>>>(G, W, h->M);
+      } else {
+        if (vk_base(h->vk) == VK_C6) k_grad<true, T><<<grad_grid(G), PLANE_THREADS, 0, s>>>(G, W, h->M);
+        else k_grad<false, T><<<grad_grid(G), PLANE_THREADS, 0, s>>>(G, W, h->M);
+      }
       h->launches++;
     }
   }
@@ -679,7 +690,7 @@ int run_stage_n(oux_handle* h, int st, cudaStream_t s, int part = 0) {
     // whole stage.
     const Geo keep = h->G;
     const int g = keep.g, nz = keep.nz;
-    const int hd = h->vk == VK_C6 ? 3 : 2;  // reach of the gradient pass along z
+    const int hd = vk_base(h->vk) == VK_C6 ? 3 : 2;  // reach of the gradient pass along z
     const bool split = keep.bcz == 2 && g >= 2 && nz - 2 * g > 2 * g;
     auto narrow = [&](int p0, int p1, int q0, int q1, int c0, int c1) {
       h->G.pk0 = p0; h->G.pk1 = p1; h->G.gk0 = q0; h->G.gk1 = q1; h->G.sk0 = c0; h->G.sk1 = c1;

@@ -219,40 +219,37 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_prim_mx(const double* __restr
 
 // ---- Ducros sensor: calc_Ducros (3D_solver/src/calc_hybrid.f90:11-72; 2D twin
 // :11-55) on cells 1..n-2, with the reference's copies to the outer faces.
-template <int DIM, class T, bool RO = false>
-__device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, const Metrics& M, int i, int j,
-                                            int k) {
-  if (i < 1 || i > G.nx - 2 || j < 1 || j > G.ny - 2) return;
-  if (DIM == 3 && (k < 1 || k > G.nz - 2)) return;
+// sensor_of_diffs takes the raw central differences df(c, a) = -vel_c(o - st_a) +
+// vel_c(o + st_a) of velocity component c along axis a (the caller has checked that
+// the cell lies in 1..n-2 on every axis), so that a pass which has loaded those
+// neighbours already (k_grad) reuses them.
+template <int DIM, class T, class DF>
+__device__ __forceinline__ void sensor_of_diffs(const Geo& G, const Fields<T>& W, const Metrics& M, int i, int j,
+                                                int k, DF df) {
   const int64_t o = G.at(i, j, k);
   const T eps = T(1.0e-12);
-  auto U = [&](int64_t q) { return ldro<RO>(W.u + q); };
-  auto V = [&](int64_t q) { return ldro<RO>(W.v + q); };
-  auto Wv = [&](int64_t q) { return ldro<RO>(W.w + q); };
   T dxt = T(0.25) * ((T)M.inv_dx[i - 1] + (T)M.inv_dx[i]);
   T dyt = T(0.25) * ((T)M.inv_dy[j - 1] + (T)M.inv_dy[j]);
   T f;
   if constexpr (DIM == 3) {
     T dzt = T(0.25) * ((T)M.inv_dz[k - 1] + (T)M.inv_dz[k]);
-    const int64_t ox = 1, oy = G.sx, oz = G.plane;
-    T dudx = (-U(o - ox) + U(o + ox)) * dxt;
-    T dvdx = (-V(o - ox) + V(o + ox)) * dxt;
-    T dwdx = (-Wv(o - ox) + Wv(o + ox)) * dxt;
-    T dudy = (-U(o - oy) + U(o + oy)) * dyt;
-    T dvdy = (-V(o - oy) + V(o + oy)) * dyt;
-    T dwdy = (-Wv(o - oy) + Wv(o + oy)) * dyt;
-    T dudz = (-U(o - oz) + U(o + oz)) * dzt;
-    T dvdz = (-V(o - oz) + V(o + oz)) * dzt;
-    T dwdz = (-Wv(o - oz) + Wv(o + oz)) * dzt;
+    T dudx = df(0, 0) * dxt;
+    T dvdx = df(1, 0) * dxt;
+    T dwdx = df(2, 0) * dxt;
+    T dudy = df(0, 1) * dyt;
+    T dvdy = df(1, 1) * dyt;
+    T dwdy = df(2, 1) * dyt;
+    T dudz = df(0, 2) * dzt;
+    T dvdz = df(1, 2) * dzt;
+    T dwdz = df(2, 2) * dzt;
     T div = dudx + dvdy + dwdz;
     T r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
     f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
   } else {
-    const int64_t ox = 1, oy = G.sx;
-    T dudx = (-U(o - ox) + U(o + ox)) * dxt;
-    T dvdx = (-V(o - ox) + V(o + ox)) * dxt;
-    T dudy = (-U(o - oy) + U(o + oy)) * dyt;
-    T dvdy = (-V(o - oy) + V(o + oy)) * dyt;
+    T dudx = df(0, 0) * dxt;
+    T dvdx = df(1, 0) * dxt;
+    T dudy = df(0, 1) * dyt;
+    T dvdy = df(1, 1) * dyt;
     T div = dudx + dvdy;
     T rot = dvdx - dudy;
     f = (div * div) / (div * div + rot * rot + eps);
@@ -264,6 +261,19 @@ __device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, co
   if constexpr (DIM == 3) {
     if (k == 1) W.sensor[G.at(i, j, 0)] = f; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = f;
   }
+}
+
+template <int DIM, class T, bool RO = false>
+__device__ __forceinline__ void sensor_cell(const Geo& G, const Fields<T>& W, const Metrics& M, int i, int j,
+                                            int k) {
+  if (i < 1 || i > G.nx - 2 || j < 1 || j > G.ny - 2) return;
+  if (DIM == 3 && (k < 1 || k > G.nz - 2)) return;
+  const int64_t o = G.at(i, j, k);
+  const T* vel[3] = {W.u, W.v, W.w};
+  const int64_t st[3] = {1, G.sx, G.plane};
+  sensor_of_diffs<DIM, T>(G, W, M, i, j, k, [&](int c, int a) -> T {
+    return -ldro<RO>(vel[c] + o - st[a]) + ldro<RO>(vel[c] + o + st[a]);
+  });
 }
 
 template <int DIM, class T, bool RO = false>
@@ -473,20 +483,22 @@ __global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_fused(const TS* __restri
 // z-marching variant with a shared-memory ring of the velocities filled by cp.async one
 // plane ahead measured slower on B200 at 518^3: 3.78 against 2.96 ms.)
 template <bool SIXTH, class T>
-__device__ __forceinline__ T node_deriv(const T* a, int64_t o, int64_t st, T inv) {
-  auto A = [&](int64_t q) { return __ldg(a + q); };
+__device__ __forceinline__ T node_deriv_of(T m3, T m2, T m1, T p1, T p2, T p3, T inv) {
   if constexpr (SIXTH)
-    return (T(1.0 / 60.0) * (-A(o - 3 * st) + A(o + 3 * st)) + T(0.15) * (A(o - 2 * st) - A(o + 2 * st)) +
-            T(0.75) * (-A(o - st) + A(o + st))) * inv;
+    return (T(1.0 / 60.0) * (-m3 + p3) + T(0.15) * (m2 - p2) + T(0.75) * (-m1 + p1)) * inv;
   else
-    return (T(2.0 / 3.0) * (-A(o - st) + A(o + st)) - T(1.0 / 12.0) * (-A(o - 2 * st) + A(o + 2 * st))) * inv;
+    return (T(2.0 / 3.0) * (-m1 + p1) - T(1.0 / 12.0) * (-m2 + p2)) * inv;
 }
 
 inline dim3 grad_grid(const Geo& G) {
   return dim3((unsigned)((G.nx * G.ny + PLANE_THREADS - 1) / PLANE_THREADS), (unsigned)(G.gk1 - G.gk0), 1);
 }
 
-template <bool SIXTH, class T>
+// SENSOR: the same pass also writes the Ducros sensor of its cells from the +-1
+// neighbours it loads for the gradients (sensor_of_diffs), so that the primitive pass
+// before it can be the plain per-cell k_prim.  Every neighbour value is loaded once
+// and feeds both.
+template <bool SIXTH, class T, bool SENSOR = false>
 __global__ void __launch_bounds__(PLANE_THREADS) k_grad(Geo G, Fields<T> W, Metrics M) {
   const int t = blockIdx.x * PLANE_THREADS + threadIdx.x;
   if (t >= G.nx * G.ny) return;
@@ -500,12 +512,35 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_grad(Geo G, Fields<T> W, Metr
   const double* invd[3] = {M.inv_dx, M.inv_dy, M.inv_dz};
   const T* vel[3] = {W.u, W.v, W.w};
   const int64_t o = G.at(c[0], c[1], c[2]);
+  // the sensor's cells: 1..n-2 on every axis
+  const bool sens = SENSOR && c[0] >= 1 && c[0] <= n[0] - 2 && c[1] >= 1 && c[1] <= n[1] - 2 && c[2] >= 1 &&
+                    c[2] <= n[2] - 2;
+  T d1[3][3];  // d1[a][q] = -vel_q(o - st_a) + vel_q(o + st_a), for the sensor
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const bool fits = c[a] >= HD && c[a] + HD < n[a];
     const T inv = fits ? (T)invd[a][c[a]] : T(0);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) W.grad[3 * q + a][o] = fits ? node_deriv<SIXTH, T>(vel[q], o, st[a], inv) : T(0);
+    for (int q = 0; q < 3; ++q) {
+      const T* f = vel[q] + o;
+      T g = T(0);
+      if (fits) {
+        const T m1 = __ldg(f - st[a]), p1 = __ldg(f + st[a]);
+        const T m2 = __ldg(f - 2 * st[a]), p2 = __ldg(f + 2 * st[a]);
+        T m3 = T(0), p3 = T(0);
+        if constexpr (SIXTH) { m3 = __ldg(f - 3 * st[a]); p3 = __ldg(f + 3 * st[a]); }
+        g = node_deriv_of<SIXTH, T>(m3, m2, m1, p1, p2, p3, inv);
+        d1[a][q] = -m1 + p1;
+      } else if (sens) {
+        d1[a][q] = -__ldg(f - st[a]) + __ldg(f + st[a]);
+      } else {
+        d1[a][q] = T(0);
+      }
+      W.grad[3 * q + a][o] = g;
+    }
+  }
+  if constexpr (SENSOR) {
+    if (sens) sensor_of_diffs<3, T>(G, W, M, c[0], c[1], c[2], [&](int q, int a) -> T { return d1[a][q]; });
   }
 }
 

@@ -27,7 +27,7 @@ int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
   dim3 grid;
   if (DIR == 0) grid = dim3((Nx + 31) / 32, (Ny + SWEEP_BR - 1) / SWEEP_BR, Nz);
   else if (DIR == 1) grid = dim3((Nx + 31) / 32, (Ny + SWEEP_BF - 1) / SWEEP_BF, Nz);
-  else grid = dim3((Nx + 31) / 32, (Nz + SWEEP_BF - 1) / SWEEP_BF, Ny);
+  else grid = dim3((Nx + 31) / 32, (Nz + SWEEP_BZ - 1) / SWEEP_BZ, Ny);
   kern<<<grid, block, smem, s>>>(A, last);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }

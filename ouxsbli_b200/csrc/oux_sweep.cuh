@@ -16,16 +16,26 @@ namespace oux {
 #ifndef OUX_SWEEP_BR
 #define OUX_SWEEP_BR 4
 #endif
+// y / z tiles of 7 cells (8 face rows, 256 threads): two blocks of 8 warps per SM leave
+// the FP64 ME4 z sweep 128 registers and no spills, where 8 cells (288 threads, 96
+// registers) spilled 120 B per thread; measured on B200 at 512^3 (Hybrid-6 / ME4): z
+// 9.64 -> 9.44 ms, and the mixed form's y sweep 6.12 -> 5.38 ms
 #ifndef OUX_SWEEP_BF
-#define OUX_SWEEP_BF 8
+#define OUX_SWEEP_BF 7
+#endif
+#ifndef OUX_SWEEP_BZ
+#define OUX_SWEEP_BZ OUX_SWEEP_BF
 #endif
 constexpr int SWEEP_BR = OUX_SWEEP_BR;  // x sweep rows per block
-constexpr int SWEEP_BF = OUX_SWEEP_BF;  // y/z sweep cells per block along the sweep
+constexpr int SWEEP_BF = OUX_SWEEP_BF;  // y sweep cells per block along the sweep
+constexpr int SWEEP_BZ = OUX_SWEEP_BZ;  // z sweep cells per block along the sweep
 
 enum TileField { TF_RHO = 0, TF_U, TF_V, TF_W, TF_P, TF_T, TF_MU, TF_MUT, TF_QC2, TF_SEN, TF_D0, TF_D1, TF_D2, TF_D3, TF_COUNT };
 
 // ROWS: pencil rows per x-sweep tile, or cells along the sweep per y/z tile.
-template <int DIR> __host__ __device__ constexpr int default_rows() { return DIR == 0 ? SWEEP_BR : SWEEP_BF; }
+template <int DIR> __host__ __device__ constexpr int default_rows() {
+  return DIR == 0 ? SWEEP_BR : DIR == 1 ? SWEEP_BF : SWEEP_BZ;
+}
 template <int DIR, int ROWS = default_rows<DIR>()> struct SweepShape {
   static constexpr int TX = (DIR == 0) ? 33 : 32;
   static constexpr int TY = (DIR == 0) ? ROWS : ROWS + 1;
@@ -700,9 +710,10 @@ namespace oux {
 // GR: the transverse node derivatives are staged from the gradient fields W.grad
 // (written by k_grad) instead of being differenced from the velocities in the tile
 // load.
-// AT: the tile fields are plain copies (no derivative is differenced in the load), so
-// they are staged with asynchronous global -> shared copies (cp.async): no register
-// staging, and every copy of the tile is in flight at once.
+// AT: the tile's plain fields (and, with GR, the gradients) are staged with
+// asynchronous global -> shared copies (cp.async): no register staging, and every
+// copy of the tile is in flight at once; derivatives differenced in the load (no GR)
+// are computed while the copies fly.
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
           bool RO = false, bool KONLY = false, int PF = 0, bool SHARE = false, bool GR = false, bool AT = false>
 __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
@@ -806,7 +817,6 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     if (!ok) continue;
     const int64_t o = G.at(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
     if constexpr (AT) {
-      static_assert(!HIGH || GR, "asynchronous tile loads need the derivatives as fields");
       cp_async<sizeof(T)>(&tile[TF_RHO * NC + c], A.W.rho + o);
       cp_async<sizeof(T)>(&tile[TF_U * NC + c], A.W.u + o);
       cp_async<sizeof(T)>(&tile[TF_V * NC + c], A.W.v + o);
@@ -820,7 +830,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         cp_async<sizeof(T)>(&tile[TF_MUT * NC + c], A.W.mut + o);
         cp_async<sizeof(T)>(&tile[TF_QC2 * NC + c], A.W.qc2 + o);
       }
-      if constexpr (HIGH) {
+      if constexpr (HIGH && GR) {
         constexpr int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
         constexpr int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
         cp_async<sizeof(T)>(&tile[TF_D0 * NC + c], A.W.grad[3 * a1 + a1] + o);
@@ -828,22 +838,26 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         cp_async<sizeof(T)>(&tile[TF_D2 * NC + c], A.W.grad[3 * n + ca] + o);
         cp_async<sizeof(T)>(&tile[TF_D3 * NC + c], A.W.grad[3 * n + cb] + o);
       }
-      continue;
+      // without gradient fields the derivatives are differenced below, while the
+      // copies above are in flight
+      if constexpr (!HIGH || GR) continue;
     }
-    tile[TF_RHO * NC + c] = ldro<RO>(A.W.rho + o);
-    tile[TF_U * NC + c] = ldro<RO>(A.W.u + o);
-    tile[TF_V * NC + c] = ldro<RO>(A.W.v + o);
-    tile[TF_W * NC + c] = (DIM == 3) ? ldro<RO>(A.W.w + o) : T(0);
-    tile[TF_P * NC + c] = ldro<RO>(A.W.p + o);
-    tile[TF_T * NC + c] = ldro<RO>(A.W.T_ + o);
-    if (!KONLY && A.scheme != 0) tile[TF_SEN * NC + c] = ldro<RO>(A.W.sensor + o);
-    if constexpr (VK != VK_EULER) tile[TF_MU * NC + c] = ldro<RO>(A.W.mu + o);
-    if constexpr (LES) {
-      tile[TF_MUT * NC + c] = ldro<RO>(A.W.mut + o);
-      tile[TF_QC2 * NC + c] = ldro<RO>(A.W.qc2 + o);
+    if constexpr (!AT) {
+      tile[TF_RHO * NC + c] = ldro<RO>(A.W.rho + o);
+      tile[TF_U * NC + c] = ldro<RO>(A.W.u + o);
+      tile[TF_V * NC + c] = ldro<RO>(A.W.v + o);
+      tile[TF_W * NC + c] = (DIM == 3) ? ldro<RO>(A.W.w + o) : T(0);
+      tile[TF_P * NC + c] = ldro<RO>(A.W.p + o);
+      tile[TF_T * NC + c] = ldro<RO>(A.W.T_ + o);
+      if (!KONLY && A.scheme != 0) tile[TF_SEN * NC + c] = ldro<RO>(A.W.sensor + o);
+      if constexpr (VK != VK_EULER) tile[TF_MU * NC + c] = ldro<RO>(A.W.mu + o);
+      if constexpr (LES) {
+        tile[TF_MUT * NC + c] = ldro<RO>(A.W.mut + o);
+        tile[TF_QC2 * NC + c] = ldro<RO>(A.W.qc2 + o);
+      }
     }
     if constexpr (HIGH && GR) {  // transverse node derivatives from the gradient fields
-      static_assert(DIM == 3 && !WALL, "gradient fields are built for periodic 3D grids");
+      static_assert(DIM == 3, "gradient fields are built for 3D grids");
       constexpr int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
       constexpr int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
       tile[TF_D0 * NC + c] = ldro<RO>(A.W.grad[3 * a1 + a1] + o);
@@ -1169,10 +1183,13 @@ template <int DIR> __host__ __device__ constexpr int sweep_threads() {
   return (SweepShape<DIR>::TX * SweepShape<DIR>::TY + 31) / 32 * 32;
 }
 
-// Single-solve sweeps of periodic 3D grids with a high-order viscous stencil read the
-// transverse node derivatives from the gradient fields (k_grad writes them).
+// Single-solve sweeps of 3D grids with a high-order viscous stencil read the transverse
+// node derivatives from the gradient fields (k_grad writes them).  On walled grids too:
+// k_grad writes 0 where a stencil leaves the grid, as the walled tile load does, and
+// the viscous faces read tile derivatives only inside the high-order guard, whose
+// cells' stencils all fit.
 template <int DIM, int VK> __host__ __device__ constexpr bool sweep_uses_grads() {
-  return DIM == 3 && (VK == VK_C6 || VK == VK_C4 || VK == VK_ME4);
+  return DIM == 3 && (vk_base(VK) == VK_C6 || vk_base(VK) == VK_C4 || vk_base(VK) == VK_ME4);
 }
 
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool SHARE = false>
