@@ -55,7 +55,9 @@ enum oux_visc_stencil { OUX_CENTRAL = 0, OUX_ME4 = 1 };
 enum oux_tvd { OUX_TVD_NONE = 0, OUX_TVD_TVD = 1, OUX_TVD_HYBRID = 2 };
 enum oux_slau_variant { OUX_SLAU1 = 0, OUX_HRSLAU2 = 1 };
 enum oux_precision { OUX_FP64 = 0, OUX_MIXED = 1 };
-/* device status bits (oux_status) */
+/* device status bits (oux_status).  OUX_FAULT_TIMEOUT: a bounded device wait gave up
+ * (a batched step's dependency wait, or a sweep block whose tensor-copied tile never
+ * arrived; that block skipped its faces, so the step's result is void). */
 enum oux_fault_bits { OUX_FAULT_NAN = 1, OUX_FAULT_NONPOSITIVE = 2, OUX_FAULT_TIMEOUT = 4 };
 
 /*
@@ -125,7 +127,10 @@ int oux_scratch_bytes(const oux_config* cfg, size_t* bytes);
 int oux_layout_of(const oux_handle* h, oux_layout* out);
 
 /* Attach caller-owned device buffers (state = QJ of oux_state_bytes; scratch
- * of oux_scratch_bytes).  Uploads the metric tables into scratch on `stream`. */
+ * of oux_scratch_bytes).  Uploads the metric tables into scratch on `stream`, and
+ * for 3D grids with a Central-4/6 or ME4 viscous stencil the tensor maps through
+ * which the y / z sweeps stage their tiles (TMA; built from the scratch's field
+ * addresses, so a buffer must stay bound where it was bound). */
 int oux_bind(oux_handle* h, void* state_dev, void* scratch_dev, size_t scratch_bytes,
              void* stream);
 

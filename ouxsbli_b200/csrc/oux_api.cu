@@ -1,6 +1,7 @@
 // Host side of liboux: configuration checks, metric tables, scratch carving,
 // the stage driver that sequences the kernels of oux_kernels.cuh /
 // oux_sweep.cuh, and the C ABI declared in include/oux.h.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <atomic>
@@ -252,7 +253,7 @@ Geo make_geo(const oux_config& c) {
 }
 
 struct ScratchPlan {
-  size_t fields = 0, racc = 0, q2 = 0, rs = 0, metrics = 0, partials = 0, status = 0, total = 0;
+  size_t fields = 0, racc = 0, q2 = 0, rs = 0, metrics = 0, partials = 0, status = 0, tmaps = 0, total = 0;
   int nfield_arrays = 0;
 };
 
@@ -290,6 +291,9 @@ ScratchPlan plan_scratch(const oux_config& c) {
   off += round_up(mcount * sizeof(double), 256);
   P.partials = off; off += round_up((size_t)3 * DIAG_BLOCKS * sizeof(double) + 3 * sizeof(double), 256);
   P.status = off; off += 256;
+  // tensor maps of the y / z sweep tiles (sweep_tma): TF_COUNT fields per direction
+  off = round_up(off, 256);
+  P.tmaps = off; off += uses_grads(c) ? round_up((size_t)2 * TF_COUNT * TMA_MAP_BYTES, 256) : 0;
   P.total = off;
   return P;
 }
@@ -796,6 +800,61 @@ unsigned long long current_ctx_id() {
   return id;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry points (no link against
+// libcuda); null when the driver does not offer it.
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_tiled() {
+  static EncodeTiled fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<EncodeTiled>(f);
+  }();
+  return fn;
+}
+static_assert(sizeof(CUtensorMap) == TMA_MAP_BYTES, "tensor map size");
+
+// Tensor maps of the y / z sweep tiles (sweep_tma, the TMA tile layout), direction-major
+// then tile field: a 3D map of the field (nx x ny x nz cells; the padded layout's row
+// and plane strides) whose box is TMA_ROW x-cells by the tile's cells along the sweep.
+// The gradient slots D0..D3 hold the four gradients that direction's viscous stencil
+// reads (the same choice as the cp.async tile load).  False if a map cannot be encoded;
+// the sweeps then stage their tiles with cp.async.
+template <class T>
+bool encode_tile_maps(const Geo& G, const Fields<T>& W, CUtensorMap* out) {
+  EncodeTiled enc = encode_tiled();
+  if (!enc) return false;
+  const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint64_t dims[3] = {(cuuint64_t)G.nx, (cuuint64_t)G.ny, (cuuint64_t)G.nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)G.sx * sizeof(T), (cuuint64_t)G.plane * sizeof(T)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  for (int dir = 1; dir <= 2; ++dir) {
+    const int n = dir, a1 = (n + 1) % 3, a2 = (n + 2) % 3, ca = 0, cb = n == 2 ? 1 : 2;
+    const T* f[TF_COUNT] = {};
+    f[TF_RHO] = W.rho; f[TF_U] = W.u; f[TF_V] = W.v; f[TF_W] = W.w; f[TF_P] = W.p; f[TF_T] = W.T_;
+    f[TF_MU] = W.mu; f[TF_MUT] = W.mut; f[TF_QC2] = W.qc2; f[TF_SEN] = W.sensor;
+    f[TF_D0] = W.grad[3 * a1 + a1]; f[TF_D1] = W.grad[3 * a2 + a2];
+    f[TF_D2] = W.grad[3 * n + ca]; f[TF_D3] = W.grad[3 * n + cb];
+    const cuuint32_t tl = (cuuint32_t)((dir == 1 ? default_rows<1>() : default_rows<2>()) + 2 * TILE_HALO);
+    const cuuint32_t box[3] = {(cuuint32_t)TMA_ROW, dir == 1 ? tl : 1u, dir == 2 ? tl : 1u};
+    for (int q = 0; q < TF_COUNT; ++q) {
+      CUtensorMap* m = out + (dir - 1) * TF_COUNT + q;
+      std::memset(m, 0, sizeof(CUtensorMap));
+      if (!f[q]) continue;
+      if ((uintptr_t)f[q] & 15) return false;
+      if (enc(m, dt, 3, (void*)f[q], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    }
+  }
+  return true;
+}
+
 // Device address of g_noalloc_scratch on the current device, looked up once per
 // device context (cudaGetSymbolAddress with that device current) and cached.
 int noalloc_scratch(unsigned char** out) {
@@ -972,6 +1031,19 @@ int oux_bind(oux_handle* h, void* state_dev, void* scratch_dev, size_t scratch_b
   h->scratch = (unsigned char*)scratch_dev;
   h->scratch_bytes = scratch_bytes;
   carve(h);
+  // the y / z sweep tiles' tensor maps (kept null where a map cannot be made)
+  h->tmaps = nullptr;
+  std::vector<CUtensorMap> maps;
+  if (uses_grads(h->cfg)) {
+    maps.resize(2 * TF_COUNT);
+    const bool ok = h->mixed ? encode_tile_maps<float>(h->G, h->Wf, maps.data())
+                             : encode_tile_maps<double>(h->G, h->W, maps.data());
+    if (ok) {
+      OUX_CUDA(cudaMemcpyAsync(h->scratch + P.tmaps, maps.data(), maps.size() * sizeof(CUtensorMap),
+                               cudaMemcpyHostToDevice, s));
+      h->tmaps = h->scratch + P.tmaps;
+    }
+  }
   // upload metric tables (contiguous block, same order as carve())
   std::vector<double> m;
   auto put = [&](const std::vector<double>& v) { m.insert(m.end(), v.begin(), v.end()); };

@@ -31,6 +31,7 @@ struct oux_handle {
   double *Racc = nullptr, *Rs = nullptr, *partials = nullptr;
   void* Qs = nullptr;           // stage state (double or float)
   int* status = nullptr;
+  const void* tmaps = nullptr;  // device tensor maps of the y / z sweep tiles (set by oux_bind)
   oux::Metrics M{};
   int64_t launches = 0;
   int diag_blocks = 0;
@@ -61,6 +62,8 @@ inline StepArgs<T> base_args(oux_handle* h) {
   A.Rs = h->Rs;
   A.Qn = h->Q;
   A.Qs = reinterpret_cast<T*>(h->Qs);
+  A.tmaps = h->tmaps;
+  A.status = h->status;
   return A;
 }
 }  // namespace oux

@@ -94,6 +94,11 @@ template <class T> struct StepArgs {
   double coef;  // metric scale (RK3 coef3 or 1)
   double c1, c2, c4;
   int mode;
+  // single solves: device copy of the y / z sweep tiles' tensor maps (TileMaps; null:
+  // the tiles are staged with cp.async) and the status word a TMA wait that runs out
+  // marks with OUX_FAULT_TIMEOUT
+  const void* tmaps;
+  int* status;
 };
 
 // Load through the read-only data path when the caller guarantees the array is
@@ -223,16 +228,37 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_prim_mx(const double* __restr
 // vel_c(o + st_a) of velocity component c along axis a (the caller has checked that
 // the cell lies in 1..n-2 on every axis), so that a pass which has loaded those
 // neighbours already (k_grad) reuses them.
+// The sensor value from the summed divergence and the rotation components, stored
+// with the reference's copies to the outer faces (3D: r1, r2, r3; 2D: r3 = rot).
+template <int DIM, class T>
+__device__ __forceinline__ void ducros_store(const Geo& G, const Fields<T>& W, int i, int j, int k, T div, T r1,
+                                             T r2, T r3) {
+  const T eps = T(1.0e-12);
+  T f;
+  if constexpr (DIM == 3) f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
+  else f = (div * div) / (div * div + r3 * r3 + eps);
+  f = fmin_f(T(1), f);
+  W.sensor[G.at(i, j, k)] = f;
+  if (i == 1) W.sensor[G.at(0, j, k)] = f; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = f;
+  if (j == 1) W.sensor[G.at(i, 0, k)] = f; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = f;
+  if constexpr (DIM == 3) {
+    if (k == 1) W.sensor[G.at(i, j, 0)] = f; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = f;
+  }
+}
+
+// Central difference scale of the sensor along an axis at cell c.
+template <class T>
+__device__ __forceinline__ T ducros_scale(const double* inv, int c) {
+  return T(0.25) * ((T)inv[c - 1] + (T)inv[c]);
+}
+
 template <int DIM, class T, class DF>
 __device__ __forceinline__ void sensor_of_diffs(const Geo& G, const Fields<T>& W, const Metrics& M, int i, int j,
                                                 int k, DF df) {
-  const int64_t o = G.at(i, j, k);
-  const T eps = T(1.0e-12);
-  T dxt = T(0.25) * ((T)M.inv_dx[i - 1] + (T)M.inv_dx[i]);
-  T dyt = T(0.25) * ((T)M.inv_dy[j - 1] + (T)M.inv_dy[j]);
-  T f;
+  T dxt = ducros_scale<T>(M.inv_dx, i);
+  T dyt = ducros_scale<T>(M.inv_dy, j);
   if constexpr (DIM == 3) {
-    T dzt = T(0.25) * ((T)M.inv_dz[k - 1] + (T)M.inv_dz[k]);
+    T dzt = ducros_scale<T>(M.inv_dz, k);
     T dudx = df(0, 0) * dxt;
     T dvdx = df(1, 0) * dxt;
     T dwdx = df(2, 0) * dxt;
@@ -243,23 +269,13 @@ __device__ __forceinline__ void sensor_of_diffs(const Geo& G, const Fields<T>& W
     T dvdz = df(1, 2) * dzt;
     T dwdz = df(2, 2) * dzt;
     T div = dudx + dvdy + dwdz;
-    T r1 = dwdy - dvdz, r2 = dudz - dwdx, r3 = dvdx - dudy;
-    f = (div * div) / (div * div + (r1 * r1 + r2 * r2 + r3 * r3) + eps);
+    ducros_store<3, T>(G, W, i, j, k, div, dwdy - dvdz, dudz - dwdx, dvdx - dudy);
   } else {
     T dudx = df(0, 0) * dxt;
     T dvdx = df(1, 0) * dxt;
     T dudy = df(0, 1) * dyt;
     T dvdy = df(1, 1) * dyt;
-    T div = dudx + dvdy;
-    T rot = dvdx - dudy;
-    f = (div * div) / (div * div + rot * rot + eps);
-  }
-  f = fmin_f(T(1), f);
-  W.sensor[o] = f;
-  if (i == 1) W.sensor[G.at(0, j, k)] = f; else if (i == G.nx - 2) W.sensor[G.at(G.nx - 1, j, k)] = f;
-  if (j == 1) W.sensor[G.at(i, 0, k)] = f; else if (j == G.ny - 2) W.sensor[G.at(i, G.ny - 1, k)] = f;
-  if constexpr (DIM == 3) {
-    if (k == 1) W.sensor[G.at(i, j, 0)] = f; else if (k == G.nz - 2) W.sensor[G.at(i, j, G.nz - 1)] = f;
+    ducros_store<2, T>(G, W, i, j, k, dudx + dvdy, T(0), T(0), dvdx - dudy);
   }
 }
 
@@ -495,9 +511,9 @@ inline dim3 grad_grid(const Geo& G) {
 }
 
 // SENSOR: the same pass also writes the Ducros sensor of its cells from the +-1
-// neighbours it loads for the gradients (sensor_of_diffs), so that the primitive pass
-// before it can be the plain per-cell k_prim.  Every neighbour value is loaded once
-// and feeds both.
+// neighbours it loads for the gradients (the arithmetic of sensor_of_diffs), so that
+// the primitive pass before it can be the plain per-cell k_prim.  Every neighbour value
+// is loaded once and feeds both.
 template <bool SIXTH, class T, bool SENSOR = false>
 __global__ void __launch_bounds__(PLANE_THREADS) k_grad(Geo G, Fields<T> W, Metrics M) {
   const int t = blockIdx.x * PLANE_THREADS + threadIdx.x;
@@ -515,32 +531,40 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_grad(Geo G, Fields<T> W, Metr
   // the sensor's cells: 1..n-2 on every axis
   const bool sens = SENSOR && c[0] >= 1 && c[0] <= n[0] - 2 && c[1] >= 1 && c[1] <= n[1] - 2 && c[2] >= 1 &&
                     c[2] <= n[2] - 2;
-  T d1[3][3];  // d1[a][q] = -vel_q(o - st_a) + vel_q(o + st_a), for the sensor
+  // the sensor's terms, summed axis by axis in the order sensor_of_diffs sums them, so
+  // that few of them are live at once
+  T div = T(0), r1 = T(0), r2 = T(0), r3 = T(0), dwdx = T(0), dwdy = T(0);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const bool fits = c[a] >= HD && c[a] + HD < n[a];
     const T inv = fits ? (T)invd[a][c[a]] : T(0);
+    const T sc = sens ? ducros_scale<T>(invd[a], c[a]) : T(0);
+    T d[3];  // (-vel_q(o - st_a) + vel_q(o + st_a)) times the sensor's scale
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const T* f = vel[q] + o;
-      T g = T(0);
+      T gq = T(0);
+      d[q] = T(0);
       if (fits) {
         const T m1 = __ldg(f - st[a]), p1 = __ldg(f + st[a]);
         const T m2 = __ldg(f - 2 * st[a]), p2 = __ldg(f + 2 * st[a]);
         T m3 = T(0), p3 = T(0);
         if constexpr (SIXTH) { m3 = __ldg(f - 3 * st[a]); p3 = __ldg(f + 3 * st[a]); }
-        g = node_deriv_of<SIXTH, T>(m3, m2, m1, p1, p2, p3, inv);
-        d1[a][q] = -m1 + p1;
+        gq = node_deriv_of<SIXTH, T>(m3, m2, m1, p1, p2, p3, inv);
+        if (sens) d[q] = (-m1 + p1) * sc;
       } else if (sens) {
-        d1[a][q] = -__ldg(f - st[a]) + __ldg(f + st[a]);
-      } else {
-        d1[a][q] = T(0);
+        d[q] = (-__ldg(f - st[a]) + __ldg(f + st[a])) * sc;
       }
-      W.grad[3 * q + a][o] = g;
+      W.grad[3 * q + a][o] = gq;
+    }
+    if constexpr (SENSOR) {
+      if (a == 0) { div = d[0]; r3 = d[1]; dwdx = d[2]; }                  // dudx, dvdx, dwdx
+      else if (a == 1) { div = div + d[1]; r3 = r3 - d[0]; dwdy = d[2]; }  // + dvdy; dvdx - dudy
+      else { div = div + d[2]; r1 = dwdy - d[1]; r2 = d[0] - dwdx; }      // + dwdz; dwdy - dvdz; dudz - dwdx
     }
   }
   if constexpr (SENSOR) {
-    if (sens) sensor_of_diffs<3, T>(G, W, M, c[0], c[1], c[2], [&](int q, int a) -> T { return d1[a][q]; });
+    if (sens) ducros_store<3, T>(G, W, c[0], c[1], c[2], div, r1, r2, r3);
   }
 }
 

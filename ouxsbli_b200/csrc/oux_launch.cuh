@@ -13,7 +13,8 @@ int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
   if constexpr (VK == VK_ME4 && !SHARE && DIR < 2) {
     if ((A.G.uni >> DIR) & 1) return launch_one<DIM, DIR, ORDER, VK, LES, T, true>(A, last, s);
   }
-  constexpr size_t smem = sweep_smem<ORDER, DIR, T>() + sweep_pf_bytes<DIR, T>(sweep_pf_mode<DIM, DIR, T>()) +
+  constexpr size_t smem = sweep_smem<ORDER, DIR, T, default_rows<DIR>(), sweep_tma<DIM, DIR, VK>()>() +
+                          sweep_pf_bytes<DIR, T>(sweep_pf_mode<DIM, DIR, T>()) +
                           (SHARE ? me4_share_bytes<DIR, T, LES>() : 0);
   auto kern = k_sweep<DIM, DIR, ORDER, VK, LES, T, SHARE>;
   static const cudaError_t attr_rc =

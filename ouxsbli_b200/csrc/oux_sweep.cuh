@@ -51,11 +51,30 @@ template <int ORDER, int DIR, int ROWS = default_rows<DIR>()> __host__ __device_
 template <int ORDER, int DIR, int ROWS = default_rows<DIR>()> __host__ __device__ constexpr int tile_cells() {
   return DIR == 0 ? tile_len<ORDER, DIR, ROWS>() * ROWS : tile_len<ORDER, DIR, ROWS>() * 32;
 }
-template <int ORDER, int DIR, class T, int ROWS = default_rows<DIR>()>
+// TMA-staged y / z tiles (TM: 3D single solves whose tile fields are all plain copies,
+// see sweep_tma): every tile field is one box copy of TMA_ROW x cells by tile_len cells
+// along the sweep, whose x origin is the block's first owned cell minus the x ghost
+// width, 32 b: 16-byte aligned for 4- and 8-byte elements, as a tiled tensor copy
+// needs, and TMA_ROW x 4 B and TMA_ROW x 8 B are multiples of 16 B.  A row then holds
+// the 32 owned cells from column gx (gx <= 3).  Each field's slab is rounded up to
+// 128 bytes of shared memory.
+constexpr int TMA_ROW = 36;
+constexpr int TMA_MAP_BYTES = 128;  // one tensor map (CUtensorMap)
+template <int ORDER, int DIR, class T, int ROWS, bool TM>
+__host__ __device__ constexpr int tile_fstride() {
+  if constexpr (TM && DIR != 0) {
+    constexpr size_t b = sizeof(T) * TMA_ROW * tile_len<ORDER, DIR, ROWS>();
+    return (int)(((b + 127) / 128) * 128 / sizeof(T));
+  } else {
+    return tile_cells<ORDER, DIR, ROWS>();
+  }
+}
+template <int ORDER, int DIR, class T, int ROWS = default_rows<DIR>(), bool TM = false>
 __host__ __device__ constexpr size_t sweep_smem() {
-  // TF_COUNT tile fields + 5 face-flux components per face thread (FP64)
-  return sizeof(T) * TF_COUNT * tile_cells<ORDER, DIR, ROWS>() +
-         sizeof(double) * 5 * SweepShape<DIR, ROWS>::TX * SweepShape<DIR, ROWS>::TY;
+  // TF_COUNT tile fields + 5 face-flux components per face thread (FP64) [+ the
+  // tile's mbarrier, 16 bytes]
+  return sizeof(T) * TF_COUNT * tile_fstride<ORDER, DIR, T, ROWS, TM>() +
+         sizeof(double) * 5 * SweepShape<DIR, ROWS>::TX * SweepShape<DIR, ROWS>::TY + (TM && DIR != 0 ? 16 : 0);
 }
 
 // Terms of one shared ME4 face position (me4_position).
@@ -102,6 +121,42 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <int N> __device__ __forceinline__ void cp_async_wait_group() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
+
+// mbarrier and tiled tensor copy (TMA, no multicast) for the y / z sweep tiles
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// box of the 3D tensor map `map` (in global memory) at (x, y, z) into shared `dst`;
+// completes `bar`'s transaction bytes
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* map, int x, int y, int z,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+// a tensor map written to global memory by a copy: make the tensor-map proxy see it
+__device__ __forceinline__ void tmap_acquire(const void* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
+}
+// polls of a tile's mbarrier before the block gives up with OUX_FAULT_TIMEOUT
+constexpr int TMA_WAIT_LIMIT = 1 << 20;
 
 // transverse node derivative of `a` along axis `ax` at offset o (4th/6th order)
 template <bool SIXTH, bool RO, class T>
@@ -714,8 +769,13 @@ namespace oux {
 // asynchronous global -> shared copies (cp.async): no register staging, and every
 // copy of the tile is in flight at once; derivatives differenced in the load (no GR)
 // are computed while the copies fly.
+// TM (y / z sweeps whose tile fields are all plain copies): the TMA tile layout
+// (TMA_ROW-wide rows, 128-byte field slabs); with A.tmaps set, one thread stages every
+// field by a tensor copy completing one mbarrier, else the threads fill the same
+// layout with cp.async.
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
-          bool RO = false, bool KONLY = false, int PF = 0, bool SHARE = false, bool GR = false, bool AT = false>
+          bool RO = false, bool KONLY = false, int PF = 0, bool SHARE = false, bool GR = false, bool AT = false,
+          bool TM = false>
 __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
                                            unsigned char* smraw, int tid, int nthr_all) {
   constexpr int H = ORDER / 2;
@@ -726,10 +786,15 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   constexpr bool WALL = vk_wall(VK);   // 3D viscous grid with a non-periodic direction
   constexpr bool HIGH = (VB == VK_C6 || VB == VK_C4 || VB == VK_ME4 || VB == VK_2D4);
   constexpr bool SIXTH = (VB == VK_C6);
+  constexpr bool TMA = TM && DIR != 0;
+  static_assert(!TMA || (AT && DIM == 3), "TMA tiles hold plain copies of 3D fields");
+  constexpr int FS = tile_fstride<ORDER, DIR, T, ROWS, TM>();  // tile field stride
+  constexpr int TW = TMA ? TMA_ROW : 32;                       // y / z tile row width
   T* tile = reinterpret_cast<T*>(smraw);
-  double* Fs = reinterpret_cast<double*>(smraw + sizeof(T) * TF_COUNT * NC);
+  double* Fs = reinterpret_cast<double*>(smraw + sizeof(T) * TF_COUNT * FS);
   const Geo& G = A.G;
   const int g = G.g, gx = G.gx, gy = G.gy;  // gx / gy: 1 with a non-periodic x / y
+  const int TOFF = TMA ? gx : 0;            // y / z tiles: column of the first owned cell
   const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * gy;
   const int gz = G.gz;                        // 1 with a non-periodic z
   const int Nz = (DIM == 3) ? G.nz - 2 * gz : 1;
@@ -756,7 +821,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   constexpr bool PF_R = PF_ON && (PF & 2);  // accumulator
   constexpr bool MXC = sizeof(T) < sizeof(double);
   constexpr int PFC = 32 * ROWS;  // owned cells per tile
-  double* pfQn = reinterpret_cast<double*>(smraw + sweep_smem<ORDER, DIR, T, ROWS>());
+  double* pfQn = reinterpret_cast<double*>(smraw + sweep_smem<ORDER, DIR, T, ROWS, TM>());
   double* pfX = pfQn + 5 * PFC;             // Qs (as T) or Rs
   T* pfQs = reinterpret_cast<T*>(pfX);
   double* pfRs = pfX;
@@ -764,8 +829,9 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   static_assert(!SHARE || VK == VK_ME4, "shared face positions are built for the periodic ME4 stencil");
   constexpr int NPOS = me4_positions<DIR, ROWS>();
   constexpr int PSTEP = DIR == 0 ? 1 : 32;                // next position along the sweep
+  constexpr int TSTEP = DIR == 0 ? 1 : TW;                // next tile cell along the sweep
   constexpr int PROW = DIR == 0 ? TX + 2 : 32;            // x sweep: positions per pencil row
-  T* Vs = reinterpret_cast<T*>(smraw + sweep_smem<ORDER, DIR, T, ROWS>() + sweep_pf_bytes<DIR, T, ROWS>(PF));
+  T* Vs = reinterpret_cast<T*>(smraw + sweep_smem<ORDER, DIR, T, ROWS, TM>() + sweep_pf_bytes<DIR, T, ROWS>(PF));
   const int md = last ? A.mode : CM_ACCUM;
   const bool needQn = (!MXC && (md == CM_RK3_1 || md == CM_RK3_2 || md == CM_RK4_S)) || md == CM_RK3_3 ||
                       md == CM_RK4_4;
@@ -796,10 +862,42 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   };
   if constexpr (PF_ON && !AT) issue_prefetch();
 
+  // ---- tile load: tensor copies (TMA layout with maps) ----
+  bool use_tma = false;
+  unsigned long long* tbar = nullptr;
+  if constexpr (TMA) {
+    tbar = reinterpret_cast<unsigned long long*>(smraw + sizeof(T) * TF_COUNT * FS +
+                                                 sizeof(double) * 5 * TX * TY);
+    use_tma = A.tmaps != nullptr && (smem_u32(smraw) & 127u) == 0;
+    if (use_tma && tid == 0) {
+      const bool sen = !KONLY && A.scheme != 0;
+      const unsigned nf = 6u + (sen ? 1u : 0u) + (VK != VK_EULER ? 1u : 0u) + (LES ? 2u : 0u) + (GR ? 4u : 0u);
+      mbar_init(tbar, 1);
+      mbar_fence_init();
+      constexpr unsigned BOX = (unsigned)(sizeof(T) * TMA_ROW * TL);
+      mbar_expect_tx(tbar, BOX * nf);
+      // box origin: x = the row's first cell (32 b), the tile's first cell along the sweep
+      const int x0 = bx0 - gx;
+      const int y0 = DIR == 1 ? by0 - TILE_HALO : by0;
+      const int z0 = DIR == 2 ? bz0 - TILE_HALO : bz0;
+      const char* maps = static_cast<const char*>(A.tmaps) + (size_t)(DIR - 1) * TF_COUNT * TMA_MAP_BYTES;
+      auto copy = [&](int field) {
+        tmap_acquire(maps + field * TMA_MAP_BYTES);
+        tma_load_3d(tile + field * FS, maps + field * TMA_MAP_BYTES, x0, y0, z0, tbar);
+      };
+      copy(TF_RHO); copy(TF_U); copy(TF_V); copy(TF_W); copy(TF_P); copy(TF_T);
+      if (sen) copy(TF_SEN);
+      if constexpr (VK != VK_EULER) copy(TF_MU);
+      if constexpr (LES) { copy(TF_MUT); copy(TF_QC2); }
+      if constexpr (GR) { copy(TF_D0); copy(TF_D1); copy(TF_D2); copy(TF_D3); }
+    }
+  }
+
   // ---- tile load (cooperative) ----
-  for (int c = tid; c < NC; c += nthr) {
+  for (int c = use_tma ? NC : tid; c < NC; c += nthr) {
     int ci[3];
     int along;
+    int sl = c;  // the cell's slot in a field's slab
     if constexpr (DIR == 0) {
       int t = c % TL, r = c / TL;
       along = bx0 - TILE_HALO + t; ci[0] = along; ci[1] = by0 + r; ci[2] = bz0;
@@ -809,6 +907,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       ci[0] = bx0 + x;
       ci[1] = (DIR == 1) ? along : by0;
       ci[2] = (DIR == 2) ? along : bz0;
+      sl = t * TW + TOFF + x;
     }
     bool ok = along >= 0 && along < nsweep;
 #pragma unroll
@@ -817,53 +916,53 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     if (!ok) continue;
     const int64_t o = G.at(ci[0], ci[1], DIM == 3 ? ci[2] : 0);
     if constexpr (AT) {
-      cp_async<sizeof(T)>(&tile[TF_RHO * NC + c], A.W.rho + o);
-      cp_async<sizeof(T)>(&tile[TF_U * NC + c], A.W.u + o);
-      cp_async<sizeof(T)>(&tile[TF_V * NC + c], A.W.v + o);
-      if constexpr (DIM == 3) cp_async<sizeof(T)>(&tile[TF_W * NC + c], A.W.w + o);
-      else tile[TF_W * NC + c] = T(0);
-      cp_async<sizeof(T)>(&tile[TF_P * NC + c], A.W.p + o);
-      cp_async<sizeof(T)>(&tile[TF_T * NC + c], A.W.T_ + o);
-      if (!KONLY && A.scheme != 0) cp_async<sizeof(T)>(&tile[TF_SEN * NC + c], A.W.sensor + o);
-      if constexpr (VK != VK_EULER) cp_async<sizeof(T)>(&tile[TF_MU * NC + c], A.W.mu + o);
+      cp_async<sizeof(T)>(&tile[TF_RHO * FS + sl], A.W.rho + o);
+      cp_async<sizeof(T)>(&tile[TF_U * FS + sl], A.W.u + o);
+      cp_async<sizeof(T)>(&tile[TF_V * FS + sl], A.W.v + o);
+      if constexpr (DIM == 3) cp_async<sizeof(T)>(&tile[TF_W * FS + sl], A.W.w + o);
+      else tile[TF_W * FS + sl] = T(0);
+      cp_async<sizeof(T)>(&tile[TF_P * FS + sl], A.W.p + o);
+      cp_async<sizeof(T)>(&tile[TF_T * FS + sl], A.W.T_ + o);
+      if (!KONLY && A.scheme != 0) cp_async<sizeof(T)>(&tile[TF_SEN * FS + sl], A.W.sensor + o);
+      if constexpr (VK != VK_EULER) cp_async<sizeof(T)>(&tile[TF_MU * FS + sl], A.W.mu + o);
       if constexpr (LES) {
-        cp_async<sizeof(T)>(&tile[TF_MUT * NC + c], A.W.mut + o);
-        cp_async<sizeof(T)>(&tile[TF_QC2 * NC + c], A.W.qc2 + o);
+        cp_async<sizeof(T)>(&tile[TF_MUT * FS + sl], A.W.mut + o);
+        cp_async<sizeof(T)>(&tile[TF_QC2 * FS + sl], A.W.qc2 + o);
       }
       if constexpr (HIGH && GR) {
         constexpr int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
         constexpr int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
-        cp_async<sizeof(T)>(&tile[TF_D0 * NC + c], A.W.grad[3 * a1 + a1] + o);
-        cp_async<sizeof(T)>(&tile[TF_D1 * NC + c], A.W.grad[3 * a2 + a2] + o);
-        cp_async<sizeof(T)>(&tile[TF_D2 * NC + c], A.W.grad[3 * n + ca] + o);
-        cp_async<sizeof(T)>(&tile[TF_D3 * NC + c], A.W.grad[3 * n + cb] + o);
+        cp_async<sizeof(T)>(&tile[TF_D0 * FS + sl], A.W.grad[3 * a1 + a1] + o);
+        cp_async<sizeof(T)>(&tile[TF_D1 * FS + sl], A.W.grad[3 * a2 + a2] + o);
+        cp_async<sizeof(T)>(&tile[TF_D2 * FS + sl], A.W.grad[3 * n + ca] + o);
+        cp_async<sizeof(T)>(&tile[TF_D3 * FS + sl], A.W.grad[3 * n + cb] + o);
       }
       // without gradient fields the derivatives are differenced below, while the
       // copies above are in flight
       if constexpr (!HIGH || GR) continue;
     }
     if constexpr (!AT) {
-      tile[TF_RHO * NC + c] = ldro<RO>(A.W.rho + o);
-      tile[TF_U * NC + c] = ldro<RO>(A.W.u + o);
-      tile[TF_V * NC + c] = ldro<RO>(A.W.v + o);
-      tile[TF_W * NC + c] = (DIM == 3) ? ldro<RO>(A.W.w + o) : T(0);
-      tile[TF_P * NC + c] = ldro<RO>(A.W.p + o);
-      tile[TF_T * NC + c] = ldro<RO>(A.W.T_ + o);
-      if (!KONLY && A.scheme != 0) tile[TF_SEN * NC + c] = ldro<RO>(A.W.sensor + o);
-      if constexpr (VK != VK_EULER) tile[TF_MU * NC + c] = ldro<RO>(A.W.mu + o);
+      tile[TF_RHO * FS + sl] = ldro<RO>(A.W.rho + o);
+      tile[TF_U * FS + sl] = ldro<RO>(A.W.u + o);
+      tile[TF_V * FS + sl] = ldro<RO>(A.W.v + o);
+      tile[TF_W * FS + sl] = (DIM == 3) ? ldro<RO>(A.W.w + o) : T(0);
+      tile[TF_P * FS + sl] = ldro<RO>(A.W.p + o);
+      tile[TF_T * FS + sl] = ldro<RO>(A.W.T_ + o);
+      if (!KONLY && A.scheme != 0) tile[TF_SEN * FS + sl] = ldro<RO>(A.W.sensor + o);
+      if constexpr (VK != VK_EULER) tile[TF_MU * FS + sl] = ldro<RO>(A.W.mu + o);
       if constexpr (LES) {
-        tile[TF_MUT * NC + c] = ldro<RO>(A.W.mut + o);
-        tile[TF_QC2 * NC + c] = ldro<RO>(A.W.qc2 + o);
+        tile[TF_MUT * FS + sl] = ldro<RO>(A.W.mut + o);
+        tile[TF_QC2 * FS + sl] = ldro<RO>(A.W.qc2 + o);
       }
     }
     if constexpr (HIGH && GR) {  // transverse node derivatives from the gradient fields
       static_assert(DIM == 3, "gradient fields are built for 3D grids");
       constexpr int n = DIR, a1 = (n + 1) % 3, a2 = (n + 2) % 3;
       constexpr int ca = n == 0 ? 1 : 0, cb = n == 2 ? 1 : 2;
-      tile[TF_D0 * NC + c] = ldro<RO>(A.W.grad[3 * a1 + a1] + o);
-      tile[TF_D1 * NC + c] = ldro<RO>(A.W.grad[3 * a2 + a2] + o);
-      tile[TF_D2 * NC + c] = ldro<RO>(A.W.grad[3 * n + ca] + o);
-      tile[TF_D3 * NC + c] = ldro<RO>(A.W.grad[3 * n + cb] + o);
+      tile[TF_D0 * FS + sl] = ldro<RO>(A.W.grad[3 * a1 + a1] + o);
+      tile[TF_D1 * FS + sl] = ldro<RO>(A.W.grad[3 * a2 + a2] + o);
+      tile[TF_D2 * FS + sl] = ldro<RO>(A.W.grad[3 * n + ca] + o);
+      tile[TF_D3 * FS + sl] = ldro<RO>(A.W.grad[3 * n + cb] + o);
     } else if constexpr (HIGH) {  // transverse node derivatives (the viscous loaders' stencils)
       const T* vel[3] = {A.W.u, A.W.v, A.W.w};
       const double* invd[3] = {A.M.inv_dx, A.M.inv_dy, A.M.inv_dz};
@@ -879,10 +978,10 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
           if (WALL && !(ci[ax] >= HD && ci[ax] + HD < na[ax])) return T(0);
           return node_d<SIXTH, RO>(f, o, stv[ax], (T)invd[ax][ci[ax]]);
         };
-        tile[TF_D0 * NC + c] = nd(vel[a1], a1);
-        tile[TF_D1 * NC + c] = nd(vel[a2], a2);
-        tile[TF_D2 * NC + c] = nd(vel[n], ca);
-        tile[TF_D3 * NC + c] = nd(vel[n], cb);
+        tile[TF_D0 * FS + sl] = nd(vel[a1], a1);
+        tile[TF_D1 * FS + sl] = nd(vel[a2], a2);
+        tile[TF_D2 * FS + sl] = nd(vel[n], ca);
+        tile[TF_D3 * FS + sl] = nd(vel[n], cb);
       } else {
         // 2D: only where the stencil stays inside the grid; the other cells lie
         // outside the 4th-order guard of calc_Ev4 / calc_Fv4, whose 2nd-order
@@ -890,11 +989,11 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         const int n = DIR, t = 1 - DIR;
         constexpr int HD = SIXTH ? 3 : 2;
         if (ci[t] >= HD && ci[t] + HD < (t == 0 ? G.nx : G.ny)) {
-          tile[TF_D0 * NC + c] = node_d<SIXTH, RO>(vel[t], o, stv[t], (T)invd[t][ci[t]]);
-          tile[TF_D2 * NC + c] = node_d<SIXTH, RO>(vel[n], o, stv[t], (T)invd[t][ci[t]]);
+          tile[TF_D0 * FS + sl] = node_d<SIXTH, RO>(vel[t], o, stv[t], (T)invd[t][ci[t]]);
+          tile[TF_D2 * FS + sl] = node_d<SIXTH, RO>(vel[n], o, stv[t], (T)invd[t][ci[t]]);
         } else {
-          tile[TF_D0 * NC + c] = T(0);
-          tile[TF_D2 * NC + c] = T(0);
+          tile[TF_D0 * FS + sl] = T(0);
+          tile[TF_D2 * FS + sl] = T(0);
         }
       }
     }
@@ -908,7 +1007,19 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       cp_async_wait_all();
     }
   }
-  __syncthreads();
+  __syncthreads();  // (also orders the mbarrier's initialisation before the waits below)
+  if constexpr (TMA) {
+    if (use_tma) {
+      bool done = false;
+      for (int it = 0; it < TMA_WAIT_LIMIT && !done; ++it) done = mbar_try_wait(tbar, 0);
+      // a tile whose copies never complete ends the whole block, flagged on the host's
+      // status word (the block's threads decide together)
+      if (!__syncthreads_and(done)) {
+        if (tid == 0 && A.status) atomicOr(A.status, 4 /* OUX_FAULT_TIMEOUT */);
+        return;
+      }
+    }
+  }
 
   // ---- shared ME4 face positions (every thread, strided) ----
   if constexpr (SHARE) {
@@ -916,8 +1027,8 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     const T inv = (T)invd[DIR][0];  // the axis' spacings are all the same double
     for (int c = tid; c < NPOS; c += nthr) {
       // tile index of the position's first stencil cell (its left cell - 1)
-      const int t0 = DIR == 0 ? (c / PROW) * TL + c % PROW : c;
-      auto sp = [&](int field, int m) -> T { return tile[field * NC + t0 + m * PSTEP]; };
+      const int t0 = DIR == 0 ? (c / PROW) * TL + c % PROW : (c / 32) * TW + TOFF + c % 32;
+      auto sp = [&](int field, int m) -> T { return tile[field * FS + t0 + m * TSTEP]; };
       T v[9];
       me4_position<LES>(A, sp, DIR, inv, v);
 #pragma unroll
@@ -939,7 +1050,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     } else {
       fc[0] = bx0 + tx;
       fc[DIR] = (DIR == 1 ? by0 : bz0) - 1 + ty;
-      base = ty * 32 + tx; step = 32;
+      base = ty * TW + TOFF + tx; step = TW;
       rowok = fc[0] < ext[0];
     }
     const int f = fc[DIR];
@@ -949,9 +1060,9 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     if (valid) {
       T F[5];
       // tile position of cell f + off is base + (2 + off) * step
-      auto st0 = [&](int field, int m) -> T { return tile[field * NC + base + m * step]; };
+      auto st0 = [&](int field, int m) -> T { return tile[field * FS + base + m * step]; };
       const int cb = base + (TILE_HALO - H) * step;
-      auto sc = [&](int field, int m) -> T { return tile[field * NC + cb + m * step]; };
+      auto sc = [&](int field, int m) -> T { return tile[field * FS + cb + m * step]; };
       T fd = T(0);
       if (!KONLY && A.scheme != 0) fd = T(0.5) * (st0(TF_SEN, 2) + st0(TF_SEN, 3));
       if constexpr (DIM == 2 || VK == VK_EULER || WALL) {
@@ -969,10 +1080,10 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
         if (lo == ORDER) {
           conv_flux<ORDER, KONLY>(A, sc, fd, DIR, F);
         } else if (lo == 4) {
-          auto s4 = [&](int field, int m) -> T { return tile[field * NC + base + (TILE_HALO - 2 + m) * step]; };
+          auto s4 = [&](int field, int m) -> T { return tile[field * FS + base + (TILE_HALO - 2 + m) * step]; };
           conv_flux<4, KONLY>(A, s4, fd, DIR, F);
         } else {
-          auto s2 = [&](int field, int m) -> T { return tile[field * NC + base + (TILE_HALO - 1 + m) * step]; };
+          auto s2 = [&](int field, int m) -> T { return tile[field * FS + base + (TILE_HALO - 1 + m) * step]; };
           conv_flux<2, KONLY>(A, s2, fd, DIR, F);
         }
       } else {
@@ -995,12 +1106,12 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
           const int64_t o = G.at(fc[0], fc[1], 0);
           T invs[2] = {(T)A.M.inv_dx[fc[0]], (T)A.M.inv_dy[fc[1]]};
           invs[DIR] = inv;
-          auto sv = [&](int field, int m) -> T { return tile[field * NC + base + m * step]; };
+          auto sv = [&](int field, int m) -> T { return tile[field * FS + base + m * step]; };
           visc_2d4(A, sv, DIR, inner, o, stv, invs, vo);
         } else {
           constexpr int off0 = (VB == VK_C4) ? -1 : -2;
           const int vb = base + (2 + off0) * step;
-          auto sv = [&](int field, int m) -> T { return tile[field * NC + vb + m * step]; };
+          auto sv = [&](int field, int m) -> T { return tile[field * FS + vb + m * step]; };
           if constexpr (WALL) {
             // high-order guard of calc_{E,F,G}v (calc_visc_high.f90.fypp:114/139/169,
             // 350/376/406, 592/618/648), 0-based: C4 faces 1..n-3 and transverse cells
@@ -1191,17 +1302,22 @@ template <int DIR> __host__ __device__ constexpr int sweep_threads() {
 template <int DIM, int VK> __host__ __device__ constexpr bool sweep_uses_grads() {
   return DIM == 3 && (vk_base(VK) == VK_C6 || vk_base(VK) == VK_C4 || vk_base(VK) == VK_ME4);
 }
+// Their y / z tiles are then all plain copies, staged by TMA in the TMA tile layout.
+template <int DIM, int DIR, int VK> __host__ __device__ constexpr bool sweep_tma() {
+  return DIR != 0 && sweep_uses_grads<DIM, VK>();
+}
 
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool SHARE = false>
 __global__ void __launch_bounds__(sweep_threads<DIR>(), DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
 k_sweep(StepArgs<T> A, int last) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+  extern __shared__ __align__(128) unsigned char smraw[];
   // coherent loads: measured as fast as the read-only path for y/z and faster for x
   constexpr int VB = vk_base(VK);
   constexpr bool HIGH = (VB == VK_C6 || VB == VK_C4 || VB == VK_ME4 || VB == VK_2D4);
   constexpr bool GR = sweep_uses_grads<DIM, VK>();
   sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>(), SHARE,
-             GR, !HIGH || GR>(A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.x, sweep_threads<DIR>());
+             GR, !HIGH || GR, sweep_tma<DIM, DIR, VK>()>(A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw,
+                                                        threadIdx.x, sweep_threads<DIR>());
 }
 
 }  // namespace oux
