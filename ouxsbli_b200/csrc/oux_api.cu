@@ -253,7 +253,7 @@ Geo make_geo(const oux_config& c) {
 }
 
 struct ScratchPlan {
-  size_t fields = 0, racc = 0, q2 = 0, rs = 0, metrics = 0, partials = 0, status = 0, tmaps = 0, total = 0;
+  size_t fields = 0, racc = 0, q2 = 0, rs = 0, metrics = 0, partials = 0, status = 0, total = 0;
   int nfield_arrays = 0;
 };
 
@@ -291,9 +291,6 @@ ScratchPlan plan_scratch(const oux_config& c) {
   off += round_up(mcount * sizeof(double), 256);
   P.partials = off; off += round_up((size_t)3 * DIAG_BLOCKS * sizeof(double) + 3 * sizeof(double), 256);
   P.status = off; off += 256;
-  // tensor maps of the y / z sweep tiles (sweep_tma): TF_COUNT fields per direction
-  off = round_up(off, 256);
-  P.tmaps = off; off += uses_grads(c) ? round_up((size_t)2 * TF_COUNT * TMA_MAP_BYTES, 256) : 0;
   P.total = off;
   return P;
 }
@@ -818,12 +815,12 @@ EncodeTiled encode_tiled() {
 }
 static_assert(sizeof(CUtensorMap) == TMA_MAP_BYTES, "tensor map size");
 
-// Tensor maps of the y / z sweep tiles (sweep_tma, the TMA tile layout), direction-major
-// then tile field: a 3D map of the field (nx x ny x nz cells; the padded layout's row
-// and plane strides) whose box is TMA_ROW x-cells by the tile's cells along the sweep.
-// The gradient slots D0..D3 hold the four gradients that direction's viscous stencil
-// reads (the same choice as the cp.async tile load).  False if a map cannot be encoded;
-// the sweeps then stage their tiles with cp.async.
+// Tensor maps of the y sweep's tiles (sweep_tma, the TMA tile layout), one per tile
+// field: a 3D map of the field (nx x ny x nz cells; the padded layout's row and plane
+// strides) whose box is TMA_ROW x-cells by the tile's cells along the sweep.  The
+// gradient slots D0..D3 hold the four gradients the y sweep's viscous stencil reads (the
+// same choice as the cp.async tile load).  False if a map cannot be encoded; the sweep
+// then stages its tiles with cp.async.
 template <class T>
 bool encode_tile_maps(const Geo& G, const Fields<T>& W, CUtensorMap* out) {
   EncodeTiled enc = encode_tiled();
@@ -832,17 +829,17 @@ bool encode_tile_maps(const Geo& G, const Fields<T>& W, CUtensorMap* out) {
   const cuuint64_t dims[3] = {(cuuint64_t)G.nx, (cuuint64_t)G.ny, (cuuint64_t)G.nz};
   const cuuint64_t strides[2] = {(cuuint64_t)G.sx * sizeof(T), (cuuint64_t)G.plane * sizeof(T)};
   const cuuint32_t estr[3] = {1, 1, 1};
-  for (int dir = 1; dir <= 2; ++dir) {
-    const int n = dir, a1 = (n + 1) % 3, a2 = (n + 2) % 3, ca = 0, cb = n == 2 ? 1 : 2;
+  {
+    const int dir = 1, n = dir, a1 = (n + 1) % 3, a2 = (n + 2) % 3, ca = 0, cb = 2;
     const T* f[TF_COUNT] = {};
     f[TF_RHO] = W.rho; f[TF_U] = W.u; f[TF_V] = W.v; f[TF_W] = W.w; f[TF_P] = W.p; f[TF_T] = W.T_;
     f[TF_MU] = W.mu; f[TF_MUT] = W.mut; f[TF_QC2] = W.qc2; f[TF_SEN] = W.sensor;
     f[TF_D0] = W.grad[3 * a1 + a1]; f[TF_D1] = W.grad[3 * a2 + a2];
     f[TF_D2] = W.grad[3 * n + ca]; f[TF_D3] = W.grad[3 * n + cb];
-    const cuuint32_t tl = (cuuint32_t)((dir == 1 ? default_rows<1>() : default_rows<2>()) + 2 * TILE_HALO);
-    const cuuint32_t box[3] = {(cuuint32_t)TMA_ROW, dir == 1 ? tl : 1u, dir == 2 ? tl : 1u};
+    const cuuint32_t tl = (cuuint32_t)(default_rows<1>() + 2 * TILE_HALO);
+    const cuuint32_t box[3] = {(cuuint32_t)TMA_ROW, tl, 1u};
     for (int q = 0; q < TF_COUNT; ++q) {
-      CUtensorMap* m = out + (dir - 1) * TF_COUNT + q;
+      CUtensorMap* m = out + q;
       std::memset(m, 0, sizeof(CUtensorMap));
       if (!f[q]) continue;
       if ((uintptr_t)f[q] & 15) return false;
@@ -1031,18 +1028,13 @@ int oux_bind(oux_handle* h, void* state_dev, void* scratch_dev, size_t scratch_b
   h->scratch = (unsigned char*)scratch_dev;
   h->scratch_bytes = scratch_bytes;
   carve(h);
-  // the y / z sweep tiles' tensor maps (kept null where a map cannot be made)
+  // the y sweep tiles' tensor maps (kept null where a map cannot be made)
   h->tmaps = nullptr;
-  std::vector<CUtensorMap> maps;
   if (uses_grads(h->cfg)) {
-    maps.resize(2 * TF_COUNT);
-    const bool ok = h->mixed ? encode_tile_maps<float>(h->G, h->Wf, maps.data())
-                             : encode_tile_maps<double>(h->G, h->W, maps.data());
-    if (ok) {
-      OUX_CUDA(cudaMemcpyAsync(h->scratch + P.tmaps, maps.data(), maps.size() * sizeof(CUtensorMap),
-                               cudaMemcpyHostToDevice, s));
-      h->tmaps = h->scratch + P.tmaps;
-    }
+    static_assert(sizeof(h->tmap_host) == TF_COUNT * sizeof(CUtensorMap), "tensor map storage");
+    CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(h->tmap_host);
+    const bool ok = h->mixed ? encode_tile_maps<float>(h->G, h->Wf, maps) : encode_tile_maps<double>(h->G, h->W, maps);
+    if (ok) h->tmaps = h->tmap_host;
   }
   // upload metric tables (contiguous block, same order as carve())
   std::vector<double> m;

@@ -31,7 +31,10 @@ struct oux_handle {
   double *Racc = nullptr, *Rs = nullptr, *partials = nullptr;
   void* Qs = nullptr;           // stage state (double or float)
   int* status = nullptr;
-  const void* tmaps = nullptr;  // device tensor maps of the y / z sweep tiles (set by oux_bind)
+  // tensor maps of the y sweep's tiles, one per tile field (CUtensorMap bytes, encoded
+  // by oux_bind); tmaps points at them once they are valid
+  alignas(64) unsigned char tmap_host[14][128] = {};
+  const void* tmaps = nullptr;
   oux::Metrics M{};
   int64_t launches = 0;
   int diag_blocks = 0;

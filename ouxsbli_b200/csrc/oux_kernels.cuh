@@ -94,9 +94,10 @@ template <class T> struct StepArgs {
   double coef;  // metric scale (RK3 coef3 or 1)
   double c1, c2, c4;
   int mode;
-  // single solves: device copy of the y / z sweep tiles' tensor maps (TileMaps; null:
-  // the tiles are staged with cp.async) and the status word a TMA wait that runs out
-  // marks with OUX_FAULT_TIMEOUT
+  // single solves: HOST address of the handle's y sweep tile tensor maps, which the
+  // launch passes to the sweep kernels by value (null: the tiles are staged with
+  // cp.async; never dereferenced on the device), and the status word a TMA wait that
+  // runs out marks with OUX_FAULT_TIMEOUT
   const void* tmaps;
   int* status;
 };
@@ -513,9 +514,11 @@ inline dim3 grad_grid(const Geo& G) {
 // SENSOR: the same pass also writes the Ducros sensor of its cells from the +-1
 // neighbours it loads for the gradients (the arithmetic of sensor_of_diffs), so that
 // the primitive pass before it can be the plain per-cell k_prim.  Every neighbour value
-// is loaded once and feeds both.
+// is loaded once and feeds both.  Bounded to 8 blocks per SM (32 registers; the FP64
+// sensor pass spills 24 B): measured on B200 at 518^3 faster than its 40 registers at
+// 6 blocks per SM, 3.79 against 4.06 ms (this latency-bound pass wants resident warps).
 template <bool SIXTH, class T, bool SENSOR = false>
-__global__ void __launch_bounds__(PLANE_THREADS) k_grad(Geo G, Fields<T> W, Metrics M) {
+__global__ void __launch_bounds__(PLANE_THREADS, 8) k_grad(Geo G, Fields<T> W, Metrics M) {
   const int t = blockIdx.x * PLANE_THREADS + threadIdx.x;
   if (t >= G.nx * G.ny) return;
   int c[3];

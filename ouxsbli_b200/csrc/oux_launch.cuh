@@ -1,5 +1,6 @@
 // Grid/block/shared-memory setup for the three sweeps of one stage.
 #pragma once
+#include <cstring>
 #include "oux_sweep.cuh"
 
 namespace oux {
@@ -16,9 +17,11 @@ int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
   constexpr size_t smem = sweep_smem<ORDER, DIR, T, default_rows<DIR>(), sweep_tma<DIM, DIR, VK>()>() +
                           sweep_pf_bytes<DIR, T>(sweep_pf_mode<DIM, DIR, T>()) +
                           (SHARE ? me4_share_bytes<DIR, T, LES>() : 0);
-  auto kern = k_sweep<DIM, DIR, ORDER, VK, LES, T, SHARE>;
-  static const cudaError_t attr_rc =
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  constexpr bool TM = sweep_tma<DIM, DIR, VK>();
+  const void* fn;
+  if constexpr (TM) fn = (const void*)k_sweep_tm<DIM, DIR, ORDER, VK, LES, T, SHARE>;
+  else fn = (const void*)k_sweep<DIM, DIR, ORDER, VK, LES, T, SHARE>;
+  static const cudaError_t attr_rc = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (attr_rc != cudaSuccess) return 1;
   const Geo& G = A.G;
   const int g = G.g;
@@ -29,7 +32,15 @@ int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
   if (DIR == 0) grid = dim3((Nx + 31) / 32, (Ny + SWEEP_BR - 1) / SWEEP_BR, Nz);
   else if (DIR == 1) grid = dim3((Nx + 31) / 32, (Ny + SWEEP_BF - 1) / SWEEP_BF, Nz);
   else grid = dim3((Nx + 31) / 32, (Nz + SWEEP_BZ - 1) / SWEEP_BZ, Ny);
-  kern<<<grid, block, smem, s>>>(A, last);
+  if constexpr (TM) {
+    // the tile tensor maps from the handle (A.tmaps, a host address)
+    SweepMaps maps;
+    if (A.tmaps) std::memcpy(&maps, A.tmaps, sizeof(SweepMaps));
+    else std::memset(&maps, 0, sizeof(SweepMaps));
+    k_sweep_tm<DIM, DIR, ORDER, VK, LES, T, SHARE><<<grid, block, smem, s>>>(A, last, maps, A.tmaps ? 1 : 0);
+  } else {
+    k_sweep<DIM, DIR, ORDER, VK, LES, T, SHARE><<<grid, block, smem, s>>>(A, last);
+  }
   return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }
 

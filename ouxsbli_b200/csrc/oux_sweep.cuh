@@ -51,8 +51,8 @@ template <int ORDER, int DIR, int ROWS = default_rows<DIR>()> __host__ __device_
 template <int ORDER, int DIR, int ROWS = default_rows<DIR>()> __host__ __device__ constexpr int tile_cells() {
   return DIR == 0 ? tile_len<ORDER, DIR, ROWS>() * ROWS : tile_len<ORDER, DIR, ROWS>() * 32;
 }
-// TMA-staged y / z tiles (TM: 3D single solves whose tile fields are all plain copies,
-// see sweep_tma): every tile field is one box copy of TMA_ROW x cells by tile_len cells
+// TMA-staged y / z tiles (TM: 3D single solves whose tile fields are all plain copies;
+// sweep_tma picks the y sweep): every tile field is one box copy of TMA_ROW x cells by tile_len cells
 // along the sweep, whose x origin is the block's first owned cell minus the x ghost
 // width, 32 b: 16-byte aligned for 4- and 8-byte elements, as a tiled tensor copy
 // needs, and TMA_ROW x 4 B and TMA_ROW x 8 B are multiples of 16 B.  A row then holds
@@ -151,10 +151,12 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* map, int x, i
       "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
-// a tensor map written to global memory by a copy: make the tensor-map proxy see it
-__device__ __forceinline__ void tmap_acquire(const void* map) {
-  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
-}
+// The tensor maps of the TMA-staged sweep's tile fields, passed to the kernel by value
+// (a __grid_constant__ parameter: the copies read them from the parameter space, with
+// no fence, where maps in global memory would need a tensor-map proxy fence per use).
+struct SweepMaps {
+  alignas(64) unsigned char m[TF_COUNT][TMA_MAP_BYTES];
+};
 // polls of a tile's mbarrier before the block gives up with OUX_FAULT_TIMEOUT
 constexpr int TMA_WAIT_LIMIT = 1 << 20;
 
@@ -770,14 +772,15 @@ namespace oux {
 // copy of the tile is in flight at once; derivatives differenced in the load (no GR)
 // are computed while the copies fly.
 // TM (y / z sweeps whose tile fields are all plain copies): the TMA tile layout
-// (TMA_ROW-wide rows, 128-byte field slabs); with A.tmaps set, one thread stages every
-// field by a tensor copy completing one mbarrier, else the threads fill the same
-// layout with cp.async.
+// (TMA_ROW-wide rows, 128-byte field slabs); given `tmaps` (the sweep's SweepMaps),
+// one thread stages every field by a tensor copy completing one mbarrier, else the
+// threads fill the same layout with cp.async.
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
           bool RO = false, bool KONLY = false, int PF = 0, bool SHARE = false, bool GR = false, bool AT = false,
           bool TM = false>
 __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b0, int b1, int b2,
-                                           unsigned char* smraw, int tid, int nthr_all) {
+                                           unsigned char* smraw, int tid, int nthr_all,
+                                           const SweepMaps* tmaps = nullptr) {
   constexpr int H = ORDER / 2;
   constexpr int TL = tile_len<ORDER, DIR, ROWS>();
   constexpr int NC = tile_cells<ORDER, DIR, ROWS>();
@@ -868,7 +871,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   if constexpr (TMA) {
     tbar = reinterpret_cast<unsigned long long*>(smraw + sizeof(T) * TF_COUNT * FS +
                                                  sizeof(double) * 5 * TX * TY);
-    use_tma = A.tmaps != nullptr && (smem_u32(smraw) & 127u) == 0;
+    use_tma = tmaps != nullptr && (smem_u32(smraw) & 127u) == 0;
     if (use_tma && tid == 0) {
       const bool sen = !KONLY && A.scheme != 0;
       const unsigned nf = 6u + (sen ? 1u : 0u) + (VK != VK_EULER ? 1u : 0u) + (LES ? 2u : 0u) + (GR ? 4u : 0u);
@@ -880,11 +883,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       const int x0 = bx0 - gx;
       const int y0 = DIR == 1 ? by0 - TILE_HALO : by0;
       const int z0 = DIR == 2 ? bz0 - TILE_HALO : bz0;
-      const char* maps = static_cast<const char*>(A.tmaps) + (size_t)(DIR - 1) * TF_COUNT * TMA_MAP_BYTES;
-      auto copy = [&](int field) {
-        tmap_acquire(maps + field * TMA_MAP_BYTES);
-        tma_load_3d(tile + field * FS, maps + field * TMA_MAP_BYTES, x0, y0, z0, tbar);
-      };
+      auto copy = [&](int field) { tma_load_3d(tile + field * FS, tmaps->m[field], x0, y0, z0, tbar); };
       copy(TF_RHO); copy(TF_U); copy(TF_V); copy(TF_W); copy(TF_P); copy(TF_T);
       if (sen) copy(TF_SEN);
       if constexpr (VK != VK_EULER) copy(TF_MU);
@@ -1302,15 +1301,18 @@ template <int DIR> __host__ __device__ constexpr int sweep_threads() {
 template <int DIM, int VK> __host__ __device__ constexpr bool sweep_uses_grads() {
   return DIM == 3 && (vk_base(VK) == VK_C6 || vk_base(VK) == VK_C4 || vk_base(VK) == VK_ME4);
 }
-// Their y / z tiles are then all plain copies, staged by TMA in the TMA tile layout.
+// Their y / z tiles are then all plain copies; the y sweep's are staged by TMA (the
+// TMA tile layout).  Measured on B200 at 512^3 (Hybrid-6 / ME4, ms per launch, TMA
+// against cp.async): y 8.74 / 8.80 (FP64) and 4.89 / 5.30 (mixed); z 9.46 / 9.11 and
+// 6.39 / 6.24, where a box is 13 rows from 13 planes 2 MB apart; so z keeps cp.async.
 template <int DIM, int DIR, int VK> __host__ __device__ constexpr bool sweep_tma() {
-  return DIR != 0 && sweep_uses_grads<DIM, VK>();
+  return DIR == 1 && sweep_uses_grads<DIM, VK>();
 }
 
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool SHARE = false>
 __global__ void __launch_bounds__(sweep_threads<DIR>(), DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
 k_sweep(StepArgs<T> A, int last) {
-  extern __shared__ __align__(128) unsigned char smraw[];
+  extern __shared__ __align__(16) unsigned char smraw[];
   // coherent loads: measured as fast as the read-only path for y/z and faster for x
   constexpr int VB = vk_base(VK);
   constexpr bool HIGH = (VB == VK_C6 || VB == VK_C4 || VB == VK_ME4 || VB == VK_2D4);
@@ -1318,6 +1320,19 @@ k_sweep(StepArgs<T> A, int last) {
   sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>(), SHARE,
              GR, !HIGH || GR, sweep_tma<DIM, DIR, VK>()>(A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw,
                                                         threadIdx.x, sweep_threads<DIR>());
+}
+
+// The sweeps of sweep_tma configurations: k_sweep with the tile's tensor maps as a
+// kernel parameter (`use` = 0: none; the tile is then filled by cp.async).
+template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool SHARE = false>
+__global__ void __launch_bounds__(sweep_threads<DIR>(), DIR == 0 ? OUX_SWEEP_MINB_X : OUX_SWEEP_MINB_YZ)
+k_sweep_tm(StepArgs<T> A, int last, const __grid_constant__ SweepMaps maps, int use) {
+  extern __shared__ __align__(128) unsigned char smtile[];  // tensor copies land 128-byte aligned
+  unsigned char* smraw = smtile;
+  static_assert(sweep_tma<DIM, DIR, VK>(), "k_sweep_tm serves the TMA-staged sweeps");
+  sweep_tile<DIM, DIR, ORDER, VK, LES, T, default_rows<DIR>(), false, false, sweep_pf_mode<DIM, DIR, T>(), SHARE,
+             true, true, true>(A, last, blockIdx.x, blockIdx.y, blockIdx.z, smraw, threadIdx.x, sweep_threads<DIR>(),
+                               use ? &maps : nullptr);
 }
 
 }  // namespace oux
