@@ -129,7 +129,7 @@ int oux_layout_of(const oux_handle* h, oux_layout* out);
 /* Attach caller-owned device buffers (state = QJ of oux_state_bytes; scratch
  * of oux_scratch_bytes).  Uploads the metric tables into scratch on `stream`, and
  * for 3D grids with a Central-4/6 or ME4 viscous stencil encodes (on the host) the
- * tensor maps through which the y sweep stages its tiles by TMA; they hold the
+ * tensor maps through which the x and y sweeps stage their tiles by TMA; they hold the
  * scratch's field addresses, so the buffers must stay where they were bound. */
 int oux_bind(oux_handle* h, void* state_dev, void* scratch_dev, size_t scratch_bytes,
              void* stream);

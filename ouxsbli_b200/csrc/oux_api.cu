@@ -815,12 +815,13 @@ EncodeTiled encode_tiled() {
 }
 static_assert(sizeof(CUtensorMap) == TMA_MAP_BYTES, "tensor map size");
 
-// Tensor maps of the y sweep's tiles (sweep_tma, the TMA tile layout), one per tile
-// field: a 3D map of the field (nx x ny x nz cells; the padded layout's row and plane
-// strides) whose box is TMA_ROW x-cells by the tile's cells along the sweep.  The
-// gradient slots D0..D3 hold the four gradients the y sweep's viscous stencil reads (the
-// same choice as the cp.async tile load).  False if a map cannot be encoded; the sweep
-// then stages its tiles with cp.async.
+// Tensor maps of the x and y sweeps' tiles (sweep_tma, the TMA tile layout), direction-
+// major then tile field: a 3D map of the field (nx x ny x nz cells; the padded layout's
+// row and plane strides) whose box is tma_row x-cells by tma_box_rows rows (x: the
+// pencil rows; y: the tile's cells along the sweep).  The gradient slots D0..D3 hold the
+// four gradients the sweep's viscous stencil reads (the same choice as the cp.async
+// tile load).  False if a map cannot be encoded; the sweeps then stage their tiles with
+// cp.async.
 template <class T>
 bool encode_tile_maps(const Geo& G, const Fields<T>& W, CUtensorMap* out) {
   EncodeTiled enc = encode_tiled();
@@ -829,17 +830,19 @@ bool encode_tile_maps(const Geo& G, const Fields<T>& W, CUtensorMap* out) {
   const cuuint64_t dims[3] = {(cuuint64_t)G.nx, (cuuint64_t)G.ny, (cuuint64_t)G.nz};
   const cuuint64_t strides[2] = {(cuuint64_t)G.sx * sizeof(T), (cuuint64_t)G.plane * sizeof(T)};
   const cuuint32_t estr[3] = {1, 1, 1};
-  {
-    const int dir = 1, n = dir, a1 = (n + 1) % 3, a2 = (n + 2) % 3, ca = 0, cb = 2;
+  for (int dir = 0; dir <= 1; ++dir) {
+    const int n = dir, a1 = (n + 1) % 3, a2 = (n + 2) % 3, ca = n == 0 ? 1 : 0, cb = 2;
     const T* f[TF_COUNT] = {};
     f[TF_RHO] = W.rho; f[TF_U] = W.u; f[TF_V] = W.v; f[TF_W] = W.w; f[TF_P] = W.p; f[TF_T] = W.T_;
     f[TF_MU] = W.mu; f[TF_MUT] = W.mut; f[TF_QC2] = W.qc2; f[TF_SEN] = W.sensor;
     f[TF_D0] = W.grad[3 * a1 + a1]; f[TF_D1] = W.grad[3 * a2 + a2];
     f[TF_D2] = W.grad[3 * n + ca]; f[TF_D3] = W.grad[3 * n + cb];
-    const cuuint32_t tl = (cuuint32_t)(default_rows<1>() + 2 * TILE_HALO);
-    const cuuint32_t box[3] = {(cuuint32_t)TMA_ROW, tl, 1u};
+    const cuuint32_t box[3] = {
+        (cuuint32_t)(dir == 0 ? tma_row<0>() : tma_row<1>()),
+        (cuuint32_t)(dir == 0 ? tma_box_rows<6, 0, default_rows<0>()>() : tma_box_rows<6, 1, default_rows<1>()>()),
+        1u};
     for (int q = 0; q < TF_COUNT; ++q) {
-      CUtensorMap* m = out + q;
+      CUtensorMap* m = out + dir * TF_COUNT + q;
       std::memset(m, 0, sizeof(CUtensorMap));
       if (!f[q]) continue;
       if ((uintptr_t)f[q] & 15) return false;
@@ -1028,10 +1031,10 @@ int oux_bind(oux_handle* h, void* state_dev, void* scratch_dev, size_t scratch_b
   h->scratch = (unsigned char*)scratch_dev;
   h->scratch_bytes = scratch_bytes;
   carve(h);
-  // the y sweep tiles' tensor maps (kept null where a map cannot be made)
+  // the x and y sweep tiles' tensor maps (kept null where a map cannot be made)
   h->tmaps = nullptr;
   if (uses_grads(h->cfg)) {
-    static_assert(sizeof(h->tmap_host) == TF_COUNT * sizeof(CUtensorMap), "tensor map storage");
+    static_assert(sizeof(h->tmap_host) == 2 * TF_COUNT * sizeof(CUtensorMap), "tensor map storage");
     CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(h->tmap_host);
     const bool ok = h->mixed ? encode_tile_maps<float>(h->G, h->Wf, maps) : encode_tile_maps<double>(h->G, h->W, maps);
     if (ok) h->tmaps = h->tmap_host;

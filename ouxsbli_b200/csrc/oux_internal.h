@@ -31,9 +31,9 @@ struct oux_handle {
   double *Racc = nullptr, *Rs = nullptr, *partials = nullptr;
   void* Qs = nullptr;           // stage state (double or float)
   int* status = nullptr;
-  // tensor maps of the y sweep's tiles, one per tile field (CUtensorMap bytes, encoded
-  // by oux_bind); tmaps points at them once they are valid
-  alignas(64) unsigned char tmap_host[14][128] = {};
+  // tensor maps of the x and y sweeps' tiles, [sweep direction][tile field] (CUtensorMap
+  // bytes, encoded by oux_bind); tmaps points at them once they are valid
+  alignas(64) unsigned char tmap_host[2][14][128] = {};
   const void* tmaps = nullptr;
   oux::Metrics M{};
   int64_t launches = 0;

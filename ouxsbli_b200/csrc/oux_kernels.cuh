@@ -94,7 +94,7 @@ template <class T> struct StepArgs {
   double coef;  // metric scale (RK3 coef3 or 1)
   double c1, c2, c4;
   int mode;
-  // single solves: HOST address of the handle's y sweep tile tensor maps, which the
+  // single solves: HOST address of the handle's x / y sweep tile tensor maps, which the
   // launch passes to the sweep kernels by value (null: the tiles are staged with
   // cp.async; never dereferenced on the device), and the status word a TMA wait that
   // runs out marks with OUX_FAULT_TIMEOUT

@@ -33,9 +33,10 @@ int launch_one(const StepArgs<T>& A, int last, cudaStream_t s) {
   else if (DIR == 1) grid = dim3((Nx + 31) / 32, (Ny + SWEEP_BF - 1) / SWEEP_BF, Nz);
   else grid = dim3((Nx + 31) / 32, (Nz + SWEEP_BZ - 1) / SWEEP_BZ, Ny);
   if constexpr (TM) {
-    // the tile tensor maps from the handle (A.tmaps, a host address)
+    // this direction's tile tensor maps from the handle (A.tmaps, a host address)
     SweepMaps maps;
-    if (A.tmaps) std::memcpy(&maps, A.tmaps, sizeof(SweepMaps));
+    if (A.tmaps) std::memcpy(&maps, static_cast<const unsigned char*>(A.tmaps) + DIR * sizeof(SweepMaps),
+                             sizeof(SweepMaps));
     else std::memset(&maps, 0, sizeof(SweepMaps));
     k_sweep_tm<DIM, DIR, ORDER, VK, LES, T, SHARE><<<grid, block, smem, s>>>(A, last, maps, A.tmaps ? 1 : 0);
   } else {

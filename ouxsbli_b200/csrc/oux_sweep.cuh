@@ -51,19 +51,28 @@ template <int ORDER, int DIR, int ROWS = default_rows<DIR>()> __host__ __device_
 template <int ORDER, int DIR, int ROWS = default_rows<DIR>()> __host__ __device__ constexpr int tile_cells() {
   return DIR == 0 ? tile_len<ORDER, DIR, ROWS>() * ROWS : tile_len<ORDER, DIR, ROWS>() * 32;
 }
-// TMA-staged y / z tiles (TM: 3D single solves whose tile fields are all plain copies;
-// sweep_tma picks the y sweep): every tile field is one box copy of TMA_ROW x cells by tile_len cells
-// along the sweep, whose x origin is the block's first owned cell minus the x ghost
-// width, 32 b: 16-byte aligned for 4- and 8-byte elements, as a tiled tensor copy
-// needs, and TMA_ROW x 4 B and TMA_ROW x 8 B are multiples of 16 B.  A row then holds
-// the 32 owned cells from column gx (gx <= 3).  Each field's slab is rounded up to
-// 128 bytes of shared memory.
+// TMA-staged tiles (TM: 3D single solves whose tile fields are all plain copies;
+// sweep_tma picks the sweeps): every tile field is one box copy into rows of tma_row
+// cells, whose x origin is 16-byte aligned for 4- and 8-byte elements, as a tiled
+// tensor copy needs (tma_row x 4 B and x 8 B are multiples of 16 B):
+//  - y / z: TMA_ROW x cells by tile_len cells along the sweep, from x = 32 b (the
+//    block's first owned cell minus the x ghost width); the 32 owned cells start at
+//    column gx (gx <= 3);
+//  - x: TMA_ROW_X x cells by ROWS rows, from x = 32 b - 4; the tile's tile_len cells
+//    start at column gx + 1.
+// Each field's slab is rounded up to 128 bytes of shared memory.
 constexpr int TMA_ROW = 36;
+constexpr int TMA_ROW_X = 44;
 constexpr int TMA_MAP_BYTES = 128;  // one tensor map (CUtensorMap)
+template <int DIR> __host__ __device__ constexpr int tma_row() { return DIR == 0 ? TMA_ROW_X : TMA_ROW; }
+// rows of a tile field's box: the pencil rows (x) or the cells along the sweep (y / z)
+template <int ORDER, int DIR, int ROWS> __host__ __device__ constexpr int tma_box_rows() {
+  return DIR == 0 ? ROWS : tile_len<ORDER, DIR, ROWS>();
+}
 template <int ORDER, int DIR, class T, int ROWS, bool TM>
 __host__ __device__ constexpr int tile_fstride() {
-  if constexpr (TM && DIR != 0) {
-    constexpr size_t b = sizeof(T) * TMA_ROW * tile_len<ORDER, DIR, ROWS>();
+  if constexpr (TM) {
+    constexpr size_t b = sizeof(T) * tma_row<DIR>() * tma_box_rows<ORDER, DIR, ROWS>();
     return (int)(((b + 127) / 128) * 128 / sizeof(T));
   } else {
     return tile_cells<ORDER, DIR, ROWS>();
@@ -74,7 +83,7 @@ __host__ __device__ constexpr size_t sweep_smem() {
   // TF_COUNT tile fields + 5 face-flux components per face thread (FP64) [+ the
   // tile's mbarrier, 16 bytes]
   return sizeof(T) * TF_COUNT * tile_fstride<ORDER, DIR, T, ROWS, TM>() +
-         sizeof(double) * 5 * SweepShape<DIR, ROWS>::TX * SweepShape<DIR, ROWS>::TY + (TM && DIR != 0 ? 16 : 0);
+         sizeof(double) * 5 * SweepShape<DIR, ROWS>::TX * SweepShape<DIR, ROWS>::TY + (TM ? 16 : 0);
 }
 
 // Terms of one shared ME4 face position (me4_position).
@@ -789,15 +798,16 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
   constexpr bool WALL = vk_wall(VK);   // 3D viscous grid with a non-periodic direction
   constexpr bool HIGH = (VB == VK_C6 || VB == VK_C4 || VB == VK_ME4 || VB == VK_2D4);
   constexpr bool SIXTH = (VB == VK_C6);
-  constexpr bool TMA = TM && DIR != 0;
+  constexpr bool TMA = TM;
   static_assert(!TMA || (AT && DIM == 3), "TMA tiles hold plain copies of 3D fields");
   constexpr int FS = tile_fstride<ORDER, DIR, T, ROWS, TM>();  // tile field stride
-  constexpr int TW = TMA ? TMA_ROW : 32;                       // y / z tile row width
+  constexpr int TW = TMA ? tma_row<DIR>() : (DIR == 0 ? TL : 32);  // tile row width
   T* tile = reinterpret_cast<T*>(smraw);
   double* Fs = reinterpret_cast<double*>(smraw + sizeof(T) * TF_COUNT * FS);
   const Geo& G = A.G;
   const int g = G.g, gx = G.gx, gy = G.gy;  // gx / gy: 1 with a non-periodic x / y
-  const int TOFF = TMA ? gx : 0;            // y / z tiles: column of the first owned cell
+  // column of a row's first tile cell (x) or first owned cell (y / z)
+  const int TOFF = TMA ? (DIR == 0 ? gx + 1 : gx) : 0;
   const int Nx = G.nx - 2 * gx, Ny = G.ny - 2 * gy;
   const int gz = G.gz;                        // 1 with a non-periodic z
   const int Nz = (DIM == 3) ? G.nz - 2 * gz : 1;
@@ -877,10 +887,11 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
       const unsigned nf = 6u + (sen ? 1u : 0u) + (VK != VK_EULER ? 1u : 0u) + (LES ? 2u : 0u) + (GR ? 4u : 0u);
       mbar_init(tbar, 1);
       mbar_fence_init();
-      constexpr unsigned BOX = (unsigned)(sizeof(T) * TMA_ROW * TL);
+      constexpr unsigned BOX = (unsigned)(sizeof(T) * TW * tma_box_rows<ORDER, DIR, ROWS>());
       mbar_expect_tx(tbar, BOX * nf);
-      // box origin: x = the row's first cell (32 b), the tile's first cell along the sweep
-      const int x0 = bx0 - gx;
+      // box origin: x = the row's first cell (32 b, or 32 b - 4 in the x sweep), the
+      // tile's first cell along the sweep
+      const int x0 = DIR == 0 ? bx0 - gx - 4 : bx0 - gx;
       const int y0 = DIR == 1 ? by0 - TILE_HALO : by0;
       const int z0 = DIR == 2 ? bz0 - TILE_HALO : bz0;
       auto copy = [&](int field) { tma_load_3d(tile + field * FS, tmaps->m[field], x0, y0, z0, tbar); };
@@ -900,6 +911,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     if constexpr (DIR == 0) {
       int t = c % TL, r = c / TL;
       along = bx0 - TILE_HALO + t; ci[0] = along; ci[1] = by0 + r; ci[2] = bz0;
+      sl = r * TW + TOFF + t;
     } else {
       int x = c % 32, t = c / 32;
       along = (DIR == 1 ? by0 : bz0) - TILE_HALO + t;
@@ -1026,7 +1038,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     const T inv = (T)invd[DIR][0];  // the axis' spacings are all the same double
     for (int c = tid; c < NPOS; c += nthr) {
       // tile index of the position's first stencil cell (its left cell - 1)
-      const int t0 = DIR == 0 ? (c / PROW) * TL + c % PROW : (c / 32) * TW + TOFF + c % 32;
+      const int t0 = DIR == 0 ? (c / PROW) * TW + TOFF + c % PROW : (c / 32) * TW + TOFF + c % 32;
       auto sp = [&](int field, int m) -> T { return tile[field * FS + t0 + m * TSTEP]; };
       T v[9];
       me4_position<LES>(A, sp, DIR, inv, v);
@@ -1044,7 +1056,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs<T>& A, int last, int b
     bool rowok;
     if constexpr (DIR == 0) {
       fc[0] = bx0 - 1 + tx; fc[1] = by0 + ty;
-      base = ty * TL + tx; step = 1;
+      base = ty * TW + TOFF + tx; step = 1;
       rowok = fc[1] < ext[1];
     } else {
       fc[0] = bx0 + tx;
@@ -1301,12 +1313,12 @@ template <int DIR> __host__ __device__ constexpr int sweep_threads() {
 template <int DIM, int VK> __host__ __device__ constexpr bool sweep_uses_grads() {
   return DIM == 3 && (vk_base(VK) == VK_C6 || vk_base(VK) == VK_C4 || vk_base(VK) == VK_ME4);
 }
-// Their y / z tiles are then all plain copies; the y sweep's are staged by TMA (the
+// Their tiles are then all plain copies; the x and y sweeps' are staged by TMA (the
 // TMA tile layout).  Measured on B200 at 512^3 (Hybrid-6 / ME4, ms per launch, TMA
 // against cp.async): y 8.74 / 8.80 (FP64) and 4.89 / 5.30 (mixed); z 9.46 / 9.11 and
 // 6.39 / 6.24, where a box is 13 rows from 13 planes 2 MB apart; so z keeps cp.async.
 template <int DIM, int DIR, int VK> __host__ __device__ constexpr bool sweep_tma() {
-  return DIR == 1 && sweep_uses_grads<DIM, VK>();
+  return DIR <= 1 && sweep_uses_grads<DIM, VK>();
 }
 
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, bool SHARE = false>
