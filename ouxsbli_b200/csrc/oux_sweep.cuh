@@ -1315,8 +1315,9 @@ template <int DIM, int VK> __host__ __device__ constexpr bool sweep_uses_grads()
 }
 // Their tiles are then all plain copies; the x and y sweeps' are staged by TMA (the
 // TMA tile layout).  Measured on B200 at 512^3 (Hybrid-6 / ME4, ms per launch, TMA
-// against cp.async): y 8.74 / 8.80 (FP64) and 4.89 / 5.30 (mixed); z 9.46 / 9.11 and
-// 6.39 / 6.24, where a box is 13 rows from 13 planes 2 MB apart; so z keeps cp.async.
+// against cp.async): x 8.12 / 8.18 (FP64) and 5.52 / 5.48 (mixed); y 8.74 / 8.80 and
+// 4.89 / 5.30; z 9.46 / 9.11 and 6.39 / 6.24, where a box is 13 rows from 13 planes
+// 2 MB apart; so z keeps cp.async.
 template <int DIM, int DIR, int VK> __host__ __device__ constexpr bool sweep_tma() {
   return DIR <= 1 && sweep_uses_grads<DIM, VK>();
 }
