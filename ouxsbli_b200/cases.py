@@ -468,6 +468,81 @@ def _bl_boundary(p: dict, J: np.ndarray) -> dict:
 
 
 # ---------------------------------------------------------------------------
+# Boundary layer from an inflow profile: 2D_solver/BL (mod_globals.f90, set.f90).  The
+# flat-plate grid and Mach-2 constants of BL0 with blt = 1 mm, Lx = 20 blt and a 4th-order
+# viscous stencil on the 2nd-order grid.  set_init reads the profile file (`inflow`;
+# the reference reads ./Qin.dat): nyi rows of 5 float64 values (y, rho, u, v, p), the
+# rows one after another; it interpolates them linearly onto the grid's y nodes (held
+# at the end rows outside the profile's range), takes one pressure, the mean of the
+# interpolated p over the first nyi grid rows, and fills every column with the
+# result.  set_bc: the inflow column keeps its initial values, zero gradient at x high
+# and at y high (Neumann), an adiabatic no-slip wall along all of y low; corners take
+# their y rule.
+# ---------------------------------------------------------------------------
+def read_inflow_profile(path) -> np.ndarray:
+    """The (nyi, 5) rows (y, rho, u, v, p) of a BL inflow profile file (little-endian
+    float64, written row after row as the reference's Qi(5, nyi) lies in memory)."""
+    a = np.fromfile(path, dtype="<f8")
+    if a.size == 0 or a.size % 5:
+        raise ValueError(f"{path}: an inflow profile holds rows of 5 float64 values, found {a.size} values")
+    return a.reshape(-1, 5)
+
+
+def interpolate_inflow(y: np.ndarray, prof: np.ndarray) -> np.ndarray:
+    """interpolate_Q (2D_solver/BL/set.f90:39-63): (ny, 4) rho, u, v, p at the nodes y."""
+    out = np.empty((y.size, 4))
+    nyi = prof.shape[0]
+    for j, yj in enumerate(y):
+        if yj <= prof[0, 0]:
+            out[j] = prof[0, 1:]
+        elif yj >= prof[nyi - 1, 0]:
+            out[j] = prof[nyi - 1, 1:]
+        else:
+            for i in range(nyi - 1):
+                y1, y2 = prof[i, 0], prof[i + 1, 0]
+                if y1 <= yj <= y2:
+                    alpha = (yj - y1) / (y2 - y1)
+                    out[j] = (1.0 - alpha) * prof[i, 1:] + alpha * prof[i + 1, 1:]
+                    break
+    return out
+
+
+def _blq_derived(p: dict) -> dict:
+    p = dict(p)
+    if p.get("Lx") is None:
+        p["Lx"] = 20.0 * p["blt"]
+    return _bl_derived(p)
+
+
+def _blq_init(p: dict, x, y, z=None) -> np.ndarray:
+    """set_init (2D_solver/BL/set.f90:66-101); keeps the inflow column for the boundary."""
+    prof = read_inflow_profile(p["inflow"])
+    nyi = prof.shape[0]
+    if nyi > y.size:
+        raise ValueError(f"the inflow profile has {nyi} rows, more than the grid's {y.size} y nodes "
+                         "(set_init averages p over the first nyi grid rows)")
+    qp = interpolate_inflow(y, prof)
+    ptbl = 0.0
+    for j in range(nyi):  # the reference's sequential sum
+        ptbl = ptbl + qp[j, 3]
+    ptbl = ptbl / float(nyi)
+    og1 = 1.0 / (p["gamma"] - 1.0)
+    rho, u, v = qp[:, 0], qp[:, 1], qp[:, 2]
+    Q = np.zeros((x.size, 4, y.size), order="F")
+    Q[:, 0] = rho
+    Q[:, 1] = rho * u
+    Q[:, 2] = rho * v
+    Q[:, 3] = ptbl * og1 + 0.5 * rho * (u * u + v * v)
+    p["inflow_q"] = Q[0].copy()  # (4, ny): what set_bc leaves in the inflow column
+    return Q
+
+
+def _blq_boundary(p: dict, J: np.ndarray) -> dict:
+    inflow = p["inflow_q"] * (1.0 / J[0, :])[None, :]
+    return {"x_lo": ("fixed", inflow), "x_hi": "zero_gradient", "y_lo": "noslip_wall", "y_hi": "zero_gradient"}
+
+
+# ---------------------------------------------------------------------------
 # Temporally developing boundary layer on a wall: 2D_solver/SBLI (mod_globals.f90,
 # set.f90, src/set_init_common.f90 set_init_tbl, src/set_compressible_bl.f90).  Its
 # set_bc copies the x ghosts periodically (the x flux kernels are the boundary
@@ -645,6 +720,15 @@ CASES: dict[str, CaseDef] = {
         _bl_init, _bl_derived,
         "Laminar boundary layer on a flat plate at Mach 2 (2D_solver/BL0)",
         grid=_bl_grid, bc_x=True, bc_y=True, boundary=_bl_boundary, boundary_order="y_last"),
+    "BL": CaseDef(
+        "BL", 2,
+        dict(VISC="NS", SCHEME="SLAU", ORDER=2, VISC_ORDER=4, TVD="none", SLAU_VARIANT="HRSLAU2", RK=3,
+             BC_X=True, BC_Y=True, RESCALE=False, COMMZ=False, RESTART=False),
+        dict(nx=257, ny=129, blt=1.0e-3, Lx=None, endT=0.3e-3, np=30, dt=3.0e-9, nt=None, R=287.03, gamma=1.4,
+             Pr=0.72, Prt=0.9, M0=2.0, p_tot=100.0e3, T_tot=295.0, rf=0.89, threshold=0.4, inflow="Qin.dat"),
+        _blq_init, _blq_derived,
+        "Boundary layer from an inflow profile file at Mach 2 (2D_solver/BL)",
+        grid=_bl_grid, bc_x=True, bc_y=True, boundary=_blq_boundary, boundary_order="y_last"),
     "SBLI": CaseDef(
         "SBLI", 2,
         dict(VISC="NS", SCHEME="SLAU", ORDER=6, TVD="hybrid", SLAU_VARIANT="HRSLAU2", RK=3,

@@ -454,6 +454,39 @@ def test_bl0_case_matches_oracle(tmp_path, cuda_device):
     np.testing.assert_allclose(c.solver.get_state(), want, rtol=1e-12, atol=0)
 
 
+def bl_profile_file(path, p, rows):
+    """A compressible laminar layer (the BL0 constants, 99 % thickness 0.75 mm) written
+    in the BL inflow profile format: rows of (y, rho, u, v, p)."""
+    from ouxsbli_b200.blasius import compressible_profile
+    from ouxsbli_b200.cases import sutherland_mu
+    y = np.linspace(0.0, 3.0e-3, rows)
+    cp = p["gamma"] * p["R"] / (p["gamma"] - 1.0)
+    rho, u, v, T = compressible_profile(y, 0.75e-3, p["u0"], p["T0"], p["p0"], p["R"], cp, p["rf"], p["Taw"],
+                                        sutherland_mu(p["T0"]))
+    prof = np.stack([y, p["p0"] / (p["R"] * T), u, v, np.full_like(y, p["p0"])], axis=1)
+    prof.astype("<f8").tofile(path)
+    return path
+
+
+def test_bl_case_matches_oracle(tmp_path, cuda_device):
+    """The BL case (an inflow profile from a file, zero-gradient outlet and top, an
+    adiabatic no-slip floor, y-last corners; NS SLAU-2 with the 4th-order viscous
+    stencil on the 2nd-order grid) through Case.run, 5 steps, bit for bit against the
+    oracle."""
+    from ouxsbli_b200 import Case
+    from ouxsbli_b200.cases import CASES, _bl_derived
+    p = _bl_derived(dict(CASES["BL"].params, Lx=0.02))
+    f = bl_profile_file(tmp_path / "Qin.dat", p, 30)
+    c = Case("2D_solver/BL", tmp_path / "bl", nx=65, ny=33, nt=5, np=1, inflow=str(f))
+    c.build()
+    c.run(device=cuda_device)
+    p, xc, yc, zc, dx, dy, dz, Q = c._initial()
+    cfg = c._solver_config(p, dx, dy, dz)
+    assert (cfg.order, cfg.visc_order) == (2, 4)
+    want = oracle.step(cfg, to_qj(Q, jacobian(dx, dy, None)), 5)
+    np.testing.assert_array_equal(c.solver.get_state(), want)
+
+
 def test_bl0_flat_plate_skin_friction(tmp_path, cuda_device):
     """BL0 at its own settings (Mach 2, 1025 x 129 nodes, 0.4 ms = 5 flow-through
     times): the laminar boundary layer on the adiabatic plate. Skin friction from the

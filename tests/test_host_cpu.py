@@ -295,9 +295,13 @@ def test_every_case_builds_its_initial_field(tmp_path):
     """Each case's defaults (scaled down) give a finite initial field of the right shape."""
     from ouxsbli_b200.cases import CASES
     small = {3: dict(nx=14, ny=14, nz=14), 2: dict(nx=22, ny=22)}
+    # BL reads its inflow profile (rows of y, rho, u, v, p) from a file
+    prof = np.array([[0.0, 0.2, 0.0, 0.0, 1.3e4], [1.0e-3, 0.25, 300.0, 0.5, 1.3e4], [3.0e-3, 0.28, 540.0, 1.4, 1.3e4]])
+    prof.astype("<f8").tofile(tmp_path / "Qin.dat")
+    extra = {"BL": dict(inflow=str(tmp_path / "Qin.dat"))}
     for name, case in CASES.items():
         src = f"{case.dim}D_solver/{name}"
-        c = Case(src, tmp_path / name, nt=1, np=1, **small[case.dim])
+        c = Case(src, tmp_path / name, nt=1, np=1, **small[case.dim], **extra.get(name, {}))
         c._setup()
         p, xc, yc, zc, dx, dy, dz, Q = c._initial()
         nv = case.dim + 2
@@ -455,3 +459,36 @@ def test_2d_neumann_rule_of_the_oracle():
     for j in range(1, ny - 1):  # x high column
         np.testing.assert_allclose(prim(q[nx - 1, :, j], J[nx - 1, j]), prim(q[nx - 2, :, j], J[nx - 2, j]),
                                    rtol=1e-13, atol=1e-15)
+
+
+def test_bl_inflow_profile_as_set_init_reads_it(tmp_path):
+    """2D_solver/BL/set.f90 set_init: the profile file's rows (y, rho, u, v, p) are
+    interpolated linearly onto the grid's y nodes, held at the end rows outside their
+    range, and one pressure, the mean of the interpolated p over the first nyi grid
+    rows, fills every column (known answers for a 3-row profile on 4 nodes)."""
+    from ouxsbli_b200.cases import _blq_init, read_inflow_profile
+    prof = np.array([[0.0, 1.0, 0.0, 0.0, 100.0],
+                     [1.0e-3, 2.0, 10.0, 1.0, 200.0],
+                     [2.0e-3, 3.0, 20.0, 2.0, 300.0]])
+    f = tmp_path / "Qin.dat"
+    prof.astype("<f8").tofile(f)
+    np.testing.assert_array_equal(read_inflow_profile(f), prof)
+    y = np.array([0.0, 0.5e-3, 1.0e-3, 2.5e-3])
+    x = np.zeros(3)
+    p = {"inflow": str(f), "gamma": 1.4}
+    Q = _blq_init(p, x, y)
+    rho = np.array([1.0, 1.5, 2.0, 3.0])
+    u = np.array([0.0, 5.0, 10.0, 20.0])
+    v = np.array([0.0, 0.5, 1.0, 2.0])
+    ptbl = (100.0 + 150.0 + 200.0) / 3.0  # the first nyi = 3 grid rows
+    for i in range(3):
+        np.testing.assert_allclose(Q[i, 0], rho, rtol=1e-15)
+        np.testing.assert_allclose(Q[i, 1], rho * u, rtol=1e-15)
+        np.testing.assert_allclose(Q[i, 2], rho * v, rtol=1e-15)
+        np.testing.assert_allclose(Q[i, 3], ptbl / 0.4 + 0.5 * rho * (u * u + v * v), rtol=1e-15)
+    np.testing.assert_array_equal(p["inflow_q"], Q[0])  # the inflow column the boundary keeps
+    (tmp_path / "bad.dat").write_bytes(np.zeros(7).tobytes())
+    with pytest.raises(ValueError, match="rows of 5"):
+        read_inflow_profile(tmp_path / "bad.dat")
+    with pytest.raises(ValueError, match="more than the grid"):
+        _blq_init(dict(p), x, y[:2])
