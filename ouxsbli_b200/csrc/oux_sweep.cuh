@@ -131,7 +131,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait_group() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// mbarrier and tiled tensor copy (TMA, no multicast) for the y / z sweep tiles
+// mbarrier and tiled tensor copy (TMA, no multicast) for the sweep tiles
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, int count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
@@ -780,8 +780,8 @@ namespace oux {
 // asynchronous global -> shared copies (cp.async): no register staging, and every
 // copy of the tile is in flight at once; derivatives differenced in the load (no GR)
 // are computed while the copies fly.
-// TM (y / z sweeps whose tile fields are all plain copies): the TMA tile layout
-// (TMA_ROW-wide rows, 128-byte field slabs); given `tmaps` (the sweep's SweepMaps),
+// TM (sweeps whose tile fields are all plain copies, sweep_tma): the TMA tile layout
+// (tma_row-wide rows, 128-byte field slabs); given `tmaps` (the sweep's SweepMaps),
 // one thread stages every field by a tensor copy completing one mbarrier, else the
 // threads fill the same layout with cp.async.
 template <int DIM, int DIR, int ORDER, int VK, bool LES, class T, int ROWS = default_rows<DIR>(),
