@@ -683,7 +683,13 @@ def main():
         lib = _lib.LIB
         h_in = torch.from_numpy(np.ascontiguousarray(qj.ravel(order="F"))).pin_memory()
         pin = C.cast(C.c_void_p(h_in.data_ptr()), C.POINTER(C.c_double))
-        NPIPE = 2 if n_el * 8 > (2 << 30) else 3
+        # three handles let one job's upload, another's step and a third's download run at
+        # once (with two, each stream's own upload, step and download follow one another;
+        # 512^3 on one B200: 826 with two, 962 with three, 961 with four Mcell-steps/s,
+        # where the host link bounds it); two where the device cannot hold three solves
+        per_handle = s.state.numel() * 8 + s.scratch.numel() * 8
+        free_b, _ = torch.cuda.mem_get_info(dev)
+        NPIPE = 3 if free_b > 2 * per_handle + (4 << 30) else 2
         pipes = [s] + [Solver(cfg, dev) for _ in range(NPIPE - 1)]
         streams = [torch.cuda.Stream(dev) for _ in range(NPIPE)]
         h_out = [torch.empty(n_el, dtype=torch.float64).pin_memory() for _ in range(NPIPE)]
