@@ -188,3 +188,37 @@ def test_stage_part_argument_checks_without_a_device():
     assert _lib.LIB.oux_stage_part(h, 0, 1, None) == _lib.OUX_E_INVALID
     assert "Navier-Stokes" in _lib.LIB.oux_last_error().decode()
     _lib.LIB.oux_destroy(h)
+
+
+def test_tma_tile_geometry_meets_the_tensor_copy_rules():
+    """The x / y sweep tiles staged by tensor copies (oux_sweep.cuh): every box starts
+    on a 16-byte boundary (x origin 32 b - 4 in the x sweep, 32 b in the y sweep), its
+    rows are a multiple of 16 bytes for 4- and 8-byte elements, every cell the tile
+    needs lies inside the row for each x ghost width (1 to 3), and each field's slab
+    is a multiple of 128 bytes.  Constants read from the header."""
+    import pathlib
+    import re
+    src = (pathlib.Path(__file__).resolve().parents[1] / "ouxsbli_b200" / "csrc" / "oux_sweep.cuh").read_text()
+    const = {k: int(re.search(rf"constexpr int {k} = (\d+);", src).group(1))
+             for k in ("TMA_ROW", "TMA_ROW_X", "TILE_HALO", "TMA_MAP_BYTES")}
+    rows_y = int(re.search(r"#define OUX_SWEEP_BF (\d+)", src).group(1))
+    rows_x = int(re.search(r"#define OUX_SWEEP_BR (\d+)", src).group(1))
+    halo = const["TILE_HALO"]
+    assert const["TMA_MAP_BYTES"] == 128
+    for elem in (4, 8):
+        for row, box_rows in ((const["TMA_ROW_X"], rows_x), (const["TMA_ROW"], rows_y + 2 * halo)):
+            assert row * elem % 16 == 0
+            slab = -(-row * box_rows * elem // 128) * 128
+            assert slab % 128 == 0 and slab >= row * box_rows * elem
+        for gx in (1, 2, 3):
+            for b0 in range(64):
+                bx0 = gx + 32 * b0
+                # x sweep: cells bx0 - halo .. bx0 + 31 + halo, row from 32 b - 4, column gx + 1 + t
+                x0 = bx0 - gx - 4
+                assert x0 * elem % 16 == 0
+                assert 0 <= (bx0 - halo) - x0 and (bx0 + 31 + halo) - x0 < const["TMA_ROW_X"]
+                assert (bx0 - halo) - x0 == gx + 1
+                # y sweep: owned cells bx0 .. bx0 + 31, row from 32 b, column gx + x
+                y0 = bx0 - gx
+                assert y0 * elem % 16 == 0 and y0 >= 0
+                assert bx0 - y0 == gx and (bx0 + 31) - y0 < const["TMA_ROW"]
