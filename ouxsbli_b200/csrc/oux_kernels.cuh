@@ -496,9 +496,12 @@ __global__ void __launch_bounds__(PS_TX * PS_TY) k_prim_fused(const TS* __restri
 // (Central-4, ME4) central node derivative of the viscous loaders
 // (load_smem_visc_cent.f90.fypp:51-70, load_smem_visc_me4_base.f90:120-127), at every
 // cell whose stencil fits in the grid (else 0: no sweep reads those), on the z planes
-// [gk0, gk1).  Plane-flattened like k_prim: the neighbours come through L1 / L2.  (A
-// z-marching variant with a shared-memory ring of the velocities filled by cp.async one
-// plane ahead measured slower on B200 at 518^3: 3.78 against 2.96 ms.)
+// [gk0, gk1).  Plane-flattened like k_prim: the neighbours come through L1 / L2.
+// Measured slower on B200 at 518^3: a z-marching variant with a shared-memory ring of
+// the velocities filled by cp.async one plane ahead (3.78 against 2.96 ms without the
+// sensor), and 32 x 8 tiles of one plane staged in shared memory with their x / y
+// ring, the z neighbours from L2 (FP64 with the sensor 4.76 against 3.84 ms; FP32
+// without it 2.06 against 2.17).
 template <bool SIXTH, class T>
 __device__ __forceinline__ T node_deriv_of(T m3, T m2, T m1, T p1, T p2, T p3, T inv) {
   if constexpr (SIXTH)
